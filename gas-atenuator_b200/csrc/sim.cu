@@ -1,0 +1,1290 @@
+// sim.cu - the resident PIC-MCC simulation (the hot path).
+//
+// One step = FDTD sub-cycle (fields t^s -> t^{s+1}) followed by one fused
+// particle pass:
+//   gather (EM4.cu:41-122) -> relativistic Boris kick -> half drift with the
+//   wall / end rules (EM4.cu:146-177) -> null-collision MCC against the
+//   tabulated N2 cross-sections (electron_transport.cu:64-227, corrected) with
+//   secondary birth -> half drift (EM2.cu:26-57) -> current deposit
+//   (EM7.cu:56-202) into 64-bit fixed point.
+// Particles never leave HBM; the per-step sequence is replayed from CUDA graphs.
+//
+// Two state forms:
+//   FP64      r, z [m]; u_r, u_theta, u_z = gamma v [m/s]; id.  Dead: r < 0.
+//   FP32      key = (iz << 16) | ir, fr, fz in-cell offsets [cells], u / c
+//             (gamma beta) in float; id.  Dead: key = 0xFFFFFFFF.
+// The collision test, branch selection, energy sharing and threshold
+// subtraction run in FP64 in both forms.
+//
+// Deposit: each particle's four node contributions (q FN v w) are rounded to
+// integers first, so the grid sum is exact and independent of order; lanes of
+// a warp that hit the same four nodes (__match_any_sync on the node key) are
+// summed with __reduce_add_sync before one 64-bit atomic per node.
+#include <cub/device/device_scan.cuh>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "fdtd.cuh"
+#include "gasatt_internal.h"
+
+using namespace gasatt;
+
+namespace {
+
+constexpr uint32_t kDead = 0xFFFFFFFFu;
+constexpr int kBlock = 256;
+
+struct SimCounters {
+  unsigned long long n_total;    // committed slots
+  unsigned long long n_births;   // slots claimed by births in the current pass
+  unsigned long long ion, ela, exc, nul, lost, cap_overflow;
+  long long step;                // index of the current particle pass
+  unsigned long long sorted_total;
+  unsigned long long kin_fx;     // diagnostic: sum E_kin * 2^16 [eV]
+  unsigned long long alive;      // diagnostic
+  unsigned long long cap;        // slot capacity
+};
+
+// slots holding particles, including births of the last pass not yet committed
+__device__ __forceinline__ long long slots_in_use(const SimCounters *cnt) {
+  const unsigned long long nt = cnt->n_total + cnt->n_births;
+  return (long long)(nt < cnt->cap ? nt : cnt->cap);
+}
+
+struct SimParams {
+  int nr, nz;
+  double dr, dz, dt, c, qe, me, mu0, FN, PHIp, n_gas, nu_max, P_null, Rp, Lp, kb, m_ion, T_gas;
+  uint64_t seed;
+  int secondaries;
+  long long cap;
+  double qm_dt2;            // -q_e/m_e dt/2
+  float aE, aB, hdr, hdz;   // FP32 form: impulse per (V/m), per (A/m); c dt/(2 dr), c dt/(2 dz)
+  double dep;               // fixed-point factor: FP64 q FN scale (x v), FP32 q FN c scale (x beta)
+  // tables
+  const double *sig;        // 3 x G (el, ion, exc)
+  const double *cdf;        // G x 181
+  int G;
+  double lnEmin, dlnE;
+  int n_exc;
+  double exc[5][16];
+  unsigned long long *Jr, *Jz;
+};
+
+template <typename Real>
+struct Fields { Real *Er, *Ez, *H; };
+
+struct State64 { double *r, *z, *ur, *ut, *uz; uint64_t *id; };
+struct State32 { uint32_t *key; float *fr, *fz, *ur, *ut, *uz; uint64_t *id; };
+
+// ------------------------------------------------------------------- MCC
+struct Birth { bool born; double ux, uy, uz; };
+
+__device__ __forceinline__ void xs_lookup(const SimParams &P, double Eev, double &se, double &si,
+                                          double &sx, double &L) {
+  L = (log(Eev) - P.lnEmin) / P.dlnE;
+  int i;
+  double f;
+  if (!(L > 0)) { i = 0; f = 0; }
+  else if (L >= P.G - 1) { i = P.G - 2; f = 1; }
+  else { i = (int)L; f = L - i; }
+  const double *s0 = P.sig, *s1 = P.sig + P.G, *s2 = P.sig + 2 * P.G;
+  se = s0[i] + f * (s0[i + 1] - s0[i]);
+  si = s1[i] + f * (s1[i + 1] - s1[i]);
+  sx = s2[i] + f * (s2[i + 1] - s2[i]);
+}
+
+__device__ __forceinline__ double cdf_theta(const SimParams &P, double L, double U) {
+  const double Lr = floor(L + 0.5);
+  const int g = Lr < 0 ? 0 : (Lr > P.G - 1 ? P.G - 1 : (int)Lr);
+  const double *C = P.cdf + (int64_t)g * 181;
+  int lo = 0, hi = 180;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (C[mid] <= U) lo = mid; else hi = mid;
+  }
+  return (lo + (U - C[lo]) / (C[lo + 1] - C[lo])) * (GASATT_PI / 180);
+}
+
+__device__ __forceinline__ double u_of_energy(double EJ, double m, double c) {
+  const double e = EJ / (m * c * c);
+  return c * sqrt(e * (2 + e));
+}
+
+// Null-collision event for one electron at step `step` (corrected form of
+// electron_transport.cu:74-227).  u in m/s, local (r, theta, z) frame.
+// Returns 0 no candidate, 1 elastic, 2 ionization, 3 excitation, 4 null.
+__device__ int mcc_event(const SimParams &P, uint64_t id, long long step, double &ux, double &uy,
+                         double &uz, Birth &b) {
+  b.born = false;
+  const U2 d0 = draw2(P.seed, id, step, 0);
+  if (!(d0.a < P.P_null)) return 0;
+  const double c = P.c, me = P.me, qe = P.qe, I = GASATT_ION_I_EV;
+  const double u2 = ux * ux + uy * uy + uz * uz;
+  const double g = sqrt(1 + u2 / (c * c));
+  const double EJ = me * c * c * ((u2 / (c * c)) / (g + 1));
+  const double Eev = EJ / qe;
+  const double um = sqrt(u2), v = um / g;
+  double se, si, sx, L;
+  xs_lookup(P, Eev, se, si, sx, L);
+  const double nu_el = P.n_gas * se * v, nu_io = P.n_gas * si * v, nu_ex = P.n_gas * sx * v;
+  const double X = d0.b * P.nu_max;
+  if (X < nu_el) {
+    const U2 d1 = draw2(P.seed, id, step, 1);
+    const double th = cdf_theta(P, L, d1.a), ph = 2 * GASATT_PI * d1.b;
+    rotate_v(ux, uy, uz, th, ph, false);
+    return 1;
+  }
+  if (X < nu_el + nu_io && Eev > I) {
+    const U2 d1 = draw2(P.seed, id, step, 1);
+    const double T = Eev;
+    const double T_a = 1000, T_b = 2 * I, t_b = I, T_s = 4.17, t_s = 13.8;
+    const double T_0 = T_s - T_a / (T + T_b);
+    const double t = t_s * T / (T + t_b);
+    const double T_m = (T - I) / 2;
+    const double k_1 = atan((T_m - T_0) / t), k_2 = atan(T_0 / t);
+    const double k0 = T_0 + t * tan(d1.a * (k_1 + k_2) - k_2);
+    const double E_1 = k0, E_2 = T - E_1 - I;
+    double E_p, E_s;
+    if (E_2 > E_1) { E_p = E_2; E_s = E_1; } else { E_p = E_1; E_s = E_2; }
+    const double E_e = me * c * c / qe;
+    const double phi_p = 2 * GASATT_PI * d1.b, phi_s = phi_p - GASATT_PI;
+    const double th_p = asin(sqrt((E_s / T) / ((1 - E_s / T) * T / (2 * E_e) + 1)));
+    const double th_s = asin(sqrt((1 - E_s / T) / (1 + E_s / (2 * E_e))));
+    const double ix = ux / um, iy = uy / um, iz = uz / um;
+    const double up = u_of_energy(E_p * qe, me, c), us = u_of_energy(E_s * qe, me, c);
+    ux = ix * up; uy = iy * up; uz = iz * up;
+    rotate_v(ux, uy, uz, th_p, phi_p, false);
+    if (P.secondaries) {
+      double sx_ = ix * us, sy_ = iy * us, sz_ = iz * us;
+      rotate_v(sx_, sy_, sz_, th_s, phi_s, false);
+      b.born = true; b.ux = sx_; b.uy = sy_; b.uz = sz_;
+    }
+    return 2;
+  }
+  if (X < nu_el + nu_io + nu_ex) {
+    double k1 = 0, k2 = 0;
+    for (int i = 0; i < P.n_exc; ++i) {
+      const double k = P.exc[0][i];
+      if (!(Eev > k)) continue;
+      const double a = P.exc[1][i] / (k * k);
+      const double bb = pow(k / Eev, P.exc[2][i]);
+      const double cc = pow(1 - pow(k / Eev, P.exc[4][i]), P.exc[3][i]);
+      k1 = k1 + a * bb * cc * k;
+      k2 = k2 + a * bb * cc;
+    }
+    if (!(k2 > 0)) return 4;
+    const double E_dep = k1 / k2;
+    const double up = u_of_energy((Eev - E_dep) * qe, me, c);
+    ux = ux / um * up; uy = uy / um * up; uz = uz / um * up;
+    return 3;
+  }
+  return 4;
+}
+
+// ------------------------------------------------------ warp deposit
+// Sum of v over the lanes of `mask` (all lanes of the group call it).
+__device__ __forceinline__ long long group_sum_i64(unsigned mask, long long v) {
+  const unsigned lo = (unsigned)(v & ((1ll << 26) - 1));
+  const int hi = (int)(v >> 26);
+  const unsigned slo = __reduce_add_sync(mask, lo);
+  const int shi = __reduce_add_sync(mask, hi);
+  return ((long long)shi << 26) + (long long)slo;
+}
+
+// 4 nodes x 2 components, grouped by node key; the lowest lane of each group
+// issues the atomics.  `act` lanes with no contribution pass zeros.
+__device__ __forceinline__ void warp_deposit(bool act, unsigned key, const int64_t a[4],
+                                             const long long vr[4], const long long vz[4],
+                                             unsigned long long *Jr, unsigned long long *Jz,
+                                             bool wide) {
+  const unsigned live = __ballot_sync(0xFFFFFFFFu, act);
+  if (!act) return;
+  const unsigned mask = __match_any_sync(live, key);
+  const bool leader = (__ffs(mask) - 1) == (int)(threadIdx.x & 31);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    long long sr, sz;
+    if (wide) {
+      sr = group_sum_i64(mask, vr[k]);
+      sz = group_sum_i64(mask, vz[k]);
+    } else {
+      sr = __reduce_add_sync(mask, (int)vr[k]);
+      sz = __reduce_add_sync(mask, (int)vz[k]);
+    }
+    if (leader) {
+      if (sr) atomicAdd(Jr + a[k], (unsigned long long)sr);
+      if (sz) atomicAdd(Jz + a[k], (unsigned long long)sz);
+    }
+  }
+}
+
+// ----------------------------------------------------------- FP64 form
+__device__ __forceinline__ void halfdrift64(double &r, double &z, double &ur, double &ut,
+                                            double &uz, bool &alive, const SimParams &P) {
+  const double g = sqrt(1 + (ur * ur + ut * ut + uz * uz) / (P.c * P.c));
+  const double X = r + 0.5 * (ur / g) * P.dt;
+  const double Y = 0.5 * (ut / g) * P.dt;
+  double Z = z + 0.5 * (uz / g) * P.dt;
+  const double rn = sqrt(X * X + Y * Y);
+  const double cs = rn > 0 ? X / rn : 1.0, sn = rn > 0 ? Y / rn : 0.0;
+  const double nur = cs * ur + sn * ut, nut = -sn * ur + cs * ut;
+  ur = nur; ut = nut;
+  if (rn > P.Rp) alive = false;
+  if (Z > P.Lp) { Z = 2 * P.Lp - Z; uz = -uz; }
+  if (Z < 0) { Z = -Z; uz = -uz; }
+  r = rn; z = Z;
+}
+
+__device__ __forceinline__ void deposit_values64(const SimParams &P, double r, double z,
+                                                 double ur, double ut, double uz, int64_t a[4],
+                                                 long long vr[4], long long vz[4],
+                                                 unsigned &key) {
+  const double g = sqrt(1 + (ur * ur + ut * ut + uz * uz) / (P.c * P.c));
+  const double vrr = ur / g, vzz = uz / g;
+  double b[4];
+  const int ar = em7_weights(r, z, P.nr, P.nz, P.dr, P.dz, a, b);
+  const int az = (int)floor(z / P.dz - 0.5);
+  key = (unsigned)((ar + 1) + (az + 1) * (P.nr + 1));
+  const double q = -P.qe;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    vr[k] = __double2ll_rn(P.FN * b[k] * q * vrr * P.dep);
+    vz[k] = __double2ll_rn(P.FN * b[k] * q * vzz * P.dep);
+  }
+}
+
+__device__ __forceinline__ void deposit_direct(const int64_t a[4], const long long vr[4],
+                                               const long long vz[4], const SimParams &P) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (vr[k]) atomicAdd(P.Jr + a[k], (unsigned long long)vr[k]);
+    if (vz[k]) atomicAdd(P.Jz + a[k], (unsigned long long)vz[k]);
+  }
+}
+
+__device__ __forceinline__ void count_event(SimCounters *cnt, int ev) {
+  if (ev == 1) atomicAdd(&cnt->ela, 1ull);
+  else if (ev == 2) atomicAdd(&cnt->ion, 1ull);
+  else if (ev == 3) atomicAdd(&cnt->exc, 1ull);
+  else if (ev == 4) atomicAdd(&cnt->nul, 1ull);
+}
+
+// mode 0: full pass; mode 1: half drift + deposit only (start of a run)
+__global__ void __launch_bounds__(kBlock) k_pass64(SimParams P, State64 S, Fields<double> F,
+                                                   SimCounters *cnt, int mode) {
+  const long long n0 = (long long)cnt->n_total;
+  const long long step = cnt->step;
+  const int lane = threadIdx.x & 31;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  unsigned lost = 0;
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n0;
+       base += stride) {
+    const long long p = base + lane;
+    bool act = p < n0;
+    double r = 0, z = 0, ur = 0, ut = 0, uz = 0;
+    if (act) {
+      r = S.r[p];
+      act = r >= 0;
+    }
+    if (act) {
+      z = S.z[p]; ur = S.ur[p]; ut = S.ut[p]; uz = S.uz[p];
+      bool alive = true;
+      if (mode == 0) {
+        double E_r, E_z, Hp;
+        gather3<double>(F.Er, F.Ez, F.H, P.nr, P.nz, P.dr, P.dz, r, z, E_r, E_z, Hp);
+        const double B = P.mu0 * Hp;
+        boris(ur, ut, uz, E_r, 0.0, E_z, 0.0, B, 0.0, P.qm_dt2, P.c);
+        halfdrift64(r, z, ur, ut, uz, alive, P);
+        if (alive) {
+          Birth b;
+          const int ev = mcc_event(P, S.id[p], step, ur, ut, uz, b);
+          if (ev) count_event(cnt, ev);
+          if (b.born) {
+            const unsigned long long k = atomicAdd(&cnt->n_births, 1ull);
+            const long long slot = n0 + (long long)k;
+            if (slot < P.cap) {
+              double cr = r, cz = z, cur = b.ux, cut = b.uy, cuz = b.uz;
+              bool calive = true;
+              halfdrift64(cr, cz, cur, cut, cuz, calive, P);
+              if (calive) {
+                int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
+                deposit_values64(P, cr, cz, cur, cut, cuz, a, vr, vz, kk);
+                deposit_direct(a, vr, vz, P);
+              } else {
+                atomicAdd(&cnt->lost, 1ull);
+              }
+              S.r[slot] = calive ? cr : -1.0; S.z[slot] = cz;
+              S.ur[slot] = cur; S.ut[slot] = cut; S.uz[slot] = cuz;
+              S.id[slot] = child_id(S.id[p], step);
+            } else {
+              atomicAdd(&cnt->cap_overflow, 1ull);
+            }
+          }
+        }
+      }
+      if (alive) halfdrift64(r, z, ur, ut, uz, alive, P);
+      if (!alive) { lost++; r = -1.0; }
+      S.r[p] = r; S.z[p] = z; S.ur[p] = ur; S.ut[p] = ut; S.uz[p] = uz;
+      act = alive;
+    }
+    int64_t a[4] = {0, 0, 0, 0};
+    long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
+    unsigned key = 0;
+    if (act) deposit_values64(P, r, z, ur, ut, uz, a, vr, vz, key);
+    warp_deposit(act, key, a, vr, vz, P.Jr, P.Jz, true);
+  }
+  lost = __reduce_add_sync(0xFFFFFFFFu, lost);
+  if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
+}
+
+// ----------------------------------------------------------- FP32 form
+// clamped bilinear interpolation on a (ncol x nrow) column-major grid
+__device__ __forceinline__ float bilin(const float *__restrict__ F, int ncol, int nrow, int c0,
+                                       float wc, int r0, float wr) {
+  const int ca = max(c0, 0), cb = min(c0 + 1, ncol - 1);
+  const int ra = max(r0, 0), rb = min(r0 + 1, nrow - 1);
+  const float f00 = __ldg(F + ca + (int64_t)ra * ncol), f10 = __ldg(F + cb + (int64_t)ra * ncol);
+  const float f01 = __ldg(F + ca + (int64_t)rb * ncol), f11 = __ldg(F + cb + (int64_t)rb * ncol);
+  return (1 - wr) * ((1 - wc) * f00 + wc * f10) + wr * ((1 - wc) * f01 + wc * f11);
+}
+
+// half-cell staggered index/weight: position ic + f measured from node ic-1/2
+__device__ __forceinline__ void half_shift(int ic, float f, int &a, float &w) {
+  if (f >= 0.5f) { a = ic; w = f - 0.5f; } else { a = ic - 1; w = f + 0.5f; }
+}
+
+__device__ __forceinline__ void halfdrift32(int &ir, int &iz, float &fr, float &fz, float &ur,
+                                            float &ut, float &uz, bool &alive,
+                                            const SimParams &P) {
+  const float ig = 1.0f / sqrtf(1.0f + ur * ur + ut * ut + uz * uz);
+  const float dx = ur * ig * P.hdr, dy = ut * ig * P.hdr, dzz = uz * ig * P.hdz;
+  const float rc = (float)ir + fr;
+  const float X = rc + dx;
+  const float rn = sqrtf(X * X + dy * dy);
+  const float den = rn + rc;
+  const float drr = den > 0.f ? (dx * (2.f * rc + dx) + dy * dy) / den : 0.f;
+  const float cs = rn > 0.f ? X / rn : 1.f, sn = rn > 0.f ? dy / rn : 0.f;
+  const float nur = cs * ur + sn * ut, nut = -sn * ur + cs * ut;
+  ur = nur; ut = nut;
+  fr += drr;
+  int k = (int)floorf(fr);
+  ir += k; fr -= (float)k;
+  if (ir < 0) { ir = 0; fr = 0.f; }
+  if (ir >= P.nr) alive = false;
+  fz += dzz;
+  k = (int)floorf(fz);
+  iz += k; fz -= (float)k;
+  if (iz < 0) {                                   // specular at z = 0
+    iz = -iz - 1; fz = 1.f - fz; uz = -uz;
+    if (fz >= 1.f) { fz = 0.f; iz += 1; }
+  } else if (iz >= P.nz) {                         // specular at z = Lp
+    iz = 2 * P.nz - iz - 1; fz = 1.f - fz; uz = -uz;
+    if (fz >= 1.f) { fz = 0.f; iz += 1; }
+  }
+  if (iz > P.nz - 1) { iz = P.nz - 1; fz = 0.99999994f; }
+  if (iz < 0) { iz = 0; fz = 0.f; }
+}
+
+__device__ __forceinline__ void deposit_values32(const SimParams &P, int ir, int iz, float fr,
+                                                 float fz, float ur, float ut, float uz,
+                                                 int64_t a[4], long long vr[4], long long vz[4],
+                                                 unsigned &key) {
+  const float ig = 1.0f / sqrtf(1.0f + ur * ur + ut * ut + uz * uz);
+  int ar, az;
+  float wr, wz;
+  half_shift(ir, fr, ar, wr);
+  half_shift(iz, fz, az, wz);
+  const int ca = max(ar, 0), cb = min(ar + 1, P.nr - 1);
+  const int ra = max(az, 0), rb = min(az + 1, P.nz - 1);
+  a[0] = ca + (int64_t)ra * P.nr; a[1] = cb + (int64_t)ra * P.nr;
+  a[2] = ca + (int64_t)rb * P.nr; a[3] = cb + (int64_t)rb * P.nr;
+  const float w[4] = {(1 - wr) * (1 - wz), wr * (1 - wz), (1 - wr) * wz, wr * wz};
+  const float kr = (float)P.dep * ur * ig, kz = (float)P.dep * uz * ig;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    vr[k] = __float2ll_rn(kr * w[k]);
+    vz[k] = __float2ll_rn(kz * w[k]);
+  }
+  key = (unsigned)((ar + 1) + (az + 1) * (P.nr + 1));
+}
+
+__global__ void __launch_bounds__(kBlock) k_pass32(SimParams P, State32 S, Fields<float> F,
+                                                   SimCounters *cnt, int mode) {
+  const long long n0 = (long long)cnt->n_total;
+  const long long step = cnt->step;
+  const int lane = threadIdx.x & 31;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  unsigned lost = 0;
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n0;
+       base += stride) {
+    const long long p = base + lane;
+    bool act = p < n0;
+    uint32_t key = kDead;
+    if (act) {
+      key = S.key[p];
+      act = key != kDead;
+    }
+    int ir = 0, iz = 0;
+    float fr = 0, fz = 0, ur = 0, ut = 0, uz = 0;
+    if (act) {
+      ir = (int)(key & 0xFFFFu); iz = (int)(key >> 16);
+      fr = S.fr[p]; fz = S.fz[p]; ur = S.ur[p]; ut = S.ut[p]; uz = S.uz[p];
+      bool alive = true;
+      if (mode == 0) {
+        int ar, az;
+        float wr, wz;
+        half_shift(ir, fr, ar, wr);
+        half_shift(iz, fz, az, wz);
+        const float Er = bilin(F.Er, P.nr, P.nz + 1, ar, wr, iz, fz);
+        const float Ez = bilin(F.Ez, P.nr + 1, P.nz, ir, fr, az, wz);
+        const float H = bilin(F.H, P.nr, P.nz, ar, wr, az, wz);
+        // Boris in gamma*beta units: E = (Er, 0, Ez), B = (0, mu0 H, 0)
+        const float umr = ur + P.aE * Er, umt = ut, umz = uz + P.aE * Ez;
+        const float gm = sqrtf(1.0f + umr * umr + umt * umt + umz * umz);
+        const float t = P.aB * H / gm;
+        const float s = 2.f * t / (1.f + t * t);
+        const float upr = umr - umz * t, upz = umz + umr * t;
+        ur = umr - upz * s + P.aE * Er;
+        uz = umz + upr * s + P.aE * Ez;
+        ut = umt;
+        halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P);
+        if (alive) {
+          double dux = (double)ur * P.c, duy = (double)ut * P.c, duz = (double)uz * P.c;
+          Birth b;
+          const int ev = mcc_event(P, S.id[p], step, dux, duy, duz, b);
+          if (ev) {
+            count_event(cnt, ev);
+            ur = (float)(dux / P.c); ut = (float)(duy / P.c); uz = (float)(duz / P.c);
+          }
+          if (b.born) {
+            const unsigned long long k = atomicAdd(&cnt->n_births, 1ull);
+            const long long slot = n0 + (long long)k;
+            if (slot < P.cap) {
+              int cir = ir, ciz = iz;
+              float cfr = fr, cfz = fz;
+              float cur = (float)(b.ux / P.c), cut = (float)(b.uy / P.c), cuz = (float)(b.uz / P.c);
+              bool calive = true;
+              halfdrift32(cir, ciz, cfr, cfz, cur, cut, cuz, calive, P);
+              if (calive) {
+                int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
+                deposit_values32(P, cir, ciz, cfr, cfz, cur, cut, cuz, a, vr, vz, kk);
+                deposit_direct(a, vr, vz, P);
+              } else {
+                atomicAdd(&cnt->lost, 1ull);
+              }
+              S.key[slot] = calive ? (((uint32_t)ciz << 16) | (uint32_t)cir) : kDead;
+              S.fr[slot] = cfr; S.fz[slot] = cfz;
+              S.ur[slot] = cur; S.ut[slot] = cut; S.uz[slot] = cuz;
+              S.id[slot] = child_id(S.id[p], step);
+            } else {
+              atomicAdd(&cnt->cap_overflow, 1ull);
+            }
+          }
+        }
+      }
+      if (alive) halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P);
+      if (!alive) lost++;
+      S.key[p] = alive ? (((uint32_t)iz << 16) | (uint32_t)ir) : kDead;
+      S.fr[p] = fr; S.fz[p] = fz; S.ur[p] = ur; S.ut[p] = ut; S.uz[p] = uz;
+      act = alive;
+    }
+    int64_t a[4] = {0, 0, 0, 0};
+    long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
+    unsigned dkey = 0;
+    if (act) deposit_values32(P, ir, iz, fr, fz, ur, ut, uz, a, vr, vz, dkey);
+    warp_deposit(act, dkey, a, vr, vz, P.Jr, P.Jz, false);
+  }
+  lost = __reduce_add_sync(0xFFFFFFFFu, lost);
+  if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
+}
+
+// ------------------------------------------------------------- FDTD
+// H update; the last H update of a step also clears the current (read by
+// the E updates before it), commits the births of the previous particle
+// pass and advances the step index read by the next pass.
+template <typename T>
+__global__ void k_sim_h(T *__restrict__ H, const T *__restrict__ Er, const T *__restrict__ Ez,
+                        int nr, int nz, double chr, double chz, unsigned long long *Jr,
+                        unsigned long long *Jz, SimCounters *cnt) {
+  const int64_t n = (int64_t)nr * nz;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % nr), j = (int)(idx / nr);
+    const int64_t ez = i + (int64_t)j * (nr + 1);
+    H[idx] = (T)((double)H[idx] + (chr * ((double)Ez[ez + 1] - (double)Ez[ez]) -
+                                   chz * ((double)Er[idx + nr] - (double)Er[idx])));
+    if (Jr) { Jr[idx] = 0; Jz[idx] = 0; }
+  }
+  if (cnt && blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long nt = cnt->n_total + cnt->n_births;
+    cnt->n_total = nt < cnt->cap ? nt : cnt->cap;
+    cnt->n_births = 0;
+    cnt->step += 1;
+  }
+}
+
+// ---------------------------------------------------------- load/read
+__global__ void k_load64(State64 S, const double *r, const double *z, const double *ur,
+                         const double *ut, const double *uz, const uint64_t *id, long long n) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    S.r[p] = r[p]; S.z[p] = z[p]; S.ur[p] = ur[p]; S.ut[p] = ut[p]; S.uz[p] = uz[p];
+    S.id[p] = id[p];
+  }
+}
+
+__global__ void k_load32(State32 S, const double *r, const double *z, const double *ur,
+                         const double *ut, const double *uz, const uint64_t *id, long long n,
+                         int nr, int nz, double dr, double dz, double c) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double R = r[p] / dr, Z = z[p] / dz;
+    int ir = (int)floor(R), iz = (int)floor(Z);
+    float fr = (float)(R - ir), fz = (float)(Z - iz);
+    if (fr >= 1.f) { fr = 0.f; ir++; }
+    if (fz >= 1.f) { fz = 0.f; iz++; }
+    if (iz >= nz) { iz = nz - 1; fz = 0.99999994f; }
+    const bool alive = r[p] >= 0 && ir < nr && iz >= 0;
+    S.key[p] = alive ? (((uint32_t)iz << 16) | (uint32_t)ir) : kDead;
+    S.fr[p] = fr; S.fz[p] = fz;
+    S.ur[p] = (float)(ur[p] / c); S.ut[p] = (float)(ut[p] / c); S.uz[p] = (float)(uz[p] / c);
+    S.id[p] = id[p];
+  }
+}
+
+__global__ void k_read64(State64 S, double *r, double *z, double *ur, double *ut, double *uz,
+                         uint64_t *id, long long n) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    r[p] = S.r[p]; z[p] = S.z[p]; ur[p] = S.ur[p]; ut[p] = S.ut[p]; uz[p] = S.uz[p];
+    id[p] = S.id[p];
+  }
+}
+
+__global__ void k_read32(State32 S, double *r, double *z, double *ur, double *ut, double *uz,
+                         uint64_t *id, long long n, double dr, double dz, double c) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const uint32_t key = S.key[p];
+    if (key == kDead) { r[p] = -1.0; z[p] = 0; }
+    else {
+      r[p] = ((double)(key & 0xFFFFu) + (double)S.fr[p]) * dr;
+      z[p] = ((double)(key >> 16) + (double)S.fz[p]) * dz;
+    }
+    ur[p] = (double)S.ur[p] * c; ut[p] = (double)S.ut[p] * c; uz[p] = (double)S.uz[p] * c;
+    id[p] = S.id[p];
+  }
+}
+
+// ---------------------------------------------------------------- sort
+// Counting sort by cell (z-major), dropping dead slots.  Order inside a cell
+// is arbitrary; nothing downstream depends on it (random streams are keyed
+// on particle ids and the deposit is an exact integer sum).
+__device__ __forceinline__ int cell_of64(const State64 &S, long long p, int nr, int nz,
+                                         double dr, double dz) {
+  const double r = S.r[p];
+  if (r < 0) return -1;
+  int ir = (int)floor(r / dr), iz = (int)floor(S.z[p] / dz);
+  ir = min(max(ir, 0), nr - 1);
+  iz = min(max(iz, 0), nz - 1);
+  return ir + iz * nr;
+}
+__device__ __forceinline__ int cell_of32(const State32 &S, long long p, int nr) {
+  const uint32_t k = S.key[p];
+  if (k == kDead) return -1;
+  return (int)(k & 0xFFFFu) + (int)(k >> 16) * nr;
+}
+
+template <int FORM>
+__global__ void k_sort_hist(State64 S64, State32 S32, const SimCounters *cnt, int nr, int nz,
+                            double dr, double dz, int *count) {
+  const long long n0 = slots_in_use(cnt);
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n0;
+       base += (long long)gridDim.x * blockDim.x) {
+    const long long p = base + (threadIdx.x & 31);
+    int c = -1;
+    if (p < n0) c = FORM == 0 ? cell_of64(S64, p, nr, nz, dr, dz) : cell_of32(S32, p, nr);
+    const unsigned live = __ballot_sync(0xFFFFFFFFu, c >= 0);
+    if (c < 0) continue;
+    const unsigned mask = __match_any_sync(live, c);
+    if ((__ffs(mask) - 1) == (int)(threadIdx.x & 31)) atomicAdd(count + c, __popc(mask));
+  }
+}
+
+template <int FORM>
+__global__ void k_sort_scatter(State64 A64, State64 B64, State32 A32, State32 B32,
+                               SimCounters *cnt, int nr, int nz, double dr, double dz,
+                               const int *offset, int *cursor) {
+  const long long n0 = slots_in_use(cnt);
+  const int lane = threadIdx.x & 31;
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n0;
+       base += (long long)gridDim.x * blockDim.x) {
+    const long long p = base + lane;
+    int c = -1;
+    if (p < n0) c = FORM == 0 ? cell_of64(A64, p, nr, nz, dr, dz) : cell_of32(A32, p, nr);
+    const unsigned live = __ballot_sync(0xFFFFFFFFu, c >= 0);
+    if (c < 0) continue;
+    const unsigned mask = __match_any_sync(live, c);
+    const int leader = __ffs(mask) - 1;
+    int basepos = 0;
+    if (lane == leader) basepos = atomicAdd(cursor + c, __popc(mask));
+    basepos = __shfl_sync(mask, basepos, leader);
+    const long long dst = (long long)offset[c] + basepos + __popc(mask & ((1u << lane) - 1));
+    if (FORM == 0) {
+      B64.r[dst] = A64.r[p]; B64.z[dst] = A64.z[p];
+      B64.ur[dst] = A64.ur[p]; B64.ut[dst] = A64.ut[p]; B64.uz[dst] = A64.uz[p];
+      B64.id[dst] = A64.id[p];
+    } else {
+      B32.key[dst] = A32.key[p]; B32.fr[dst] = A32.fr[p]; B32.fz[dst] = A32.fz[p];
+      B32.ur[dst] = A32.ur[p]; B32.ut[dst] = A32.ut[p]; B32.uz[dst] = A32.uz[p];
+      B32.id[dst] = A32.id[p];
+    }
+  }
+}
+
+__global__ void k_sort_finish(SimCounters *cnt, const int *offset, int ncell) {
+  cnt->n_total = (unsigned long long)offset[ncell];
+  cnt->n_births = 0;
+  cnt->sorted_total = cnt->n_total;
+}
+
+// ---------------------------------------------------------- diagnostics
+template <int FORM>
+__global__ void k_diag(State64 S64, State32 S32, SimCounters *cnt, double c, double me,
+                       double qe) {
+  const long long n0 = slots_in_use(cnt);
+  unsigned long long kin = 0, alive = 0;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n0;
+       p += (long long)gridDim.x * blockDim.x) {
+    double u2;
+    if (FORM == 0) {
+      if (S64.r[p] < 0) continue;
+      u2 = (S64.ur[p] * S64.ur[p] + S64.ut[p] * S64.ut[p] + S64.uz[p] * S64.uz[p]) / (c * c);
+    } else {
+      if (S32.key[p] == kDead) continue;
+      const double a = S32.ur[p], b = S32.ut[p], d = S32.uz[p];
+      u2 = a * a + b * b + d * d;
+    }
+    const double g = sqrt(1 + u2);
+    const double Eev = me * c * c * (u2 / (g + 1)) / qe;
+    kin += (unsigned long long)__double2ll_rn(Eev * 65536.0);
+    alive++;
+  }
+  for (int o = 16; o; o >>= 1) {
+    kin += __shfl_down_sync(0xFFFFFFFFu, kin, o);
+    alive += __shfl_down_sync(0xFFFFFFFFu, alive, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&cnt->kin_fx, kin);
+    atomicAdd(&cnt->alive, alive);
+  }
+}
+
+// trapezoid-weighted field energy (electricmagneticfield6.m:153-154),
+// per-block partial sums in a fixed order
+template <typename T>
+__global__ void k_field_energy(const T *Er, const T *Ez, const T *H, int nr, int nz, double dr,
+                               double dz, double *partial) {
+  __shared__ double sh[kBlock];
+  const int64_t nE = (int64_t)nr * (nz + 1), nZ = (int64_t)(nr + 1) * nz, nH = (int64_t)nr * nz;
+  double acc[3] = {0, 0, 0};
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < nE + nZ + nH;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    int f, ncol, nrow;
+    int64_t k;
+    double r0;
+    const T *A;
+    if (idx < nE) { f = 0; k = idx; ncol = nr; nrow = nz + 1; r0 = dr / 2; A = Er; }
+    else if (idx < nE + nZ) { f = 0; k = idx - nE; ncol = nr + 1; nrow = nz; r0 = 0; A = Ez; }
+    else { f = 1; k = idx - nE - nZ; ncol = nr; nrow = nz; r0 = dr / 2; A = H; }
+    const int i = (int)(k % ncol), j = (int)(k / ncol);
+    const double wi = (i == 0 || i == ncol - 1) ? 0.5 : 1.0;
+    const double wj = (j == 0 || j == nrow - 1) ? 0.5 : 1.0;
+    const double v = (double)A[k];
+    acc[f] += wi * wj * v * v * (r0 + i * dr) * dr * dz;
+  }
+  for (int f = 0; f < 2; ++f) {
+    sh[threadIdx.x] = acc[f];
+    __syncthreads();
+    for (int s = kBlock / 2; s; s >>= 1) {
+      if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x * 2 + f] = sh[0];
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+// ================================================================ sim object
+struct gasatt_sim {
+  gasatt_ctx *ctx = nullptr;
+  gasatt_sim_config cfg{};
+  SimTables tabs;
+  SimParams P{};
+  int form = 0;
+  // state (double-buffered for the sort)
+  State64 s64[2]{};
+  State32 s32[2]{};
+  int cur = 0;
+  void *Er = nullptr, *Ez = nullptr, *H = nullptr;
+  unsigned long long *Jr = nullptr, *Jz = nullptr;
+  double *d_tab = nullptr;
+  SimCounters *cnt = nullptr;
+  SimCounters *h_cnt = nullptr;   // pinned
+  int *cell_count = nullptr, *cell_offset = nullptr, *cell_cursor = nullptr;
+  void *scan_tmp = nullptr;
+  size_t scan_bytes = 0;
+  double *partial = nullptr;
+  int partial_blocks = 0;
+  std::vector<void *> allocs;
+  bool primed = false;
+  int64_t host_step = 0;          // particle passes completed
+  int64_t since_sort = 0;
+  cudaGraphExec_t g_step[2] = {nullptr, nullptr};
+  cudaGraphExec_t g_sort[2] = {nullptr, nullptr};
+  double scale = 1.0;
+  unsigned pass_grid = 0;
+};
+
+namespace {
+
+template <typename T>
+int sim_alloc(gasatt_sim *s, T **p, size_t n) {
+  cudaError_t e = cudaMalloc((void **)p, (n ? n : 1) * sizeof(T));
+  if (e != cudaSuccess) return cuda_fail(s->ctx, e, "cudaMalloc");
+  s->allocs.push_back((void *)*p);
+  return GASATT_OK;
+}
+
+#define SIM_TRY(x) do { int rc__ = (x); if (rc__) return rc__; } while (0)
+
+int launch_fdtd(gasatt_sim *s, cudaStream_t st) {
+  const auto &c = s->cfg;
+  const int nr = c.n_r, nz = c.n_z, R = c.fdtd_ratio;
+  const double dt = c.dt / R, mu = c.mu0, eps = c.eps0;
+  FdtdCoef fc;
+  fc.dr = c.dr; fc.dz = c.dz; fc.PHIp = c.PHIp; fc.inv_scale = 1.0 / s->scale;
+  fc.dt_eps = (dt / 2) / eps;
+  fc.dt_eps_dz = (dt / 2) / (eps * c.dz);
+  fc.axis = 4 * (dt / 2) / (eps * c.dr);
+  const unsigned gh = grid_for((int64_t)nr * nz, kBlock), ge = grid_for((int64_t)(nr + 1) * (nz + 1), kBlock);
+  auto H = [&](double h, bool last) {
+    if (s->form == 0)
+      k_sim_h<double><<<gh, kBlock, 0, st>>>((double *)s->H, (const double *)s->Er, (const double *)s->Ez,
+                                            nr, nz, h / (mu * c.dr), h / (mu * c.dz),
+                                            last ? s->Jr : nullptr, last ? s->Jz : nullptr,
+                                            last ? s->cnt : nullptr);
+    else
+      k_sim_h<float><<<gh, kBlock, 0, st>>>((float *)s->H, (const float *)s->Er, (const float *)s->Ez,
+                                           nr, nz, h / (mu * c.dr), h / (mu * c.dz),
+                                           last ? s->Jr : nullptr, last ? s->Jz : nullptr,
+                                           last ? s->cnt : nullptr);
+    s->ctx->launches++;
+  };
+  auto E = [&]() {
+    if (s->form == 0)
+      k_fdtd_e<double><<<ge, kBlock, 0, st>>>((double *)s->Er, (double *)s->Ez, (const double *)s->H,
+                                             s->Jr, s->Jz, nr, nz, fc, c.flags);
+    else
+      k_fdtd_e<float><<<ge, kBlock, 0, st>>>((float *)s->Er, (float *)s->Ez, (const float *)s->H,
+                                            s->Jr, s->Jz, nr, nz, fc, c.flags);
+    s->ctx->launches++;
+  };
+  // H(-dt/4) + H(dt/2) of the reference sequence merged into H(dt/4)
+  H(dt / 4, false);
+  for (int i = 0; i < 2 * R; ++i) {
+    E();
+    H(i == 2 * R - 1 ? dt / 4 : dt / 2, i == 2 * R - 1);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(s->ctx, e, "fdtd launch");
+  return GASATT_OK;
+}
+
+int launch_pass(gasatt_sim *s, cudaStream_t st, int mode) {
+  SimParams P = s->P;
+  const int b = s->cur;
+  if (s->form == 0)
+    k_pass64<<<s->pass_grid, kBlock, 0, st>>>(P, s->s64[b],
+                                              Fields<double>{(double *)s->Er, (double *)s->Ez, (double *)s->H},
+                                              s->cnt, mode);
+  else
+    k_pass32<<<s->pass_grid, kBlock, 0, st>>>(P, s->s32[b],
+                                              Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H},
+                                              s->cnt, mode);
+  s->ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(s->ctx, e, "particle pass launch");
+  return GASATT_OK;
+}
+
+// sort from buffer `from` into 1 - from
+int launch_sort(gasatt_sim *s, cudaStream_t st, int from) {
+  const auto &c = s->cfg;
+  const int ncell = c.n_r * c.n_z;
+  GASATT_CUDA(s->ctx, cudaMemsetAsync(s->cell_count, 0, (size_t)(ncell + 1) * 4, st));
+  GASATT_CUDA(s->ctx, cudaMemsetAsync(s->cell_cursor, 0, (size_t)ncell * 4, st));
+  const unsigned g = s->pass_grid;
+  if (s->form == 0)
+    k_sort_hist<0><<<g, kBlock, 0, st>>>(s->s64[from], s->s32[from], s->cnt, c.n_r, c.n_z, c.dr, c.dz, s->cell_count);
+  else
+    k_sort_hist<1><<<g, kBlock, 0, st>>>(s->s64[from], s->s32[from], s->cnt, c.n_r, c.n_z, c.dr, c.dz, s->cell_count);
+  s->ctx->launches++;
+  size_t nb = s->scan_bytes;
+  GASATT_CUDA(s->ctx, cub::DeviceScan::ExclusiveSum(s->scan_tmp, nb, s->cell_count, s->cell_offset, ncell + 1, st));
+  s->ctx->launches++;
+  if (s->form == 0)
+    k_sort_scatter<0><<<g, kBlock, 0, st>>>(s->s64[from], s->s64[1 - from], s->s32[from], s->s32[1 - from],
+                                            s->cnt, c.n_r, c.n_z, c.dr, c.dz, s->cell_offset, s->cell_cursor);
+  else
+    k_sort_scatter<1><<<g, kBlock, 0, st>>>(s->s64[from], s->s64[1 - from], s->s32[from], s->s32[1 - from],
+                                            s->cnt, c.n_r, c.n_z, c.dr, c.dz, s->cell_offset, s->cell_cursor);
+  s->ctx->launches++;
+  k_sort_finish<<<1, 1, 0, st>>>(s->cnt, s->cell_offset, ncell);
+  s->ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(s->ctx, e, "sort launch");
+  return GASATT_OK;
+}
+
+void drop_graphs(gasatt_sim *s) {
+  for (int i = 0; i < 2; ++i) {
+    if (s->g_step[i]) cudaGraphExecDestroy(s->g_step[i]);
+    if (s->g_sort[i]) cudaGraphExecDestroy(s->g_sort[i]);
+    s->g_step[i] = s->g_sort[i] = nullptr;
+  }
+}
+
+// capture one step (FDTD + pass) for state buffer b, and one sort b -> 1-b
+int build_graphs(gasatt_sim *s) {
+  cudaStream_t cs;
+  GASATT_CUDA(s->ctx, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  const int save = s->cur;
+  const int64_t save_launch = s->ctx->launches;
+  for (int b = 0; b < 2; ++b) {
+    cudaGraph_t g;
+    s->cur = b;
+    GASATT_CUDA(s->ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    int rc = launch_fdtd(s, cs);
+    if (!rc) rc = launch_pass(s, cs, 0);
+    cudaError_t e = cudaStreamEndCapture(cs, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(s->ctx, e, "capture step");
+    GASATT_CUDA(s->ctx, cudaGraphInstantiate(&s->g_step[b], g, 0));
+    cudaGraphDestroy(g);
+    GASATT_CUDA(s->ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    rc = launch_sort(s, cs, b);
+    e = cudaStreamEndCapture(cs, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(s->ctx, e, "capture sort");
+    GASATT_CUDA(s->ctx, cudaGraphInstantiate(&s->g_sort[b], g, 0));
+    cudaGraphDestroy(g);
+  }
+  s->cur = save;
+  s->ctx->launches = save_launch;
+  cudaStreamDestroy(cs);
+  return GASATT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gasatt_sim_default_config(gasatt_sim_config *c) {
+  if (!c) return GASATT_E_ARG;
+  std::memset(c, 0, sizeof(*c));
+  c->n_r = 256; c->n_z = 1024; c->dr = 5e-6; c->dz = 5e-6; c->dt = 1e-14;
+  c->fdtd_ratio = 1;
+  c->PHIp = 2 * GASATT_PI;
+  c->FN = 1.0;
+  c->gas_temperature = 300.0;
+  c->kb = 1.380649e-23;
+  c->gas_density = 133.322368 / (c->kb * 300.0);     // 1 Torr
+  c->q_e = 1.602176634e-19; c->m_e = 9.1093837015e-31; c->c = 299792458.0;
+  c->eps0 = 8.8541878128e-12; c->mu0 = 1.25663706212e-6;
+  c->m_ion = 28.0134 * 1.66053906660e-27;
+  c->precision = GASATT_FP32_SPLIT;
+  c->capacity = 1 << 20;
+  c->ion_capacity = 0;
+  c->seed = 0;
+  c->flags = 0;
+  c->sort_period = 20;
+  c->secondaries = 1;
+  c->table_n = 2048; c->table_emin_ev = 0.1; c->table_emax_ev = 30000.0;
+  return GASATT_OK;
+}
+
+int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasatt_tables *tab,
+                      gasatt_sim **out) {
+  if (!ctx || !cfg || !out) return GASATT_E_ARG;
+  *out = nullptr;
+  const gasatt_sim_config &c = *cfg;
+  if (c.n_r < 2 || c.n_z < 2 || c.n_r > 65535 || c.n_z > 65535 || !(c.dr > 0) || !(c.dz > 0) ||
+      !(c.dt > 0) || c.fdtd_ratio < 1 || c.capacity < 1 ||
+      (c.precision != GASATT_FP64 && c.precision != GASATT_FP32_SPLIT))
+    return fail(ctx, GASATT_E_ARG, "sim config out of range");
+  if (c.flags & ~(unsigned)(GASATT_Q_ER_END_COPY | GASATT_Q_EZ_AXIS_JSIGN | GASATT_Q_EZ_RSHIFT))
+    return fail(ctx, GASATT_E_ARG, "the resident simulation accepts only the field quirk flags");
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  gasatt_sim *s = new gasatt_sim();
+  s->ctx = ctx;
+  s->cfg = c;
+  s->form = c.precision;
+  std::string err;
+  int rc = build_sim_tables(tab, c.table_n, c.table_emin_ev, c.table_emax_ev, c.gas_density, c.c,
+                            c.m_e, c.q_e, s->tabs, err);
+  if (rc) { delete s; return fail(ctx, rc, err); }
+  const int64_t cap = c.capacity;
+  const int nr = c.n_r, nz = c.n_z, ncell = nr * nz;
+  auto cleanup = [&](int code) { gasatt_sim_destroy(s); return code; };
+  for (int b = 0; b < 2; ++b) {
+    if (s->form == 0) {
+      State64 &S = s->s64[b];
+      if ((rc = sim_alloc(s, &S.r, cap)) || (rc = sim_alloc(s, &S.z, cap)) || (rc = sim_alloc(s, &S.ur, cap)) ||
+          (rc = sim_alloc(s, &S.ut, cap)) || (rc = sim_alloc(s, &S.uz, cap)) || (rc = sim_alloc(s, &S.id, cap)))
+        return cleanup(rc);
+    } else {
+      State32 &S = s->s32[b];
+      if ((rc = sim_alloc(s, &S.key, cap)) || (rc = sim_alloc(s, &S.fr, cap)) || (rc = sim_alloc(s, &S.fz, cap)) ||
+          (rc = sim_alloc(s, &S.ur, cap)) || (rc = sim_alloc(s, &S.ut, cap)) || (rc = sim_alloc(s, &S.uz, cap)) ||
+          (rc = sim_alloc(s, &S.id, cap)))
+        return cleanup(rc);
+    }
+  }
+  const size_t esz = s->form == 0 ? 8 : 4;
+  double *tmpd;
+  if ((rc = sim_alloc(s, (char **)&s->Er, (size_t)nr * (nz + 1) * esz)) ||
+      (rc = sim_alloc(s, (char **)&s->Ez, (size_t)(nr + 1) * nz * esz)) ||
+      (rc = sim_alloc(s, (char **)&s->H, (size_t)nr * nz * esz)) ||
+      (rc = sim_alloc(s, &s->Jr, (size_t)ncell)) || (rc = sim_alloc(s, &s->Jz, (size_t)ncell)) ||
+      (rc = sim_alloc(s, &s->cnt, 1)) || (rc = sim_alloc(s, &s->cell_count, (size_t)ncell + 1)) ||
+      (rc = sim_alloc(s, &s->cell_offset, (size_t)ncell + 1)) ||
+      (rc = sim_alloc(s, &s->cell_cursor, (size_t)ncell)) ||
+      (rc = sim_alloc(s, &tmpd, (size_t)3 * c.table_n + (size_t)181 * c.table_n)))
+    return cleanup(rc);
+  s->d_tab = tmpd;
+  cub::DeviceScan::ExclusiveSum(nullptr, s->scan_bytes, s->cell_count, s->cell_offset, ncell + 1);
+  if ((rc = sim_alloc(s, (char **)&s->scan_tmp, s->scan_bytes))) return cleanup(rc);
+  s->partial_blocks = 296;
+  if ((rc = sim_alloc(s, &s->partial, (size_t)2 * s->partial_blocks))) return cleanup(rc);
+  if (cudaMallocHost((void **)&s->h_cnt, sizeof(SimCounters)) != cudaSuccess)
+    return cleanup(fail(ctx, GASATT_E_CUDA, "cudaMallocHost"));
+  // tables
+  std::vector<double> host((size_t)3 * c.table_n + (size_t)181 * c.table_n);
+  std::memcpy(host.data(), s->tabs.sig_el.data(), c.table_n * 8);
+  std::memcpy(host.data() + c.table_n, s->tabs.sig_ion.data(), c.table_n * 8);
+  std::memcpy(host.data() + 2 * c.table_n, s->tabs.sig_exc.data(), c.table_n * 8);
+  std::memcpy(host.data() + 3 * c.table_n, s->tabs.cdf.data(), (size_t)181 * c.table_n * 8);
+  if (cudaMemcpy(s->d_tab, host.data(), host.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+    return cleanup(fail(ctx, GASATT_E_CUDA, "table upload"));
+  // parameters
+  SimParams &P = s->P;
+  P.nr = nr; P.nz = nz; P.dr = c.dr; P.dz = c.dz; P.dt = c.dt; P.c = c.c; P.qe = c.q_e;
+  P.me = c.m_e; P.mu0 = c.mu0; P.FN = c.FN; P.PHIp = c.PHIp; P.n_gas = c.gas_density;
+  P.nu_max = s->tabs.nu_max; P.P_null = -std::expm1(-s->tabs.nu_max * c.dt);
+  P.Rp = nr * c.dr; P.Lp = nz * c.dz; P.kb = c.kb; P.m_ion = c.m_ion; P.T_gas = c.gas_temperature;
+  P.seed = c.seed; P.secondaries = c.secondaries; P.cap = cap;
+  P.qm_dt2 = -c.q_e / c.m_e * c.dt / 2;
+  P.aE = (float)(-c.q_e * c.dt / (2 * c.m_e * c.c));
+  P.aB = (float)(-c.q_e * c.dt * c.mu0 / (2 * c.m_e));
+  P.hdr = (float)(c.c * c.dt / (2 * c.dr));
+  P.hdz = (float)(c.c * c.dt / (2 * c.dz));
+  // fixed point: FP64 |q FN v w| * scale <= 2^48; FP32 <= 2^25 (one warp sum fits int32)
+  const double qfc = c.q_e * std::fabs(c.FN) * c.c;
+  s->scale = s->form == 0 ? std::ldexp(1.0, 48) / qfc : std::ldexp(1.0, 25) / qfc;
+  P.dep = s->form == 0 ? s->scale : -c.q_e * c.FN * c.c * s->scale;
+  P.sig = s->d_tab;
+  P.cdf = s->d_tab + 3 * c.table_n;
+  P.G = c.table_n; P.lnEmin = s->tabs.lnEmin; P.dlnE = s->tabs.dlnE;
+  P.n_exc = s->tabs.n_exc;
+  std::memcpy(P.exc, s->tabs.exc, sizeof(P.exc));
+  P.Jr = s->Jr; P.Jz = s->Jz;
+  int dev = ctx->device, nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  int occ = 4;
+  if (s->form == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass64, kBlock, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass32, kBlock, 0);
+  s->pass_grid = (unsigned)(nsm * (occ > 0 ? occ : 1));
+  // zero state
+  SimCounters z{};
+  z.step = -1;
+  z.cap = (unsigned long long)cap;
+  if (cudaMemcpy(s->cnt, &z, sizeof(z), cudaMemcpyHostToDevice) != cudaSuccess)
+    return cleanup(fail(ctx, GASATT_E_CUDA, "counter init"));
+  cudaMemset(s->Er, 0, (size_t)nr * (nz + 1) * esz);
+  cudaMemset(s->Ez, 0, (size_t)(nr + 1) * nz * esz);
+  cudaMemset(s->H, 0, (size_t)nr * nz * esz);
+  cudaMemset(s->Jr, 0, (size_t)ncell * 8);
+  cudaMemset(s->Jz, 0, (size_t)ncell * 8);
+  rc = build_graphs(s);
+  if (rc) return cleanup(rc);
+  if (cudaDeviceSynchronize() != cudaSuccess) return cleanup(fail(ctx, GASATT_E_CUDA, "sim init"));
+  *out = s;
+  return GASATT_OK;
+}
+
+int gasatt_sim_destroy(gasatt_sim *s) {
+  if (!s) return GASATT_OK;
+  cudaSetDevice(s->ctx->device);
+  cudaDeviceSynchronize();
+  drop_graphs(s);
+  for (void *p : s->allocs) cudaFree(p);
+  if (s->h_cnt) cudaFreeHost(s->h_cnt);
+  delete s;
+  return GASATT_OK;
+}
+
+int gasatt_sim_load(gasatt_sim *s, const double *r, const double *z, const double *ur,
+                    const double *ut, const double *uz, const uint64_t *id, int64_t n,
+                    int on_device) {
+  if (!s) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  if (n < 0 || n > s->cfg.capacity) return fail(ctx, GASATT_E_CAPACITY, "load exceeds capacity");
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const double *src[5] = {r, z, ur, ut, uz};
+  const double *d[5];
+  const uint64_t *did = id;
+  void *buf = nullptr;
+  if (!on_device && n > 0) {
+    int rc = scratch(ctx, (size_t)n * 48, &buf);
+    if (rc) return rc;
+    for (int i = 0; i < 5; ++i) {
+      d[i] = (double *)buf + (size_t)i * n;
+      GASATT_CUDA(ctx, cudaMemcpyAsync((void *)d[i], src[i], (size_t)n * 8, cudaMemcpyHostToDevice, st));
+    }
+    did = (uint64_t *)((double *)buf + 5 * (size_t)n);
+    GASATT_CUDA(ctx, cudaMemcpyAsync((void *)did, id, (size_t)n * 8, cudaMemcpyHostToDevice, st));
+  } else {
+    for (int i = 0; i < 5; ++i) d[i] = src[i];
+  }
+  s->cur = 0;
+  if (n > 0) {
+    if (s->form == 0)
+      k_load64<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->s64[0], d[0], d[1], d[2], d[3], d[4], did, n);
+    else
+      k_load32<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->s32[0], d[0], d[1], d[2], d[3], d[4], did, n,
+                                                       s->cfg.n_r, s->cfg.n_z, s->cfg.dr, s->cfg.dz, s->cfg.c);
+    GASATT_LAUNCHED(ctx);
+  }
+  SimCounters zc{};
+  zc.n_total = (unsigned long long)n;
+  zc.step = -1;
+  zc.cap = (unsigned long long)s->cfg.capacity;
+  GASATT_CUDA(ctx, cudaMemcpyAsync(s->cnt, &zc, sizeof(zc), cudaMemcpyHostToDevice, st));
+  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  s->primed = false;
+  s->host_step = 0;
+  s->since_sort = 0;
+  return GASATT_OK;
+}
+
+int gasatt_sim_read(gasatt_sim *s, double *r, double *z, double *ur, double *ut, double *uz,
+                    uint64_t *id, int64_t cap, int64_t *n_out, int on_device) {
+  if (!s) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  GASATT_CUDA(ctx, cudaMemcpyAsync(s->h_cnt, s->cnt, sizeof(SimCounters), cudaMemcpyDeviceToHost, st));
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  const unsigned long long nt = s->h_cnt->n_total + s->h_cnt->n_births;
+  const int64_t n = (int64_t)(nt < s->h_cnt->cap ? nt : s->h_cnt->cap);
+  if (n_out) *n_out = n;
+  if (n > cap) return fail(ctx, GASATT_E_CAPACITY, "read buffer too small");
+  if (n == 0) return GASATT_OK;
+  double *d[5] = {r, z, ur, ut, uz};
+  uint64_t *did = id;
+  void *buf = nullptr;
+  if (!on_device) {
+    int rc = scratch(ctx, (size_t)n * 48, &buf);
+    if (rc) return rc;
+    for (int i = 0; i < 5; ++i) d[i] = (double *)buf + (size_t)i * n;
+    did = (uint64_t *)((double *)buf + 5 * (size_t)n);
+  }
+  if (s->form == 0)
+    k_read64<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->s64[s->cur], d[0], d[1], d[2], d[3], d[4], did, n);
+  else
+    k_read32<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->s32[s->cur], d[0], d[1], d[2], d[3], d[4], did, n,
+                                                     s->cfg.dr, s->cfg.dz, s->cfg.c);
+  GASATT_LAUNCHED(ctx);
+  if (!on_device) {
+    double *h[5] = {r, z, ur, ut, uz};
+    for (int i = 0; i < 5; ++i)
+      GASATT_CUDA(ctx, cudaMemcpyAsync(h[i], d[i], (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    GASATT_CUDA(ctx, cudaMemcpyAsync(id, did, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+  }
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  return GASATT_OK;
+}
+
+namespace {
+__global__ void k_f64_to_f32(const double *a, float *b, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+__global__ void k_f32_to_f64(const float *a, double *b, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (double)a[i];
+}
+__global__ void k_j_to_density(const unsigned long long *J, int nr, int nz, double inv_scale,
+                               double dr, double dz, double PHIp, double *out) {
+  const int64_t n = (int64_t)nr * nz;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (double)(long long)J[i] * inv_scale / shell_volume((int)(i % nr), dr, dz, PHIp);
+}
+
+int fields_io(gasatt_sim *s, double *Er, double *Ez, double *H, int on_device, bool set) {
+  gasatt_ctx *ctx = s->ctx;
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int nr = s->cfg.n_r, nz = s->cfg.n_z;
+  const int64_t n[3] = {(int64_t)nr * (nz + 1), (int64_t)(nr + 1) * nz, (int64_t)nr * nz};
+  double *u[3] = {Er, Ez, H};
+  void *dev[3] = {s->Er, s->Ez, s->H};
+  void *buf = nullptr;
+  if (!on_device || s->form == 1) {
+    int rc = scratch(ctx, (size_t)(n[0] + n[1] + n[2]) * 8, &buf);
+    if (rc) return rc;
+  }
+  int64_t off = 0;
+  for (int f = 0; f < 3; ++f) {
+    double *stage = on_device ? u[f] : (double *)buf + off;
+    if (set) {
+      if (!on_device)
+        GASATT_CUDA(ctx, cudaMemcpyAsync(stage, u[f], n[f] * 8, cudaMemcpyHostToDevice, st));
+      if (s->form == 0) GASATT_CUDA(ctx, cudaMemcpyAsync(dev[f], stage, n[f] * 8, cudaMemcpyDeviceToDevice, st));
+      else { k_f64_to_f32<<<grid_for(n[f], kBlock), kBlock, 0, st>>>(stage, (float *)dev[f], n[f]); GASATT_LAUNCHED(ctx); }
+    } else {
+      if (s->form == 0) GASATT_CUDA(ctx, cudaMemcpyAsync(stage, dev[f], n[f] * 8, cudaMemcpyDeviceToDevice, st));
+      else { k_f32_to_f64<<<grid_for(n[f], kBlock), kBlock, 0, st>>>((float *)dev[f], stage, n[f]); GASATT_LAUNCHED(ctx); }
+      if (!on_device)
+        GASATT_CUDA(ctx, cudaMemcpyAsync(u[f], stage, n[f] * 8, cudaMemcpyDeviceToHost, st));
+    }
+    off += n[f];
+  }
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  return GASATT_OK;
+}
+}  // namespace
+
+int gasatt_sim_set_fields(gasatt_sim *s, const double *Er, const double *Ez, const double *H,
+                          int on_device) {
+  if (!s) return GASATT_E_ARG;
+  return fields_io(s, (double *)Er, (double *)Ez, (double *)H, on_device, true);
+}
+
+int gasatt_sim_get_fields(gasatt_sim *s, double *Er, double *Ez, double *H, int on_device) {
+  if (!s) return GASATT_E_ARG;
+  return fields_io(s, Er, Ez, H, on_device, false);
+}
+
+int gasatt_sim_get_current(gasatt_sim *s, double *jr, double *jz, int on_device) {
+  if (!s) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int nr = s->cfg.n_r, nz = s->cfg.n_z;
+  const int64_t n = (int64_t)nr * nz;
+  double *d[2] = {jr, jz};
+  void *buf = nullptr;
+  if (!on_device) {
+    int rc = scratch(ctx, (size_t)n * 16, &buf);
+    if (rc) return rc;
+    d[0] = (double *)buf; d[1] = (double *)buf + n;
+  }
+  const unsigned long long *J[2] = {s->Jr, s->Jz};
+  for (int f = 0; f < 2; ++f) {
+    k_j_to_density<<<grid_for(n, kBlock), kBlock, 0, st>>>(J[f], nr, nz, 1.0 / s->scale, s->cfg.dr,
+                                                           s->cfg.dz, s->cfg.PHIp, d[f]);
+    GASATT_LAUNCHED(ctx);
+  }
+  if (!on_device) {
+    GASATT_CUDA(ctx, cudaMemcpyAsync(jr, d[0], n * 8, cudaMemcpyDeviceToHost, st));
+    GASATT_CUDA(ctx, cudaMemcpyAsync(jz, d[1], n * 8, cudaMemcpyDeviceToHost, st));
+  }
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  return GASATT_OK;
+}
+
+int gasatt_sim_sort(gasatt_sim *s) {
+  if (!s) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  GASATT_CUDA(ctx, cudaGraphLaunch(s->g_sort[s->cur], ctx->stream));
+  ctx->launches += 4;
+  s->cur = 1 - s->cur;
+  s->since_sort = 0;
+  return GASATT_OK;
+}
+
+int gasatt_sim_step(gasatt_sim *s, int nsteps) {
+  if (!s || nsteps < 0) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  if (!s->primed) {
+    // start of a run: particles at x^0 move to x^{1/2} and deposit j^{1/2}
+    if (s->cfg.sort_period > 0) SIM_TRY(gasatt_sim_sort(s));
+    SIM_TRY(launch_pass(s, st, 1));
+    s->primed = true;
+  }
+  const int per_step = 4 * s->cfg.fdtd_ratio + 2;
+  for (int k = 0; k < nsteps; ++k) {
+    if (s->cfg.sort_period > 0 && s->since_sort >= s->cfg.sort_period) SIM_TRY(gasatt_sim_sort(s));
+    GASATT_CUDA(ctx, cudaGraphLaunch(s->g_step[s->cur], st));
+    ctx->launches += per_step;
+    s->host_step++;
+    s->since_sort++;
+  }
+  return GASATT_OK;
+}
+
+int gasatt_sim_diag(gasatt_sim *s, gasatt_diag *d) {
+  if (!s || !d) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  GASATT_CUDA(ctx, cudaMemsetAsync((char *)s->cnt + offsetof(SimCounters, kin_fx), 0, 16, st));
+  if (s->form == 0) k_diag<0><<<s->pass_grid, kBlock, 0, st>>>(s->s64[s->cur], s->s32[s->cur], s->cnt, s->cfg.c, s->cfg.m_e, s->cfg.q_e);
+  else k_diag<1><<<s->pass_grid, kBlock, 0, st>>>(s->s64[s->cur], s->s32[s->cur], s->cnt, s->cfg.c, s->cfg.m_e, s->cfg.q_e);
+  GASATT_LAUNCHED(ctx);
+  const int nr = s->cfg.n_r, nz = s->cfg.n_z;
+  if (s->form == 0)
+    k_field_energy<double><<<s->partial_blocks, kBlock, 0, st>>>((double *)s->Er, (double *)s->Ez, (double *)s->H, nr, nz, s->cfg.dr, s->cfg.dz, s->partial);
+  else
+    k_field_energy<float><<<s->partial_blocks, kBlock, 0, st>>>((float *)s->Er, (float *)s->Ez, (float *)s->H, nr, nz, s->cfg.dr, s->cfg.dz, s->partial);
+  GASATT_LAUNCHED(ctx);
+  std::vector<double> part(2 * s->partial_blocks);
+  GASATT_CUDA(ctx, cudaMemcpyAsync(s->h_cnt, s->cnt, sizeof(SimCounters), cudaMemcpyDeviceToHost, st));
+  GASATT_CUDA(ctx, cudaMemcpyAsync(part.data(), s->partial, part.size() * 8, cudaMemcpyDeviceToHost, st));
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  const SimCounters &h = *s->h_cnt;
+  double we = 0, wm = 0;
+  for (int b = 0; b < s->partial_blocks; ++b) { we += part[2 * b]; wm += part[2 * b + 1]; }
+  d->n_alive = (int64_t)h.alive;
+  d->n_total = (int64_t)(h.n_total + h.n_births < h.cap ? h.n_total + h.n_births : h.cap);
+  d->n_ionizations = (int64_t)h.ion;
+  d->n_elastic = (int64_t)h.ela;
+  d->n_excitation = (int64_t)h.exc;
+  d->n_null = (int64_t)h.nul;
+  d->n_lost_wall = (int64_t)h.lost;
+  d->n_ions = 0;
+  d->kinetic_ev = (double)h.kin_fx / 65536.0;
+  d->field_energy_j = s->cfg.PHIp * 0.5 * s->cfg.eps0 * we + s->cfg.PHIp * 0.5 * s->cfg.mu0 * wm;
+  d->steps = s->host_step;
+  d->status_flags = (h.cap_overflow ? 2 : 0);
+  return GASATT_OK;
+}
+
+int gasatt_sim_run_host(gasatt_sim *s, double *pos, double *vel, int64_t *n_io, int64_t cap,
+                        int nsteps) {
+  (void)pos; (void)vel; (void)n_io; (void)cap; (void)nsteps;
+  if (!s) return GASATT_E_ARG;
+  return fail(s->ctx, GASATT_E_STATE, "gasatt_sim_run_host: not available yet");
+}
+
+}  // extern "C"

@@ -1,0 +1,277 @@
+/*
+ * gasatt.h - C ABI of the B200 PIC-MCC electron step for the N2 X-ray gas
+ * attenuator (axisymmetric r-z, Yee FDTD, null-collision Monte Carlo).
+ *
+ * Two groups of entry points:
+ *
+ *  1. Drop-ins for the MATLAB functions of the reference driver.  Each takes
+ *     DEVICE pointers to column-major (MATLAB layout) arrays plus sizes and a
+ *     context, and replaces one reference function:
+ *        gasatt_find_CS0               find_CS0.m:1-61
+ *        gasatt_free_motion            free_motion.m:1-9
+ *        gasatt_particle_density       particle_density.m:1-38
+ *        gasatt_electricmagneticfield6 electricmagneticfield6.m:1-188
+ *                                      (EM2.cu, EM7.cu, EM3_1.cu, EM3.cu, EM4.cu)
+ *        gasatt_electron_collision     electron_collision.m:1-75
+ *                                      (electron_transport.cu:3-229)
+ *     The cross-section tables are passed as HOST pointers in the shapes that
+ *     MATLAB's readtable produces (see gasatt_tables below).
+ *
+ *  2. The resident simulation ("sim"): particles live in HBM in the
+ *     library's own SoA layout (plain FP64 or FP32 split precision) and one
+ *     call advances N steps of push + MCC + deposit + FDTD.
+ *
+ * Every function returns a gasatt status (0 = OK).  gasatt_last_error()
+ * gives the message of the last failure on a context.  A context is used by
+ * one host thread at a time; different contexts are independent.
+ */
+#ifndef GASATT_H
+#define GASATT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define GASATT_OK            0
+#define GASATT_E_ARG         1   /* bad argument / shape                     */
+#define GASATT_E_CUDA        2   /* CUDA runtime error                       */
+#define GASATT_E_CAPACITY    3   /* particle capacity exceeded               */
+#define GASATT_E_NAN         4   /* non-finite value detected in a kernel    */
+#define GASATT_E_TABLES      5   /* cross-section tables missing / invalid   */
+#define GASATT_E_STATE       6   /* call out of order                        */
+#define GASATT_E_NODEVICE    7   /* no CUDA device / library built without   */
+
+/* ---------------------------------------------------------- quirk flags
+ * Each bit reproduces one behaviour of the reference that the resident
+ * simulation corrects.  The drop-ins default to GASATT_FAITHFUL (reference
+ * behaviour); the simulation uses 0.
+ */
+#define GASATT_Q_EULER_KICK     (1u << 0)  /* EM4.cu:134-138 explicit kick, not Boris        */
+#define GASATT_Q_ATAN_PHI       (1u << 1)  /* EM2.cu:30, EM4.cu:151 phi=atan(y/x) (axis mirror)*/
+#define GASATT_Q_ER_END_COPY    (1u << 2)  /* EM3.cu:21-27 Er(z=0,Lp) copied, not PEC zero      */
+#define GASATT_Q_EZ_AXIS_JSIGN  (1u << 3)  /* EM3.cu:35 axis Ez adds +jz                         */
+#define GASATT_Q_EZ_RSHIFT      (1u << 4)  /* EM3.cu:39 radius (nr+1)dr at Ez node nr            */
+#define GASATT_Q_XS_LINEAR_E    (1u << 5)  /* electron_transport.cu:89 keV compared to log(E)     */
+#define GASATT_Q_COLL_LINEAR_P  (1u << 6)  /* electron_transport.cu:74-79 p=v dt n sigma         */
+#define GASATT_Q_SEC_LAB_FRAME  (1u << 7)  /* electron_transport.cu:198-200 secondary about lab z */
+#define GASATT_Q_EXC_POWF       (1u << 8)  /* electron_transport.cu:214-215 single-precision pow  */
+#define GASATT_Q_XS_NAN         (1u << 9)  /* find_CS0.m:16-56 NaN/neg. outside the tables        */
+#define GASATT_Q_PI7            (1u << 10) /* electron_transport.cu:53 pi = 3.1415926             */
+#define GASATT_Q_CDF_NEXTBIN    (1u << 11) /* electron_transport.cu:103-121 rectangle CDF, next-bin inverse */
+#define GASATT_FAITHFUL         0x0FFFu
+/* input-convention bit for gasatt_electricmagneticfield6: positions arrive as
+ * (r, phi, z) columns (electricmagneticfield6.m:113-115) instead of (x, y, z) */
+#define GASATT_POS_IN_CYL       (1u << 16)
+
+/* ------------------------------------------------ reference constants
+ * The reference uses different values per file; the drop-ins use the value of
+ * the file they replace.
+ */
+#define GASATT_EM_E        1.6e-19          /* electricmagneticfield6.m:11 */
+#define GASATT_EM_ME       9.1096e-31       /* electricmagneticfield6.m:5  */
+#define GASATT_EM_MION     4.65e-26         /* electricmagneticfield6.m:6-7 */
+#define GASATT_EM_C        3e8              /* electricmagneticfield6.m:8  */
+#define GASATT_EM_EPS      8.854187817e-12  /* electricmagneticfield6.m:9  */
+#define GASATT_PI          3.141592653589793
+#define GASATT_EM_MU       (4.0 * GASATT_PI * 1e-7) /* electricmagneticfield6.m:10 */
+#define GASATT_MCC_E       1.6022e-19       /* electron_transport.cu:47 */
+#define GASATT_MCC_C       3e8              /* electron_transport.cu:48 */
+#define GASATT_MCC_ME      9.109e-31        /* electron_transport.cu:49 */
+#define GASATT_MCC_MION    4.65e-26         /* electron_transport.cu:50 */
+#define GASATT_MCC_KB      1.38064853e-23   /* electron_transport.cu:51 */
+#define GASATT_MCC_PI7     3.1415926        /* electron_transport.cu:53 */
+#define GASATT_MCC_Q0      6.514e-14        /* electron_transport.cu:208 */
+#define GASATT_ION_I_EV    15.6             /* electron_transport.cu:60 */
+#define GASATT_CS_Q0       6.542e-14        /* find_CS0.m:42 */
+#define GASATT_A0SQ        2.8002852e-21    /* find_CS0.m:17, electron_collision.m:12 */
+
+/* injected random draws per particle for gasatt_electron_collision:
+ * [0] p1  [1] p2  [2] elastic angle / ionization split  [3] azimuth
+ * [4..6] three standard normals (ion Maxwellian), used as float like curand_normal */
+#define GASATT_MCC_NDRAW   8
+
+/* --------------------------------------------------------------- tables
+ * Raw N2 tables as MATLAB readtable gives them (electron_transport_field3.m:8-37),
+ * column-major, HOST memory:
+ *   t_el    2 x n_el      row 0 energy [keV], row 1 sigma [a0^2 per N atom]
+ *   t_sel   n_sel x 2     energy [eV], sigma [1e-20 m^2]          (1..50 eV)
+ *   t_sel_1 n_sel1 x 2    energy [eV], sigma [1e-20 m^2]          (5..50 eV)
+ *   t_del   181+1 x n_del row 0 energies [keV], col 0 angles, DCS body
+ *   t_sdel  181+1 x n_sdel same, low-energy DCS
+ *   t_ion   n_ion x 2     energy [eV], sigma [1e-20 m^2]
+ *   t_exc   n_exc x 5     k [eV], A, omega, nu, gamma
+ */
+typedef struct gasatt_tables {
+  const double *t_el;    int n_el;
+  const double *t_sel;   int n_sel;
+  const double *t_sel_1; int n_sel1;
+  const double *t_del;   int del_rows;  int del_cols;
+  const double *t_sdel;  int sdel_rows; int sdel_cols;
+  const double *t_ion;   int n_ion;
+  const double *t_exc;   int n_exc;
+} gasatt_tables;
+
+/* -------------------------------------------------------------- context */
+typedef struct gasatt_ctx gasatt_ctx;
+
+int         gasatt_create(gasatt_ctx **ctx, int device, uint64_t seed);
+int         gasatt_destroy(gasatt_ctx *ctx);
+const char *gasatt_last_error(const gasatt_ctx *ctx);
+/* stream (cudaStream_t as void*) used for every launch on this context; NULL = legacy default */
+int         gasatt_set_stream(gasatt_ctx *ctx, void *stream);
+int         gasatt_synchronize(gasatt_ctx *ctx);
+/* number of kernels this context launched since creation (monotone counter) */
+int64_t     gasatt_kernel_launches(const gasatt_ctx *ctx);
+const char *gasatt_version(void);
+
+/* ------------------------------------------------------------- drop-ins */
+
+/* find_CS0.m:1-61.  E_keV, sig_* : device, length n.  Tables: host. */
+int gasatt_find_CS0(gasatt_ctx *ctx, const gasatt_tables *tab,
+                    const double *E_keV, int64_t n,
+                    double *sig_el, double *sig_ion, double *sig_exc,
+                    unsigned flags);
+
+/* free_motion.m:1-9.  All device arrays of length n. */
+int gasatt_free_motion(gasatt_ctx *ctx,
+                       const double *vx, const double *vy, const double *vz,
+                       const double *x, const double *y, const double *z,
+                       int64_t n, double dt,
+                       double *xn, double *yn, double *zn, double *rn, double *phin);
+
+/* particle_density.m:1-38 (10-argument form).
+ * dphi, sum_cell: device arrays of length rmax (sum_cell(k) = cells with r index <= k).
+ * r, phi, z: device, length n.  VC: device, length cellnumxy (volume of the
+ * cells of one z layer, calculate_VC.m).  density: device, length ncell
+ * (= cellnumxy * zmax), overwritten.  Particles whose cell index falls
+ * outside [1, ncell] are not counted. */
+int gasatt_particle_density(gasatt_ctx *ctx, double dr, double dz,
+                            const double *dphi, int rmax,
+                            const double *r, const double *phi, const double *z,
+                            int64_t n, int cellnumxy, const double *sum_cell,
+                            const double *VC, int64_t ncell, double FN,
+                            double *density);
+
+/* electricmagneticfield6.m:1-188.  Species arrays are device, column-major
+ * with leading dimension equal to their count (n x 3).  Positions arrive as
+ * (r,phi,z) when GASATT_POS_IN_CYL is set (the reference convention) else
+ * (x,y,z); they leave as (x,y,z).  Deleted particles (r > Rp) are removed in
+ * place, order kept; the new counts are returned in *_out and the first
+ * n_out rows of each array (leading dimension unchanged) hold the survivors.
+ * Er: n_r x (n_z+1), Ez: (n_r+1) x n_z, Hphi: n_r x n_z, updated in place.
+ * electron_kinetic: device, length n_e, kinetic energy [keV] of the surviving
+ * electrons.  cycle_time/5 particle steps of 5*dt are taken
+ * (electricmagneticfield6.m:134-138). */
+int gasatt_electricmagneticfield6(gasatt_ctx *ctx,
+                                  double *e_pos, double *e_vel, int64_t n_e,
+                                  double *i1_pos, double *i1_vel, int64_t n_i1,
+                                  double *i2_pos, double *i2_vel, int64_t n_i2,
+                                  double *Er, double *Ez, double *Hphi,
+                                  int n_r, int n_z,
+                                  double delta, double dt, double Rp, double Lp,
+                                  double PHIp, double FN, int cycle_time,
+                                  double *electron_kinetic,
+                                  int64_t *n_e_out, int64_t *n_i1_out, int64_t *n_i2_out,
+                                  unsigned flags);
+
+/* electron_collision.m:1-75 with electron_transport.cu:3-229.
+ * e_pos/e_vel: device, column-major with leading dimension cap_e (>= n_e plus
+ * room for one secondary per electron); i1_pos/i1_vel likewise with cap_i1.
+ * electron_kinetic, sig_*: device length n_e.  density, temperature: device,
+ * length ncell.  sum_cell, phimax: host, length rmax.  draws: optional device
+ * array n_e x GASATT_MCC_NDRAW (row-major per particle) of injected draws;
+ * NULL draws from Philox keyed on (context seed, particle index, call count).
+ * Secondaries are appended to the electrons and ions to ion1 in parent order
+ * (MATLAB logical indexing, electron_collision.m:63-75). */
+int gasatt_electron_collision(gasatt_ctx *ctx,
+                              double *e_pos, double *e_vel, int64_t n_e, int64_t cap_e,
+                              double *i1_pos, double *i1_vel, int64_t n_i1, int64_t cap_i1,
+                              const gasatt_tables *tab,
+                              const double *electron_kinetic,
+                              const double *sum_cell, int rmax, int cellnumxy,
+                              const double *density, const double *temperature, int64_t ncell,
+                              double PHIp, const double *phimax, double dr, double dz,
+                              const double *sig_el, const double *sig_ion, const double *sig_exc,
+                              double dt_transport, const double *draws,
+                              int64_t *n_e_out, int64_t *n_i1_out, unsigned flags);
+
+/* ------------------------------------------------------ resident simulation */
+#define GASATT_FP64        0   /* plain FP64: r, z, u_r, u_theta, u_z (+ id)       */
+#define GASATT_FP32_SPLIT  1   /* int32 cell key + FP32 offsets + FP32 u (+ id)    */
+
+typedef struct gasatt_sim_config {
+  int      n_r, n_z;        /* cells; Er n_r x (n_z+1), Ez (n_r+1) x n_z, Hphi n_r x n_z */
+  double   dr, dz;          /* cell size [m] */
+  double   dt;              /* particle step [s] */
+  int      fdtd_ratio;      /* field sub-cycle: 2*ratio half-updates of dt/2 each per ratio*dt of
+                               particle time; the product uses 1 (electricmagneticfield6.m:134-151 uses 5) */
+  double   PHIp;            /* azimuthal extent of a macro-particle shell [rad] (2*pi: full ring) */
+  double   FN;              /* real electrons per macro-particle */
+  double   gas_density;     /* N2 number density [m^-3] */
+  double   gas_temperature; /* [K] */
+  double   q_e, m_e, c, eps0, mu0, kb, m_ion;  /* constants (SI); q_e > 0 */
+  int      precision;       /* GASATT_FP64 / GASATT_FP32_SPLIT */
+  int64_t  capacity;        /* max electrons */
+  int64_t  ion_capacity;    /* max ions (0: ions are counted, not stored) */
+  uint64_t seed;
+  unsigned flags;           /* quirk flags (0 for the product) */
+  int      sort_period;     /* steps between cell re-sorts (0 = never) */
+  int      secondaries;     /* 1: ionization births enabled */
+  int      table_n;         /* log-energy grid points (2048) */
+  double   table_emin_ev, table_emax_ev;  /* 0.1 eV, 30 keV */
+} gasatt_sim_config;
+
+typedef struct gasatt_diag {
+  int64_t n_alive;          /* electrons alive */
+  int64_t n_total;          /* slots in use (alive + dead not yet compacted) */
+  int64_t n_ionizations;    /* cumulative ionization events (= secondaries born) */
+  int64_t n_elastic, n_excitation, n_null;   /* cumulative collision branches */
+  int64_t n_lost_wall;      /* cumulative electrons absorbed at r = Rp */
+  int64_t n_ions;           /* ions stored (ion_capacity > 0) */
+  double  kinetic_ev;       /* sum of electron kinetic energy [eV] (x FN not applied) */
+  double  field_energy_j;   /* electromagnetic field energy [J] */
+  int64_t steps;            /* steps taken */
+  int32_t status_flags;     /* bit0 NaN seen, bit1 capacity overflow */
+} gasatt_diag;
+
+typedef struct gasatt_sim gasatt_sim;
+
+int gasatt_sim_default_config(gasatt_sim_config *cfg);
+int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg,
+                      const gasatt_tables *tab, gasatt_sim **sim);
+int gasatt_sim_destroy(gasatt_sim *sim);
+/* particle state in SI, axisymmetric frame: r, z [m]; u = gamma*v [m/s] in
+ * (r, theta, z); id: 64-bit identity keying the random stream.
+ * on_device: 1 = pointers are device memory, 0 = host memory. */
+int gasatt_sim_load(gasatt_sim *sim, const double *r, const double *z,
+                    const double *ur, const double *ut, const double *uz,
+                    const uint64_t *id, int64_t n, int on_device);
+int gasatt_sim_read(gasatt_sim *sim, double *r, double *z,
+                    double *ur, double *ut, double *uz, uint64_t *id,
+                    int64_t cap, int64_t *n, int on_device);
+/* fields in the reference layout (column-major): Er n_r x (n_z+1), Ez (n_r+1) x n_z, Hphi n_r x n_z */
+int gasatt_sim_set_fields(gasatt_sim *sim, const double *Er, const double *Ez,
+                          const double *Hphi, int on_device);
+int gasatt_sim_get_fields(gasatt_sim *sim, double *Er, double *Ez, double *Hphi,
+                          int on_device);
+/* current density [A/m^2] deposited by the last particle pass (n_r x n_z each) */
+int gasatt_sim_get_current(gasatt_sim *sim, double *jr, double *jz, int on_device);
+/* advance nsteps steps of push + MCC + deposit + FDTD (captured in a CUDA graph) */
+int gasatt_sim_step(gasatt_sim *sim, int nsteps);
+/* cell re-sort + compaction of dead slots now */
+int gasatt_sim_sort(gasatt_sim *sim);
+int gasatt_sim_diag(gasatt_sim *sim, gasatt_diag *out);
+/* end-to-end entry: copy host particle arrays (x,y,z,vx,vy,vz Cartesian, SI,
+ * n x 3 column-major like the MATLAB host) in, run nsteps, copy them out.
+ * n_io is in/out (births may grow it up to cap rows). */
+int gasatt_sim_run_host(gasatt_sim *sim, double *pos, double *vel,
+                        int64_t *n_io, int64_t cap, int nsteps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GASATT_H */

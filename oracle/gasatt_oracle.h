@@ -1,0 +1,133 @@
+/*
+ * gasatt_oracle.h - CPU FP64 oracle for the PIC-MCC electron step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference's
+ * algorithm (its CUDA kernels and MATLAB functions), used by tests/, by the
+ * smoke check and by bench.py's CPU baseline leg as the checker.  The product
+ * (libgasatt) never links, loads or calls it.
+ *
+ * Every function cites the reference file:line it restates.  The quirk flags
+ * (GASATT_Q_*, include/gasatt.h) select between reproducing a reference
+ * behaviour and its corrected form.
+ */
+#ifndef GASATT_ORACLE_H
+#define GASATT_ORACLE_H
+
+#include <stdint.h>
+#include "../include/gasatt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void orc_set_threads(int n);
+int  orc_get_threads(void);
+
+/* ---- counter-based RNG (Philox4x32-10, Salmon et al. SC'11) ---- */
+void   orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+double orc_u01(uint32_t hi, uint32_t lo);           /* (0,1) from 52 bits */
+uint64_t orc_child_id(uint64_t parent, int64_t step);
+
+/* ---- MATLAB built-ins restated ---- */
+double orc_interp1(const double *x, int sx, const double *y, int sy, int n, double xq);
+
+/* ---- find_CS0.m ---- */
+void orc_find_cs0(const gasatt_tables *t, const double *E_keV, int64_t n,
+                  double *s_el, double *s_ion, double *s_exc, unsigned flags);
+/* electron_collision.m:12-33 : xInterp[ne], yInterp[ne], V_interp[181*ne]; returns ne or <0 */
+int orc_elastic_tables(const gasatt_tables *t, double *xInterp, double *yInterp, double *V_interp);
+
+/* ---- kernels of the reference, one call = one launch ---- */
+void orc_em2(double *x, double *y, double *z, double *vx, double *vy, double *vz,
+             double *r, double *phi, double *vr, int *del, int64_t n,
+             double Rp, double Lp, double PHIp, double dt, unsigned flags);
+void orc_em7(const double *r, const double *z, const double *q, const double *vr,
+             const double *vz, double *jr, double *jz, const int *del, int64_t n,
+             int nr, int nz, double dr, double dz, double FN, double PHIp);
+void orc_em3_1(double *Er, double *Ez, double *H, int nr, int nz,
+               double mu, double dr, double dz, double dt);
+void orc_em3(const double *Er0, const double *Ez0, const double *H0, double *Er, double *Ez,
+             const double *jr, const double *jz, int nr, int nz,
+             double eps, double dr, double dz, double dt, unsigned flags);
+void orc_em4(double *x, double *y, double *z, double *vx, double *vy, double *vz,
+             double *r, double *phi, const double *vr, const double *Er, const double *Ez,
+             const double *H, const double *q, const double *m, double *E, int *del,
+             int64_t n, double Rp, double Lp, double PHIp, int nr, int nz,
+             double mu, double c, double dr, double dz, double dt, unsigned flags);
+/* electron_transport.cu:3-229 with injected draws (n x GASATT_MCC_NDRAW) */
+void orc_electron_transport(double *x, double *y, double *z, double *vx, double *vy, double *vz,
+                            const double *sig_el, const double *sig_ion, const double *sig_exc,
+                            const double *energy, const double *xInterp, const double *yInterp,
+                            const double *V_interp, int ne,
+                            const double *density, const double *temperature, int64_t ncell,
+                            const double *dphi, const double *t_exc, int n_exc,
+                            uint8_t *sec, double *svx, double *svy, double *svz,
+                            double *sample_out, double *ivx, double *ivy, double *ivz,
+                            const int *sum_cell0, int rmax, int cellnumxy,
+                            double dr, double dz, double dt, int64_t n,
+                            const double *draws, unsigned flags);
+
+/* ---- MATLAB drop-ins ---- */
+void orc_free_motion(const double *vx, const double *vy, const double *vz,
+                     const double *x, const double *y, const double *z, int64_t n, double dt,
+                     double *xn, double *yn, double *zn, double *rn, double *phin);
+void orc_particle_density(double dr, double dz, const double *dphi, int rmax,
+                          const double *r, const double *phi, const double *z, int64_t n,
+                          int cellnumxy, const double *sum_cell, const double *VC,
+                          int64_t ncell, double FN, double *density);
+/* species arrays n x 3 column-major; see gasatt_electricmagneticfield6 */
+int orc_electricmagneticfield6(double *e_pos, double *e_vel, int64_t n_e,
+                               double *i1_pos, double *i1_vel, int64_t n_i1,
+                               double *i2_pos, double *i2_vel, int64_t n_i2,
+                               double *Er, double *Ez, double *H, int nr, int nz,
+                               double delta, double dt, double Rp, double Lp,
+                               double PHIp, double FN, int cycle_time, double *kin,
+                               int64_t *n_e_out, int64_t *n_i1_out, int64_t *n_i2_out,
+                               unsigned flags);
+int orc_electron_collision(double *e_pos, double *e_vel, int64_t n_e, int64_t cap_e,
+                           double *i1_pos, double *i1_vel, int64_t n_i1, int64_t cap_i1,
+                           const gasatt_tables *tab, const double *kin,
+                           const double *sum_cell, int rmax, int cellnumxy,
+                           const double *density, const double *temperature, int64_t ncell,
+                           double PHIp, const double *phimax, double dr, double dz,
+                           const double *sig_el, const double *sig_ion, const double *sig_exc,
+                           double dt, const double *draws,
+                           int64_t *n_e_out, int64_t *n_i1_out, unsigned flags);
+
+/* ---- resident step, corrected physics (Cartesian u = gamma v form) ---- */
+typedef struct orc_xs {
+  int G;  double lnEmin, dlnE;        /* log grid */
+  double *sig_el, *sig_ion, *sig_exc; /* [G], m^2 */
+  double *cdf;                        /* [G*181] normalised elastic CDF */
+  double nu_max;                      /* s^-1, FP64 bound */
+  double exc_k[16], exc_A[16], exc_om[16], exc_nu[16], exc_ga[16]; int n_exc;
+} orc_xs;
+orc_xs *orc_xs_create(const gasatt_tables *t, int G, double emin_ev, double emax_ev,
+                      double n_gas, double c, double me, double qe);
+void orc_xs_free(orc_xs *xs);
+double orc_xs_nu_max(const orc_xs *xs);
+/* 0 sig_el, 1 sig_ion, 2 sig_exc (length G), 3 cdf (G x 181) */
+const double *orc_xs_array(const orc_xs *xs, int which);
+
+typedef struct orc_counters {
+  int64_t ion, ela, exc, nul, lost, cap_overflow;
+} orc_counters;
+
+/* one particle pass of step s: gather + kick + half drift + MCC + half drift +
+ * deposit.  Arrays x..alive have capacity cap; *n grows with births.
+ * jr/jz receive the current density [A/m^2] (overwritten). */
+int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step,
+                 double *x, double *y, double *z, double *ux, double *uy, double *uz,
+                 uint64_t *id, uint8_t *alive, int64_t *n, int64_t cap,
+                 const double *Er, const double *Ez, const double *H,
+                 double *jr, double *jz, int do_kick, int do_mcc, orc_counters *cnt);
+/* field sub-cycle: H(-dt/4), [H(dt/2), E(dt/2)] x 2 ratio, H(dt/4), dt = cfg->dt/ratio */
+void orc_sim_fdtd(const gasatt_sim_config *cfg, double *Er, double *Ez, double *H,
+                  const double *jr, const double *jz);
+double orc_field_energy(const gasatt_sim_config *cfg, const double *Er, const double *Ez,
+                        const double *H);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,125 @@
+"""Resident simulation (the hot path) against the CPU oracle, plus the
+FP32-split-vs-FP64 accuracy gates and run-to-run bit-exactness."""
+import numpy as np
+import pytest
+
+import pyoracle as O
+from _cases import close, grid_fields
+from gasatt import _lib
+from gasatt.sim import Sim, births, config
+
+pytestmark = pytest.mark.gpu
+
+NR, NZ, D = 32, 64, 5e-6
+
+
+def small_cfg(precision, torr=300.0, sort_period=0, seed=7, cap=40000):
+    return config(NR, NZ, D, 1e-14, torr, precision=precision, capacity=cap, seed=seed,
+                  sort_period=sort_period)
+
+
+def start(precision, n_photo=2000, sort_period=0, fields=True, torr=300.0):
+    cfg = small_cfg(precision, torr=torr, sort_period=sort_period)
+    r, z, ur, ut, uz, ids = births(n_photo, 8.0, NZ * D, seed=3, sigma_r=30e-6, Rp=NR * D)
+    sim = Sim(cfg)
+    sim.load(r, z, ur, ut, uz, ids)
+    Er = Ez = H = None
+    if fields:
+        Er, Ez, H = grid_fields(NR, NZ, np.random.default_rng(8), E0=3e6, H0=2e3)
+        Er[:, 0] = 0; Er[:, -1] = 0; Ez[-1, :] = 0
+        sim.set_fields(Er, Ez, H)
+    return cfg, sim, (r, z, ur, ut, uz, ids), (Er, Ez, H)
+
+
+def oracle_run(cfg, tables, parts, flds, steps):
+    orc = O.Sim(cfg, tables, cap=cfg.capacity)
+    orc.load(*parts)
+    if flds[0] is not None:
+        orc.Er[:], orc.Ez[:], orc.H[:] = flds
+    orc.prologue()
+    for _ in range(steps):
+        orc.step()
+    return orc
+
+
+def by_id(state_ids, *arrays):
+    order = np.argsort(state_ids)
+    return [a[order] for a in arrays]
+
+
+@pytest.mark.parametrize("steps", [1, 4])
+def test_fp64_matches_oracle(tables, steps):
+    cfg, sim, parts, flds = start(_lib.FP64)
+    sim.step(steps)
+    got = sim.read()
+    orc = oracle_run(cfg, tables, parts, flds, steps)
+    r, z, ur, ut, uz, ids, alive = orc.state_rz()
+    # same population: alive ids (births included) identical
+    g_alive = got["r"] >= 0
+    assert set(got["id"][g_alive].tolist()) == set(ids[alive.astype(bool)].tolist())
+    assert len(got["id"]) == len(ids)
+    a = alive.astype(bool)
+    want = by_id(ids[a], r[a], z[a], ur[a], ut[a], uz[a])
+    have = by_id(got["id"][g_alive], got["r"][g_alive], got["z"][g_alive], got["ur"][g_alive],
+                 got["ut"][g_alive], got["uz"][g_alive])
+    for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
+        close(h, w, 1e-10, k)
+    d = sim.diag()
+    ion, ela, exc, nul, lost, ovf = orc.counters
+    assert (d["n_ionizations"], d["n_elastic"], d["n_excitation"], d["n_null"]) == (ion, ela, exc, nul)
+    assert d["n_lost_wall"] == lost
+    if steps > 1:
+        assert ion > 10 and ela > 10 and exc > 10
+    Er, Ez, H = sim.fields()
+    close(Er, orc.Er, 1e-10, "Er"); close(Ez, orc.Ez, 1e-10, "Ez"); close(H, orc.H, 1e-10, "H")
+    jr, jz = sim.current()
+    close(jr, orc.jr, 1e-10, "jr"); close(jz, orc.jz, 1e-10, "jz")
+
+
+def test_fp64_field_energy_diag_matches_oracle(tables):
+    cfg, sim, parts, flds = start(_lib.FP64)
+    sim.step(2)
+    orc = oracle_run(cfg, tables, parts, flds, 2)
+    close(sim.diag()["field_energy_j"], orc.field_energy(), 1e-10, "field energy")
+
+
+@pytest.mark.parametrize("precision", [_lib.FP64, _lib.FP32_SPLIT])
+def test_bit_exact_run_to_run_and_sort_invariant(precision):
+    outs = []
+    for sp in (0, 0, 1):
+        cfg, sim, _, _ = start(precision, sort_period=sp)
+        sim.step(6)
+        jr, jz = sim.current()
+        Er, Ez, H = sim.fields()
+        d = sim.diag()
+        outs.append((jr, jz, Er, Ez, H, d["n_ionizations"], d["n_alive"]))
+        sim.close()
+    for o in outs[1:]:
+        for a, b in zip(outs[0], o):
+            assert np.array_equal(a, b)
+
+
+def test_fp32_split_tracks_fp64():
+    res = {}
+    for prec in (_lib.FP64, _lib.FP32_SPLIT):
+        cfg, sim, parts, _ = start(prec, n_photo=4000, sort_period=5, torr=100.0)
+        sim.step(40)
+        res[prec] = (sim.diag(), sim.fields(), sim.read())
+    d64, f64, p64 = res[_lib.FP64]
+    d32, f32, p32 = res[_lib.FP32_SPLIT]
+    assert d64["n_ionizations"] > 200
+    assert abs(d32["n_ionizations"] - d64["n_ionizations"]) <= 0.005 * d64["n_ionizations"] + 2
+    assert abs(d32["kinetic_ev"] / d64["kinetic_ev"] - 1) < 1e-4
+    for a, b in zip(f32, f64):
+        close(a, b, 1e-4, "field FP32 vs FP64")
+
+
+def test_capacity_overflow_is_reported():
+    cfg = small_cfg(_lib.FP32_SPLIT, cap=4100)
+    r, z, ur, ut, uz, ids = births(2000, 8.0, NZ * D, seed=3, sigma_r=30e-6, Rp=NR * D)
+    sim = Sim(cfg)
+    sim.load(r, z, ur, ut, uz, ids)
+    sim.step(20)
+    d = sim.diag()
+    assert d["n_total"] <= 4100
+    assert d["status_flags"] & 2
