@@ -1,0 +1,439 @@
+"""Benchmark: particle-steps/s of the PIC-MCC electron step (push + MCC +
+deposit, with the FDTD field update inside every timed step) on the 2,000,000
+electron workload (1,000,000 photoionizations by 8 keV photons in N2 at 1 Torr,
+256 x 1024 cells of 5 um, dt = 1e-14 s, secondaries on, seed 1).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1); each rank runs an independent
+replica of the workload (no data-path collective), timing is device-side
+(CUDA events), max over ranks.  Rank 0 prints one JSON line.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gas-atenuator_b200"))
+
+METRIC = "particle-steps/s (push+MCC+deposit), FP32 vs FP64 GPU at ≤0.5% yield error"
+UNIT = "particle-steps/s"
+WORKLOAD = dict(n_r=256, n_z=1024, delta=5e-6, dt=1e-14, torr=1.0, photo=1_000_000, e_keV=8.0,
+                seed=1)
+WORKLOAD_NAME = ("2,000,000 e- from 1,000,000 photoionizations at 8 keV (photoelectron 7.59 keV, "
+                 "dipole about x; Auger 360 eV isotropic), N2 1 Torr 300 K, 256x1024 cells at 5 um, "
+                 "dt 1e-14 s, Rayleigh sigma 50 um, secondaries on, seed 1")
+L2_FLUSH_BYTES = 256 << 20
+# algorithmic bytes: per alive particle-step, FP32 split: 24 B state read + 24 B written
+# + 8 B id read; FP64: 40 + 40 + 8.  Grid term per step: field gather (3 fields) + current.
+BYTES_PER_PARTICLE = {"fp32_split": 56, "fp64": 88}
+GRID_BYTES_PER_CELL = {"fp32_split": 3 * 4 + 2 * 8, "fp64": 3 * 8 + 2 * 8}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1])); mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ ours (GPU)
+def make_sim(precision, device, rank, torch):
+    from gasatt import _lib
+    from gasatt.sim import Sim, births, config
+    w = WORKLOAD
+    prec = _lib.FP32_SPLIT if precision == "fp32_split" else _lib.FP64
+    cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=prec,
+                 capacity=4_000_000, seed=w["seed"] + 1000 * rank, sort_period=20)
+    parts = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=w["seed"] + 1000 * rank,
+                   Rp=w["n_r"] * w["delta"])
+    sim = Sim(cfg, device=device)
+    sim.bind_stream()
+    sim.load(*parts)
+    return sim, parts
+
+
+def counts(sim):
+    from gasatt._lib import lib
+    a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    lib.gasatt_sim_counts(sim.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    return a.value, b.value, c.value
+
+
+def timed_run(sim, steps, warmup, torch, flush, dist_barrier):
+    from gasatt._lib import lib
+    lib.gasatt_sim_enable_timing(sim.h, 1)
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        sim.step(1)
+    torch.cuda.synchronize()
+    d0 = sim.diag()
+    l0 = sim.ctx.launches
+    fd = ctypes.c_float(); ps = ctypes.c_float()
+    step_ms, pass_ms, fdtd_ms = [], [], []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    dist_barrier()
+    torch.cuda.synchronize()
+    for _ in range(steps):
+        flush()                                      # L2 cold before every timed step
+        e0.record(stream)
+        sim.step(1)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        lib.gasatt_sim_last_timing(sim.h, ctypes.byref(fd), ctypes.byref(ps))
+        fdtd_ms.append(fd.value); pass_ms.append(ps.value)
+    torch.cuda.synchronize()
+    dist_barrier()
+    launches = sim.ctx.launches - l0
+    d1 = sim.diag()
+    lib.gasatt_sim_enable_timing(sim.h, 0)
+    return dict(step_ms=step_ms, pass_ms=pass_ms, fdtd_ms=fdtd_ms, d0=d0, d1=d1,
+                launches=launches)
+
+
+def e2e_run(precision, device, rank, torch, steps_per_call=200):
+    """Through the public C ABI with pinned HOST buffers: H2D of the electrons,
+    steps_per_call steps, D2H of the result, all inside the timed region."""
+    from gasatt._lib import lib
+    sim, parts = make_sim(precision, device, rank, torch)
+    r, z, ur, ut, uz, ids = parts
+    n = len(r)
+    cap = int(n * 1.1)
+    c = 299792458.0
+    g = np.sqrt(1 + (ur * ur + ut * ut + uz * uz) / (c * c))
+    pos = torch.zeros(3 * cap, dtype=torch.float64).pin_memory()
+    vel = torch.zeros(3 * cap, dtype=torch.float64).pin_memory()
+    P, V = pos.numpy(), vel.numpy()
+
+    def fill():
+        P[:n] = r; P[cap:cap + n] = 0.0; P[2 * cap:2 * cap + n] = z
+        V[:n] = ur / g; V[cap:cap + n] = ut / g; V[2 * cap:2 * cap + n] = uz / g
+
+    def call(k):
+        nio = ctypes.c_int64(n)
+        rc = lib.gasatt_sim_run_host(sim.h, ctypes.c_void_p(pos.data_ptr()),
+                                     ctypes.c_void_p(vel.data_ptr()), ctypes.byref(nio), cap, k)
+        assert rc == 0, lib.gasatt_last_error(sim.ctx.handle)
+        return nio.value
+
+    fill()
+    call(5)                                          # warm-up call
+    fill()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    nout = call(steps_per_call)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    sim.close()
+    return dict(ms=ms, n_in=n, n_out=nout, steps=steps_per_call,
+                h2d=n * 6 * 8, d2h=nout * 6 * 8)
+
+
+def cpu_baseline(target_s=12.0):
+    """CPU oracle (plain C FP64 restatement, OpenMP on all host cores) on the
+    same workload: full population, a bounded number of steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    from gasatt import _lib
+    from gasatt.sim import births, config
+    from gasatt.tables import N2Tables
+    w = WORKLOAD
+    threads = os.cpu_count() or 1
+    O.lib.orc_set_threads(threads)
+    cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=_lib.FP64,
+                 capacity=2_200_000, seed=w["seed"], sort_period=0)
+    parts = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=w["seed"],
+                   Rp=w["n_r"] * w["delta"])
+    orc = O.Sim(cfg, N2Tables(), cap=cfg.capacity)
+    orc.load(*parts)
+    orc.prologue()
+    t0 = time.perf_counter()
+    orc.step()
+    one = time.perf_counter() - t0
+    steps = max(1, min(200, int(target_s / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        orc.step()
+    dt = time.perf_counter() - t0
+    n_alive = int(orc.alive[:orc.n].sum())
+    return {"value": n_alive * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"full 2,000,000-electron population, {steps} steps after 1 warm-up step "
+                      f"(plain C FP64 oracle, OpenMP {threads} threads, FDTD included)"}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    flush_buf = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def flush():
+        flush_buf.fill_(1)
+
+    results = {}
+    clocks = None
+    for prec in ("fp32_split", "fp64"):
+        sim, _ = make_sim(prec, local, rank, torch)
+        if prec == "fp32_split":
+            with ClockSampler(local) as cs:
+                res = timed_run(sim, args.steps, args.warmup, torch, flush, barrier)
+            clocks = cs.summary()
+        else:
+            res = timed_run(sim, args.steps, args.warmup, torch, flush, barrier)
+        res["fields"] = sim.fields()
+        results[prec] = res
+        sim.close()
+    e2e = e2e_run("fp32_split", local, rank, torch, steps_per_call=200)
+
+    pk, pk_src = peaks()
+    hbm = float(pk.get("hbm_gbs", 6650.0))
+    out = {}
+    for prec, res in results.items():
+        t_ms = sum(res["step_ms"])
+        t_ms_max = max_over_ranks(t_ms)
+        alive = 0.5 * (res["d0"]["n_alive"] + res["d1"]["n_alive"])
+        tot = sum_over_ranks(alive * args.steps)
+        pass_avg = sum(res["pass_ms"]) / len(res["pass_ms"])
+        fdtd_avg = sum(res["fdtd_ms"]) / len(res["fdtd_ms"])
+        ncell = WORKLOAD["n_r"] * WORKLOAD["n_z"]
+        bytes_launch = alive * BYTES_PER_PARTICLE[prec] + ncell * GRID_BYTES_PER_CELL[prec]
+        out[prec] = dict(value=tot / (t_ms_max / 1e3), ms_per_step=t_ms_max / args.steps,
+                         pass_ms=pass_avg, fdtd_ms=fdtd_avg, alive=alive,
+                         achieved_gbs=bytes_launch / (pass_avg / 1e3) / 1e9,
+                         ionizations=res["d1"]["n_ionizations"] - res["d0"]["n_ionizations"],
+                         ion_total=res["d1"]["n_ionizations"], launches=res["launches"],
+                         bytes_launch=bytes_launch,
+                         cell_updates_per_s=ncell * (4 + 1) / (fdtd_avg / 1e3))
+    f32, f64 = out["fp32_split"], out["fp64"]
+    yerr = abs(f32["ion_total"] - f64["ion_total"]) / max(f64["ion_total"], 1)
+    ferr = max(float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+               for a, b in zip(results["fp32_split"]["fields"], results["fp64"]["fields"]))
+    e2e_ms = max_over_ranks(e2e["ms"])
+    e2e_val = sum_over_ranks(e2e["n_in"] * e2e["steps"]) / (e2e_ms / 1e3)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "pass32_c2_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": f32["value"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": f32["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded photoionization births; N2 cross-sections from the reference CSVs)",
+        "config": {"workload": WORKLOAD_NAME, "precision": "fp32_split (int32 cell key + f32 offsets "
+                   "+ f32 gamma*v; f64 collision test, energy sharing, threshold subtraction)",
+                   "global_electrons": int(sum_over_ranks(f32["alive"])),
+                   "per_rank": "independent replica", "parallelism": f"replicas x{world}",
+                   "l2": "flushed before every timed step (256 MiB write, outside the events)",
+                   "sort_period": 20, "fdtd_ratio": 1, "timed": "whole step: FDTD + particle pass (+ periodic sort)"},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"] / e2e["steps"],
+                "d2h_bytes_per_step": e2e["d2h"] / e2e["steps"],
+                "call": f"gasatt_sim_run_host, {e2e['steps']} steps per call, pinned host x,y,z,vx,vy,vz in/out"},
+        "gpu_launches": int(f32["launches"]),
+        "roofline": {"bound": "hbm", "achieved": f32["achieved_gbs"], "peak": hbm, "unit": "GB/s",
+                     "frac": f32["achieved_gbs"] / hbm, "traffic": traffic,
+                     "kernel": "k_pass32 (fused push+MCC+deposit)",
+                     "peak_source": f"{pk_src} hbm_gbs",
+                     "bytes_per_launch": f32["bytes_launch"]},
+        "fp64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"], "pass_ms": f64["pass_ms"],
+                 "achieved_gbs": f64["achieved_gbs"], "frac": f64["achieved_gbs"] / hbm},
+        "fp32_over_fp64": f32["value"] / f64["value"],
+        "accuracy": {"yield_rel_err_fp32_vs_fp64": yerr, "field_rel_err_fp32_vs_fp64": ferr,
+                     "ionizations_fp32": f32["ion_total"], "ionizations_fp64": f64["ion_total"]},
+        "fdtd": {"cell_updates_per_s": f32["cell_updates_per_s"], "ms": f32["fdtd_ms"]},
+        "pass_ms": f32["pass_ms"],
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------ reference arm (CPU)
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    from gasatt import _lib
+    from gasatt.sim import births, config
+    from gasatt.tables import N2Tables
+    w = WORKLOAD
+    threads = os.cpu_count() or 1
+    O.lib.orc_set_threads(threads)
+    sample_photo = w["photo"] // 4                     # 500,000 electrons per step
+    cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=_lib.FP64,
+                 capacity=2 * sample_photo + 100_000, seed=w["seed"], sort_period=0)
+    parts = births(sample_photo, w["e_keV"], w["n_z"] * w["delta"], seed=w["seed"],
+                   Rp=w["n_r"] * w["delta"])
+    orc = O.Sim(cfg, N2Tables(), cap=cfg.capacity)
+    orc.load(*parts)
+    orc.prologue()
+    for _ in range(args.warmup):
+        orc.step()
+    alive0 = int(orc.alive[:orc.n].sum())
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.step()
+    dt = time.perf_counter() - t0
+    alive1 = int(orc.alive[:orc.n].sum())
+    value = 0.5 * (alive0 + alive1) * args.steps / dt
+    sample = (f"500,000 of the 2,000,000 electrons (the first 250,000 photoionizations) on the full "
+              f"256x1024 grid, FDTD every step; plain C FP64 oracle of the same step, OpenMP "
+              f"{threads} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD_NAME, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's CPU path is MATLAB (not installed); its algorithm is timed as "
+                    "the plain C restatement"}
+    print(json.dumps(line), flush=True)
+
+
+def run_profile(args):
+    """The step loop alone (warm-up then timed steps, no flush/e2e/baseline),
+    for kernel profilers."""
+    import torch
+    torch.cuda.set_device(0)
+    sim, _ = make_sim(args.precision, 0, 0, torch)
+    sim.step(args.warmup + args.steps)
+    torch.cuda.synchronize()
+    d = sim.diag()
+    print(json.dumps({"mode": "profile", "precision": args.precision, "steps": args.steps,
+                      "warmup": args.warmup, "alive": d["n_alive"],
+                      "ionizations": d["n_ionizations"], "launches": sim.ctx.launches}))
+    sim.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="bench", choices=["bench", "profile"],
+                    help="profile: only the step loop of one precision (for ncu)")
+    ap.add_argument("--precision", default="fp32_split", choices=["fp32_split", "fp64"])
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.mode == "profile":
+        run_profile(args)
+    elif args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -269,7 +269,8 @@ __device__ __forceinline__ void count_event(SimCounters *cnt, int ev) {
   else if (ev == 4) atomicAdd(&cnt->nul, 1ull);
 }
 
-// mode 0: full pass; mode 1: half drift + deposit only (start of a run)
+// mode 0: full pass; mode 1: half drift + deposit only (start of a run);
+// mode 2: kick + half drift only, ending at integer time (end of a run)
 __global__ void __launch_bounds__(kBlock) k_pass64(SimParams P, State64 S, Fields<double> F,
                                                    SimCounters *cnt, int mode) {
   const long long n0 = (long long)cnt->n_total;
@@ -289,13 +290,13 @@ __global__ void __launch_bounds__(kBlock) k_pass64(SimParams P, State64 S, Field
     if (act) {
       z = S.z[p]; ur = S.ur[p]; ut = S.ut[p]; uz = S.uz[p];
       bool alive = true;
-      if (mode == 0) {
+      if (mode != 1) {
         double E_r, E_z, Hp;
         gather3<double>(F.Er, F.Ez, F.H, P.nr, P.nz, P.dr, P.dz, r, z, E_r, E_z, Hp);
         const double B = P.mu0 * Hp;
         boris(ur, ut, uz, E_r, 0.0, E_z, 0.0, B, 0.0, P.qm_dt2, P.c);
         halfdrift64(r, z, ur, ut, uz, alive, P);
-        if (alive) {
+        if (alive && mode == 0) {
           Birth b;
           const int ev = mcc_event(P, S.id[p], step, ur, ut, uz, b);
           if (ev) count_event(cnt, ev);
@@ -322,10 +323,10 @@ __global__ void __launch_bounds__(kBlock) k_pass64(SimParams P, State64 S, Field
           }
         }
       }
-      if (alive) halfdrift64(r, z, ur, ut, uz, alive, P);
+      if (alive && mode != 2) halfdrift64(r, z, ur, ut, uz, alive, P);
       if (!alive) { lost++; r = -1.0; }
       S.r[p] = r; S.z[p] = z; S.ur[p] = ur; S.ut[p] = ut; S.uz[p] = uz;
-      act = alive;
+      act = alive && mode != 2;
     }
     int64_t a[4] = {0, 0, 0, 0};
     long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
@@ -430,7 +431,7 @@ __global__ void __launch_bounds__(kBlock) k_pass32(SimParams P, State32 S, Field
       ir = (int)(key & 0xFFFFu); iz = (int)(key >> 16);
       fr = S.fr[p]; fz = S.fz[p]; ur = S.ur[p]; ut = S.ut[p]; uz = S.uz[p];
       bool alive = true;
-      if (mode == 0) {
+      if (mode != 1) {
         int ar, az;
         float wr, wz;
         half_shift(ir, fr, ar, wr);
@@ -448,7 +449,7 @@ __global__ void __launch_bounds__(kBlock) k_pass32(SimParams P, State32 S, Field
         uz = umz + upr * s + P.aE * Ez;
         ut = umt;
         halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P);
-        if (alive) {
+        if (alive && mode == 0) {
           double dux = (double)ur * P.c, duy = (double)ut * P.c, duz = (double)uz * P.c;
           Birth b;
           const int ev = mcc_event(P, S.id[p], step, dux, duy, duz, b);
@@ -482,11 +483,11 @@ __global__ void __launch_bounds__(kBlock) k_pass32(SimParams P, State32 S, Field
           }
         }
       }
-      if (alive) halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P);
+      if (alive && mode != 2) halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P);
       if (!alive) lost++;
       S.key[p] = alive ? (((uint32_t)iz << 16) | (uint32_t)ir) : kDead;
       S.fr[p] = fr; S.fz[p] = fz; S.ur[p] = ur; S.ut[p] = ut; S.uz[p] = uz;
-      act = alive;
+      act = alive && mode != 2;
     }
     int64_t a[4] = {0, 0, 0, 0};
     long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
@@ -746,6 +747,8 @@ struct gasatt_sim {
   cudaGraphExec_t g_sort[2] = {nullptr, nullptr};
   double scale = 1.0;
   unsigned pass_grid = 0;
+  bool timing = false;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};   // before FDTD, before pass, after pass
 };
 
 namespace {
@@ -867,8 +870,11 @@ int build_graphs(gasatt_sim *s) {
     cudaGraph_t g;
     s->cur = b;
     GASATT_CUDA(s->ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    if (s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[0], cs, cudaEventRecordExternal));
     int rc = launch_fdtd(s, cs);
+    if (!rc && s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[1], cs, cudaEventRecordExternal));
     if (!rc) rc = launch_pass(s, cs, 0);
+    if (!rc && s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[2], cs, cudaEventRecordExternal));
     cudaError_t e = cudaStreamEndCapture(cs, &g);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_fail(s->ctx, e, "capture step");
@@ -1018,6 +1024,8 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   cudaMemset(s->H, 0, (size_t)nr * nz * esz);
   cudaMemset(s->Jr, 0, (size_t)ncell * 8);
   cudaMemset(s->Jz, 0, (size_t)ncell * 8);
+  for (int i = 0; i < 3; ++i)
+    if (cudaEventCreate(&s->ev[i]) != cudaSuccess) return cleanup(fail(ctx, GASATT_E_CUDA, "event"));
   rc = build_graphs(s);
   if (rc) return cleanup(rc);
   if (cudaDeviceSynchronize() != cudaSuccess) return cleanup(fail(ctx, GASATT_E_CUDA, "sim init"));
@@ -1030,6 +1038,8 @@ int gasatt_sim_destroy(gasatt_sim *s) {
   cudaSetDevice(s->ctx->device);
   cudaDeviceSynchronize();
   drop_graphs(s);
+  for (int i = 0; i < 3; ++i)
+    if (s->ev[i]) cudaEventDestroy(s->ev[i]);
   for (void *p : s->allocs) cudaFree(p);
   if (s->h_cnt) cudaFreeHost(s->h_cnt);
   delete s;
@@ -1280,11 +1290,149 @@ int gasatt_sim_diag(gasatt_sim *s, gasatt_diag *d) {
   return GASATT_OK;
 }
 
+int gasatt_sim_counts(gasatt_sim *s, int64_t *n_slots, int64_t *n_ion, int64_t *n_lost) {
+  if (!s) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  GASATT_CUDA(ctx, cudaMemcpyAsync(s->h_cnt, s->cnt, sizeof(SimCounters), cudaMemcpyDeviceToHost, ctx->stream));
+  GASATT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const SimCounters &h = *s->h_cnt;
+  const unsigned long long nt = h.n_total + h.n_births;
+  if (n_slots) *n_slots = (int64_t)(nt < h.cap ? nt : h.cap);
+  if (n_ion) *n_ion = (int64_t)h.ion;
+  if (n_lost) *n_lost = (int64_t)h.lost;
+  return GASATT_OK;
+}
+
+int gasatt_sim_enable_timing(gasatt_sim *s, int enable) {
+  if (!s) return GASATT_E_ARG;
+  if ((bool)enable == s->timing) return GASATT_OK;
+  GASATT_CUDA(s->ctx, cudaSetDevice(s->ctx->device));
+  GASATT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  drop_graphs(s);
+  s->timing = enable != 0;
+  return build_graphs(s);
+}
+
+int gasatt_sim_last_timing(gasatt_sim *s, float *fdtd_ms, float *pass_ms) {
+  if (!s) return GASATT_E_ARG;
+  if (!s->timing) return fail(s->ctx, GASATT_E_STATE, "timing not enabled");
+  GASATT_CUDA(s->ctx, cudaEventSynchronize(s->ev[2]));
+  float a = 0, b = 0;
+  GASATT_CUDA(s->ctx, cudaEventElapsedTime(&a, s->ev[0], s->ev[1]));
+  GASATT_CUDA(s->ctx, cudaEventElapsedTime(&b, s->ev[1], s->ev[2]));
+  if (fdtd_ms) *fdtd_ms = a;
+  if (pass_ms) *pass_ms = b;
+  return GASATT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Cartesian (x, y, z, v) columns -> axisymmetric state (r, z, u = gamma v local), id = slot
+__global__ void k_cart_in(const double *pos, const double *vel, int64_t ld, int64_t n, double c,
+                          double *r, double *z, double *ur, double *ut, double *uz, uint64_t *id,
+                          uint64_t id_base) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const double x = pos[p], y = pos[ld + p];
+    const double vx = vel[p], vy = vel[ld + p], vz = vel[2 * ld + p];
+    const double rr = sqrt(x * x + y * y);
+    const double cp = rr > 0 ? x / rr : 1.0, sp = rr > 0 ? y / rr : 0.0;
+    const double g = 1 / sqrt(1 - (vx * vx + vy * vy + vz * vz) / (c * c));
+    r[p] = rr; z[p] = pos[2 * ld + p];
+    ur[p] = g * (vx * cp + vy * sp); ut[p] = g * (-vx * sp + vy * cp); uz[p] = g * vz;
+    id[p] = id_base + (uint64_t)p;
+  }
+}
+
+// axisymmetric state -> Cartesian columns at azimuth 0, velocity v = u / gamma
+__global__ void k_cart_out(const double *r, const double *z, const double *ur, const double *ut,
+                           const double *uz, int64_t n, double c, double *pos, double *vel,
+                           int64_t ld) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const double g = sqrt(1 + (ur[p] * ur[p] + ut[p] * ut[p] + uz[p] * uz[p]) / (c * c));
+    pos[p] = r[p]; pos[ld + p] = 0.0; pos[2 * ld + p] = z[p];
+    vel[p] = ur[p] / g; vel[ld + p] = ut[p] / g; vel[2 * ld + p] = uz[p] / g;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
 int gasatt_sim_run_host(gasatt_sim *s, double *pos, double *vel, int64_t *n_io, int64_t cap,
                         int nsteps) {
-  (void)pos; (void)vel; (void)n_io; (void)cap; (void)nsteps;
-  if (!s) return GASATT_E_ARG;
-  return fail(s->ctx, GASATT_E_STATE, "gasatt_sim_run_host: not available yet");
+  if (!s || !n_io || nsteps < 1) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  const int64_t n = *n_io;
+  if (n < 0 || n > cap || n > s->cfg.capacity) return fail(ctx, GASATT_E_ARG, "run_host: bad count");
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  // device staging: 6 columns in, reused for the way out; plus state scratch
+  void *buf;
+  const int64_t m = s->cfg.capacity;
+  int rc = scratch(ctx, (size_t)m * 8 * 12, &buf);
+  if (rc) return rc;
+  double *dpos = (double *)buf, *dvel = dpos + 3 * m;
+  double *sr = dvel + 3 * m, *sz = sr + m, *sur = sz + m, *sut = sur + m, *suz = sut + m;
+  uint64_t *sid = (uint64_t *)(suz + m);
+  for (int d = 0; d < 3; ++d) {
+    GASATT_CUDA(ctx, cudaMemcpyAsync(dpos + d * m, pos + d * cap, (size_t)n * 8, cudaMemcpyHostToDevice, st));
+    GASATT_CUDA(ctx, cudaMemcpyAsync(dvel + d * m, vel + d * cap, (size_t)n * 8, cudaMemcpyHostToDevice, st));
+  }
+  // the step counter keeps running across calls, so (id = slot, step) never repeats
+  GASATT_CUDA(ctx, cudaMemcpyAsync(s->h_cnt, s->cnt, sizeof(SimCounters), cudaMemcpyDeviceToHost, st));
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  if (n > 0) {
+    k_cart_in<<<grid_for(n, kBlock), kBlock, 0, st>>>(dpos, dvel, m, n, s->cfg.c, sr, sz, sur, sut, suz, sid, 0);
+    GASATT_LAUNCHED(ctx);
+    if (s->form == 0)
+      k_load64<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->s64[s->cur], sr, sz, sur, sut, suz, sid, n);
+    else
+      k_load32<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->s32[s->cur], sr, sz, sur, sut, suz, sid, n,
+                                                       s->cfg.n_r, s->cfg.n_z, s->cfg.dr, s->cfg.dz, s->cfg.c);
+    GASATT_LAUNCHED(ctx);
+  }
+  SimCounters h = *s->h_cnt;
+  h.n_total = (unsigned long long)n;
+  h.n_births = 0;
+  GASATT_CUDA(ctx, cudaMemcpyAsync(s->cnt, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+  s->primed = false;
+  s->since_sort = s->cfg.sort_period;       // sort the fresh population first
+  SIM_TRY(gasatt_sim_step(s, nsteps - 1));
+  // last step: fields, then a push that ends at integer time
+  SIM_TRY(launch_fdtd(s, st));
+  SIM_TRY(launch_pass(s, st, 2));
+  SIM_TRY(gasatt_sim_sort(s));               // compacts away the dead
+  s->host_step++;
+  s->primed = false;
+  GASATT_CUDA(ctx, cudaMemcpyAsync(s->h_cnt, s->cnt, sizeof(SimCounters), cudaMemcpyDeviceToHost, st));
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  const int64_t nout = (int64_t)s->h_cnt->n_total;
+  const int64_t nw = nout < cap ? nout : cap;
+  if (nw > 0) {
+    if (s->form == 0)
+      k_read64<<<grid_for(nw, kBlock), kBlock, 0, st>>>(s->s64[s->cur], sr, sz, sur, sut, suz, sid, nw);
+    else
+      k_read32<<<grid_for(nw, kBlock), kBlock, 0, st>>>(s->s32[s->cur], sr, sz, sur, sut, suz, sid, nw,
+                                                        s->cfg.dr, s->cfg.dz, s->cfg.c);
+    GASATT_LAUNCHED(ctx);
+    k_cart_out<<<grid_for(nw, kBlock), kBlock, 0, st>>>(sr, sz, sur, sut, suz, nw, s->cfg.c, dpos, dvel, m);
+    GASATT_LAUNCHED(ctx);
+    for (int d = 0; d < 3; ++d) {
+      GASATT_CUDA(ctx, cudaMemcpyAsync(pos + d * cap, dpos + d * m, (size_t)nw * 8, cudaMemcpyDeviceToHost, st));
+      GASATT_CUDA(ctx, cudaMemcpyAsync(vel + d * cap, dvel + d * m, (size_t)nw * 8, cudaMemcpyDeviceToHost, st));
+    }
+  }
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  *n_io = nw;
+  if (nout > cap) return fail(ctx, GASATT_E_CAPACITY, "run_host: more electrons than cap rows");
+  return GASATT_OK;
 }
 
 }  // extern "C"

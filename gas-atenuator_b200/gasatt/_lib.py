@@ -97,6 +97,11 @@ _SIGS = {
     "gasatt_sim_sort": (c_i, [c_p]),
     "gasatt_sim_diag": (c_i, [c_p, ctypes.POINTER(Diag)]),
     "gasatt_sim_run_host": (c_i, [c_p, c_p, c_p, ctypes.POINTER(c_i64), c_i64, c_i]),
+    "gasatt_sim_counts": (c_i, [c_p, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64),
+                                ctypes.POINTER(c_i64)]),
+    "gasatt_sim_enable_timing": (c_i, [c_p, c_i]),
+    "gasatt_sim_last_timing": (c_i, [c_p, ctypes.POINTER(ctypes.c_float),
+                                     ctypes.POINTER(ctypes.c_float)]),
 }
 
 # every entry point declared in include/gasatt.h

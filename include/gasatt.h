@@ -265,11 +265,27 @@ int gasatt_sim_step(gasatt_sim *sim, int nsteps);
 /* cell re-sort + compaction of dead slots now */
 int gasatt_sim_sort(gasatt_sim *sim);
 int gasatt_sim_diag(gasatt_sim *sim, gasatt_diag *out);
-/* end-to-end entry: copy host particle arrays (x,y,z,vx,vy,vz Cartesian, SI,
- * n x 3 column-major like the MATLAB host) in, run nsteps, copy them out.
- * n_io is in/out (births may grow it up to cap rows). */
+/* End-to-end entry with HOST buffers (the call a MATLAB host makes):
+ * pos/vel are n x 3 column-major Cartesian arrays in SI (leading dimension
+ * cap) holding electrons at time t and their velocities v (not gamma v).
+ * They are copied to the device, advanced nsteps particle steps in the
+ * resident fields (each interior step with the null-collision MCC and
+ * secondary birth; the last push ends at integer time without a collision
+ * test), compacted, and copied back: positions in the axisymmetric frame at
+ * azimuth 0 (x = r, y = 0), velocities in the matching local components.
+ * *n_io is in/out; births may grow it up to cap rows (GASATT_E_CAPACITY if
+ * more would be needed; the surplus is dropped). Pinned host memory gives
+ * full copy bandwidth. */
 int gasatt_sim_run_host(gasatt_sim *sim, double *pos, double *vel,
                         int64_t *n_io, int64_t cap, int nsteps);
+/* cheap counter read (one small device->host copy) */
+int gasatt_sim_counts(gasatt_sim *sim, int64_t *n_slots, int64_t *n_ionizations,
+                      int64_t *n_lost);
+/* device-side phase timing: with timing enabled the step graphs record CUDA
+ * events around the field sub-cycle and the particle pass; last_timing gives
+ * the durations of the most recent step (milliseconds) */
+int gasatt_sim_enable_timing(gasatt_sim *sim, int enable);
+int gasatt_sim_last_timing(gasatt_sim *sim, float *fdtd_ms, float *pass_ms);
 
 #ifdef __cplusplus
 }

@@ -294,6 +294,7 @@ void orc_em7(const double *r, const double *z, const double *q, const double *vr
 /* EM3_1.cu:89-95: Faraday update of H_phi (n_r x n_z), in place. */
 void orc_em3_1(double *Er, double *Ez, double *H, int nr, int nz, double mu, double dr,
                double dz, double dt) {
+#pragma omp parallel for schedule(static) num_threads(g_threads)
   for (int j = 0; j < nz; ++j)
     for (int i = 0; i < nr; ++i) {
       int64_t nr_ = i + (int64_t)j * nr, nz_ = i + (int64_t)j * (nr + 1);
@@ -306,6 +307,7 @@ void orc_em3_1(double *Er, double *Ez, double *H, int nr, int nz, double mu, dou
 void orc_em3(const double *Er0, const double *Ez0, const double *H0, double *Er, double *Ez,
              const double *jr, const double *jz, int nr, int nz, double eps, double dr,
              double dz, double dt, unsigned flags) {
+#pragma omp parallel for schedule(static) num_threads(g_threads)
   for (int j = 0; j <= nz; ++j) {
     for (int i = 0; i <= nr; ++i) {
       int64_t n_r = i + (int64_t)j * nr, n_z = i + (int64_t)j * (nr + 1);
@@ -928,6 +930,31 @@ static void deposit_u(double x, double y, double z, double ux, double uy, double
           cfg->PHIp);
 }
 
+/* births of one thread: state rows appended after the parallel loop */
+typedef struct births_t {
+  int64_t n, cap;
+  double *st;        /* 6 per birth: x y z ux uy uz */
+  uint64_t *id;
+  uint8_t *alive;
+} births_t;
+
+static void births_push(births_t *b, const double s[6], uint64_t id, uint8_t alive) {
+  if (b->n == b->cap) {
+    b->cap = b->cap ? 2 * b->cap : 256;
+    b->st = (double *)realloc(b->st, (size_t)b->cap * 6 * sizeof(double));
+    b->id = (uint64_t *)realloc(b->id, (size_t)b->cap * sizeof(uint64_t));
+    b->alive = (uint8_t *)realloc(b->alive, (size_t)b->cap);
+  }
+  memcpy(b->st + 6 * b->n, s, 6 * sizeof(double));
+  b->id[b->n] = id;
+  b->alive[b->n] = alive;
+  b->n++;
+}
+
+/* per-thread current buffers, kept between calls */
+static double *g_tj = NULL;
+static size_t g_tj_len = 0;
+
 int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, double *x,
                  double *y, double *z, double *ux, double *uy, double *uz, uint64_t *id,
                  uint8_t *alive, int64_t *n_io, int64_t cap, const double *Er, const double *Ez,
@@ -939,102 +966,141 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
   const double P_null = -expm1(-xs->nu_max * cfg->dt);
   const double I = GASATT_ION_I_EV;
   const int64_t ncel = (int64_t)nr * nz;
-  memset(jr, 0, (size_t)ncel * sizeof(double));
-  memset(jz, 0, (size_t)ncel * sizeof(double));
+  const int nt = g_threads;
+  const size_t need = (size_t)nt * 2 * (size_t)ncel;
+  if (need > g_tj_len) {
+    free(g_tj);
+    g_tj = (double *)malloc(need * sizeof(double));
+    g_tj_len = need;
+  }
+  births_t *bt = (births_t *)calloc((size_t)nt, sizeof(births_t));
+  orc_counters *ct = (orc_counters *)calloc((size_t)nt, sizeof(orc_counters));
   const int64_t n0 = *n_io;
-  int64_t n = n0;
-  for (int64_t p = 0; p < n0; ++p) {
-    if (!alive[p]) continue;
-    if (do_kick) {
-      double r0 = sqrt(x[p] * x[p] + y[p] * y[p]);
-      double cp = r0 > 0 ? x[p] / r0 : 1.0, sp = r0 > 0 ? y[p] / r0 : 0.0;
-      double E_r, E_z, Hp;
-      gather(Er, Ez, H, nr, nz, cfg->dr, cfg->dz, r0, z[p], &E_r, &E_z, &Hp);
-      double B = cfg->mu0 * Hp;
-      if (cfg->flags & GASATT_Q_EULER_KICK) {
-        double g = sqrt(1 + (ux[p] * ux[p] + uy[p] * uy[p] + uz[p] * uz[p]) / (c * c));
-        double vr = (ux[p] * cp + uy[p] * sp) / g, vz = uz[p] / g;
-        double Fr = -qe * (E_r + (-vz * Hp * cfg->mu0)), Fz = -qe * (E_z + (vr * Hp * cfg->mu0));
-        ux[p] += Fr * cp / me * cfg->dt; uy[p] += Fr * sp / me * cfg->dt; uz[p] += Fz / me * cfg->dt;
-      } else {
-        boris(&ux[p], &uy[p], &uz[p], E_r * cp, E_r * sp, E_z, -B * sp, B * cp, 0.0, qm_dt2, c);
-      }
-      halfdrift_u(&x[p], &y[p], &z[p], &ux[p], &uy[p], &uz[p], &alive[p], cfg, Rp, Lp);
-      if (!alive[p]) { cnt->lost++; continue; }
-    }
-    if (do_mcc) {
-      double U1, U2;
-      draw_block(cfg->seed, id[p], step, 0, &U1, &U2);
-      if (U1 < P_null) {
-        double u2 = ux[p] * ux[p] + uy[p] * uy[p] + uz[p] * uz[p];
-        double g = sqrt(1 + u2 / (c * c));
-        double EJ = me * c * c * ((u2 / (c * c)) / (g + 1));
-        double Eev = EJ / qe;
-        double um = sqrt(u2), v = um / g;
-        double se, si, sx, L;
-        xs_lookup(xs, Eev, &se, &si, &sx, &L);
-        double nu_el = cfg->gas_density * se * v, nu_io = cfg->gas_density * si * v;
-        double nu_ex = cfg->gas_density * sx * v;
-        double X = U2 * xs->nu_max;
-        if (X < nu_el) {
-          double U3, U4;
-          draw_block(cfg->seed, id[p], step, 1, &U3, &U4);
-          double th = cdf_theta(xs, L, U3), ph = 2 * GASATT_PI * U4;
-          rotate_v(&ux[p], &uy[p], &uz[p], th, ph, 0);
-          cnt->ela++;
-        } else if (X < nu_el + nu_io && Eev > I) {
-          double U3, U4;
-          draw_block(cfg->seed, id[p], step, 1, &U3, &U4);
-          double T = Eev;
-          double T_a = 1000, T_b = 2 * I, t_b = I, T_s = 4.17, t_s = 13.8;
-          double T_0 = T_s - T_a / (T + T_b);
-          double t = t_s * T / (T + t_b);
-          double T_m = (T - I) / 2;
-          double k_1 = atan((T_m - T_0) / t), k_2 = atan(T_0 / t);
-          double k0 = T_0 + t * tan(U3 * (k_1 + k_2) - k_2);
-          double E_1 = k0, E_2 = T - E_1 - I, E_p, E_s;
-          if (E_2 > E_1) { E_p = E_2; E_s = E_1; } else { E_p = E_1; E_s = E_2; }
-          double E_e = me * c * c / qe;
-          double phi_p = 2 * GASATT_PI * U4, phi_s = phi_p - GASATT_PI;
-          double th_p = asin(sqrt((E_s / T) / ((1 - E_s / T) * T / (2 * E_e) + 1)));
-          double th_s = asin(sqrt((1 - E_s / T) / (1 + E_s / (2 * E_e))));
-          double ix = ux[p] / um, iy = uy[p] / um, iz_ = uz[p] / um;
-          double up = u_of_energy(E_p * qe, me, c), us = u_of_energy(E_s * qe, me, c);
-          ux[p] = ix * up; uy[p] = iy * up; uz[p] = iz_ * up;
-          rotate_v(&ux[p], &uy[p], &uz[p], th_p, phi_p, 0);
-          cnt->ion++;
-          if (cfg->secondaries) {
-            if (n >= cap) { cnt->cap_overflow++; }
-            else {
-              double sx_ = ix * us, sy_ = iy * us, sz_ = iz_ * us;
-              rotate_v(&sx_, &sy_, &sz_, th_s, phi_s, 0);
-              x[n] = x[p]; y[n] = y[p]; z[n] = z[p];
-              ux[n] = sx_; uy[n] = sy_; uz[n] = sz_;
-              id[n] = orc_child_id(id[p], step);
-              alive[n] = 1;
-              halfdrift_u(&x[n], &y[n], &z[n], &ux[n], &uy[n], &uz[n], &alive[n], cfg, Rp, Lp);
-              if (alive[n]) deposit_u(x[n], y[n], z[n], ux[n], uy[n], uz[n], cfg, jr, jz);
-              else cnt->lost++;
-              ++n;
-            }
-          }
-        } else if (X < nu_el + nu_io + nu_ex) {
-          int ok;
-          double E_dep = exc_loss_sim(xs, Eev, &ok);
-          if (ok) {
-            double up = u_of_energy((Eev - E_dep) * qe, me, c);
-            ux[p] = ux[p] / um * up; uy[p] = uy[p] / um * up; uz[p] = uz[p] / um * up;
-            cnt->exc++;
-          } else cnt->nul++;
+#pragma omp parallel num_threads(nt)
+  {
+#ifdef _OPENMP
+    const int tid = omp_get_thread_num();
+#else
+    const int tid = 0;
+#endif
+    double *tjr = g_tj + (size_t)tid * 2 * ncel, *tjz = tjr + ncel;
+    memset(tjr, 0, 2 * (size_t)ncel * sizeof(double));
+    births_t *B = &bt[tid];
+    orc_counters *C = &ct[tid];
+#pragma omp for schedule(static)
+    for (int64_t p = 0; p < n0; ++p) {
+      if (!alive[p]) continue;
+      if (do_kick) {
+        double r0 = sqrt(x[p] * x[p] + y[p] * y[p]);
+        double cp = r0 > 0 ? x[p] / r0 : 1.0, sp = r0 > 0 ? y[p] / r0 : 0.0;
+        double E_r, E_z, Hp;
+        gather(Er, Ez, H, nr, nz, cfg->dr, cfg->dz, r0, z[p], &E_r, &E_z, &Hp);
+        double B_ = cfg->mu0 * Hp;
+        if (cfg->flags & GASATT_Q_EULER_KICK) {
+          double g = sqrt(1 + (ux[p] * ux[p] + uy[p] * uy[p] + uz[p] * uz[p]) / (c * c));
+          double vr = (ux[p] * cp + uy[p] * sp) / g, vz = uz[p] / g;
+          double Fr = -qe * (E_r + (-vz * Hp * cfg->mu0)), Fz = -qe * (E_z + (vr * Hp * cfg->mu0));
+          ux[p] += Fr * cp / me * cfg->dt; uy[p] += Fr * sp / me * cfg->dt; uz[p] += Fz / me * cfg->dt;
         } else {
-          cnt->nul++;
+          boris(&ux[p], &uy[p], &uz[p], E_r * cp, E_r * sp, E_z, -B_ * sp, B_ * cp, 0.0, qm_dt2, c);
+        }
+        halfdrift_u(&x[p], &y[p], &z[p], &ux[p], &uy[p], &uz[p], &alive[p], cfg, Rp, Lp);
+        if (!alive[p]) { C->lost++; continue; }
+      }
+      if (do_mcc) {
+        double U1, U2;
+        draw_block(cfg->seed, id[p], step, 0, &U1, &U2);
+        if (U1 < P_null) {
+          double u2 = ux[p] * ux[p] + uy[p] * uy[p] + uz[p] * uz[p];
+          double g = sqrt(1 + u2 / (c * c));
+          double EJ = me * c * c * ((u2 / (c * c)) / (g + 1));
+          double Eev = EJ / qe;
+          double um = sqrt(u2), v = um / g;
+          double se, si, sx, L;
+          xs_lookup(xs, Eev, &se, &si, &sx, &L);
+          double nu_el = cfg->gas_density * se * v, nu_io = cfg->gas_density * si * v;
+          double nu_ex = cfg->gas_density * sx * v;
+          double X = U2 * xs->nu_max;
+          if (X < nu_el) {
+            double U3, U4;
+            draw_block(cfg->seed, id[p], step, 1, &U3, &U4);
+            double th = cdf_theta(xs, L, U3), ph = 2 * GASATT_PI * U4;
+            rotate_v(&ux[p], &uy[p], &uz[p], th, ph, 0);
+            C->ela++;
+          } else if (X < nu_el + nu_io && Eev > I) {
+            double U3, U4;
+            draw_block(cfg->seed, id[p], step, 1, &U3, &U4);
+            double T = Eev;
+            double T_a = 1000, T_b = 2 * I, t_b = I, T_s = 4.17, t_s = 13.8;
+            double T_0 = T_s - T_a / (T + T_b);
+            double t = t_s * T / (T + t_b);
+            double T_m = (T - I) / 2;
+            double k_1 = atan((T_m - T_0) / t), k_2 = atan(T_0 / t);
+            double k0 = T_0 + t * tan(U3 * (k_1 + k_2) - k_2);
+            double E_1 = k0, E_2 = T - E_1 - I, E_p, E_s;
+            if (E_2 > E_1) { E_p = E_2; E_s = E_1; } else { E_p = E_1; E_s = E_2; }
+            double E_e = me * c * c / qe;
+            double phi_p = 2 * GASATT_PI * U4, phi_s = phi_p - GASATT_PI;
+            double th_p = asin(sqrt((E_s / T) / ((1 - E_s / T) * T / (2 * E_e) + 1)));
+            double th_s = asin(sqrt((1 - E_s / T) / (1 + E_s / (2 * E_e))));
+            double ix = ux[p] / um, iy = uy[p] / um, iz_ = uz[p] / um;
+            double up = u_of_energy(E_p * qe, me, c), us = u_of_energy(E_s * qe, me, c);
+            ux[p] = ix * up; uy[p] = iy * up; uz[p] = iz_ * up;
+            rotate_v(&ux[p], &uy[p], &uz[p], th_p, phi_p, 0);
+            C->ion++;
+            if (cfg->secondaries) {
+              double s[6] = {x[p], y[p], z[p], ix * us, iy * us, iz_ * us};
+              rotate_v(&s[3], &s[4], &s[5], th_s, phi_s, 0);
+              uint8_t ca = 1;
+              halfdrift_u(&s[0], &s[1], &s[2], &s[3], &s[4], &s[5], &ca, cfg, Rp, Lp);
+              if (ca) deposit_u(s[0], s[1], s[2], s[3], s[4], s[5], cfg, tjr, tjz);
+              else C->lost++;
+              births_push(B, s, orc_child_id(id[p], step), ca);
+            }
+          } else if (X < nu_el + nu_io + nu_ex) {
+            int ok;
+            double E_dep = exc_loss_sim(xs, Eev, &ok);
+            if (ok) {
+              double up = u_of_energy((Eev - E_dep) * qe, me, c);
+              ux[p] = ux[p] / um * up; uy[p] = uy[p] / um * up; uz[p] = uz[p] / um * up;
+              C->exc++;
+            } else C->nul++;
+          } else {
+            C->nul++;
+          }
         }
       }
+      halfdrift_u(&x[p], &y[p], &z[p], &ux[p], &uy[p], &uz[p], &alive[p], cfg, Rp, Lp);
+      if (!alive[p]) { C->lost++; continue; }
+      deposit_u(x[p], y[p], z[p], ux[p], uy[p], uz[p], cfg, tjr, tjz);
     }
-    halfdrift_u(&x[p], &y[p], &z[p], &ux[p], &uy[p], &uz[p], &alive[p], cfg, Rp, Lp);
-    if (!alive[p]) { cnt->lost++; continue; }
-    deposit_u(x[p], y[p], z[p], ux[p], uy[p], uz[p], cfg, jr, jz);
+    /* reduce the per-thread currents in thread order */
+#pragma omp for schedule(static)
+    for (int64_t k = 0; k < ncel; ++k) {
+      double a = 0, b = 0;
+      for (int t = 0; t < nt; ++t) {
+        a += g_tj[(size_t)t * 2 * ncel + k];
+        b += g_tj[(size_t)t * 2 * ncel + ncel + k];
+      }
+      jr[k] = a;
+      jz[k] = b;
+    }
   }
+  int64_t n = n0;
+  for (int t = 0; t < nt; ++t) {
+    cnt->ion += ct[t].ion; cnt->ela += ct[t].ela; cnt->exc += ct[t].exc;
+    cnt->nul += ct[t].nul; cnt->lost += ct[t].lost;
+    for (int64_t k = 0; k < bt[t].n; ++k) {
+      if (n >= cap) { cnt->cap_overflow++; continue; }
+      const double *s = bt[t].st + 6 * k;
+      x[n] = s[0]; y[n] = s[1]; z[n] = s[2]; ux[n] = s[3]; uy[n] = s[4]; uz[n] = s[5];
+      id[n] = bt[t].id[k];
+      alive[n] = bt[t].alive[k];
+      ++n;
+    }
+    free(bt[t].st); free(bt[t].id); free(bt[t].alive);
+  }
+  free(bt); free(ct);
   *n_io = n;
   return 0;
 }
