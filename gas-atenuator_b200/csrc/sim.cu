@@ -43,6 +43,7 @@ struct SimCounters {
   unsigned long long kin_fx;     // diagnostic: sum E_kin * 2^16 [eV]
   unsigned long long alive;      // diagnostic
   unsigned long long cap;        // slot capacity
+  unsigned long long n_cand;     // collision candidates queued by the current pass
 };
 
 // slots holding particles, including births of the last pass not yet committed
@@ -59,7 +60,9 @@ struct SimParams {
   long long cap;
   double qm_dt2;            // -q_e/m_e dt/2
   float aE, aB, hdr, hdz;   // FP32 form: impulse per (V/m), per (A/m); c dt/(2 dr), c dt/(2 dz)
-  double dep;               // fixed-point factor: FP64 q FN scale (x v), FP32 q FN c scale (x beta)
+  double dep;               // fixed-point factor: FP64 q FN scale (x v)
+  float depf;               // FP32: q FN c scale (x beta)
+  uint64_t cand_below;      // null-collision candidate iff the 52-bit draw is below this
   // tables
   const double *sig;        // 3 x G (el, ion, exc)
   const double *cdf;        // G x 181
@@ -73,8 +76,9 @@ struct SimParams {
 template <typename Real>
 struct Fields { Real *Er, *Ez, *H; };
 
-struct State64 { double *r, *z, *ur, *ut, *uz; uint64_t *id; };
-struct State32 { uint32_t *key; float *fr, *fz, *ur, *ut, *uz; uint64_t *id; };
+// FP64: (r, z), (u_r, u_theta), u_z, id.   FP32: (key, fr, fz, u_r), (u_theta, u_z), id.
+struct State64 { double2 *rz; double2 *urt; double *uz; uint64_t *id; };
+struct State32 { uint4 *a; float2 *b; uint64_t *id; };
 
 // ------------------------------------------------------------------- MCC
 struct Birth { bool born; double ux, uy, uz; };
@@ -110,14 +114,23 @@ __device__ __forceinline__ double u_of_energy(double EJ, double m, double c) {
   return c * sqrt(e * (2 + e));
 }
 
-// Null-collision event for one electron at step `step` (corrected form of
+// Null-collision candidate test U1 < P_null on the integer draw: with
+// U1 = (2b+1) 2^-53 (b the top 52 bits of the first two words) this is
+// exactly b < P.cand_below.
+__device__ __forceinline__ bool null_candidate(const SimParams &P, uint64_t id, long long step) {
+  uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
+  philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+  const uint64_t b = ((((uint64_t)c[0]) << 32) | c[1]) >> 12;
+  return b < P.cand_below;
+}
+
+// Collision of a candidate electron at step `step` (corrected form of
 // electron_transport.cu:74-227).  u in m/s, local (r, theta, z) frame.
-// Returns 0 no candidate, 1 elastic, 2 ionization, 3 excitation, 4 null.
-__device__ int mcc_event(const SimParams &P, uint64_t id, long long step, double &ux, double &uy,
-                         double &uz, Birth &b) {
+// Returns 1 elastic, 2 ionization, 3 excitation, 4 null.
+__device__ __noinline__ int mcc_event(const SimParams &P, uint64_t id, long long step, double &ux,
+                                      double &uy, double &uz, Birth &b) {
   b.born = false;
   const U2 d0 = draw2(P.seed, id, step, 0);
-  if (!(d0.a < P.P_null)) return 0;
   const double c = P.c, me = P.me, qe = P.qe, I = GASATT_ION_I_EV;
   const double u2 = ux * ux + uy * uy + uz * uz;
   const double g = sqrt(1 + u2 / (c * c));
@@ -181,6 +194,24 @@ __device__ int mcc_event(const SimParams &P, uint64_t id, long long step, double
   return 4;
 }
 
+__device__ __forceinline__ void count_event(SimCounters *cnt, int ev) {
+  if (ev == 1) atomicAdd(&cnt->ela, 1ull);
+  else if (ev == 2) atomicAdd(&cnt->ion, 1ull);
+  else if (ev == 3) atomicAdd(&cnt->exc, 1ull);
+  else if (ev == 4) atomicAdd(&cnt->nul, 1ull);
+}
+
+// warp-aggregated append of candidate slots to the collision queue
+__device__ __forceinline__ void queue_push(bool want, long long p, SimCounters *cnt, int *queue) {
+  const unsigned m = __ballot_sync(0xFFFFFFFFu, want);
+  if (!m) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(&cnt->n_cand, (unsigned long long)__popc(m));
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  if (want) queue[base + __popc(m & ((1u << lane) - 1))] = (int)p;
+}
+
 // ------------------------------------------------------ warp deposit
 // Sum of v over the lanes of `mask` (all lanes of the group call it).
 __device__ __forceinline__ long long group_sum_i64(unsigned mask, long long v) {
@@ -192,7 +223,7 @@ __device__ __forceinline__ long long group_sum_i64(unsigned mask, long long v) {
 }
 
 // 4 nodes x 2 components, grouped by node key; the lowest lane of each group
-// issues the atomics.  `act` lanes with no contribution pass zeros.
+// issues the atomics.  Must be reached by all 32 lanes of the warp.
 __device__ __forceinline__ void warp_deposit(bool act, unsigned key, const int64_t a[4],
                                              const long long vr[4], const long long vz[4],
                                              unsigned long long *Jr, unsigned long long *Jz,
@@ -215,6 +246,15 @@ __device__ __forceinline__ void warp_deposit(bool act, unsigned key, const int64
       if (sr) atomicAdd(Jr + a[k], (unsigned long long)sr);
       if (sz) atomicAdd(Jz + a[k], (unsigned long long)sz);
     }
+  }
+}
+
+__device__ __forceinline__ void deposit_direct(const int64_t a[4], const long long vr[4],
+                                               const long long vz[4], const SimParams &P) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (vr[k]) atomicAdd(P.Jr + a[k], (unsigned long long)vr[k]);
+    if (vz[k]) atomicAdd(P.Jz + a[k], (unsigned long long)vz[k]);
   }
 }
 
@@ -253,26 +293,11 @@ __device__ __forceinline__ void deposit_values64(const SimParams &P, double r, d
   }
 }
 
-__device__ __forceinline__ void deposit_direct(const int64_t a[4], const long long vr[4],
-                                               const long long vz[4], const SimParams &P) {
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (vr[k]) atomicAdd(P.Jr + a[k], (unsigned long long)vr[k]);
-    if (vz[k]) atomicAdd(P.Jz + a[k], (unsigned long long)vz[k]);
-  }
-}
-
-__device__ __forceinline__ void count_event(SimCounters *cnt, int ev) {
-  if (ev == 1) atomicAdd(&cnt->ela, 1ull);
-  else if (ev == 2) atomicAdd(&cnt->ion, 1ull);
-  else if (ev == 3) atomicAdd(&cnt->exc, 1ull);
-  else if (ev == 4) atomicAdd(&cnt->nul, 1ull);
-}
-
-// mode 0: full pass; mode 1: half drift + deposit only (start of a run);
-// mode 2: kick + half drift only, ending at integer time (end of a run)
-__global__ void __launch_bounds__(kBlock) k_pass64(SimParams P, State64 S, Fields<double> F,
-                                                   SimCounters *cnt, int mode) {
+// mode 0: full pass (collision candidates go to the queue and are finished by
+// k_mcc64); mode 1: half drift + deposit only (start of a run); mode 2: kick
+// + half drift only, ending at integer time (end of a run)
+__global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fields<double> F,
+                                                      SimCounters *cnt, int *queue, int mode) {
   const long long n0 = (long long)cnt->n_total;
   const long long step = cnt->step;
   const int lane = threadIdx.x & 31;
@@ -282,13 +307,16 @@ __global__ void __launch_bounds__(kBlock) k_pass64(SimParams P, State64 S, Field
        base += stride) {
     const long long p = base + lane;
     bool act = p < n0;
-    double r = 0, z = 0, ur = 0, ut = 0, uz = 0;
+    double2 rz = make_double2(-1.0, 0.0), urt = make_double2(0.0, 0.0);
+    double uz = 0;
     if (act) {
-      r = S.r[p];
-      act = r >= 0;
+      rz = S.rz[p];
+      act = rz.x >= 0;
     }
+    bool cand = false;
     if (act) {
-      z = S.z[p]; ur = S.ur[p]; ut = S.ut[p]; uz = S.uz[p];
+      urt = S.urt[p]; uz = S.uz[p];
+      double r = rz.x, z = rz.y, ur = urt.x, ut = urt.y;
       bool alive = true;
       if (mode != 1) {
         double E_r, E_z, Hp;
@@ -296,46 +324,73 @@ __global__ void __launch_bounds__(kBlock) k_pass64(SimParams P, State64 S, Field
         const double B = P.mu0 * Hp;
         boris(ur, ut, uz, E_r, 0.0, E_z, 0.0, B, 0.0, P.qm_dt2, P.c);
         halfdrift64(r, z, ur, ut, uz, alive, P);
-        if (alive && mode == 0) {
-          Birth b;
-          const int ev = mcc_event(P, S.id[p], step, ur, ut, uz, b);
-          if (ev) count_event(cnt, ev);
-          if (b.born) {
-            const unsigned long long k = atomicAdd(&cnt->n_births, 1ull);
-            const long long slot = n0 + (long long)k;
-            if (slot < P.cap) {
-              double cr = r, cz = z, cur = b.ux, cut = b.uy, cuz = b.uz;
-              bool calive = true;
-              halfdrift64(cr, cz, cur, cut, cuz, calive, P);
-              if (calive) {
-                int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
-                deposit_values64(P, cr, cz, cur, cut, cuz, a, vr, vz, kk);
-                deposit_direct(a, vr, vz, P);
-              } else {
-                atomicAdd(&cnt->lost, 1ull);
-              }
-              S.r[slot] = calive ? cr : -1.0; S.z[slot] = cz;
-              S.ur[slot] = cur; S.ut[slot] = cut; S.uz[slot] = cuz;
-              S.id[slot] = child_id(S.id[p], step);
-            } else {
-              atomicAdd(&cnt->cap_overflow, 1ull);
-            }
-          }
-        }
+        if (alive && mode == 0) cand = null_candidate(P, S.id[p], step);
       }
-      if (alive && mode != 2) halfdrift64(r, z, ur, ut, uz, alive, P);
+      if (alive && mode != 2 && !cand) halfdrift64(r, z, ur, ut, uz, alive, P);
       if (!alive) { lost++; r = -1.0; }
-      S.r[p] = r; S.z[p] = z; S.ur[p] = ur; S.ut[p] = ut; S.uz[p] = uz;
-      act = alive && mode != 2;
+      rz = make_double2(r, z); urt = make_double2(ur, ut);
+      S.rz[p] = rz; S.urt[p] = urt; S.uz[p] = uz;
+      act = alive && mode != 2 && !cand;
     }
+    queue_push(cand, p, cnt, queue);
     int64_t a[4] = {0, 0, 0, 0};
     long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
     unsigned key = 0;
-    if (act) deposit_values64(P, r, z, ur, ut, uz, a, vr, vz, key);
+    if (act) deposit_values64(P, rz.x, rz.y, urt.x, urt.y, uz, a, vr, vz, key);
     warp_deposit(act, key, a, vr, vz, P.Jr, P.Jz, true);
   }
   lost = __reduce_add_sync(0xFFFFFFFFu, lost);
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
+}
+
+// collision candidates of this step: MCC, births, second half drift, deposit
+__global__ void __launch_bounds__(128) k_mcc64(SimParams P, State64 S, SimCounters *cnt,
+                                               const int *queue) {
+  const long long n0 = (long long)cnt->n_total;
+  const long long step = cnt->step;
+  const long long nq = (long long)cnt->n_cand;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
+       q += (long long)gridDim.x * blockDim.x) {
+    const long long p = queue[q];
+    double2 rz = S.rz[p], urt = S.urt[p];
+    double r = rz.x, z = rz.y, ur = urt.x, ut = urt.y, uz = S.uz[p];
+    const uint64_t id = S.id[p];
+    Birth b;
+    count_event(cnt, mcc_event(P, id, step, ur, ut, uz, b));
+    if (b.born) {
+      const unsigned long long k = atomicAdd(&cnt->n_births, 1ull);
+      const long long slot = n0 + (long long)k;
+      if (slot < P.cap) {
+        double cr = r, cz = z, cur = b.ux, cut = b.uy, cuz = b.uz;
+        bool calive = true;
+        halfdrift64(cr, cz, cur, cut, cuz, calive, P);
+        if (calive) {
+          int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
+          deposit_values64(P, cr, cz, cur, cut, cuz, a, vr, vz, kk);
+          deposit_direct(a, vr, vz, P);
+        } else {
+          atomicAdd(&cnt->lost, 1ull);
+        }
+        S.rz[slot] = make_double2(calive ? cr : -1.0, cz);
+        S.urt[slot] = make_double2(cur, cut);
+        S.uz[slot] = cuz;
+        S.id[slot] = child_id(id, step);
+      } else {
+        atomicAdd(&cnt->cap_overflow, 1ull);
+      }
+    }
+    bool alive = true;
+    halfdrift64(r, z, ur, ut, uz, alive, P);
+    if (alive) {
+      int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
+      deposit_values64(P, r, z, ur, ut, uz, a, vr, vz, kk);
+      deposit_direct(a, vr, vz, P);
+    } else {
+      atomicAdd(&cnt->lost, 1ull);
+      r = -1.0;
+    }
+    S.rz[p] = make_double2(r, z); S.urt[p] = make_double2(ur, ut); S.uz[p] = uz;
+  }
 }
 
 // ----------------------------------------------------------- FP32 form
@@ -344,53 +399,103 @@ __device__ __forceinline__ float bilin(const float *__restrict__ F, int ncol, in
                                        float wc, int r0, float wr) {
   const int ca = max(c0, 0), cb = min(c0 + 1, ncol - 1);
   const int ra = max(r0, 0), rb = min(r0 + 1, nrow - 1);
-  const float f00 = __ldg(F + ca + (int64_t)ra * ncol), f10 = __ldg(F + cb + (int64_t)ra * ncol);
-  const float f01 = __ldg(F + ca + (int64_t)rb * ncol), f11 = __ldg(F + cb + (int64_t)rb * ncol);
-  return (1 - wr) * ((1 - wc) * f00 + wc * f10) + wr * ((1 - wc) * f01 + wc * f11);
+  const float *pa = F + (int64_t)ra * ncol, *pb = F + (int64_t)rb * ncol;
+  const float f00 = __ldg(pa + ca), f10 = __ldg(pa + cb);
+  const float f01 = __ldg(pb + ca), f11 = __ldg(pb + cb);
+  const float lo = fmaf(wc, f10 - f00, f00), hi = fmaf(wc, f11 - f01, f01);
+  return fmaf(wr, hi - lo, lo);
+}
+
+// 1/sqrt(x) refined by one Newton step: the hardware estimate is biased, and
+// a biased rotation normaliser or gamma makes the FP32 energy drift steadily
+__device__ __forceinline__ float rsqrt_nr(float x) {
+  const float y = rsqrtf(x);
+  return y * fmaf(-0.5f * x * y, y, 1.5f);
+}
+
+// a + d with stochastic rounding.  The per-step velocity changes of the FP32
+// form (a drift rotation by a small angle, a kick in a weak field) are often
+// below one float ulp of u; rounding them to nearest would bias |u| steadily.
+// The exact residual of a + d (TwoSum) picks the neighbour float with
+// probability |residual| / ulp, using 16 random bits r16.
+__device__ __forceinline__ float sround_add(float a, float d, uint32_t r16) {
+  const float s = a + d;
+  const float bb = s - a;
+  const float e = (a - (s - bb)) + (d - bb);
+  if (e == 0.f || s == 0.f) return s;
+  const int dir = ((e > 0.f) == (s > 0.f)) ? 1 : -1;
+  const float nb = __int_as_float(__float_as_int(s) + dir);
+  const float p = __fdividef(fabsf(e), fabsf(nb - s));
+  const float u = ((float)(r16 & 0xFFFFu) + 0.5f) * (1.0f / 65536.0f);
+  return u < p ? nb : s;
+}
+
+// 32 fresh bits from a 32-bit input (integer finaliser)
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352du;
+  x ^= x >> 15; x *= 0x846ca68bu;
+  return x ^ (x >> 16);
 }
 
 // half-cell staggered index/weight: position ic + f measured from node ic-1/2
 __device__ __forceinline__ void half_shift(int ic, float f, int &a, float &w) {
-  if (f >= 0.5f) { a = ic; w = f - 0.5f; } else { a = ic - 1; w = f + 0.5f; }
+  const bool up = f >= 0.5f;
+  a = up ? ic : ic - 1;
+  w = up ? f - 0.5f : f + 0.5f;
 }
 
+// specular reflection of the cell coordinate (iz, fz) into [0, nz)
+__device__ __forceinline__ void reflect_z(int &iz, float &fz, float &uz, int nz) {
+  if (iz < 0 || iz >= nz) {
+    iz = iz < 0 ? -iz - 1 : 2 * nz - iz - 1;
+    fz = 1.f - fz;
+    uz = -uz;
+    if (fz >= 1.f) { fz = 0.f; iz += 1; }
+    if (iz > nz - 1) { iz = nz - 1; fz = 0.99999994f; }
+    if (iz < 0) { iz = 0; fz = 0.f; }
+  }
+}
+
+// Half drift in cell units.  The new radius comes from the exact difference
+// r' - rc = (dx (2 rc + dx) + dy^2) / (r' + rc) (no cancellation at large rc);
+// (u_r, u_theta) turn by the drift angle a, written with the small
+// quantities sin a and 1 - cos a = sin^2 a / (1 + cos a) and added to u with
+// stochastic rounding (rb: two 16-bit random numbers).
 __device__ __forceinline__ void halfdrift32(int &ir, int &iz, float &fr, float &fz, float &ur,
                                             float &ut, float &uz, bool &alive,
-                                            const SimParams &P) {
-  const float ig = 1.0f / sqrtf(1.0f + ur * ur + ut * ut + uz * uz);
+                                            const SimParams &P, uint32_t rb) {
+  const float ig = rsqrt_nr(fmaf(ur, ur, fmaf(ut, ut, fmaf(uz, uz, 1.0f))));
   const float dx = ur * ig * P.hdr, dy = ut * ig * P.hdr, dzz = uz * ig * P.hdz;
   const float rc = (float)ir + fr;
   const float X = rc + dx;
-  const float rn = sqrtf(X * X + dy * dy);
+  const float r2 = fmaf(X, X, dy * dy);
+  const float irn = rsqrt_nr(r2);                    // 1/r' (inf at r' = 0)
+  const float rn = r2 * irn;
+  const float sn = r2 > 0.f ? dy * irn : 0.f;
+  const float s2 = sn * sn;
+  const float sq = sqrtf(fmaxf(0.f, 1.f - s2));
+  const float c1 = X >= 0.f ? __fdividef(s2, 1.f + sq) : 1.f + sq;   // 1 - cos a
+  const float dur = fmaf(sn, ut, -c1 * ur), dut = fmaf(-sn, ur, -c1 * ut);
+  ur = sround_add(ur, dur, rb);
+  ut = sround_add(ut, dut, rb >> 16);
   const float den = rn + rc;
-  const float drr = den > 0.f ? (dx * (2.f * rc + dx) + dy * dy) / den : 0.f;
-  const float cs = rn > 0.f ? X / rn : 1.f, sn = rn > 0.f ? dy / rn : 0.f;
-  const float nur = cs * ur + sn * ut, nut = -sn * ur + cs * ut;
-  ur = nur; ut = nut;
+  const float drr = den > 0.f ? __fdividef(fmaf(dx, 2.f * rc + dx, dy * dy), den) : 0.f;
   fr += drr;
-  int k = (int)floorf(fr);
-  ir += k; fr -= (float)k;
+  float k = floorf(fr);
+  ir += (int)k; fr -= k;
   if (ir < 0) { ir = 0; fr = 0.f; }
-  if (ir >= P.nr) alive = false;
+  alive = alive && ir < P.nr;
   fz += dzz;
-  k = (int)floorf(fz);
-  iz += k; fz -= (float)k;
-  if (iz < 0) {                                   // specular at z = 0
-    iz = -iz - 1; fz = 1.f - fz; uz = -uz;
-    if (fz >= 1.f) { fz = 0.f; iz += 1; }
-  } else if (iz >= P.nz) {                         // specular at z = Lp
-    iz = 2 * P.nz - iz - 1; fz = 1.f - fz; uz = -uz;
-    if (fz >= 1.f) { fz = 0.f; iz += 1; }
-  }
-  if (iz > P.nz - 1) { iz = P.nz - 1; fz = 0.99999994f; }
-  if (iz < 0) { iz = 0; fz = 0.f; }
+  k = floorf(fz);
+  iz += (int)k; fz -= k;
+  reflect_z(iz, fz, uz, P.nz);
 }
 
 __device__ __forceinline__ void deposit_values32(const SimParams &P, int ir, int iz, float fr,
                                                  float fz, float ur, float ut, float uz,
                                                  int64_t a[4], long long vr[4], long long vz[4],
                                                  unsigned &key) {
-  const float ig = 1.0f / sqrtf(1.0f + ur * ur + ut * ut + uz * uz);
+  const float ig = rsqrt_nr(fmaf(ur, ur, fmaf(ut, ut, fmaf(uz, uz, 1.0f))));
   int ar, az;
   float wr, wz;
   half_shift(ir, fr, ar, wr);
@@ -400,17 +505,22 @@ __device__ __forceinline__ void deposit_values32(const SimParams &P, int ir, int
   a[0] = ca + (int64_t)ra * P.nr; a[1] = cb + (int64_t)ra * P.nr;
   a[2] = ca + (int64_t)rb * P.nr; a[3] = cb + (int64_t)rb * P.nr;
   const float w[4] = {(1 - wr) * (1 - wz), wr * (1 - wz), (1 - wr) * wz, wr * wz};
-  const float kr = (float)P.dep * ur * ig, kz = (float)P.dep * uz * ig;
+  const float kr = P.depf * ur * ig, kz = P.depf * uz * ig;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    vr[k] = __float2ll_rn(kr * w[k]);
-    vz[k] = __float2ll_rn(kz * w[k]);
+    vr[k] = __float2int_rn(kr * w[k]);
+    vz[k] = __float2int_rn(kz * w[k]);
   }
   key = (unsigned)((ar + 1) + (az + 1) * (P.nr + 1));
 }
 
-__global__ void __launch_bounds__(kBlock) k_pass32(SimParams P, State32 S, Fields<float> F,
-                                                   SimCounters *cnt, int mode) {
+__device__ __forceinline__ uint4 pack32(int ir, int iz, float fr, float fz, float ur, bool alive) {
+  return make_uint4(alive ? (((uint32_t)iz << 16) | (uint32_t)ir) : kDead, __float_as_uint(fr),
+                    __float_as_uint(fz), __float_as_uint(ur));
+}
+
+__global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fields<float> F,
+                                                      SimCounters *cnt, int *queue, int mode) {
   const long long n0 = (long long)cnt->n_total;
   const long long step = cnt->step;
   const int lane = threadIdx.x & 31;
@@ -420,16 +530,24 @@ __global__ void __launch_bounds__(kBlock) k_pass32(SimParams P, State32 S, Field
        base += stride) {
     const long long p = base + lane;
     bool act = p < n0;
-    uint32_t key = kDead;
+    uint4 A = make_uint4(kDead, 0, 0, 0);
     if (act) {
-      key = S.key[p];
-      act = key != kDead;
+      A = S.a[p];
+      act = A.x != kDead;
     }
-    int ir = 0, iz = 0;
-    float fr = 0, fz = 0, ur = 0, ut = 0, uz = 0;
+    int ir = (int)(A.x & 0xFFFFu), iz = (int)(A.x >> 16);
+    float fr = __uint_as_float(A.y), fz = __uint_as_float(A.z), ur = __uint_as_float(A.w);
+    float ut = 0.f, uz = 0.f;
+    bool cand = false;
     if (act) {
-      ir = (int)(key & 0xFFFFu); iz = (int)(key >> 16);
-      fr = S.fr[p]; fz = S.fz[p]; ur = S.ur[p]; ut = S.ut[p]; uz = S.uz[p];
+      const float2 B = S.b[p];
+      ut = B.x; uz = B.y;
+      // block 0 of this particle's stream: words 0-1 decide the null-collision
+      // candidate, words 2-3 (mixed) drive the stochastic rounding
+      const uint64_t id = S.id[p];
+      uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
+      philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+      const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]), rb2 = mix32(c[2] ^ (c[3] * 0x9E3779B9u));
       bool alive = true;
       if (mode != 1) {
         int ar, az;
@@ -439,56 +557,27 @@ __global__ void __launch_bounds__(kBlock) k_pass32(SimParams P, State32 S, Field
         const float Er = bilin(F.Er, P.nr, P.nz + 1, ar, wr, iz, fz);
         const float Ez = bilin(F.Ez, P.nr + 1, P.nz, ir, fr, az, wz);
         const float H = bilin(F.H, P.nr, P.nz, ar, wr, az, wz);
-        // Boris in gamma*beta units: E = (Er, 0, Ez), B = (0, mu0 H, 0)
-        const float umr = ur + P.aE * Er, umt = ut, umz = uz + P.aE * Ez;
-        const float gm = sqrtf(1.0f + umr * umr + umt * umt + umz * umz);
-        const float t = P.aB * H / gm;
-        const float s = 2.f * t / (1.f + t * t);
-        const float upr = umr - umz * t, upz = umz + umr * t;
-        ur = umr - upz * s + P.aE * Er;
-        uz = umz + upr * s + P.aE * Ez;
-        ut = umt;
-        halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P);
-        if (alive && mode == 0) {
-          double dux = (double)ur * P.c, duy = (double)ut * P.c, duz = (double)uz * P.c;
-          Birth b;
-          const int ev = mcc_event(P, S.id[p], step, dux, duy, duz, b);
-          if (ev) {
-            count_event(cnt, ev);
-            ur = (float)(dux / P.c); ut = (float)(duy / P.c); uz = (float)(duz / P.c);
-          }
-          if (b.born) {
-            const unsigned long long k = atomicAdd(&cnt->n_births, 1ull);
-            const long long slot = n0 + (long long)k;
-            if (slot < P.cap) {
-              int cir = ir, ciz = iz;
-              float cfr = fr, cfz = fz;
-              float cur = (float)(b.ux / P.c), cut = (float)(b.uy / P.c), cuz = (float)(b.uz / P.c);
-              bool calive = true;
-              halfdrift32(cir, ciz, cfr, cfz, cur, cut, cuz, calive, P);
-              if (calive) {
-                int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
-                deposit_values32(P, cir, ciz, cfr, cfz, cur, cut, cuz, a, vr, vz, kk);
-                deposit_direct(a, vr, vz, P);
-              } else {
-                atomicAdd(&cnt->lost, 1ull);
-              }
-              S.key[slot] = calive ? (((uint32_t)ciz << 16) | (uint32_t)cir) : kDead;
-              S.fr[slot] = cfr; S.fz[slot] = cfz;
-              S.ur[slot] = cur; S.ut[slot] = cut; S.uz[slot] = cuz;
-              S.id[slot] = child_id(S.id[p], step);
-            } else {
-              atomicAdd(&cnt->cap_overflow, 1ull);
-            }
-          }
-        }
+        // Boris in gamma*beta units: E = (Er, 0, Ez), B = (0, mu0 H, 0); the
+        // increment u+ - u is formed first, then added with stochastic rounding
+        const float her = P.aE * Er, hez = P.aE * Ez;
+        const float umr = ur + her, umz = uz + hez;
+        const float igm = rsqrt_nr(fmaf(umr, umr, fmaf(ut, ut, fmaf(umz, umz, 1.0f))));
+        const float t = P.aB * H * igm;
+        const float s = __fdividef(2.f * t, fmaf(t, t, 1.f));
+        const float upr = fmaf(-umz, t, umr), upz = fmaf(umr, t, umz);
+        ur = sround_add(ur, fmaf(-upz, s, 2.f * her), rb0);
+        uz = sround_add(uz, fmaf(upr, s, 2.f * hez), rb0 >> 16);
+        halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1);
+        if (alive && mode == 0)
+          cand = (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
       }
-      if (alive && mode != 2) halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P);
+      if (alive && mode != 2 && !cand) halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb2);
       if (!alive) lost++;
-      S.key[p] = alive ? (((uint32_t)iz << 16) | (uint32_t)ir) : kDead;
-      S.fr[p] = fr; S.fz[p] = fz; S.ur[p] = ur; S.ut[p] = ut; S.uz[p] = uz;
-      act = alive && mode != 2;
+      S.a[p] = pack32(ir, iz, fr, fz, ur, alive);
+      S.b[p] = make_float2(ut, uz);
+      act = alive && mode != 2 && !cand;
     }
+    queue_push(cand, p, cnt, queue);
     int64_t a[4] = {0, 0, 0, 0};
     long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
     unsigned dkey = 0;
@@ -499,10 +588,64 @@ __global__ void __launch_bounds__(kBlock) k_pass32(SimParams P, State32 S, Field
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
 }
 
+__global__ void __launch_bounds__(128) k_mcc32(SimParams P, State32 S, SimCounters *cnt,
+                                               const int *queue) {
+  const long long n0 = (long long)cnt->n_total;
+  const long long step = cnt->step;
+  const long long nq = (long long)cnt->n_cand;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
+       q += (long long)gridDim.x * blockDim.x) {
+    const long long p = queue[q];
+    const uint4 A = S.a[p];
+    const float2 B = S.b[p];
+    int ir = (int)(A.x & 0xFFFFu), iz = (int)(A.x >> 16);
+    float fr = __uint_as_float(A.y), fz = __uint_as_float(A.z);
+    double dux = (double)__uint_as_float(A.w) * P.c, duy = (double)B.x * P.c, duz = (double)B.y * P.c;
+    const uint64_t id = S.id[p];
+    Birth b;
+    count_event(cnt, mcc_event(P, id, step, dux, duy, duz, b));
+    float ur = (float)(dux / P.c), ut = (float)(duy / P.c), uz = (float)(duz / P.c);
+    if (b.born) {
+      const unsigned long long k = atomicAdd(&cnt->n_births, 1ull);
+      const long long slot = n0 + (long long)k;
+      if (slot < P.cap) {
+        int cir = ir, ciz = iz;
+        float cfr = fr, cfz = fz;
+        float cur = (float)(b.ux / P.c), cut = (float)(b.uy / P.c), cuz = (float)(b.uz / P.c);
+        bool calive = true;
+        halfdrift32(cir, ciz, cfr, cfz, cur, cut, cuz, calive, P, mix32((uint32_t)(id ^ (id >> 32)) ^ 0xA5A5A5A5u ^ (uint32_t)step));
+        if (calive) {
+          int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
+          deposit_values32(P, cir, ciz, cfr, cfz, cur, cut, cuz, a, vr, vz, kk);
+          deposit_direct(a, vr, vz, P);
+        } else {
+          atomicAdd(&cnt->lost, 1ull);
+        }
+        S.a[slot] = pack32(cir, ciz, cfr, cfz, cur, calive);
+        S.b[slot] = make_float2(cut, cuz);
+        S.id[slot] = child_id(id, step);
+      } else {
+        atomicAdd(&cnt->cap_overflow, 1ull);
+      }
+    }
+    bool alive = true;
+    halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P, mix32((uint32_t)(id ^ (id >> 32)) ^ (uint32_t)step));
+    if (alive) {
+      int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
+      deposit_values32(P, ir, iz, fr, fz, ur, ut, uz, a, vr, vz, kk);
+      deposit_direct(a, vr, vz, P);
+    } else {
+      atomicAdd(&cnt->lost, 1ull);
+    }
+    S.a[p] = pack32(ir, iz, fr, fz, ur, alive);
+    S.b[p] = make_float2(ut, uz);
+  }
+}
+
 // ------------------------------------------------------------- FDTD
 // H update; the last H update of a step also clears the current (read by
 // the E updates before it), commits the births of the previous particle
-// pass and advances the step index read by the next pass.
+// pass, empties the collision queue and advances the step index.
 template <typename T>
 __global__ void k_sim_h(T *__restrict__ H, const T *__restrict__ Er, const T *__restrict__ Ez,
                         int nr, int nz, double chr, double chz, unsigned long long *Jr,
@@ -520,6 +663,7 @@ __global__ void k_sim_h(T *__restrict__ H, const T *__restrict__ Er, const T *__
     const unsigned long long nt = cnt->n_total + cnt->n_births;
     cnt->n_total = nt < cnt->cap ? nt : cnt->cap;
     cnt->n_births = 0;
+    cnt->n_cand = 0;
     cnt->step += 1;
   }
 }
@@ -529,7 +673,9 @@ __global__ void k_load64(State64 S, const double *r, const double *z, const doub
                          const double *ut, const double *uz, const uint64_t *id, long long n) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
        p += (long long)gridDim.x * blockDim.x) {
-    S.r[p] = r[p]; S.z[p] = z[p]; S.ur[p] = ur[p]; S.ut[p] = ut[p]; S.uz[p] = uz[p];
+    S.rz[p] = make_double2(r[p], z[p]);
+    S.urt[p] = make_double2(ur[p], ut[p]);
+    S.uz[p] = uz[p];
     S.id[p] = id[p];
   }
 }
@@ -546,9 +692,8 @@ __global__ void k_load32(State32 S, const double *r, const double *z, const doub
     if (fz >= 1.f) { fz = 0.f; iz++; }
     if (iz >= nz) { iz = nz - 1; fz = 0.99999994f; }
     const bool alive = r[p] >= 0 && ir < nr && iz >= 0;
-    S.key[p] = alive ? (((uint32_t)iz << 16) | (uint32_t)ir) : kDead;
-    S.fr[p] = fr; S.fz[p] = fz;
-    S.ur[p] = (float)(ur[p] / c); S.ut[p] = (float)(ut[p] / c); S.uz[p] = (float)(uz[p] / c);
+    S.a[p] = pack32(ir, iz, fr, fz, (float)(ur[p] / c), alive);
+    S.b[p] = make_float2((float)(ut[p] / c), (float)(uz[p] / c));
     S.id[p] = id[p];
   }
 }
@@ -557,7 +702,8 @@ __global__ void k_read64(State64 S, double *r, double *z, double *ur, double *ut
                          uint64_t *id, long long n) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
        p += (long long)gridDim.x * blockDim.x) {
-    r[p] = S.r[p]; z[p] = S.z[p]; ur[p] = S.ur[p]; ut[p] = S.ut[p]; uz[p] = S.uz[p];
+    const double2 a = S.rz[p], b = S.urt[p];
+    r[p] = a.x; z[p] = a.y; ur[p] = b.x; ut[p] = b.y; uz[p] = S.uz[p];
     id[p] = S.id[p];
   }
 }
@@ -566,13 +712,14 @@ __global__ void k_read32(State32 S, double *r, double *z, double *ur, double *ut
                          uint64_t *id, long long n, double dr, double dz, double c) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
        p += (long long)gridDim.x * blockDim.x) {
-    const uint32_t key = S.key[p];
-    if (key == kDead) { r[p] = -1.0; z[p] = 0; }
+    const uint4 A = S.a[p];
+    const float2 B = S.b[p];
+    if (A.x == kDead) { r[p] = -1.0; z[p] = 0; }
     else {
-      r[p] = ((double)(key & 0xFFFFu) + (double)S.fr[p]) * dr;
-      z[p] = ((double)(key >> 16) + (double)S.fz[p]) * dz;
+      r[p] = ((double)(A.x & 0xFFFFu) + (double)__uint_as_float(A.y)) * dr;
+      z[p] = ((double)(A.x >> 16) + (double)__uint_as_float(A.z)) * dz;
     }
-    ur[p] = (double)S.ur[p] * c; ut[p] = (double)S.ut[p] * c; uz[p] = (double)S.uz[p] * c;
+    ur[p] = (double)__uint_as_float(A.w) * c; ut[p] = (double)B.x * c; uz[p] = (double)B.y * c;
     id[p] = S.id[p];
   }
 }
@@ -583,15 +730,15 @@ __global__ void k_read32(State32 S, double *r, double *z, double *ur, double *ut
 // on particle ids and the deposit is an exact integer sum).
 __device__ __forceinline__ int cell_of64(const State64 &S, long long p, int nr, int nz,
                                          double dr, double dz) {
-  const double r = S.r[p];
-  if (r < 0) return -1;
-  int ir = (int)floor(r / dr), iz = (int)floor(S.z[p] / dz);
+  const double2 rz = S.rz[p];
+  if (rz.x < 0) return -1;
+  int ir = (int)floor(rz.x / dr), iz = (int)floor(rz.y / dz);
   ir = min(max(ir, 0), nr - 1);
   iz = min(max(iz, 0), nz - 1);
   return ir + iz * nr;
 }
 __device__ __forceinline__ int cell_of32(const State32 &S, long long p, int nr) {
-  const uint32_t k = S.key[p];
+  const uint32_t k = S.a[p].x;
   if (k == kDead) return -1;
   return (int)(k & 0xFFFFu) + (int)(k >> 16) * nr;
 }
@@ -632,13 +779,10 @@ __global__ void k_sort_scatter(State64 A64, State64 B64, State32 A32, State32 B3
     basepos = __shfl_sync(mask, basepos, leader);
     const long long dst = (long long)offset[c] + basepos + __popc(mask & ((1u << lane) - 1));
     if (FORM == 0) {
-      B64.r[dst] = A64.r[p]; B64.z[dst] = A64.z[p];
-      B64.ur[dst] = A64.ur[p]; B64.ut[dst] = A64.ut[p]; B64.uz[dst] = A64.uz[p];
+      B64.rz[dst] = A64.rz[p]; B64.urt[dst] = A64.urt[p]; B64.uz[dst] = A64.uz[p];
       B64.id[dst] = A64.id[p];
     } else {
-      B32.key[dst] = A32.key[p]; B32.fr[dst] = A32.fr[p]; B32.fz[dst] = A32.fz[p];
-      B32.ur[dst] = A32.ur[p]; B32.ut[dst] = A32.ut[p]; B32.uz[dst] = A32.uz[p];
-      B32.id[dst] = A32.id[p];
+      B32.a[dst] = A32.a[p]; B32.b[dst] = A32.b[p]; B32.id[dst] = A32.id[p];
     }
   }
 }
@@ -659,11 +803,15 @@ __global__ void k_diag(State64 S64, State32 S32, SimCounters *cnt, double c, dou
        p += (long long)gridDim.x * blockDim.x) {
     double u2;
     if (FORM == 0) {
-      if (S64.r[p] < 0) continue;
-      u2 = (S64.ur[p] * S64.ur[p] + S64.ut[p] * S64.ut[p] + S64.uz[p] * S64.uz[p]) / (c * c);
+      if (S64.rz[p].x < 0) continue;
+      const double2 a = S64.urt[p];
+      const double w = S64.uz[p];
+      u2 = (a.x * a.x + a.y * a.y + w * w) / (c * c);
     } else {
-      if (S32.key[p] == kDead) continue;
-      const double a = S32.ur[p], b = S32.ut[p], d = S32.uz[p];
+      const uint4 A = S32.a[p];
+      if (A.x == kDead) continue;
+      const float2 B = S32.b[p];
+      const double a = __uint_as_float(A.w), b = B.x, d = B.y;
       u2 = a * a + b * b + d * d;
     }
     const double g = sqrt(1 + u2);
@@ -746,7 +894,8 @@ struct gasatt_sim {
   cudaGraphExec_t g_step[2] = {nullptr, nullptr};
   cudaGraphExec_t g_sort[2] = {nullptr, nullptr};
   double scale = 1.0;
-  unsigned pass_grid = 0;
+  unsigned pass_grid = 0, mcc_grid = 0;
+  int *queue = nullptr;           // collision candidates of the current pass
   bool timing = false;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};   // before FDTD, before pass, after pass
 };
@@ -806,18 +955,25 @@ int launch_fdtd(gasatt_sim *s, cudaStream_t st) {
   return GASATT_OK;
 }
 
+// particle pass; a full pass (mode 0) is followed by the collision kernel
+// that finishes the queued candidates
 int launch_pass(gasatt_sim *s, cudaStream_t st, int mode) {
   SimParams P = s->P;
   const int b = s->cur;
   if (s->form == 0)
     k_pass64<<<s->pass_grid, kBlock, 0, st>>>(P, s->s64[b],
                                               Fields<double>{(double *)s->Er, (double *)s->Ez, (double *)s->H},
-                                              s->cnt, mode);
+                                              s->cnt, s->queue, mode);
   else
     k_pass32<<<s->pass_grid, kBlock, 0, st>>>(P, s->s32[b],
                                               Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H},
-                                              s->cnt, mode);
+                                              s->cnt, s->queue, mode);
   s->ctx->launches++;
+  if (mode == 0) {
+    if (s->form == 0) k_mcc64<<<s->mcc_grid, 128, 0, st>>>(P, s->s64[b], s->cnt, s->queue);
+    else k_mcc32<<<s->mcc_grid, 128, 0, st>>>(P, s->s32[b], s->cnt, s->queue);
+    s->ctx->launches++;
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "particle pass launch");
   return GASATT_OK;
@@ -948,17 +1104,16 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   for (int b = 0; b < 2; ++b) {
     if (s->form == 0) {
       State64 &S = s->s64[b];
-      if ((rc = sim_alloc(s, &S.r, cap)) || (rc = sim_alloc(s, &S.z, cap)) || (rc = sim_alloc(s, &S.ur, cap)) ||
-          (rc = sim_alloc(s, &S.ut, cap)) || (rc = sim_alloc(s, &S.uz, cap)) || (rc = sim_alloc(s, &S.id, cap)))
+      if ((rc = sim_alloc(s, &S.rz, cap)) || (rc = sim_alloc(s, &S.urt, cap)) ||
+          (rc = sim_alloc(s, &S.uz, cap)) || (rc = sim_alloc(s, &S.id, cap)))
         return cleanup(rc);
     } else {
       State32 &S = s->s32[b];
-      if ((rc = sim_alloc(s, &S.key, cap)) || (rc = sim_alloc(s, &S.fr, cap)) || (rc = sim_alloc(s, &S.fz, cap)) ||
-          (rc = sim_alloc(s, &S.ur, cap)) || (rc = sim_alloc(s, &S.ut, cap)) || (rc = sim_alloc(s, &S.uz, cap)) ||
-          (rc = sim_alloc(s, &S.id, cap)))
+      if ((rc = sim_alloc(s, &S.a, cap)) || (rc = sim_alloc(s, &S.b, cap)) || (rc = sim_alloc(s, &S.id, cap)))
         return cleanup(rc);
     }
   }
+  if ((rc = sim_alloc(s, &s->queue, cap))) return cleanup(rc);
   const size_t esz = s->form == 0 ? 8 : 4;
   double *tmpd;
   if ((rc = sim_alloc(s, (char **)&s->Er, (size_t)nr * (nz + 1) * esz)) ||
@@ -1000,7 +1155,15 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   // fixed point: FP64 |q FN v w| * scale <= 2^48; FP32 <= 2^25 (one warp sum fits int32)
   const double qfc = c.q_e * std::fabs(c.FN) * c.c;
   s->scale = s->form == 0 ? std::ldexp(1.0, 48) / qfc : std::ldexp(1.0, 25) / qfc;
-  P.dep = s->form == 0 ? s->scale : -c.q_e * c.FN * c.c * s->scale;
+  P.dep = s->scale;
+  P.depf = (float)(-c.q_e * c.FN * c.c * s->scale);
+  {
+    // largest count of 52-bit draws b with (2b+1) 2^-53 < P_null (exact in double)
+    uint64_t t = (uint64_t)std::floor(P.P_null * 0x1.0p52);
+    while ((2.0 * (double)t + 1.0) * 0x1.0p-53 < P.P_null) ++t;
+    while (t > 0 && !((2.0 * (double)(t - 1) + 1.0) * 0x1.0p-53 < P.P_null)) --t;
+    P.cand_below = t;
+  }
   P.sig = s->d_tab;
   P.cdf = s->d_tab + 3 * c.table_n;
   P.G = c.table_n; P.lnEmin = s->tabs.lnEmin; P.dlnE = s->tabs.dlnE;
@@ -1013,6 +1176,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   if (s->form == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass64, kBlock, 0);
   else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass32, kBlock, 0);
   s->pass_grid = (unsigned)(nsm * (occ > 0 ? occ : 1));
+  s->mcc_grid = (unsigned)nsm;
   // zero state
   SimCounters z{};
   z.step = -1;
@@ -1242,7 +1406,7 @@ int gasatt_sim_step(gasatt_sim *s, int nsteps) {
     SIM_TRY(launch_pass(s, st, 1));
     s->primed = true;
   }
-  const int per_step = 4 * s->cfg.fdtd_ratio + 2;
+  const int per_step = 4 * s->cfg.fdtd_ratio + 3;
   for (int k = 0; k < nsteps; ++k) {
     if (s->cfg.sort_period > 0 && s->since_sort >= s->cfg.sort_period) SIM_TRY(gasatt_sim_sort(s));
     GASATT_CUDA(ctx, cudaGraphLaunch(s->g_step[s->cur], st));
