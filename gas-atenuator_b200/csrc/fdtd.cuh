@@ -84,3 +84,124 @@ __global__ void k_fdtd_e(T *__restrict__ Er, T *__restrict__ Ez, const T *__rest
 }
 
 }  // namespace gasatt
+
+namespace gasatt {
+
+// ---------------------------------------------------------------------------
+// Fused field sub-cycle for the resident simulation: one launch advances the
+// fields by one particle step, H(dt/4), [E(dt/2), H(dt/2)] x (2R - 1), E(dt/2),
+// H(dt/4) (the reference's H(-dt/4) [H(dt/2) E(dt/2)] x 2R H(dt/4) with the
+// first two H updates merged).  Each block loads a 32 x 32 patch = a tile of
+// (32 - 4R - 1)^2 cells plus a halo of 2R cells on the low side and 2R + 1 on
+// the high side (each H update needs E one cell up in r and z, each E update
+// needs H one cell down) into shared memory, runs all sub-updates there, and
+// writes back its tile.  A warp covers one 32-cell row of the patch.  The
+// current it reads (Jr, Jz, fixed point) was deposited by the previous
+// particle pass; the block clears its tile of the other buffer (Jr_next,
+// Jz_next) for the next pass.  Storage in T, arithmetic in double (float
+// arithmetic here costs the FP32 form two orders of magnitude in field
+// accuracy).
+constexpr int kFdtdPatch = 32;
+constexpr int kFdtdRows = 16;                          // blockDim = (32, kFdtdRows)
+
+__host__ __device__ inline int fdtd_tile(int R) { return kFdtdPatch - 4 * R - 1; }
+
+template <typename T>
+__device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ Ez,
+                                           T *__restrict__ H,
+                                           const unsigned long long *__restrict__ Jr,
+                                           const unsigned long long *__restrict__ Jz,
+                                           unsigned long long *__restrict__ Jr_next,
+                                           unsigned long long *__restrict__ Jz_next, int nr,
+                                           int nz, const FdtdCoef &c, const double *__restrict__ invV,
+                                           double mu, double dt, int R, unsigned flags) {
+  constexpr int TW = kFdtdPatch;
+  __shared__ T sEr[TW * TW], sEz[TW * TW], sH[TW * TW], sJr[TW * TW], sJz[TW * TW];
+  const int tile = fdtd_tile(R), hl = 2 * R, hh = 2 * R + 1;
+  const int i0 = blockIdx.x * tile, j0 = blockIdx.y * tile;
+  const int I0 = max(i0 - hl, 0), J0 = max(j0 - hl, 0);
+  const int I1 = min(i0 + tile + hh, nr + 1), J1 = min(j0 + tile + hh, nz + 1);
+  const int W = I1 - I0, Hn = J1 - J0;
+  const int li = threadIdx.x, i = I0 + li;
+  const bool col = li < W;
+  for (int lj = threadIdx.y; lj < Hn; lj += kFdtdRows) {
+    const int j = J0 + lj, s = li + lj * TW;
+    if (!col) continue;
+    if (i < nr && j <= nz) sEr[s] = Er[i + (int64_t)j * nr];
+    if (i <= nr && j < nz) sEz[s] = Ez[i + (int64_t)j * (nr + 1)];
+    if (i < nr && j < nz) {
+      const int64_t g = i + (int64_t)j * nr;
+      sH[s] = H[g];
+      sJr[s] = (T)((double)(long long)Jr[g] * invV[i]);
+      sJz[s] = (T)((double)(long long)Jz[g] * invV[i]);
+    }
+  }
+  __syncthreads();
+  const bool endcopy = (flags & GASATT_Q_ER_END_COPY) != 0;
+  const double dt_eps = c.dt_eps, dt_eps_dz = c.dt_eps_dz, axis = c.axis, inv_dr = 1 / c.dr;
+  const double ri = ((flags & GASATT_Q_EZ_RSHIFT) ? (i + 1) : i) * c.dr;
+  const double ezp = i > 0 ? dt_eps * (1 / (2 * ri) + inv_dr) : 0.0;   // coefficient of H(i)
+  const double ezm = i > 0 ? dt_eps * (1 / (2 * ri) - inv_dr) : 0.0;   // coefficient of H(i-1)
+  const int nsub = 4 * R + 1;
+  for (int sub = 0; sub < nsub; ++sub) {
+    if ((sub & 1) == 0) {                              // H update
+      const double h = (sub == 0 || sub == nsub - 1) ? dt / 4 : dt / 2;
+      const double chr = h / (mu * c.dr), chz = h / (mu * c.dz);
+      if (col && i < nr && i + 1 < I1) {
+        for (int lj = threadIdx.y; lj < Hn; lj += kFdtdRows) {
+          const int j = J0 + lj, s = li + lj * TW;
+          if (j < nz && j + 1 < J1)
+            sH[s] = (T)((double)sH[s] + (chr * ((double)sEz[s + 1] - (double)sEz[s]) -
+                                         chz * ((double)sEr[s + TW] - (double)sEr[s])));
+        }
+      }
+    } else if (col) {                                  // E update (dt/2)
+      for (int lj = threadIdx.y; lj < Hn; lj += kFdtdRows) {
+        const int j = J0 + lj, s = li + lj * TW;
+        if (i < nr) {
+          if (j >= 1 && j < nz) {
+            if (j - 1 >= J0) {
+              const T old = sEr[s];
+              sEr[s] = (T)((double)old - dt_eps * ((double)sJr[s - TW] + (double)sJr[s]) / 2 -
+                           dt_eps_dz * ((double)sH[s] - (double)sH[s - TW]));
+              if (endcopy) {
+                if (j == 1 && J0 == 0) sEr[s - TW] = old;
+                if (j == nz - 1 && J1 == nz + 1) sEr[s + TW] = old;
+              }
+            }
+          } else if (!endcopy && j <= nz) {
+            sEr[s] = (T)0;
+          }
+        }
+        if (j < nz) {
+          if (i == 0) {
+            const double jz0 = (double)sJz[s];
+            const double jterm = (flags & GASATT_Q_EZ_AXIS_JSIGN) ? dt_eps * jz0 : -(dt_eps * jz0);
+            sEz[s] = (T)((double)sEz[s] + jterm + axis * (double)sH[s]);
+          } else if (i < nr && i - 1 >= I0) {
+            sEz[s] = (T)((double)sEz[s] - dt_eps * ((double)sJz[s - 1] + (double)sJz[s]) / 2 +
+                         ezp * (double)sH[s] + ezm * (double)sH[s - 1]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const int ie = min(i0 + tile, nr + 1), je = min(j0 + tile, nz + 1);
+  if (i >= i0 && i < ie) {
+    for (int j = J0 + threadIdx.y; j < je; j += kFdtdRows) {
+      if (j < j0) continue;
+      const int s = li + (j - J0) * TW;
+      if (i < nr && j <= nz) Er[i + (int64_t)j * nr] = sEr[s];
+      if (i <= nr && j < nz) Ez[i + (int64_t)j * (nr + 1)] = sEz[s];
+      if (i < nr && j < nz) {
+        const int64_t g = i + (int64_t)j * nr;
+        H[g] = sH[s];
+        Jr_next[g] = 0;
+        Jz_next[g] = 0;
+      }
+    }
+  }
+}
+
+}  // namespace gasatt

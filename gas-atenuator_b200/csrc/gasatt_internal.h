@@ -64,6 +64,8 @@ struct SimTables {
   int G = 0;
   double lnEmin = 0, dlnE = 0;
   std::vector<double> sig_el, sig_ion, sig_exc, cdf;   // G, G, G, G*181
+  std::vector<double> edep;                            // G: mean excitation loss [eV]
+  double exc_kmin = 0;                                 // lowest excitation threshold [eV]
   double nu_max = 0;
   int n_exc = 0;
   double exc[5][16] = {};   // k, A, omega, nu, gamma

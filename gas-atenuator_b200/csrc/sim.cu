@@ -66,6 +66,8 @@ struct SimParams {
   // tables
   const double *sig;        // 3 x G (el, ion, exc)
   const double *cdf;        // G x 181
+  const double *edep;       // G: mean excitation energy loss [eV]
+  double exc_kmin;          // lowest excitation threshold [eV]
   int G;
   double lnEmin, dlnE;
   int n_exc;
@@ -97,16 +99,30 @@ __device__ __forceinline__ void xs_lookup(const SimParams &P, double Eev, double
   sx = s2[i] + f * (s2[i + 1] - s2[i]);
 }
 
+// Inverse CDF: the largest k in [0, 179] with C[k] <= U, then linear in
+// between (interp1 of the cumtrapz, get_ElasticSc_sub1.m:16-19).  Found in two
+// rounds of independent loads (every 12th entry, then the 12 in the bracket)
+// instead of eight dependent ones; same k as a bisection.
 __device__ __forceinline__ double cdf_theta(const SimParams &P, double L, double U) {
   const double Lr = floor(L + 0.5);
   const int g = Lr < 0 ? 0 : (Lr > P.G - 1 ? P.G - 1 : (int)Lr);
   const double *C = P.cdf + (int64_t)g * 181;
-  int lo = 0, hi = 180;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (C[mid] <= U) lo = mid; else hi = mid;
-  }
-  return (lo + (U - C[lo]) / (C[lo + 1] - C[lo])) * (GASATT_PI / 180);
+  double coarse[15];
+#pragma unroll
+  for (int m = 0; m < 15; ++m) coarse[m] = C[12 * (m + 1)];
+  int seg = 0;                                     // C[12 seg] <= U
+#pragma unroll
+  for (int m = 0; m < 15; ++m) seg += coarse[m] <= U ? 1 : 0;
+  const int base = 12 * seg;
+  double fine[12];
+#pragma unroll
+  for (int m = 0; m < 12; ++m) fine[m] = C[min(base + 1 + m, 180)];
+  int lo = base;
+#pragma unroll
+  for (int m = 0; m < 12; ++m) lo += (base + 1 + m <= 179 && fine[m] <= U) ? 1 : 0;
+  const double c0 = lo == base ? C[base] : fine[lo - base - 1];
+  const double c1 = fine[lo - base];
+  return (lo + (U - c0) / (c1 - c0)) * (GASATT_PI / 180);
 }
 
 __device__ __forceinline__ double u_of_energy(double EJ, double m, double c) {
@@ -175,18 +191,15 @@ __device__ __noinline__ int mcc_event(const SimParams &P, uint64_t id, long long
     return 2;
   }
   if (X < nu_el + nu_io + nu_ex) {
-    double k1 = 0, k2 = 0;
-    for (int i = 0; i < P.n_exc; ++i) {
-      const double k = P.exc[0][i];
-      if (!(Eev > k)) continue;
-      const double a = P.exc[1][i] / (k * k);
-      const double bb = pow(k / Eev, P.exc[2][i]);
-      const double cc = pow(1 - pow(k / Eev, P.exc[4][i]), P.exc[3][i]);
-      k1 = k1 + a * bb * cc * k;
-      k2 = k2 + a * bb * cc;
-    }
-    if (!(k2 > 0)) return 4;
-    const double E_dep = k1 / k2;
+    // tabulated mean energy loss, interpolated like the cross-sections
+    if (!(Eev > P.exc_kmin)) return 4;
+    int i;
+    double f;
+    if (!(L > 0)) { i = 0; f = 0; }
+    else if (L >= P.G - 1) { i = P.G - 2; f = 1; }
+    else { i = (int)L; f = L - i; }
+    const double E_dep = P.edep[i] + f * (P.edep[i + 1] - P.edep[i]);
+    if (!(E_dep > 0) || !(E_dep < Eev)) return 4;
     const double up = u_of_energy((Eev - E_dep) * qe, me, c);
     ux = ux / um * up; uy = uy / um * up; uz = uz / um * up;
     return 3;
@@ -212,40 +225,88 @@ __device__ __forceinline__ void queue_push(bool want, long long p, SimCounters *
   if (want) queue[base + __popc(m & ((1u << lane) - 1))] = (int)p;
 }
 
-// ------------------------------------------------------ warp deposit
-// Sum of v over the lanes of `mask` (all lanes of the group call it).
-__device__ __forceinline__ long long group_sum_i64(unsigned mask, long long v) {
-  const unsigned lo = (unsigned)(v & ((1ll << 26) - 1));
-  const int hi = (int)(v >> 26);
-  const unsigned slo = __reduce_add_sync(mask, lo);
-  const int shi = __reduce_add_sync(mask, hi);
-  return ((long long)shi << 26) + (long long)slo;
+// ------------------------------------------------------ deposit
+// Two-level reduction of the per-particle fixed-point contributions (4 nodes x
+// 2 components).  (1) A warp sums runs of consecutive lanes with the same node
+// quad by a segmented shuffle scan (fixed cost whatever the run pattern).
+// (2) The last lane of each run adds the sums into a shared-memory window of
+// whole grid rows held by the block; nodes outside the window go straight to
+// global memory.  (3) The block adds its window to the grid with one 64-bit
+// atomic per touched node.  All sums are integer, so the result is exact and
+// independent of order.
+constexpr int kWinNodes = 2048;      // window capacity (nodes) per component
+
+struct DepWindow {
+  unsigned long long *r, *z;          // shared memory, kWinNodes each
+  int row0, rows, nr;                 // window = grid rows [row0, row0 + rows)
+};
+
+__device__ __forceinline__ void win_add(const DepWindow &w, unsigned long long *J,
+                                        unsigned long long *wJ, int64_t node, long long v) {
+  if (!v) return;
+  const int row = (int)(node / w.nr);
+  if (row >= w.row0 && row < w.row0 + w.rows)
+    atomicAdd(wJ + (node - (int64_t)w.row0 * w.nr), (unsigned long long)v);
+  else
+    atomicAdd(J + node, (unsigned long long)v);
 }
 
-// 4 nodes x 2 components, grouped by node key; the lowest lane of each group
-// issues the atomics.  Must be reached by all 32 lanes of the warp.
+// segmented inclusive scan over runs of equal keys; VT = int (FP32 form,
+// |value| <= 2^25 so a 32-lane sum fits) or long long (FP64 form)
+template <typename VT>
 __device__ __forceinline__ void warp_deposit(bool act, unsigned key, const int64_t a[4],
                                              const long long vr[4], const long long vz[4],
                                              unsigned long long *Jr, unsigned long long *Jz,
-                                             bool wide) {
-  const unsigned live = __ballot_sync(0xFFFFFFFFu, act);
-  if (!act) return;
-  const unsigned mask = __match_any_sync(live, key);
-  const bool leader = (__ffs(mask) - 1) == (int)(threadIdx.x & 31);
+                                             const DepWindow &w) {
+  const int lane = threadIdx.x & 31;
+  const unsigned k = act ? key : (0xFFFFFFFFu - (unsigned)lane);
+  const unsigned pk = __shfl_up_sync(0xFFFFFFFFu, k, 1);
+  const bool head = lane == 0 || pk != k;
+  const unsigned hm = __ballot_sync(0xFFFFFFFFu, head);
+  const int rid = __popc(hm & (0xFFFFFFFFu >> (31 - lane)));
+  VT v[8];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    long long sr, sz;
-    if (wide) {
-      sr = group_sum_i64(mask, vr[k]);
-      sz = group_sum_i64(mask, vz[k]);
-    } else {
-      sr = __reduce_add_sync(mask, (int)vr[k]);
-      sz = __reduce_add_sync(mask, (int)vz[k]);
+  for (int q = 0; q < 4; ++q) { v[q] = (VT)vr[q]; v[4 + q] = (VT)vz[q]; }
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int rd = __shfl_up_sync(0xFFFFFFFFu, rid, d);
+    const bool same = lane >= d && rd == rid;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const VT t = __shfl_up_sync(0xFFFFFFFFu, v[q], d);
+      v[q] += same ? t : (VT)0;
     }
-    if (leader) {
-      if (sr) atomicAdd(Jr + a[k], (unsigned long long)sr);
-      if (sz) atomicAdd(Jz + a[k], (unsigned long long)sz);
+  }
+  const bool tail = lane == 31 || ((hm >> (lane + 1)) & 1u);
+  if (act && tail) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      win_add(w, Jr, w.r, a[q], (long long)v[q]);
+      win_add(w, Jz, w.z, a[q], (long long)v[4 + q]);
     }
+  }
+}
+
+// block setup of the window: rows from `lead_row` - 2 on; zeroed
+__device__ __forceinline__ DepWindow win_open(unsigned long long *smem, int lead_row, int nr,
+                                              int nz) {
+  DepWindow w;
+  w.r = smem;
+  w.z = smem + kWinNodes;
+  w.nr = nr;
+  w.rows = min(kWinNodes / nr, nz);
+  w.row0 = max(0, min(lead_row - 2, nz - w.rows));
+  for (int i = threadIdx.x; i < 2 * kWinNodes; i += blockDim.x) smem[i] = 0;
+  return w;
+}
+
+__device__ __forceinline__ void win_flush(const DepWindow &w, unsigned long long *Jr,
+                                          unsigned long long *Jz) {
+  const int n = w.rows * w.nr;
+  const int64_t off = (int64_t)w.row0 * w.nr;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (w.r[i]) atomicAdd(Jr + off + i, w.r[i]);
+    if (w.z[i]) atomicAdd(Jz + off + i, w.z[i]);
   }
 }
 
@@ -298,15 +359,25 @@ __device__ __forceinline__ void deposit_values64(const SimParams &P, double r, d
 // + half drift only, ending at integer time (end of a run)
 __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fields<double> F,
                                                       SimCounters *cnt, int *queue, int mode) {
+  __shared__ unsigned long long wmem[2 * kWinNodes];
+  __shared__ int lead_row;
   const long long n0 = (long long)cnt->n_total;
   const long long step = cnt->step;
   const int lane = threadIdx.x & 31;
-  const long long stride = (long long)gridDim.x * blockDim.x;
+  // each block takes a contiguous chunk of the (cell-sorted) particles
+  const long long chunk = (n0 + gridDim.x - 1) / gridDim.x;
+  const long long beg = (long long)blockIdx.x * chunk, end = min(beg + chunk, n0);
+  if (threadIdx.x == 0) {
+    const double2 rz = beg < end ? S.rz[beg] : make_double2(-1.0, 0.0);
+    lead_row = rz.x >= 0 ? (int)floor(rz.y / P.dz - 0.5) : 0;
+  }
+  __syncthreads();
+  const DepWindow win = win_open(wmem, lead_row, P.nr, P.nz);
+  __syncthreads();
   unsigned lost = 0;
-  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n0;
-       base += stride) {
+  for (long long base = beg + (threadIdx.x & ~31); base < end; base += blockDim.x) {
     const long long p = base + lane;
-    bool act = p < n0;
+    bool act = p < end;
     double2 rz = make_double2(-1.0, 0.0), urt = make_double2(0.0, 0.0);
     double uz = 0;
     if (act) {
@@ -337,10 +408,12 @@ __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fi
     long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
     unsigned key = 0;
     if (act) deposit_values64(P, rz.x, rz.y, urt.x, urt.y, uz, a, vr, vz, key);
-    warp_deposit(act, key, a, vr, vz, P.Jr, P.Jz, true);
+    warp_deposit<long long>(act, key, a, vr, vz, P.Jr, P.Jz, win);
   }
   lost = __reduce_add_sync(0xFFFFFFFFu, lost);
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
+  __syncthreads();
+  win_flush(win, P.Jr, P.Jz);
 }
 
 // collision candidates of this step: MCC, births, second half drift, deposit
@@ -521,15 +594,25 @@ __device__ __forceinline__ uint4 pack32(int ir, int iz, float fr, float fz, floa
 
 __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fields<float> F,
                                                       SimCounters *cnt, int *queue, int mode) {
+  __shared__ unsigned long long wmem[2 * kWinNodes];
+  __shared__ int lead_row;
   const long long n0 = (long long)cnt->n_total;
   const long long step = cnt->step;
   const int lane = threadIdx.x & 31;
-  const long long stride = (long long)gridDim.x * blockDim.x;
+  // each block takes a contiguous chunk of the (cell-sorted) particles
+  const long long chunk = (n0 + gridDim.x - 1) / gridDim.x;
+  const long long beg = (long long)blockIdx.x * chunk, end = min(beg + chunk, n0);
+  if (threadIdx.x == 0) {
+    const uint4 A0 = beg < end ? S.a[beg] : make_uint4(kDead, 0, 0, 0);
+    lead_row = A0.x != kDead ? (int)(A0.x >> 16) - (__uint_as_float(A0.z) >= 0.5f ? 0 : 1) : 0;
+  }
+  __syncthreads();
+  const DepWindow win = win_open(wmem, lead_row, P.nr, P.nz);
+  __syncthreads();
   unsigned lost = 0;
-  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n0;
-       base += stride) {
+  for (long long base = beg + (threadIdx.x & ~31); base < end; base += blockDim.x) {
     const long long p = base + lane;
-    bool act = p < n0;
+    bool act = p < end;
     uint4 A = make_uint4(kDead, 0, 0, 0);
     if (act) {
       A = S.a[p];
@@ -582,10 +665,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
     long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
     unsigned dkey = 0;
     if (act) deposit_values32(P, ir, iz, fr, fz, ur, ut, uz, a, vr, vz, dkey);
-    warp_deposit(act, dkey, a, vr, vz, P.Jr, P.Jz, false);
+    warp_deposit<int>(act, dkey, a, vr, vz, P.Jr, P.Jz, win);
   }
   lost = __reduce_add_sync(0xFFFFFFFFu, lost);
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
+  __syncthreads();
+  win_flush(win, P.Jr, P.Jz);
 }
 
 __global__ void __launch_bounds__(128) k_mcc32(SimParams P, State32 S, SimCounters *cnt,
@@ -643,29 +728,25 @@ __global__ void __launch_bounds__(128) k_mcc32(SimParams P, State32 S, SimCounte
 }
 
 // ------------------------------------------------------------- FDTD
-// H update; the last H update of a step also clears the current (read by
-// the E updates before it), commits the births of the previous particle
-// pass, empties the collision queue and advances the step index.
+// One fused field sub-cycle per step (fdtd_tiled).  Block (0,0) also commits
+// the births of the previous particle pass, empties the collision queue and
+// advances the step index; no other block of this kernel reads them.
 template <typename T>
-__global__ void k_sim_h(T *__restrict__ H, const T *__restrict__ Er, const T *__restrict__ Ez,
-                        int nr, int nz, double chr, double chz, unsigned long long *Jr,
-                        unsigned long long *Jz, SimCounters *cnt) {
-  const int64_t n = (int64_t)nr * nz;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int i = (int)(idx % nr), j = (int)(idx / nr);
-    const int64_t ez = i + (int64_t)j * (nr + 1);
-    H[idx] = (T)((double)H[idx] + (chr * ((double)Ez[ez + 1] - (double)Ez[ez]) -
-                                   chz * ((double)Er[idx + nr] - (double)Er[idx])));
-    if (Jr) { Jr[idx] = 0; Jz[idx] = 0; }
-  }
-  if (cnt && blockIdx.x == 0 && threadIdx.x == 0) {
+__global__ void __launch_bounds__(32 * kFdtdRows) k_sim_fdtd(T *Er, T *Ez, T *H, const unsigned long long *Jr,
+                                                  const unsigned long long *Jz,
+                                                  unsigned long long *Jr_next,
+                                                  unsigned long long *Jz_next, int nr, int nz,
+                                                  FdtdCoef c, const double *invV, double mu,
+                                                  double dt, int R, unsigned flags,
+                                                  SimCounters *cnt) {
+  if (cnt && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
     const unsigned long long nt = cnt->n_total + cnt->n_births;
     cnt->n_total = nt < cnt->cap ? nt : cnt->cap;
     cnt->n_births = 0;
     cnt->n_cand = 0;
     cnt->step += 1;
   }
+  fdtd_tiled<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, c, invV, mu, dt, R, flags);
 }
 
 // ---------------------------------------------------------- load/read
@@ -728,19 +809,24 @@ __global__ void k_read32(State32 S, double *r, double *z, double *ur, double *ut
 // Counting sort by cell (z-major), dropping dead slots.  Order inside a cell
 // is arbitrary; nothing downstream depends on it (random streams are keyed
 // on particle ids and the deposit is an exact integer sum).
+// sort key: the deposit node quad (ar, az) = cell shifted by half a cell, so
+// that lanes of a warp share their four deposit nodes right after a sort;
+// (nr + 1) x (nz + 1) bins
 __device__ __forceinline__ int cell_of64(const State64 &S, long long p, int nr, int nz,
                                          double dr, double dz) {
   const double2 rz = S.rz[p];
   if (rz.x < 0) return -1;
-  int ir = (int)floor(rz.x / dr), iz = (int)floor(rz.y / dz);
-  ir = min(max(ir, 0), nr - 1);
-  iz = min(max(iz, 0), nz - 1);
-  return ir + iz * nr;
+  int ar = (int)floor(rz.x / dr - 0.5) + 1, az = (int)floor(rz.y / dz - 0.5) + 1;
+  ar = min(max(ar, 0), nr);
+  az = min(max(az, 0), nz);
+  return ar + az * (nr + 1);
 }
 __device__ __forceinline__ int cell_of32(const State32 &S, long long p, int nr) {
-  const uint32_t k = S.a[p].x;
-  if (k == kDead) return -1;
-  return (int)(k & 0xFFFFu) + (int)(k >> 16) * nr;
+  const uint4 A = S.a[p];
+  if (A.x == kDead) return -1;
+  const int ar = (int)(A.x & 0xFFFFu) + (__uint_as_float(A.y) >= 0.5f ? 1 : 0);
+  const int az = (int)(A.x >> 16) + (__uint_as_float(A.z) >= 0.5f ? 1 : 0);
+  return ar + az * (nr + 1);
 }
 
 template <int FORM>
@@ -878,8 +964,11 @@ struct gasatt_sim {
   State32 s32[2]{};
   int cur = 0;
   void *Er = nullptr, *Ez = nullptr, *H = nullptr;
-  unsigned long long *Jr = nullptr, *Jz = nullptr;
+  // current accumulators, double-buffered: the field update of step s reads
+  // buffer s & 1 and clears the other one, which the pass of step s fills
+  unsigned long long *Jr[2] = {nullptr, nullptr}, *Jz[2] = {nullptr, nullptr};
   double *d_tab = nullptr;
+  double *invV = nullptr;         // per column: 2^-S / shell volume
   SimCounters *cnt = nullptr;
   SimCounters *h_cnt = nullptr;   // pinned
   int *cell_count = nullptr, *cell_offset = nullptr, *cell_cursor = nullptr;
@@ -891,13 +980,13 @@ struct gasatt_sim {
   bool primed = false;
   int64_t host_step = 0;          // particle passes completed
   int64_t since_sort = 0;
-  cudaGraphExec_t g_step[2] = {nullptr, nullptr};
+  cudaGraphExec_t g_step[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [state buffer][step parity]
   cudaGraphExec_t g_sort[2] = {nullptr, nullptr};
   double scale = 1.0;
   unsigned pass_grid = 0, mcc_grid = 0;
   int *queue = nullptr;           // collision candidates of the current pass
   bool timing = false;
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};   // before FDTD, before pass, after pass
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // before FDTD, pass, collision kernel, end
 };
 
 namespace {
@@ -912,44 +1001,36 @@ int sim_alloc(gasatt_sim *s, T **p, size_t n) {
 
 #define SIM_TRY(x) do { int rc__ = (x); if (rc__) return rc__; } while (0)
 
-int launch_fdtd(gasatt_sim *s, cudaStream_t st) {
+FdtdCoef fdtd_coef(const gasatt_sim *s) {
   const auto &c = s->cfg;
-  const int nr = c.n_r, nz = c.n_z, R = c.fdtd_ratio;
-  const double dt = c.dt / R, mu = c.mu0, eps = c.eps0;
+  const double dt = c.dt / c.fdtd_ratio, eps = c.eps0;
   FdtdCoef fc;
   fc.dr = c.dr; fc.dz = c.dz; fc.PHIp = c.PHIp; fc.inv_scale = 1.0 / s->scale;
   fc.dt_eps = (dt / 2) / eps;
   fc.dt_eps_dz = (dt / 2) / (eps * c.dz);
   fc.axis = 4 * (dt / 2) / (eps * c.dr);
-  const unsigned gh = grid_for((int64_t)nr * nz, kBlock), ge = grid_for((int64_t)(nr + 1) * (nz + 1), kBlock);
-  auto H = [&](double h, bool last) {
-    if (s->form == 0)
-      k_sim_h<double><<<gh, kBlock, 0, st>>>((double *)s->H, (const double *)s->Er, (const double *)s->Ez,
-                                            nr, nz, h / (mu * c.dr), h / (mu * c.dz),
-                                            last ? s->Jr : nullptr, last ? s->Jz : nullptr,
-                                            last ? s->cnt : nullptr);
-    else
-      k_sim_h<float><<<gh, kBlock, 0, st>>>((float *)s->H, (const float *)s->Er, (const float *)s->Ez,
-                                           nr, nz, h / (mu * c.dr), h / (mu * c.dz),
-                                           last ? s->Jr : nullptr, last ? s->Jz : nullptr,
-                                           last ? s->cnt : nullptr);
-    s->ctx->launches++;
-  };
-  auto E = [&]() {
-    if (s->form == 0)
-      k_fdtd_e<double><<<ge, kBlock, 0, st>>>((double *)s->Er, (double *)s->Ez, (const double *)s->H,
-                                             s->Jr, s->Jz, nr, nz, fc, c.flags);
-    else
-      k_fdtd_e<float><<<ge, kBlock, 0, st>>>((float *)s->Er, (float *)s->Ez, (const float *)s->H,
-                                            s->Jr, s->Jz, nr, nz, fc, c.flags);
-    s->ctx->launches++;
-  };
-  // H(-dt/4) + H(dt/2) of the reference sequence merged into H(dt/4)
-  H(dt / 4, false);
-  for (int i = 0; i < 2 * R; ++i) {
-    E();
-    H(i == 2 * R - 1 ? dt / 4 : dt / 2, i == 2 * R - 1);
-  }
+  fc.chr = fc.chz = 0;
+  return fc;
+}
+
+// field sub-cycle of step with parity q: reads current buffer q, clears 1 - q
+int launch_fdtd(gasatt_sim *s, cudaStream_t st, int q) {
+  const auto &c = s->cfg;
+  const int nr = c.n_r, nz = c.n_z, R = c.fdtd_ratio;
+  const FdtdCoef fc = fdtd_coef(s);
+  const int tile = fdtd_tile(R);
+  const dim3 grid((nr + 1 + tile - 1) / tile, (nz + 1 + tile - 1) / tile);
+  const dim3 block(32, kFdtdRows);
+  const double dt = c.dt / R;
+  if (s->form == 0)
+    k_sim_fdtd<double><<<grid, block, 0, st>>>(
+        (double *)s->Er, (double *)s->Ez, (double *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
+        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt);
+  else
+    k_sim_fdtd<float><<<grid, block, 0, st>>>(
+        (float *)s->Er, (float *)s->Ez, (float *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
+        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt);
+  s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "fdtd launch");
   return GASATT_OK;
@@ -957,8 +1038,10 @@ int launch_fdtd(gasatt_sim *s, cudaStream_t st) {
 
 // particle pass; a full pass (mode 0) is followed by the collision kernel
 // that finishes the queued candidates
-int launch_pass(gasatt_sim *s, cudaStream_t st, int mode) {
+int launch_pass(gasatt_sim *s, cudaStream_t st, int mode, int jb, cudaEvent_t mid = nullptr) {
   SimParams P = s->P;
+  P.Jr = s->Jr[jb];
+  P.Jz = s->Jz[jb];
   const int b = s->cur;
   if (s->form == 0)
     k_pass64<<<s->pass_grid, kBlock, 0, st>>>(P, s->s64[b],
@@ -969,6 +1052,10 @@ int launch_pass(gasatt_sim *s, cudaStream_t st, int mode) {
                                               Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H},
                                               s->cnt, s->queue, mode);
   s->ctx->launches++;
+  if (mid) {
+    cudaError_t e = cudaEventRecordWithFlags(mid, st, cudaEventRecordExternal);
+    if (e != cudaSuccess) return cuda_fail(s->ctx, e, "event");
+  }
   if (mode == 0) {
     if (s->form == 0) k_mcc64<<<s->mcc_grid, 128, 0, st>>>(P, s->s64[b], s->cnt, s->queue);
     else k_mcc32<<<s->mcc_grid, 128, 0, st>>>(P, s->s32[b], s->cnt, s->queue);
@@ -982,7 +1069,7 @@ int launch_pass(gasatt_sim *s, cudaStream_t st, int mode) {
 // sort from buffer `from` into 1 - from
 int launch_sort(gasatt_sim *s, cudaStream_t st, int from) {
   const auto &c = s->cfg;
-  const int ncell = c.n_r * c.n_z;
+  const int ncell = (c.n_r + 1) * (c.n_z + 1);    // sort bins
   GASATT_CUDA(s->ctx, cudaMemsetAsync(s->cell_count, 0, (size_t)(ncell + 1) * 4, st));
   GASATT_CUDA(s->ctx, cudaMemsetAsync(s->cell_cursor, 0, (size_t)ncell * 4, st));
   const unsigned g = s->pass_grid;
@@ -1010,9 +1097,12 @@ int launch_sort(gasatt_sim *s, cudaStream_t st, int from) {
 
 void drop_graphs(gasatt_sim *s) {
   for (int i = 0; i < 2; ++i) {
-    if (s->g_step[i]) cudaGraphExecDestroy(s->g_step[i]);
+    for (int q = 0; q < 2; ++q) {
+      if (s->g_step[i][q]) cudaGraphExecDestroy(s->g_step[i][q]);
+      s->g_step[i][q] = nullptr;
+    }
     if (s->g_sort[i]) cudaGraphExecDestroy(s->g_sort[i]);
-    s->g_step[i] = s->g_sort[i] = nullptr;
+    s->g_sort[i] = nullptr;
   }
 }
 
@@ -1025,20 +1115,22 @@ int build_graphs(gasatt_sim *s) {
   for (int b = 0; b < 2; ++b) {
     cudaGraph_t g;
     s->cur = b;
+    for (int q = 0; q < 2; ++q) {
+      GASATT_CUDA(s->ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      if (s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[0], cs, cudaEventRecordExternal));
+      int rc = launch_fdtd(s, cs, q);
+      if (!rc && s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[1], cs, cudaEventRecordExternal));
+      if (!rc) rc = launch_pass(s, cs, 0, 1 - q, s->timing ? s->ev[2] : nullptr);
+      if (!rc && s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[3], cs, cudaEventRecordExternal));
+      cudaError_t e = cudaStreamEndCapture(cs, &g);
+      if (rc) return rc;
+      if (e != cudaSuccess) return cuda_fail(s->ctx, e, "capture step");
+      GASATT_CUDA(s->ctx, cudaGraphInstantiate(&s->g_step[b][q], g, 0));
+      cudaGraphDestroy(g);
+    }
     GASATT_CUDA(s->ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    if (s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[0], cs, cudaEventRecordExternal));
-    int rc = launch_fdtd(s, cs);
-    if (!rc && s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[1], cs, cudaEventRecordExternal));
-    if (!rc) rc = launch_pass(s, cs, 0);
-    if (!rc && s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[2], cs, cudaEventRecordExternal));
+    int rc = launch_sort(s, cs, b);
     cudaError_t e = cudaStreamEndCapture(cs, &g);
-    if (rc) return rc;
-    if (e != cudaSuccess) return cuda_fail(s->ctx, e, "capture step");
-    GASATT_CUDA(s->ctx, cudaGraphInstantiate(&s->g_step[b], g, 0));
-    cudaGraphDestroy(g);
-    GASATT_CUDA(s->ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    rc = launch_sort(s, cs, b);
-    e = cudaStreamEndCapture(cs, &g);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_fail(s->ctx, e, "capture sort");
     GASATT_CUDA(s->ctx, cudaGraphInstantiate(&s->g_sort[b], g, 0));
@@ -1099,7 +1191,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
                             c.m_e, c.q_e, s->tabs, err);
   if (rc) { delete s; return fail(ctx, rc, err); }
   const int64_t cap = c.capacity;
-  const int nr = c.n_r, nz = c.n_z, ncell = nr * nz;
+  const int nr = c.n_r, nz = c.n_z, ncell = nr * nz, nbin = (nr + 1) * (nz + 1);
   auto cleanup = [&](int code) { gasatt_sim_destroy(s); return code; };
   for (int b = 0; b < 2; ++b) {
     if (s->form == 0) {
@@ -1119,25 +1211,28 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   if ((rc = sim_alloc(s, (char **)&s->Er, (size_t)nr * (nz + 1) * esz)) ||
       (rc = sim_alloc(s, (char **)&s->Ez, (size_t)(nr + 1) * nz * esz)) ||
       (rc = sim_alloc(s, (char **)&s->H, (size_t)nr * nz * esz)) ||
-      (rc = sim_alloc(s, &s->Jr, (size_t)ncell)) || (rc = sim_alloc(s, &s->Jz, (size_t)ncell)) ||
-      (rc = sim_alloc(s, &s->cnt, 1)) || (rc = sim_alloc(s, &s->cell_count, (size_t)ncell + 1)) ||
-      (rc = sim_alloc(s, &s->cell_offset, (size_t)ncell + 1)) ||
-      (rc = sim_alloc(s, &s->cell_cursor, (size_t)ncell)) ||
-      (rc = sim_alloc(s, &tmpd, (size_t)3 * c.table_n + (size_t)181 * c.table_n)))
+      (rc = sim_alloc(s, &s->Jr[0], (size_t)ncell)) || (rc = sim_alloc(s, &s->Jz[0], (size_t)ncell)) ||
+      (rc = sim_alloc(s, &s->Jr[1], (size_t)ncell)) || (rc = sim_alloc(s, &s->Jz[1], (size_t)ncell)) ||
+      (rc = sim_alloc(s, &s->cnt, 1)) || (rc = sim_alloc(s, &s->cell_count, (size_t)nbin + 1)) ||
+      (rc = sim_alloc(s, &s->cell_offset, (size_t)nbin + 1)) ||
+      (rc = sim_alloc(s, &s->cell_cursor, (size_t)nbin)) ||
+      (rc = sim_alloc(s, &tmpd, (size_t)4 * c.table_n + (size_t)181 * c.table_n)))
     return cleanup(rc);
   s->d_tab = tmpd;
-  cub::DeviceScan::ExclusiveSum(nullptr, s->scan_bytes, s->cell_count, s->cell_offset, ncell + 1);
+  if ((rc = sim_alloc(s, &s->invV, (size_t)nr))) return cleanup(rc);
+  cub::DeviceScan::ExclusiveSum(nullptr, s->scan_bytes, s->cell_count, s->cell_offset, nbin + 1);
   if ((rc = sim_alloc(s, (char **)&s->scan_tmp, s->scan_bytes))) return cleanup(rc);
   s->partial_blocks = 296;
   if ((rc = sim_alloc(s, &s->partial, (size_t)2 * s->partial_blocks))) return cleanup(rc);
   if (cudaMallocHost((void **)&s->h_cnt, sizeof(SimCounters)) != cudaSuccess)
     return cleanup(fail(ctx, GASATT_E_CUDA, "cudaMallocHost"));
   // tables
-  std::vector<double> host((size_t)3 * c.table_n + (size_t)181 * c.table_n);
+  std::vector<double> host((size_t)4 * c.table_n + (size_t)181 * c.table_n);
   std::memcpy(host.data(), s->tabs.sig_el.data(), c.table_n * 8);
   std::memcpy(host.data() + c.table_n, s->tabs.sig_ion.data(), c.table_n * 8);
   std::memcpy(host.data() + 2 * c.table_n, s->tabs.sig_exc.data(), c.table_n * 8);
-  std::memcpy(host.data() + 3 * c.table_n, s->tabs.cdf.data(), (size_t)181 * c.table_n * 8);
+  std::memcpy(host.data() + 3 * c.table_n, s->tabs.edep.data(), c.table_n * 8);
+  std::memcpy(host.data() + 4 * c.table_n, s->tabs.cdf.data(), (size_t)181 * c.table_n * 8);
   if (cudaMemcpy(s->d_tab, host.data(), host.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
     return cleanup(fail(ctx, GASATT_E_CUDA, "table upload"));
   // parameters
@@ -1165,11 +1260,21 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
     P.cand_below = t;
   }
   P.sig = s->d_tab;
-  P.cdf = s->d_tab + 3 * c.table_n;
+  P.edep = s->d_tab + 3 * c.table_n;
+  P.cdf = s->d_tab + 4 * c.table_n;
+  P.exc_kmin = s->tabs.exc_kmin;
   P.G = c.table_n; P.lnEmin = s->tabs.lnEmin; P.dlnE = s->tabs.dlnE;
   P.n_exc = s->tabs.n_exc;
   std::memcpy(P.exc, s->tabs.exc, sizeof(P.exc));
-  P.Jr = s->Jr; P.Jz = s->Jz;
+  P.Jr = s->Jr[0]; P.Jz = s->Jz[0];
+  {
+    std::vector<double> iv(nr);
+    for (int i = 0; i < nr; ++i) iv[i] = (1.0 / s->scale) / shell_volume(i, c.dr, c.dz, c.PHIp);
+    if (cudaMemcpy(s->invV, iv.data(), (size_t)nr * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+      return cleanup(fail(ctx, GASATT_E_CUDA, "volume table upload"));
+  }
+  if (fdtd_tile(c.fdtd_ratio) < 4)
+    return cleanup(fail(ctx, GASATT_E_ARG, "fdtd_ratio too large for the fused field update (max 6)"));
   int dev = ctx->device, nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   int occ = 4;
@@ -1186,9 +1291,11 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   cudaMemset(s->Er, 0, (size_t)nr * (nz + 1) * esz);
   cudaMemset(s->Ez, 0, (size_t)(nr + 1) * nz * esz);
   cudaMemset(s->H, 0, (size_t)nr * nz * esz);
-  cudaMemset(s->Jr, 0, (size_t)ncell * 8);
-  cudaMemset(s->Jz, 0, (size_t)ncell * 8);
-  for (int i = 0; i < 3; ++i)
+  for (int q = 0; q < 2; ++q) {
+    cudaMemset(s->Jr[q], 0, (size_t)ncell * 8);
+    cudaMemset(s->Jz[q], 0, (size_t)ncell * 8);
+  }
+  for (int i = 0; i < 4; ++i)
     if (cudaEventCreate(&s->ev[i]) != cudaSuccess) return cleanup(fail(ctx, GASATT_E_CUDA, "event"));
   rc = build_graphs(s);
   if (rc) return cleanup(rc);
@@ -1202,7 +1309,7 @@ int gasatt_sim_destroy(gasatt_sim *s) {
   cudaSetDevice(s->ctx->device);
   cudaDeviceSynchronize();
   drop_graphs(s);
-  for (int i = 0; i < 3; ++i)
+  for (int i = 0; i < 4; ++i)
     if (s->ev[i]) cudaEventDestroy(s->ev[i]);
   for (void *p : s->allocs) cudaFree(p);
   if (s->h_cnt) cudaFreeHost(s->h_cnt);
@@ -1248,8 +1355,10 @@ int gasatt_sim_load(gasatt_sim *s, const double *r, const double *z, const doubl
   zc.step = -1;
   zc.cap = (unsigned long long)s->cfg.capacity;
   GASATT_CUDA(ctx, cudaMemcpyAsync(s->cnt, &zc, sizeof(zc), cudaMemcpyHostToDevice, st));
-  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
-  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+  for (int q = 0; q < 2; ++q) {
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+  }
   GASATT_CUDA(ctx, cudaStreamSynchronize(st));
   s->primed = false;
   s->host_step = 0;
@@ -1370,7 +1479,8 @@ int gasatt_sim_get_current(gasatt_sim *s, double *jr, double *jz, int on_device)
     if (rc) return rc;
     d[0] = (double *)buf; d[1] = (double *)buf + n;
   }
-  const unsigned long long *J[2] = {s->Jr, s->Jz};
+  const int q = (int)(s->host_step & 1);   // buffer of the most recent deposit
+  const unsigned long long *J[2] = {s->Jr[q], s->Jz[q]};
   for (int f = 0; f < 2; ++f) {
     k_j_to_density<<<grid_for(n, kBlock), kBlock, 0, st>>>(J[f], nr, nz, 1.0 / s->scale, s->cfg.dr,
                                                            s->cfg.dz, s->cfg.PHIp, d[f]);
@@ -1403,13 +1513,13 @@ int gasatt_sim_step(gasatt_sim *s, int nsteps) {
   if (!s->primed) {
     // start of a run: particles at x^0 move to x^{1/2} and deposit j^{1/2}
     if (s->cfg.sort_period > 0) SIM_TRY(gasatt_sim_sort(s));
-    SIM_TRY(launch_pass(s, st, 1));
+    SIM_TRY(launch_pass(s, st, 1, 0));
     s->primed = true;
   }
-  const int per_step = 4 * s->cfg.fdtd_ratio + 3;
+  const int per_step = 3;   // field update, particle pass, collision kernel
   for (int k = 0; k < nsteps; ++k) {
     if (s->cfg.sort_period > 0 && s->since_sort >= s->cfg.sort_period) SIM_TRY(gasatt_sim_sort(s));
-    GASATT_CUDA(ctx, cudaGraphLaunch(s->g_step[s->cur], st));
+    GASATT_CUDA(ctx, cudaGraphLaunch(s->g_step[s->cur][s->host_step & 1], st));
     ctx->launches += per_step;
     s->host_step++;
     s->since_sort++;
@@ -1478,15 +1588,17 @@ int gasatt_sim_enable_timing(gasatt_sim *s, int enable) {
   return build_graphs(s);
 }
 
-int gasatt_sim_last_timing(gasatt_sim *s, float *fdtd_ms, float *pass_ms) {
+int gasatt_sim_last_timing(gasatt_sim *s, float *fdtd_ms, float *pass_ms, float *mcc_ms) {
   if (!s) return GASATT_E_ARG;
   if (!s->timing) return fail(s->ctx, GASATT_E_STATE, "timing not enabled");
-  GASATT_CUDA(s->ctx, cudaEventSynchronize(s->ev[2]));
-  float a = 0, b = 0;
+  GASATT_CUDA(s->ctx, cudaEventSynchronize(s->ev[3]));
+  float a = 0, b = 0, m = 0;
   GASATT_CUDA(s->ctx, cudaEventElapsedTime(&a, s->ev[0], s->ev[1]));
   GASATT_CUDA(s->ctx, cudaEventElapsedTime(&b, s->ev[1], s->ev[2]));
+  GASATT_CUDA(s->ctx, cudaEventElapsedTime(&m, s->ev[2], s->ev[3]));
   if (fdtd_ms) *fdtd_ms = a;
   if (pass_ms) *pass_ms = b;
+  if (mcc_ms) *mcc_ms = m;
   return GASATT_OK;
 }
 
@@ -1564,14 +1676,17 @@ int gasatt_sim_run_host(gasatt_sim *s, double *pos, double *vel, int64_t *n_io, 
   h.n_total = (unsigned long long)n;
   h.n_births = 0;
   GASATT_CUDA(ctx, cudaMemcpyAsync(s->cnt, &h, sizeof(h), cudaMemcpyHostToDevice, st));
-  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
-  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+  for (int q = 0; q < 2; ++q) {
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+  }
   s->primed = false;
+  s->host_step = 0;                          // the prologue deposits into buffer 0
   s->since_sort = s->cfg.sort_period;       // sort the fresh population first
   SIM_TRY(gasatt_sim_step(s, nsteps - 1));
   // last step: fields, then a push that ends at integer time
-  SIM_TRY(launch_fdtd(s, st));
-  SIM_TRY(launch_pass(s, st, 2));
+  SIM_TRY(launch_fdtd(s, st, (int)(s->host_step & 1)));
+  SIM_TRY(launch_pass(s, st, 2, (int)((s->host_step + 1) & 1)));
   SIM_TRY(gasatt_sim_sort(s));               // compacts away the dead
   s->host_step++;
   s->primed = false;

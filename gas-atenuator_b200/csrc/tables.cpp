@@ -8,6 +8,7 @@
 //    log-spaced energies, per-energy normalised elastic CDFs (the
 //    get_ElasticSc_sub1.m recipe: log DCS linear in log E, PDF = 2 pi sin
 //    theta DCS, trapezoid CDF), and the FP64 null-collision bound.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include "gasatt_internal.h"
@@ -131,6 +132,7 @@ int build_sim_tables(const gasatt_tables *t, int G, double emin_ev, double emax_
   o.lnEmin = std::log(emin_ev);
   o.dlnE = (std::log(emax_ev) - o.lnEmin) / (G - 1);
   o.sig_el.assign(G, 0.0); o.sig_ion.assign(G, 0.0); o.sig_exc.assign(G, 0.0);
+  o.edep.assign(G, 0.0);
   o.cdf.assign((size_t)G * 181, 0.0);
   std::vector<double> Eg(G);
   for (int g = 0; g < G; ++g) {
@@ -180,6 +182,25 @@ int build_sim_tables(const gasatt_tables *t, int G, double emin_ev, double emax_
     if (sg * vg > vmax) vmax = sg * vg;
   }
   o.nu_max = n_gas * vmax;
+  // mean excitation energy loss sum_j k_j s_j / sum_j s_j over the terms above
+  // threshold (electron_transport.cu:207-219, get_ImpExc2.m; q0 cancels)
+  o.exc_kmin = 1e300;
+  for (int i = 0; i < t->n_exc; ++i) o.exc_kmin = std::min(o.exc_kmin, t->t_exc[i]);
+  for (int g = 0; g < G; ++g) {
+    const double T = Eg[g];
+    double k1 = 0, k2 = 0;
+    for (int i = 0; i < t->n_exc; ++i) {
+      const double k = t->t_exc[i], A = t->t_exc[t->n_exc + i], om = t->t_exc[2 * t->n_exc + i];
+      const double nu = t->t_exc[3 * t->n_exc + i], ga = t->t_exc[4 * t->n_exc + i];
+      if (!(T > k)) continue;
+      const double a = A / (k * k);
+      const double b = std::pow(k / T, om);
+      const double cc = std::pow(1 - std::pow(k / T, ga), nu);
+      k1 = k1 + a * b * cc * k;
+      k2 = k2 + a * b * cc;
+    }
+    o.edep[g] = k2 > 0 ? k1 / k2 : 0.0;
+  }
   o.n_exc = t->n_exc;
   for (int j = 0; j < 5; ++j)
     for (int i = 0; i < t->n_exc; ++i) o.exc[j][i] = t->t_exc[j * t->n_exc + i];

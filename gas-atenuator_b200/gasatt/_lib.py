@@ -7,7 +7,8 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), "libgasatt.so")
+# GASATT_LIB may point at another build of the same library (e.g. a debug build)
+LIB_PATH = os.environ.get("GASATT_LIB") or os.path.join(os.path.dirname(_HERE), "libgasatt.so")
 
 c_p = ctypes.c_void_p
 c_i64 = ctypes.c_int64
@@ -101,6 +102,7 @@ _SIGS = {
                                 ctypes.POINTER(c_i64)]),
     "gasatt_sim_enable_timing": (c_i, [c_p, c_i]),
     "gasatt_sim_last_timing": (c_i, [c_p, ctypes.POINTER(ctypes.c_float),
+                                     ctypes.POINTER(ctypes.c_float),
                                      ctypes.POINTER(ctypes.c_float)]),
 }
 

@@ -282,10 +282,10 @@ int gasatt_sim_run_host(gasatt_sim *sim, double *pos, double *vel,
 int gasatt_sim_counts(gasatt_sim *sim, int64_t *n_slots, int64_t *n_ionizations,
                       int64_t *n_lost);
 /* device-side phase timing: with timing enabled the step graphs record CUDA
- * events around the field sub-cycle and the particle pass; last_timing gives
- * the durations of the most recent step (milliseconds) */
+ * events around the field sub-cycle, the particle pass and the collision
+ * kernel; last_timing gives their durations in the most recent step (ms) */
 int gasatt_sim_enable_timing(gasatt_sim *sim, int enable);
-int gasatt_sim_last_timing(gasatt_sim *sim, float *fdtd_ms, float *pass_ms);
+int gasatt_sim_last_timing(gasatt_sim *sim, float *fdtd_ms, float *pass_ms, float *mcc_ms);
 
 #ifdef __cplusplus
 }

@@ -889,7 +889,23 @@ static double cdf_theta(const orc_xs *xs, double L, double U) {
   return (lo + (U - C[lo]) / (C[lo + 1] - C[lo])) * (GASATT_PI / 180);
 }
 
-static double exc_loss_sim(const orc_xs *xs, double T, int *ok) {
+/* mean excitation energy loss (electron_transport.cu:207-219, get_ImpExc2.m)
+ * tabulated on the grid at build time and interpolated like the
+ * cross-sections; *ok = 0 below the lowest threshold or for a loss outside
+ * (0, T) */
+static double exc_loss_sim(const orc_xs *xs, double T, double L, int *ok) {
+  *ok = 0;
+  if (!(T > xs->exc_kmin)) return 0;
+  int i; double f;
+  if (!(L > 0)) { i = 0; f = 0; }
+  else if (L >= xs->G - 1) { i = xs->G - 2; f = 1; }
+  else { i = (int)L; f = L - i; }
+  double e = xs->edep[i] + f * (xs->edep[i + 1] - xs->edep[i]);
+  *ok = (e > 0) && (e < T);
+  return e;
+}
+
+static double exc_loss_exact(const orc_xs *xs, double T) {
   double k1 = 0, k2 = 0;
   for (int i = 0; i < xs->n_exc; ++i) {
     double k = xs->exc_k[i];
@@ -900,8 +916,7 @@ static double exc_loss_sim(const orc_xs *xs, double T, int *ok) {
     k1 = k1 + a * b * c * k;
     k2 = k2 + a * b * c;
   }
-  *ok = k2 > 0;
-  return k1 / k2;
+  return k2 > 0 ? k1 / k2 : 0.0;
 }
 
 /* u magnitude for kinetic energy E [J]: c sqrt(eps (2 + eps)), eps = E / (m c^2) */
@@ -1059,7 +1074,7 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
             }
           } else if (X < nu_el + nu_io + nu_ex) {
             int ok;
-            double E_dep = exc_loss_sim(xs, Eev, &ok);
+            double E_dep = exc_loss_sim(xs, Eev, L, &ok);
             if (ok) {
               double up = u_of_energy((Eev - E_dep) * qe, me, c);
               ux[p] = ux[p] / um * up; uy[p] = uy[p] / um * up; uz[p] = uz[p] / um * up;
@@ -1158,6 +1173,7 @@ orc_xs *orc_xs_create(const gasatt_tables *t, int G, double emin_ev, double emax
   xs->sig_ion = (double *)malloc((size_t)G * sizeof(double));
   xs->sig_exc = (double *)malloc((size_t)G * sizeof(double));
   xs->cdf = (double *)malloc((size_t)G * 181 * sizeof(double));
+  xs->edep = (double *)malloc((size_t)G * sizeof(double));
   if (xs_fill(t, G, emin_ev, emax_ev, n_gas, c, me, qe, xs->sig_el, xs->sig_ion, xs->sig_exc,
               xs->cdf, &xs->nu_max) != 0) {
     orc_xs_free(xs);
@@ -1171,12 +1187,16 @@ orc_xs *orc_xs_create(const gasatt_tables *t, int G, double emin_ev, double emax
     xs->exc_nu[i] = t->t_exc[3 * t->n_exc + i];
     xs->exc_ga[i] = t->t_exc[4 * t->n_exc + i];
   }
+  xs->exc_kmin = 1e300;
+  for (int i = 0; i < t->n_exc; ++i)
+    if (xs->exc_k[i] < xs->exc_kmin) xs->exc_kmin = xs->exc_k[i];
+  for (int g = 0; g < G; ++g) xs->edep[g] = exc_loss_exact(xs, exp(xs->lnEmin + g * xs->dlnE));
   return xs;
 }
 
 void orc_xs_free(orc_xs *xs) {
   if (!xs) return;
-  free(xs->sig_el); free(xs->sig_ion); free(xs->sig_exc); free(xs->cdf); free(xs);
+  free(xs->sig_el); free(xs->sig_ion); free(xs->sig_exc); free(xs->cdf); free(xs->edep); free(xs);
 }
 
 double orc_xs_nu_max(const orc_xs *xs) { return xs->nu_max; }
@@ -1185,6 +1205,7 @@ const double *orc_xs_array(const orc_xs *xs, int which) {
     case 0: return xs->sig_el;
     case 1: return xs->sig_ion;
     case 2: return xs->sig_exc;
+    case 4: return xs->edep;
     default: return xs->cdf;
   }
 }

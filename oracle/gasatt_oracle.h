@@ -99,6 +99,8 @@ typedef struct orc_xs {
   int G;  double lnEmin, dlnE;        /* log grid */
   double *sig_el, *sig_ion, *sig_exc; /* [G], m^2 */
   double *cdf;                        /* [G*181] normalised elastic CDF */
+  double *edep;                       /* [G] mean excitation energy loss [eV] */
+  double exc_kmin;                    /* lowest excitation threshold [eV] */
   double nu_max;                      /* s^-1, FP64 bound */
   double exc_k[16], exc_A[16], exc_om[16], exc_nu[16], exc_ga[16]; int n_exc;
 } orc_xs;
@@ -106,7 +108,7 @@ orc_xs *orc_xs_create(const gasatt_tables *t, int G, double emin_ev, double emax
                       double n_gas, double c, double me, double qe);
 void orc_xs_free(orc_xs *xs);
 double orc_xs_nu_max(const orc_xs *xs);
-/* 0 sig_el, 1 sig_ion, 2 sig_exc (length G), 3 cdf (G x 181) */
+/* 0 sig_el, 1 sig_ion, 2 sig_exc, 4 edep (length G), 3 cdf (G x 181) */
 const double *orc_xs_array(const orc_xs *xs, int which);
 
 typedef struct orc_counters {

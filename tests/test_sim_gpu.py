@@ -123,3 +123,56 @@ def test_capacity_overflow_is_reported():
     d = sim.diag()
     assert d["n_total"] <= 4100
     assert d["status_flags"] & 2
+
+
+def test_fp64_matches_oracle_multi_window(tables):
+    """A grid large enough for several deposit windows and field tiles per
+    direction (64 x 256 cells), 20,000 electrons, three steps."""
+    cfg = config(64, 256, 5e-6, 1e-14, 300.0, precision=_lib.FP64, capacity=60000, seed=11,
+                 sort_period=2)
+    r, z, ur, ut, uz, ids = births(10000, 8.0, 256 * 5e-6, seed=5, sigma_r=60e-6, Rp=64 * 5e-6)
+    Er, Ez, H = grid_fields(64, 256, np.random.default_rng(2), E0=3e6, H0=2e3)
+    Er[:, 0] = 0; Er[:, -1] = 0; Ez[-1, :] = 0
+    sim = Sim(cfg)
+    sim.load(r, z, ur, ut, uz, ids)
+    sim.set_fields(Er, Ez, H)
+    sim.step(3)
+    orc = oracle_run(cfg, tables, (r, z, ur, ut, uz, ids), (Er, Ez, H), 3)
+    got = sim.read()
+    rr, zz, urr, utt, uzz, oid, alive = orc.state_rz()
+    a = alive.astype(bool)
+    ga = got["r"] >= 0
+    assert set(got["id"][ga].tolist()) == set(oid[a].tolist())
+    want = by_id(oid[a], rr[a], zz[a], urr[a], utt[a], uzz[a])
+    have = by_id(got["id"][ga], got["r"][ga], got["z"][ga], got["ur"][ga], got["ut"][ga], got["uz"][ga])
+    for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
+        close(h, w, 1e-10, k)
+    jr, jz = sim.current()
+    close(jr, orc.jr, 1e-10, "jr"); close(jz, orc.jz, 1e-10, "jz")
+    f = sim.fields()
+    for g, w, k in zip(f, (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
+        close(g, w, 1e-10, k)
+    d = sim.diag()
+    assert (d["n_ionizations"], d["n_elastic"], d["n_excitation"]) == tuple(orc.counters[:3])
+
+
+@pytest.mark.parametrize("precision", [_lib.FP64, _lib.FP32_SPLIT])
+@pytest.mark.parametrize("sort_period", [0, 3])
+def test_births_conserved(precision, sort_period):
+    """Every ionization appends exactly one secondary (secondaries=1): over many
+    steps, one at a time and in bursts, the alive count equals the loaded count
+    plus the ionizations minus the wall losses, the state agrees with it, and
+    no id repeats; without sorting no slot is ever reused."""
+    cfg, sim, parts, _ = start(precision, n_photo=4000, sort_period=sort_period, torr=600.0)
+    n0 = len(parts[0])
+    for burst in (1, 1, 1, 2, 5, 1, 10, 1, 20):
+        sim.step(burst)
+        d = sim.diag()
+        got = sim.read()
+        alive = got["r"] >= 0
+        assert d["n_alive"] == n0 + d["n_ionizations"] - d["n_lost_wall"]
+        assert int(alive.sum()) == d["n_alive"]
+        if sort_period == 0:
+            assert d["n_total"] == n0 + d["n_ionizations"]
+        assert len(np.unique(got["id"][alive])) == int(alive.sum())
+    assert d["n_ionizations"] > 50
