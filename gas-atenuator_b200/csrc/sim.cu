@@ -18,8 +18,12 @@
 //
 // Deposit: each particle's four node contributions (q FN v w) are rounded to
 // integers first, so the grid sum is exact and independent of order; lanes of
-// a warp that hit the same four nodes (__match_any_sync on the node key) are
-// summed with __reduce_add_sync before one 64-bit atomic per node.
+// a warp that hit the same four nodes (equal sort key) are summed with
+// __reduce_add_sync before one 64-bit atomic per node.
+//
+// The FP32 form drifts a particle that is not a collision candidate by the
+// whole step at once (the two half drifts of the reference joined); a
+// candidate stops at integer time and the collision kernel finishes it.
 #include <cub/device/device_scan.cuh>
 #include <cmath>
 #include <cstring>
@@ -226,97 +230,66 @@ __device__ __forceinline__ void queue_push(bool want, long long p, SimCounters *
 }
 
 // ------------------------------------------------------ deposit
-// Two-level reduction of the per-particle fixed-point contributions (4 nodes x
-// 2 components).  (1) A warp sums runs of consecutive lanes with the same node
-// quad by a segmented shuffle scan (fixed cost whatever the run pattern).
-// (2) The last lane of each run adds the sums into a shared-memory window of
-// whole grid rows held by the block; nodes outside the window go straight to
-// global memory.  (3) The block adds its window to the grid with one 64-bit
-// atomic per touched node.  All sums are integer, so the result is exact and
-// independent of order.
-constexpr int kWinNodes = 2048;      // window capacity (nodes) per component
+// Each particle's four node contributions (q FN v w, both components) are
+// integers, so every summation order gives the same grid.  The lanes of a warp
+// that share a node quad (the sort key; the quad fixes the four node indices)
+// are summed with redux.sync, one quad per round, and the first lane of the
+// quad adds the eight sums with 64-bit atomics.  Sorted particles put one to
+// three quads in a warp; after kDepRounds rounds the lanes left add their own
+// contributions.
+constexpr int kDepRounds = 4;
 
-struct DepWindow {
-  unsigned long long *r, *z;          // shared memory, kWinNodes each
-  int row0, rows, nr;                 // window = grid rows [row0, row0 + rows)
-};
-
-__device__ __forceinline__ void win_add(const DepWindow &w, unsigned long long *J,
-                                        unsigned long long *wJ, int64_t node, long long v) {
-  if (!v) return;
-  const int row = (int)(node / w.nr);
-  if (row >= w.row0 && row < w.row0 + w.rows)
-    atomicAdd(wJ + (node - (int64_t)w.row0 * w.nr), (unsigned long long)v);
-  else
-    atomicAdd(J + node, (unsigned long long)v);
+// warp-wide sum of an FP32-form contribution (|v| <= 2^25: 32 lanes fit int32)
+__device__ __forceinline__ long long warp_sum(int v) {
+  return (long long)__reduce_add_sync(0xFFFFFFFFu, v);
+}
+// FP64-form contribution, |v| <= 2^48, summed as hi 2^24 + lo with lo in
+// [0, 2^24): both 32-lane partial sums fit int32, the recombination is exact
+__device__ __forceinline__ long long warp_sum(long long v) {
+  const int lo = (int)(v & 0xFFFFFFLL), hi = (int)(v >> 24);
+  const long long slo = __reduce_add_sync(0xFFFFFFFFu, lo);
+  const long long shi = __reduce_add_sync(0xFFFFFFFFu, hi);
+  return shi * (1LL << 24) + slo;
 }
 
-// segmented inclusive scan over runs of equal keys; VT = int (FP32 form,
-// |value| <= 2^25 so a 32-lane sum fits) or long long (FP64 form)
 template <typename VT>
-__device__ __forceinline__ void warp_deposit(bool act, unsigned key, const int64_t a[4],
-                                             const long long vr[4], const long long vz[4],
-                                             unsigned long long *Jr, unsigned long long *Jz,
-                                             const DepWindow &w) {
-  const int lane = threadIdx.x & 31;
-  const unsigned k = act ? key : (0xFFFFFFFFu - (unsigned)lane);
-  const unsigned pk = __shfl_up_sync(0xFFFFFFFFu, k, 1);
-  const bool head = lane == 0 || pk != k;
-  const unsigned hm = __ballot_sync(0xFFFFFFFFu, head);
-  const int rid = __popc(hm & (0xFFFFFFFFu >> (31 - lane)));
-  VT v[8];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) { v[q] = (VT)vr[q]; v[4 + q] = (VT)vz[q]; }
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const int rd = __shfl_up_sync(0xFFFFFFFFu, rid, d);
-    const bool same = lane >= d && rd == rid;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const VT t = __shfl_up_sync(0xFFFFFFFFu, v[q], d);
-      v[q] += same ? t : (VT)0;
-    }
-  }
-  const bool tail = lane == 31 || ((hm >> (lane + 1)) & 1u);
-  if (act && tail) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      win_add(w, Jr, w.r, a[q], (long long)v[q]);
-      win_add(w, Jz, w.z, a[q], (long long)v[4 + q]);
-    }
-  }
-}
-
-// block setup of the window: rows from `lead_row` - 2 on; zeroed
-__device__ __forceinline__ DepWindow win_open(unsigned long long *smem, int lead_row, int nr,
-                                              int nz) {
-  DepWindow w;
-  w.r = smem;
-  w.z = smem + kWinNodes;
-  w.nr = nr;
-  w.rows = min(kWinNodes / nr, nz);
-  w.row0 = max(0, min(lead_row - 2, nz - w.rows));
-  for (int i = threadIdx.x; i < 2 * kWinNodes; i += blockDim.x) smem[i] = 0;
-  return w;
-}
-
-__device__ __forceinline__ void win_flush(const DepWindow &w, unsigned long long *Jr,
-                                          unsigned long long *Jz) {
-  const int n = w.rows * w.nr;
-  const int64_t off = (int64_t)w.row0 * w.nr;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    if (w.r[i]) atomicAdd(Jr + off + i, w.r[i]);
-    if (w.z[i]) atomicAdd(Jz + off + i, w.z[i]);
-  }
-}
-
-__device__ __forceinline__ void deposit_direct(const int64_t a[4], const long long vr[4],
-                                               const long long vz[4], const SimParams &P) {
+__device__ __forceinline__ void deposit_atomic(const int64_t a[4], const VT vr[4],
+                                               const VT vz[4], unsigned long long *Jr,
+                                               unsigned long long *Jz) {
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    if (vr[k]) atomicAdd(P.Jr + a[k], (unsigned long long)vr[k]);
-    if (vz[k]) atomicAdd(P.Jz + a[k], (unsigned long long)vz[k]);
+    if (vr[k]) atomicAdd(Jr + a[k], (unsigned long long)(long long)vr[k]);
+    if (vz[k]) atomicAdd(Jz + a[k], (unsigned long long)(long long)vz[k]);
   }
+}
+
+template <typename VT>
+__device__ __forceinline__ void warp_deposit(bool act, unsigned key, const int64_t a[4],
+                                             const VT vr[4], const VT vz[4],
+                                             unsigned long long *Jr, unsigned long long *Jz) {
+  const int lane = threadIdx.x & 31;
+  unsigned pending = __ballot_sync(0xFFFFFFFFu, act);
+#pragma unroll 1
+  for (int round = 0; round < kDepRounds && pending; ++round) {
+    const int leader = __ffs(pending) - 1;
+    const unsigned lk = __shfl_sync(0xFFFFFFFFu, key, leader);
+    const bool mine = act && key == lk;
+    pending &= ~__ballot_sync(0xFFFFFFFFu, mine);
+    long long sr[4], sz[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      sr[q] = warp_sum(mine ? vr[q] : (VT)0);
+      sz[q] = warp_sum(mine ? vz[q] : (VT)0);
+    }
+    if (lane == leader) deposit_atomic<long long>(a, sr, sz, Jr, Jz);
+  }
+  if ((pending >> lane) & 1u) deposit_atomic<VT>(a, vr, vz, Jr, Jz);
+}
+
+template <typename VT>
+__device__ __forceinline__ void deposit_direct(const int64_t a[4], const VT vr[4],
+                                               const VT vz[4], const SimParams &P) {
+  deposit_atomic<VT>(a, vr, vz, P.Jr, P.Jz);
 }
 
 // ----------------------------------------------------------- FP64 form
@@ -359,21 +332,13 @@ __device__ __forceinline__ void deposit_values64(const SimParams &P, double r, d
 // + half drift only, ending at integer time (end of a run)
 __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fields<double> F,
                                                       SimCounters *cnt, int *queue, int mode) {
-  __shared__ unsigned long long wmem[2 * kWinNodes];
-  __shared__ int lead_row;
   const long long n0 = (long long)cnt->n_total;
   const long long step = cnt->step;
   const int lane = threadIdx.x & 31;
-  // each block takes a contiguous chunk of the (cell-sorted) particles
+  // each block takes a contiguous chunk of the (cell-sorted) particles, so its
+  // field reads stay in a narrow band of grid rows
   const long long chunk = (n0 + gridDim.x - 1) / gridDim.x;
   const long long beg = (long long)blockIdx.x * chunk, end = min(beg + chunk, n0);
-  if (threadIdx.x == 0) {
-    const double2 rz = beg < end ? S.rz[beg] : make_double2(-1.0, 0.0);
-    lead_row = rz.x >= 0 ? (int)floor(rz.y / P.dz - 0.5) : 0;
-  }
-  __syncthreads();
-  const DepWindow win = win_open(wmem, lead_row, P.nr, P.nz);
-  __syncthreads();
   unsigned lost = 0;
   for (long long base = beg + (threadIdx.x & ~31); base < end; base += blockDim.x) {
     const long long p = base + lane;
@@ -408,12 +373,10 @@ __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fi
     long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
     unsigned key = 0;
     if (act) deposit_values64(P, rz.x, rz.y, urt.x, urt.y, uz, a, vr, vz, key);
-    warp_deposit<long long>(act, key, a, vr, vz, P.Jr, P.Jz, win);
+    warp_deposit<long long>(act, key, a, vr, vz, P.Jr, P.Jz);
   }
   lost = __reduce_add_sync(0xFFFFFFFFu, lost);
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
-  __syncthreads();
-  win_flush(win, P.Jr, P.Jz);
 }
 
 // collision candidates of this step: MCC, births, second half drift, deposit
@@ -529,16 +492,21 @@ __device__ __forceinline__ void reflect_z(int &iz, float &fz, float &uz, int nz)
   }
 }
 
-// Half drift in cell units.  The new radius comes from the exact difference
-// r' - rc = (dx (2 rc + dx) + dy^2) / (r' + rc) (no cancellation at large rc);
-// (u_r, u_theta) turn by the drift angle a, written with the small
-// quantities sin a and 1 - cos a = sin^2 a / (1 + cos a) and added to u with
-// stochastic rounding (rb: two 16-bit random numbers).
-__device__ __forceinline__ void halfdrift32(int &ir, int &iz, float &fr, float &fz, float &ur,
-                                            float &ut, float &uz, bool &alive,
-                                            const SimParams &P, uint32_t rb) {
+// Straight-line drift in cell units over (hr, hz) cells per unit beta:
+// (P.hdr, P.hdz) is a half step, twice that a full step.  Two half drifts at
+// the same velocity are one full drift: the Cartesian path is the same line,
+// the radius along a line is convex (a particle inside the wall at both ends
+// is inside at the midpoint), and the end reflection is specular.  The new
+// radius comes from the exact difference r' - rc = (dx (2 rc + dx) + dy^2) /
+// (r' + rc) (no cancellation at large rc); (u_r, u_theta) turn by the drift
+// angle a, written with the small quantities sin a and 1 - cos a = sin^2 a /
+// (1 + cos a) and added to u with stochastic rounding (rb: two 16-bit random
+// numbers).
+__device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, float &ur,
+                                        float &ut, float &uz, bool &alive, const SimParams &P,
+                                        uint32_t rb, float hr, float hz) {
   const float ig = rsqrt_nr(fmaf(ur, ur, fmaf(ut, ut, fmaf(uz, uz, 1.0f))));
-  const float dx = ur * ig * P.hdr, dy = ut * ig * P.hdr, dzz = uz * ig * P.hdz;
+  const float dx = ur * ig * hr, dy = ut * ig * hr, dzz = uz * ig * hz;
   const float rc = (float)ir + fr;
   const float X = rc + dx;
   const float r2 = fmaf(X, X, dy * dy);
@@ -566,7 +534,7 @@ __device__ __forceinline__ void halfdrift32(int &ir, int &iz, float &fr, float &
 
 __device__ __forceinline__ void deposit_values32(const SimParams &P, int ir, int iz, float fr,
                                                  float fz, float ur, float ut, float uz,
-                                                 int64_t a[4], long long vr[4], long long vz[4],
+                                                 int64_t a[4], int vr[4], int vz[4],
                                                  unsigned &key) {
   const float ig = rsqrt_nr(fmaf(ur, ur, fmaf(ut, ut, fmaf(uz, uz, 1.0f))));
   int ar, az;
@@ -594,21 +562,13 @@ __device__ __forceinline__ uint4 pack32(int ir, int iz, float fr, float fz, floa
 
 __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fields<float> F,
                                                       SimCounters *cnt, int *queue, int mode) {
-  __shared__ unsigned long long wmem[2 * kWinNodes];
-  __shared__ int lead_row;
   const long long n0 = (long long)cnt->n_total;
   const long long step = cnt->step;
   const int lane = threadIdx.x & 31;
-  // each block takes a contiguous chunk of the (cell-sorted) particles
+  // each block takes a contiguous chunk of the (cell-sorted) particles, so its
+  // field reads stay in a narrow band of grid rows
   const long long chunk = (n0 + gridDim.x - 1) / gridDim.x;
   const long long beg = (long long)blockIdx.x * chunk, end = min(beg + chunk, n0);
-  if (threadIdx.x == 0) {
-    const uint4 A0 = beg < end ? S.a[beg] : make_uint4(kDead, 0, 0, 0);
-    lead_row = A0.x != kDead ? (int)(A0.x >> 16) - (__uint_as_float(A0.z) >= 0.5f ? 0 : 1) : 0;
-  }
-  __syncthreads();
-  const DepWindow win = win_open(wmem, lead_row, P.nr, P.nz);
-  __syncthreads();
   unsigned lost = 0;
   for (long long base = beg + (threadIdx.x & ~31); base < end; base += blockDim.x) {
     const long long p = base + lane;
@@ -630,9 +590,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
       const uint64_t id = S.id[p];
       uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
       philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
-      const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]), rb2 = mix32(c[2] ^ (c[3] * 0x9E3779B9u));
+      const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]);
       bool alive = true;
-      if (mode != 1) {
+      if (mode == 1) {
+        drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, P.hdr, P.hdz);
+      } else {
         int ar, az;
         float wr, wz;
         half_shift(ir, fr, ar, wr);
@@ -650,11 +612,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
         const float upr = fmaf(-umz, t, umr), upz = fmaf(umr, t, umz);
         ur = sround_add(ur, fmaf(-upz, s, 2.f * her), rb0);
         uz = sround_add(uz, fmaf(upr, s, 2.f * hez), rb0 >> 16);
-        halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1);
-        if (alive && mode == 0)
-          cand = (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
+        // a collision candidate stops at integer time (k_mcc32 finishes it);
+        // the others drift the whole step
+        const bool c0 = mode == 0 && (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
+        const float h = (mode == 0 && !c0) ? 2.f : 1.f;
+        drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, h * P.hdr, h * P.hdz);
+        cand = alive && c0;
       }
-      if (alive && mode != 2 && !cand) halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb2);
       if (!alive) lost++;
       S.a[p] = pack32(ir, iz, fr, fz, ur, alive);
       S.b[p] = make_float2(ut, uz);
@@ -662,15 +626,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
     }
     queue_push(cand, p, cnt, queue);
     int64_t a[4] = {0, 0, 0, 0};
-    long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
+    int vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
     unsigned dkey = 0;
     if (act) deposit_values32(P, ir, iz, fr, fz, ur, ut, uz, a, vr, vz, dkey);
-    warp_deposit<int>(act, dkey, a, vr, vz, P.Jr, P.Jz, win);
+    warp_deposit<int>(act, dkey, a, vr, vz, P.Jr, P.Jz);
   }
   lost = __reduce_add_sync(0xFFFFFFFFu, lost);
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
-  __syncthreads();
-  win_flush(win, P.Jr, P.Jz);
 }
 
 __global__ void __launch_bounds__(128) k_mcc32(SimParams P, State32 S, SimCounters *cnt,
@@ -698,9 +660,10 @@ __global__ void __launch_bounds__(128) k_mcc32(SimParams P, State32 S, SimCounte
         float cfr = fr, cfz = fz;
         float cur = (float)(b.ux / P.c), cut = (float)(b.uy / P.c), cuz = (float)(b.uz / P.c);
         bool calive = true;
-        halfdrift32(cir, ciz, cfr, cfz, cur, cut, cuz, calive, P, mix32((uint32_t)(id ^ (id >> 32)) ^ 0xA5A5A5A5u ^ (uint32_t)step));
+        drift32(cir, ciz, cfr, cfz, cur, cut, cuz, calive, P,
+                mix32((uint32_t)(id ^ (id >> 32)) ^ 0xA5A5A5A5u ^ (uint32_t)step), P.hdr, P.hdz);
         if (calive) {
-          int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
+          int64_t a[4]; int vr[4], vz[4]; unsigned kk;
           deposit_values32(P, cir, ciz, cfr, cfz, cur, cut, cuz, a, vr, vz, kk);
           deposit_direct(a, vr, vz, P);
         } else {
@@ -714,9 +677,10 @@ __global__ void __launch_bounds__(128) k_mcc32(SimParams P, State32 S, SimCounte
       }
     }
     bool alive = true;
-    halfdrift32(ir, iz, fr, fz, ur, ut, uz, alive, P, mix32((uint32_t)(id ^ (id >> 32)) ^ (uint32_t)step));
+    drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, mix32((uint32_t)(id ^ (id >> 32)) ^ (uint32_t)step),
+            P.hdr, P.hdz);
     if (alive) {
-      int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
+      int64_t a[4]; int vr[4], vz[4]; unsigned kk;
       deposit_values32(P, ir, iz, fr, fz, ur, ut, uz, a, vr, vz, kk);
       deposit_direct(a, vr, vz, P);
     } else {
