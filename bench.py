@@ -126,34 +126,42 @@ def counts(sim):
     return a.value, b.value, c.value
 
 
-def timed_run(sim, steps, warmup, torch, flush, dist_barrier):
+def timed_run(sim, steps, warmup, torch, flush, dist_barrier, phase_steps=50):
+    """K steps enqueued back to back, each preceded by an L2 flush (outside
+    its event pair); the host synchronises once at the end.  A second, short
+    loop with the library's per-kernel events on gives the field / pass /
+    collision split (those events add graph nodes, so they stay out of the
+    headline loop)."""
     from gasatt._lib import lib
-    lib.gasatt_sim_enable_timing(sim.h, 1)
     stream = torch.cuda.current_stream()
     for _ in range(warmup):
         sim.step(1)
     torch.cuda.synchronize()
     d0 = sim.diag()
     l0 = sim.ctx.launches
-    fd = ctypes.c_float(); ps = ctypes.c_float(); mc = ctypes.c_float()
-    step_ms, pass_ms, fdtd_ms, mcc_ms = [], [], [], []
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
     dist_barrier()
     torch.cuda.synchronize()
-    for _ in range(steps):
+    for e0, e1 in evs:
         flush()                                      # L2 cold before every timed step
         e0.record(stream)
         sim.step(1)
         e1.record(stream)
-        e1.synchronize()
-        step_ms.append(e0.elapsed_time(e1))
-        lib.gasatt_sim_last_timing(sim.h, ctypes.byref(fd), ctypes.byref(ps), ctypes.byref(mc))
-        fdtd_ms.append(fd.value); pass_ms.append(ps.value); mcc_ms.append(mc.value)
     torch.cuda.synchronize()
     dist_barrier()
     launches = sim.ctx.launches - l0
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in evs]
     d1 = sim.diag()
+    fd = ctypes.c_float(); ps = ctypes.c_float(); mc = ctypes.c_float()
+    pass_ms, fdtd_ms, mcc_ms = [], [], []
+    lib.gasatt_sim_enable_timing(sim.h, 1)
+    for _ in range(phase_steps):
+        flush()
+        sim.step(1)
+        torch.cuda.synchronize()
+        lib.gasatt_sim_last_timing(sim.h, ctypes.byref(fd), ctypes.byref(ps), ctypes.byref(mc))
+        fdtd_ms.append(fd.value); pass_ms.append(ps.value); mcc_ms.append(mc.value)
     lib.gasatt_sim_enable_timing(sim.h, 0)
     return dict(step_ms=step_ms, pass_ms=pass_ms, fdtd_ms=fdtd_ms, mcc_ms=mcc_ms, d0=d0, d1=d1,
                 launches=launches)
@@ -305,8 +313,13 @@ def run_ours(args):
                          cell_updates_per_s=ncell / (fdtd_avg / 1e3))
     f32, f64 = out["fp32_split"], out["fp64"]
     yerr = abs(f32["ion_total"] - f64["ion_total"]) / max(f64["ion_total"], 1)
-    ferr = max(float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
-               for a, b in zip(results["fp32_split"]["fields"], results["fp64"]["fields"]))
+    # relative field error of the FP32 form against FP64 after the same steps:
+    # norm-wise ||F32 - F64||_2 / ||F64||_2 (the gated figure), and the
+    # max-abs form max|F32 - F64| / max|F64|, both the worst of Er, Ez, H
+    pairs = list(zip(results["fp32_split"]["fields"], results["fp64"]["fields"]))
+    ferr = max(float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+               for a, b in pairs)
+    ferr_max = max(float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)) for a, b in pairs)
     e2e_ms = max_over_ranks(e2e["ms"])
     e2e_val = sum_over_ranks(e2e["n_in"] * e2e["steps"]) / (e2e_ms / 1e3)
     cpu = None
@@ -344,6 +357,8 @@ def run_ours(args):
                  "achieved_gbs": f64["achieved_gbs"], "frac": f64["achieved_gbs"] / hbm},
         "fp32_over_fp64": f32["value"] / f64["value"],
         "accuracy": {"yield_rel_err_fp32_vs_fp64": yerr, "field_rel_err_fp32_vs_fp64": ferr,
+                     "field_rel_err_definition": "max over Er, Ez, H of ||F32 - F64||_2 / ||F64||_2",
+                     "field_max_abs_rel_err_fp32_vs_fp64": ferr_max,
                      "ionizations_fp32": f32["ion_total"], "ionizations_fp64": f64["ion_total"]},
         "fdtd": {"cell_updates_per_s": f32["cell_updates_per_s"], "ms": f32["fdtd_ms"],
                  "note": "one cell-update = one cell advanced by a full particle step (H, E, H, E, H sub-updates)"},

@@ -239,10 +239,6 @@ __device__ __forceinline__ void queue_push(bool want, long long p, SimCounters *
 // contributions.
 constexpr int kDepRounds = 4;
 
-// warp-wide sum of an FP32-form contribution (|v| <= 2^25: 32 lanes fit int32)
-__device__ __forceinline__ long long warp_sum(int v) {
-  return (long long)__reduce_add_sync(0xFFFFFFFFu, v);
-}
 // FP64-form contribution, |v| <= 2^48, summed as hi 2^24 + lo with lo in
 // [0, 2^24): both 32-lane partial sums fit int32, the recombination is exact
 __device__ __forceinline__ long long warp_sum(long long v) {
@@ -532,19 +528,20 @@ __device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, 
   reflect_z(iz, fz, uz, P.nz);
 }
 
-__device__ __forceinline__ void deposit_values32(const SimParams &P, int ir, int iz, float fr,
-                                                 float fz, float ur, float ut, float uz,
-                                                 int64_t a[4], int vr[4], int vz[4],
-                                                 unsigned &key) {
+// The four deposit nodes (columns ca, cb; rows ra, rb; clamped one-sided at
+// the edges as EM7.cu:56-202) and the fixed-point contributions, node order
+// (ca,ra), (cb,ra), (ca,rb), (cb,rb).  The weights sum to 1, so one particle
+// adds at most 2^20 in magnitude to any node, even where clamped nodes merge.
+__device__ __forceinline__ void deposit_nodes32(const SimParams &P, int ir, int iz, float fr,
+                                                float fz, float ur, float ut, float uz, int &ca,
+                                                int &cb, int &ra, int &rb, int vr[4], int vz[4]) {
   const float ig = rsqrt_nr(fmaf(ur, ur, fmaf(ut, ut, fmaf(uz, uz, 1.0f))));
   int ar, az;
   float wr, wz;
   half_shift(ir, fr, ar, wr);
   half_shift(iz, fz, az, wz);
-  const int ca = max(ar, 0), cb = min(ar + 1, P.nr - 1);
-  const int ra = max(az, 0), rb = min(az + 1, P.nz - 1);
-  a[0] = ca + (int64_t)ra * P.nr; a[1] = cb + (int64_t)ra * P.nr;
-  a[2] = ca + (int64_t)rb * P.nr; a[3] = cb + (int64_t)rb * P.nr;
+  ca = max(ar, 0); cb = min(ar + 1, P.nr - 1);
+  ra = max(az, 0); rb = min(az + 1, P.nz - 1);
   const float w[4] = {(1 - wr) * (1 - wz), wr * (1 - wz), (1 - wr) * wz, wr * wz};
   const float kr = P.depf * ur * ig, kz = P.depf * uz * ig;
 #pragma unroll
@@ -552,7 +549,44 @@ __device__ __forceinline__ void deposit_values32(const SimParams &P, int ir, int
     vr[k] = __float2int_rn(kr * w[k]);
     vz[k] = __float2int_rn(kz * w[k]);
   }
-  key = (unsigned)((ar + 1) + (az + 1) * (P.nr + 1));
+}
+
+__device__ __forceinline__ void deposit_values32(const SimParams &P, int ir, int iz, float fr,
+                                                 float fz, float ur, float ut, float uz,
+                                                 int64_t a[4], int vr[4], int vz[4],
+                                                 unsigned &key) {
+  int ca, cb, ra, rb;
+  deposit_nodes32(P, ir, iz, fr, fz, ur, ut, uz, ca, cb, ra, rb, vr, vz);
+  a[0] = ca + (int64_t)ra * P.nr; a[1] = cb + (int64_t)ra * P.nr;
+  a[2] = ca + (int64_t)rb * P.nr; a[3] = cb + (int64_t)rb * P.nr;
+  key = 0;
+}
+
+// FP32-form deposit window: int32 sums of one chunk of particles on the grid
+// rows [row0, row0 + rows) in shared memory.  A chunk holds at most kChunk
+// particles, so a node's window sum stays below kChunk * 2^20 < 2^31.  Nodes
+// outside the window go straight to the grid with 64-bit atomics; the window
+// is added to the grid with one 64-bit atomic per touched node.
+constexpr int kWinNodes = 4096;           // per component
+constexpr int kChunk = 7 * kBlock;        // 1792 particles
+
+struct Win32 {
+  int *r, *z;
+  int row0, rows;
+};
+
+__device__ __forceinline__ void win_node(const Win32 &w, const SimParams &P, int col, int row,
+                                         int vr, int vz) {
+  const unsigned lr = (unsigned)(row - w.row0);
+  if (lr < (unsigned)w.rows) {
+    const int k = (int)lr * P.nr + col;
+    atomicAdd(w.r + k, vr);
+    atomicAdd(w.z + k, vz);
+  } else {
+    const int64_t g = col + (int64_t)row * P.nr;
+    if (vr) atomicAdd(P.Jr + g, (unsigned long long)(long long)vr);
+    if (vz) atomicAdd(P.Jz + g, (unsigned long long)(long long)vz);
+  }
 }
 
 __device__ __forceinline__ uint4 pack32(int ir, int iz, float fr, float fz, float ur, bool alive) {
@@ -562,74 +596,115 @@ __device__ __forceinline__ uint4 pack32(int ir, int iz, float fr, float fz, floa
 
 __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fields<float> F,
                                                       SimCounters *cnt, int *queue, int mode) {
+  __shared__ int win_r[kWinNodes], win_z[kWinNodes];
+  __shared__ int win_row0, win_rows;
   const long long n0 = (long long)cnt->n_total;
   const long long step = cnt->step;
   const int lane = threadIdx.x & 31;
-  // each block takes a contiguous chunk of the (cell-sorted) particles, so its
-  // field reads stay in a narrow band of grid rows
-  const long long chunk = (n0 + gridDim.x - 1) / gridDim.x;
-  const long long beg = (long long)blockIdx.x * chunk, end = min(beg + chunk, n0);
+  const int maxrows = min(kWinNodes / P.nr, P.nz);
+  // every block takes the same number of consecutive chunks of the
+  // (cell-sorted) particles, each chunk at most kChunk long
+  const long long per = (n0 + (long long)gridDim.x * kChunk - 1) / ((long long)gridDim.x * kChunk);
+  const long long csize = per > 0 ? (n0 + per * gridDim.x - 1) / (per * gridDim.x) : 0;
   unsigned lost = 0;
-  for (long long base = beg + (threadIdx.x & ~31); base < end; base += blockDim.x) {
-    const long long p = base + lane;
-    bool act = p < end;
-    uint4 A = make_uint4(kDead, 0, 0, 0);
-    if (act) {
-      A = S.a[p];
-      act = A.x != kDead;
-    }
-    int ir = (int)(A.x & 0xFFFFu), iz = (int)(A.x >> 16);
-    float fr = __uint_as_float(A.y), fz = __uint_as_float(A.z), ur = __uint_as_float(A.w);
-    float ut = 0.f, uz = 0.f;
-    bool cand = false;
-    if (act) {
-      const float2 B = S.b[p];
-      ut = B.x; uz = B.y;
-      // block 0 of this particle's stream: words 0-1 decide the null-collision
-      // candidate, words 2-3 (mixed) drive the stochastic rounding
-      const uint64_t id = S.id[p];
-      uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
-      philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
-      const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]);
-      bool alive = true;
-      if (mode == 1) {
-        drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, P.hdr, P.hdz);
-      } else {
-        int ar, az;
-        float wr, wz;
-        half_shift(ir, fr, ar, wr);
-        half_shift(iz, fz, az, wz);
-        const float Er = bilin(F.Er, P.nr, P.nz + 1, ar, wr, iz, fz);
-        const float Ez = bilin(F.Ez, P.nr + 1, P.nz, ir, fr, az, wz);
-        const float H = bilin(F.H, P.nr, P.nz, ar, wr, az, wz);
-        // Boris in gamma*beta units: E = (Er, 0, Ez), B = (0, mu0 H, 0); the
-        // increment u+ - u is formed first, then added with stochastic rounding
-        const float her = P.aE * Er, hez = P.aE * Ez;
-        const float umr = ur + her, umz = uz + hez;
-        const float igm = rsqrt_nr(fmaf(umr, umr, fmaf(ut, ut, fmaf(umz, umz, 1.0f))));
-        const float t = P.aB * H * igm;
-        const float s = __fdividef(2.f * t, fmaf(t, t, 1.f));
-        const float upr = fmaf(-umz, t, umr), upz = fmaf(umr, t, umz);
-        ur = sround_add(ur, fmaf(-upz, s, 2.f * her), rb0);
-        uz = sround_add(uz, fmaf(upr, s, 2.f * hez), rb0 >> 16);
-        // a collision candidate stops at integer time (k_mcc32 finishes it);
-        // the others drift the whole step
-        const bool c0 = mode == 0 && (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
-        const float h = (mode == 0 && !c0) ? 2.f : 1.f;
-        drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, h * P.hdr, h * P.hdz);
-        cand = alive && c0;
+  for (long long ch = (long long)blockIdx.x * per; ch < (long long)(blockIdx.x + 1) * per; ++ch) {
+    const long long beg = ch * csize, end = min(beg + csize, n0);
+    if (beg >= end) break;
+    if (threadIdx.x == 0) {
+      // window rows: the node rows of the chunk's first and last particles, with
+      // a margin for the drift since the last sort
+      const uint32_t k0 = reinterpret_cast<const uint32_t *>(S.a + beg)[0];
+      const uint32_t k1 = reinterpret_cast<const uint32_t *>(S.a + end - 1)[0];
+      int lo = P.nz, hi = -1;
+      if (k0 != kDead) { lo = min(lo, (int)(k0 >> 16)); hi = max(hi, (int)(k0 >> 16)); }
+      if (k1 != kDead) { lo = min(lo, (int)(k1 >> 16)); hi = max(hi, (int)(k1 >> 16)); }
+      int row0 = 0, rows = maxrows;
+      if (hi >= 0) {
+        row0 = min(max(0, lo - 3), P.nz - maxrows);
+        rows = min(maxrows, hi + 4 - row0);
       }
-      if (!alive) lost++;
-      S.a[p] = pack32(ir, iz, fr, fz, ur, alive);
-      S.b[p] = make_float2(ut, uz);
-      act = alive && mode != 2 && !cand;
+      win_row0 = row0;
+      win_rows = rows;
     }
-    queue_push(cand, p, cnt, queue);
-    int64_t a[4] = {0, 0, 0, 0};
-    int vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
-    unsigned dkey = 0;
-    if (act) deposit_values32(P, ir, iz, fr, fz, ur, ut, uz, a, vr, vz, dkey);
-    warp_deposit<int>(act, dkey, a, vr, vz, P.Jr, P.Jz);
+    __syncthreads();
+    const Win32 w{win_r, win_z, win_row0, win_rows};
+    const int nwin = w.rows * P.nr;
+    for (int i = threadIdx.x; i < nwin; i += kBlock) { win_r[i] = 0; win_z[i] = 0; }
+    __syncthreads();
+    for (long long base = beg + (threadIdx.x & ~31); base < end; base += blockDim.x) {
+      const long long p = base + lane;
+      bool act = p < end;
+      uint4 A = make_uint4(kDead, 0, 0, 0);
+      if (act) {
+        A = S.a[p];
+        act = A.x != kDead;
+      }
+      int ir = (int)(A.x & 0xFFFFu), iz = (int)(A.x >> 16);
+      float fr = __uint_as_float(A.y), fz = __uint_as_float(A.z), ur = __uint_as_float(A.w);
+      float ut = 0.f, uz = 0.f;
+      bool cand = false;
+      if (act) {
+        const float2 B = S.b[p];
+        ut = B.x; uz = B.y;
+        // block 0 of this particle's stream: words 0-1 decide the null-collision
+        // candidate, words 2-3 (mixed) drive the stochastic rounding
+        const uint64_t id = S.id[p];
+        uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
+        philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+        const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]);
+        bool alive = true;
+        if (mode == 1) {
+          drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, P.hdr, P.hdz);
+        } else {
+          int ar, az;
+          float wr, wz;
+          half_shift(ir, fr, ar, wr);
+          half_shift(iz, fz, az, wz);
+          const float Er = bilin(F.Er, P.nr, P.nz + 1, ar, wr, iz, fz);
+          const float Ez = bilin(F.Ez, P.nr + 1, P.nz, ir, fr, az, wz);
+          const float H = bilin(F.H, P.nr, P.nz, ar, wr, az, wz);
+          // Boris in gamma*beta units: E = (Er, 0, Ez), B = (0, mu0 H, 0); the
+          // increment u+ - u is formed first, then added with stochastic rounding
+          const float her = P.aE * Er, hez = P.aE * Ez;
+          const float umr = ur + her, umz = uz + hez;
+          const float igm = rsqrt_nr(fmaf(umr, umr, fmaf(ut, ut, fmaf(umz, umz, 1.0f))));
+          const float t = P.aB * H * igm;
+          const float s = __fdividef(2.f * t, fmaf(t, t, 1.f));
+          const float upr = fmaf(-umz, t, umr), upz = fmaf(umr, t, umz);
+          ur = sround_add(ur, fmaf(-upz, s, 2.f * her), rb0);
+          uz = sround_add(uz, fmaf(upr, s, 2.f * hez), rb0 >> 16);
+          // a collision candidate stops at integer time (k_mcc32 finishes it);
+          // the others drift the whole step
+          const bool c0 = mode == 0 && (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
+          const float h = (mode == 0 && !c0) ? 2.f : 1.f;
+          drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, h * P.hdr, h * P.hdz);
+          cand = alive && c0;
+        }
+        if (!alive) lost++;
+        S.a[p] = pack32(ir, iz, fr, fz, ur, alive);
+        S.b[p] = make_float2(ut, uz);
+        act = alive && mode != 2 && !cand;
+      }
+      queue_push(cand, p, cnt, queue);
+      if (act) {
+        int ca, cb, ra, rb, vr[4], vz[4];
+        deposit_nodes32(P, ir, iz, fr, fz, ur, ut, uz, ca, cb, ra, rb, vr, vz);
+        win_node(w, P, ca, ra, vr[0], vz[0]);
+        win_node(w, P, cb, ra, vr[1], vz[1]);
+        win_node(w, P, ca, rb, vr[2], vz[2]);
+        win_node(w, P, cb, rb, vr[3], vz[3]);
+      }
+    }
+    __syncthreads();
+    {
+      const int64_t off = (int64_t)w.row0 * P.nr;
+      for (int i = threadIdx.x; i < nwin; i += kBlock) {
+        const int vr = win_r[i], vz = win_z[i];
+        if (vr) atomicAdd(P.Jr + off + i, (unsigned long long)(long long)vr);
+        if (vz) atomicAdd(P.Jz + off + i, (unsigned long long)(long long)vz);
+      }
+    }
+    __syncthreads();
   }
   lost = __reduce_add_sync(0xFFFFFFFFu, lost);
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
@@ -1211,9 +1286,10 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   P.aB = (float)(-c.q_e * c.dt * c.mu0 / (2 * c.m_e));
   P.hdr = (float)(c.c * c.dt / (2 * c.dr));
   P.hdz = (float)(c.c * c.dt / (2 * c.dz));
-  // fixed point: FP64 |q FN v w| * scale <= 2^48; FP32 <= 2^25 (one warp sum fits int32)
+  // fixed point: FP64 |q FN v w| * scale <= 2^48; FP32 <= 2^20 (the int32
+  // deposit window of a chunk of particles cannot overflow)
   const double qfc = c.q_e * std::fabs(c.FN) * c.c;
-  s->scale = s->form == 0 ? std::ldexp(1.0, 48) / qfc : std::ldexp(1.0, 25) / qfc;
+  s->scale = s->form == 0 ? std::ldexp(1.0, 48) / qfc : std::ldexp(1.0, 20) / qfc;
   P.dep = s->scale;
   P.depf = (float)(-c.q_e * c.FN * c.c * s->scale);
   {
