@@ -426,15 +426,20 @@ __global__ void __launch_bounds__(128) k_mcc64(SimParams P, State64 S, SimCounte
 }
 
 // ----------------------------------------------------------- FP32 form
-// clamped bilinear interpolation on a (ncol x nrow) column-major grid
-__device__ __forceinline__ float bilin(const float *__restrict__ F, int ncol, int nrow, int c0,
-                                       float wc, int r0, float wr) {
+// clamped bilinear interpolation on a (ncol x nrow) column-major grid, split
+// into the four loads and the blend so that the loads can be issued early
+struct Quad4 { float f00, f10, f01, f11; };
+
+__device__ __forceinline__ Quad4 bilin_load(const float *__restrict__ F, int ncol, int nrow,
+                                            int c0, int r0) {
   const int ca = max(c0, 0), cb = min(c0 + 1, ncol - 1);
   const int ra = max(r0, 0), rb = min(r0 + 1, nrow - 1);
-  const float *pa = F + (int64_t)ra * ncol, *pb = F + (int64_t)rb * ncol;
-  const float f00 = __ldg(pa + ca), f10 = __ldg(pa + cb);
-  const float f01 = __ldg(pb + ca), f11 = __ldg(pb + cb);
-  const float lo = fmaf(wc, f10 - f00, f00), hi = fmaf(wc, f11 - f01, f01);
+  const float *pa = F + ra * ncol, *pb = F + rb * ncol;
+  return Quad4{__ldg(pa + ca), __ldg(pa + cb), __ldg(pb + ca), __ldg(pb + cb)};
+}
+
+__device__ __forceinline__ float bilin_mix(const Quad4 &q, float wc, float wr) {
+  const float lo = fmaf(wc, q.f10 - q.f00, q.f00), hi = fmaf(wc, q.f11 - q.f01, q.f01);
   return fmaf(wr, hi - lo, lo);
 }
 
@@ -448,18 +453,31 @@ __device__ __forceinline__ float rsqrt_nr(float x) {
 // a + d with stochastic rounding.  The per-step velocity changes of the FP32
 // form (a drift rotation by a small angle, a kick in a weak field) are often
 // below one float ulp of u; rounding them to nearest would bias |u| steadily.
-// The exact residual of a + d (TwoSum) picks the neighbour float with
-// probability |residual| / ulp, using 16 random bits r16.
-__device__ __forceinline__ float sround_add(float a, float d, uint32_t r16) {
+// The exact residual e of a + d (TwoSum) moves the rounded sum s to its
+// neighbour nb on the side of e with probability |e| / |nb - s|.  The uniform
+// u = (k + 1/2) 2^-16 (k: the low 16 bits of r) is built as a float in [1, 2)
+// minus 1, so no conversion or division is issued; e = 0 keeps s.
+__device__ __forceinline__ float sround_add(float a, float d, uint32_t r) {
   const float s = a + d;
   const float bb = s - a;
   const float e = (a - (s - bb)) + (d - bb);
-  if (e == 0.f || s == 0.f) return s;
-  const int dir = ((e > 0.f) == (s > 0.f)) ? 1 : -1;
+  const int dir = ((__float_as_int(e) ^ __float_as_int(s)) >> 31) | 1;   // +1: away from 0
   const float nb = __int_as_float(__float_as_int(s) + dir);
-  const float p = __fdividef(fabsf(e), fabsf(nb - s));
-  const float u = ((float)(r16 & 0xFFFFu) + 0.5f) * (1.0f / 65536.0f);
-  return u < p ? nb : s;
+  const float u = __uint_as_float(0x3F800040u | ((r & 0xFFFFu) << 7)) - 1.0f;
+  return fabsf(e) > u * fabsf(nb - s) ? nb : s;
+}
+
+// floor(x) for |x| < 2^22, subtracted from x and returned as an int: x + 1.5
+// 2^23 rounded down is 1.5 2^23 + floor(x) exactly (unit spacing there)
+__device__ __forceinline__ int take_floor(float &x) {
+  const float t = __fadd_rd(x, 12582912.0f);
+  x -= t - 12582912.0f;
+  return __float_as_int(t) - 0x4B400000;
+}
+
+// nearest integer (ties to even) of a * b for |a b| < 2^22, rounded once
+__device__ __forceinline__ int fma_rint(float a, float b) {
+  return __float_as_int(fmaf(a, b, 12582912.0f)) - 0x4B400000;
 }
 
 // 32 fresh bits from a 32-bit input (integer finaliser)
@@ -510,7 +528,8 @@ __device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, 
   const float rn = r2 * irn;
   const float sn = r2 > 0.f ? dy * irn : 0.f;
   const float s2 = sn * sn;
-  const float sq = sqrtf(fmaxf(0.f, 1.f - s2));
+  const float cc = 1.f - s2;                         // cos^2 a
+  const float sq = cc > 0.f ? cc * rsqrtf(cc) : 0.f;
   const float c1 = X >= 0.f ? __fdividef(s2, 1.f + sq) : 1.f + sq;   // 1 - cos a
   const float dur = fmaf(sn, ut, -c1 * ur), dut = fmaf(-sn, ur, -c1 * ut);
   ur = sround_add(ur, dur, rb);
@@ -518,13 +537,11 @@ __device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, 
   const float den = rn + rc;
   const float drr = den > 0.f ? __fdividef(fmaf(dx, 2.f * rc + dx, dy * dy), den) : 0.f;
   fr += drr;
-  float k = floorf(fr);
-  ir += (int)k; fr -= k;
+  ir += take_floor(fr);
   if (ir < 0) { ir = 0; fr = 0.f; }
   alive = alive && ir < P.nr;
   fz += dzz;
-  k = floorf(fz);
-  iz += (int)k; fz -= k;
+  iz += take_floor(fz);
   reflect_z(iz, fz, uz, P.nz);
 }
 
@@ -546,8 +563,8 @@ __device__ __forceinline__ void deposit_nodes32(const SimParams &P, int ir, int 
   const float kr = P.depf * ur * ig, kz = P.depf * uz * ig;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    vr[k] = __float2int_rn(kr * w[k]);
-    vz[k] = __float2int_rn(kz * w[k]);
+    vr[k] = fma_rint(kr, w[k]);
+    vz[k] = fma_rint(kz, w[k]);
   }
 }
 
@@ -650,19 +667,24 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
         // candidate, words 2-3 (mixed) drive the stochastic rounding
         const uint64_t id = S.id[p];
         uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
-        philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
-        const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]);
         bool alive = true;
         if (mode == 1) {
-          drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, P.hdr, P.hdz);
+          philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+          drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, mix32(c[3]), P.hdr, P.hdz);
         } else {
           int ar, az;
           float wr, wz;
           half_shift(ir, fr, ar, wr);
           half_shift(iz, fz, az, wz);
-          const float Er = bilin(F.Er, P.nr, P.nz + 1, ar, wr, iz, fz);
-          const float Ez = bilin(F.Ez, P.nr + 1, P.nz, ir, fr, az, wz);
-          const float H = bilin(F.H, P.nr, P.nz, ar, wr, az, wz);
+          // the field loads go out first; their latency hides behind Philox
+          const Quad4 qEr = bilin_load(F.Er, P.nr, P.nz + 1, ar, iz);
+          const Quad4 qEz = bilin_load(F.Ez, P.nr + 1, P.nz, ir, az);
+          const Quad4 qH = bilin_load(F.H, P.nr, P.nz, ar, az);
+          philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+          const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]);
+          const float Er = bilin_mix(qEr, wr, fz);
+          const float Ez = bilin_mix(qEz, fr, wz);
+          const float H = bilin_mix(qH, wr, wz);
           // Boris in gamma*beta units: E = (Er, 0, Ez), B = (0, mu0 H, 0); the
           // increment u+ - u is formed first, then added with stochastic rounding
           const float her = P.aE * Er, hez = P.aE * Ez;
@@ -689,10 +711,19 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
       if (act) {
         int ca, cb, ra, rb, vr[4], vz[4];
         deposit_nodes32(P, ir, iz, fr, fz, ur, ut, uz, ca, cb, ra, rb, vr, vz);
-        win_node(w, P, ca, ra, vr[0], vz[0]);
-        win_node(w, P, cb, ra, vr[1], vz[1]);
-        win_node(w, P, ca, rb, vr[2], vz[2]);
-        win_node(w, P, cb, rb, vr[3], vz[3]);
+        const unsigned la = (unsigned)(ra - w.row0), lb = (unsigned)(rb - w.row0);
+        if (la < (unsigned)w.rows && lb < (unsigned)w.rows) {
+          const int ka = (int)la * P.nr, kb = (int)lb * P.nr;
+          atomicAdd(win_r + ka + ca, vr[0]); atomicAdd(win_z + ka + ca, vz[0]);
+          atomicAdd(win_r + ka + cb, vr[1]); atomicAdd(win_z + ka + cb, vz[1]);
+          atomicAdd(win_r + kb + ca, vr[2]); atomicAdd(win_z + kb + ca, vz[2]);
+          atomicAdd(win_r + kb + cb, vr[3]); atomicAdd(win_z + kb + cb, vz[3]);
+        } else {
+          win_node(w, P, ca, ra, vr[0], vz[0]);
+          win_node(w, P, cb, ra, vr[1], vz[1]);
+          win_node(w, P, ca, rb, vr[2], vz[2]);
+          win_node(w, P, cb, rb, vr[3], vz[3]);
+        }
       }
     }
     __syncthreads();
@@ -1214,7 +1245,8 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   if (!ctx || !cfg || !out) return GASATT_E_ARG;
   *out = nullptr;
   const gasatt_sim_config &c = *cfg;
-  if (c.n_r < 2 || c.n_z < 2 || c.n_r > 65535 || c.n_z > 65535 || !(c.dr > 0) || !(c.dz > 0) ||
+  if (c.n_r < 2 || c.n_z < 2 || c.n_r > 65535 || c.n_z > 65535 ||
+      (int64_t)(c.n_r + 1) * (c.n_z + 1) > 0x7FFFFFFFLL || !(c.dr > 0) || !(c.dz > 0) ||
       !(c.dt > 0) || c.fdtd_ratio < 1 || c.capacity < 1 ||
       (c.precision != GASATT_FP64 && c.precision != GASATT_FP32_SPLIT))
     return fail(ctx, GASATT_E_ARG, "sim config out of range");
