@@ -37,6 +37,7 @@ namespace {
 
 constexpr uint32_t kDead = 0xFFFFFFFFu;
 constexpr int kBlock = 256;
+constexpr int kMccBlock = 64;             // collision kernels: two warps per block
 
 struct SimCounters {
   unsigned long long n_total;    // committed slots
@@ -144,10 +145,57 @@ __device__ __forceinline__ bool null_candidate(const SimParams &P, uint64_t id, 
   return b < P.cand_below;
 }
 
+// Turn (vx, vy, vz) by the polar angle th and the azimuth ph about its own
+// direction, from their sines and cosines (the rotation of
+// electron_transport.cu:118-135 in the corrected frame, p2 = vx^2 + vy^2).
+template <typename R>
+__device__ __forceinline__ void rotate_sc(R &vx, R &vy, R &vz, R st, R ct, R sp, R cp) {
+  const R v = sqrt(vx * vx + vy * vy + vz * vz);
+  const R p2 = vx * vx + vy * vy;
+  R x0, y0, z0;
+  if (p2 > R(0.0001)) {
+    const R s = sqrt(p2);
+    const R f = st / s;
+    x0 = vx * ct + f * (vx * vz * cp - v * vy * sp);
+    y0 = vy * ct + f * (vy * vz * cp + v * vx * sp);
+    z0 = vz * ct - s * st * cp;
+  } else {
+    x0 = v * st * cp;
+    y0 = v * st * sp;
+    z0 = v * ct;
+  }
+  vx = x0; vy = y0; vz = z0;
+}
+
+// Apply the rotation with (st, ct) given and azimuth 2 pi b (sign = -1: the
+// opposite azimuth, phi - pi).  FAST (the FP32 form): float arithmetic with
+// the hardware sine and cosine on the azimuth folded into [-pi, pi].
+template <bool FAST>
+__device__ __forceinline__ void turn(double &ux, double &uy, double &uz, double st, double ct,
+                                     double b, double sign) {
+  if (FAST) {
+    float sp, cp;
+    const float ph = (float)(2 * GASATT_PI * (b > 0.5 ? b - 1 : b));
+    __sincosf(ph, &sp, &cp);
+    float x = (float)ux, y = (float)uy, z = (float)uz;
+    rotate_sc<float>(x, y, z, (float)st, (float)ct, (float)sign * sp, (float)sign * cp);
+    ux = x; uy = y; uz = z;
+  } else {
+    double sp, cp;
+    sincos(2 * GASATT_PI * b, &sp, &cp);
+    rotate_sc<double>(ux, uy, uz, st, ct, sign * sp, sign * cp);
+  }
+}
+
 // Collision of a candidate electron at step `step` (corrected form of
 // electron_transport.cu:74-227).  u in m/s, local (r, theta, z) frame.
-// Returns 1 elastic, 2 ionization, 3 excitation, 4 null.
-__device__ __noinline__ int mcc_event(const SimParams &P, uint64_t id, long long step, double &ux,
+// Returns 1 elastic, 2 ionization, 3 excitation, 4 null.  The collision test,
+// the branch choice, the ionization energy sharing and the threshold
+// subtractions are FP64 in both forms; FAST (the FP32 form) turns the
+// velocity in float.  The code is kept short: one candidate runs it alone,
+// mostly from a cold instruction cache.
+template <bool FAST>
+__device__ __forceinline__ int mcc_event(const SimParams &P, uint64_t id, long long step, double &ux,
                                       double &uy, double &uz, Birth &b) {
   b.born = false;
   const U2 d0 = draw2(P.seed, id, step, 0);
@@ -163,8 +211,16 @@ __device__ __noinline__ int mcc_event(const SimParams &P, uint64_t id, long long
   const double X = d0.b * P.nu_max;
   if (X < nu_el) {
     const U2 d1 = draw2(P.seed, id, step, 1);
-    const double th = cdf_theta(P, L, d1.a), ph = 2 * GASATT_PI * d1.b;
-    rotate_v(ux, uy, uz, th, ph, false);
+    const double th = cdf_theta(P, L, d1.a);
+    double st, ct;
+    if (FAST) {
+      float sf, cf;
+      __sincosf((float)th, &sf, &cf);
+      st = sf; ct = cf;
+    } else {
+      sincos(th, &st, &ct);
+    }
+    turn<FAST>(ux, uy, uz, st, ct, d1.b, 1.0);
     return 1;
   }
   if (X < nu_el + nu_io && Eev > I) {
@@ -174,22 +230,26 @@ __device__ __noinline__ int mcc_event(const SimParams &P, uint64_t id, long long
     const double T_0 = T_s - T_a / (T + T_b);
     const double t = t_s * T / (T + t_b);
     const double T_m = (T - I) / 2;
-    const double k_1 = atan((T_m - T_0) / t), k_2 = atan(T_0 / t);
-    const double k0 = T_0 + t * tan(d1.a * (k_1 + k_2) - k_2);
+    // E_1 = T_0 + t tan(U (k_1 + k_2) - k_2), k_1 = atan((T_m - T_0)/t),
+    // k_2 = atan(T_0/t): with k_1 + k_2 from one atan2 and
+    // tan(x - k_2) = (tan x - tan k_2) / (1 + tan x tan k_2)
+    const double a1 = (T_m - T_0) / t, a2 = T_0 / t;
+    const double tx = tan(d1.a * atan2(a1 + a2, 1 - a1 * a2));
+    const double k0 = T_0 + t * ((tx - a2) / (1 + a2 * tx));
     const double E_1 = k0, E_2 = T - E_1 - I;
     double E_p, E_s;
     if (E_2 > E_1) { E_p = E_2; E_s = E_1; } else { E_p = E_1; E_s = E_2; }
     const double E_e = me * c * c / qe;
-    const double phi_p = 2 * GASATT_PI * d1.b, phi_s = phi_p - GASATT_PI;
-    const double th_p = asin(sqrt((E_s / T) / ((1 - E_s / T) * T / (2 * E_e) + 1)));
-    const double th_s = asin(sqrt((1 - E_s / T) / (1 + E_s / (2 * E_e))));
+    // polar angles as sines (the reference's asin arguments) and cosines
+    const double sp2 = (E_s / T) / ((1 - E_s / T) * T / (2 * E_e) + 1);
+    const double ss2 = (1 - E_s / T) / (1 + E_s / (2 * E_e));
     const double ix = ux / um, iy = uy / um, iz = uz / um;
     const double up = u_of_energy(E_p * qe, me, c), us = u_of_energy(E_s * qe, me, c);
     ux = ix * up; uy = iy * up; uz = iz * up;
-    rotate_v(ux, uy, uz, th_p, phi_p, false);
+    turn<FAST>(ux, uy, uz, sqrt(sp2), sqrt(1 - sp2), d1.b, 1.0);
     if (P.secondaries) {
       double sx_ = ix * us, sy_ = iy * us, sz_ = iz * us;
-      rotate_v(sx_, sy_, sz_, th_s, phi_s, false);
+      turn<FAST>(sx_, sy_, sz_, sqrt(ss2), sqrt(1 - ss2), d1.b, -1.0);
       b.born = true; b.ux = sx_; b.uy = sy_; b.uz = sz_;
     }
     return 2;
@@ -376,19 +436,22 @@ __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fi
 }
 
 // collision candidates of this step: MCC, births, second half drift, deposit
-__global__ void __launch_bounds__(128) k_mcc64(SimParams P, State64 S, SimCounters *cnt,
-                                               const int *queue) {
+__global__ void __launch_bounds__(kMccBlock) k_mcc64(SimParams P, State64 S, SimCounters *cnt,
+                                                     const int *queue) {
+  // one candidate per warp (lane 0): the collision branches differ a lot in
+  // length, and lanes on different branches would run them one after another
+  if ((threadIdx.x & 31) != 0) return;
   const long long n0 = (long long)cnt->n_total;
   const long long step = cnt->step;
   const long long nq = (long long)cnt->n_cand;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
-       q += (long long)gridDim.x * blockDim.x) {
+  const long long nwarps = (long long)gridDim.x * (kMccBlock / 32);
+  for (long long q = (blockIdx.x * (long long)kMccBlock + threadIdx.x) >> 5; q < nq; q += nwarps) {
     const long long p = queue[q];
     double2 rz = S.rz[p], urt = S.urt[p];
     double r = rz.x, z = rz.y, ur = urt.x, ut = urt.y, uz = S.uz[p];
     const uint64_t id = S.id[p];
     Birth b;
-    count_event(cnt, mcc_event(P, id, step, ur, ut, uz, b));
+    count_event(cnt, mcc_event<false>(P, id, step, ur, ut, uz, b));
     if (b.born) {
       const unsigned long long k = atomicAdd(&cnt->n_births, 1ull);
       const long long slot = n0 + (long long)k;
@@ -741,13 +804,16 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
 }
 
-__global__ void __launch_bounds__(128) k_mcc32(SimParams P, State32 S, SimCounters *cnt,
-                                               const int *queue) {
+__global__ void __launch_bounds__(kMccBlock) k_mcc32(SimParams P, State32 S, SimCounters *cnt,
+                                                     const int *queue) {
+  // one candidate per warp (lane 0): the collision branches differ a lot in
+  // length, and lanes on different branches would run them one after another
+  if ((threadIdx.x & 31) != 0) return;
   const long long n0 = (long long)cnt->n_total;
   const long long step = cnt->step;
   const long long nq = (long long)cnt->n_cand;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
-       q += (long long)gridDim.x * blockDim.x) {
+  const long long nwarps = (long long)gridDim.x * (kMccBlock / 32);
+  for (long long q = (blockIdx.x * (long long)kMccBlock + threadIdx.x) >> 5; q < nq; q += nwarps) {
     const long long p = queue[q];
     const uint4 A = S.a[p];
     const float2 B = S.b[p];
@@ -756,7 +822,7 @@ __global__ void __launch_bounds__(128) k_mcc32(SimParams P, State32 S, SimCounte
     double dux = (double)__uint_as_float(A.w) * P.c, duy = (double)B.x * P.c, duz = (double)B.y * P.c;
     const uint64_t id = S.id[p];
     Birth b;
-    count_event(cnt, mcc_event(P, id, step, dux, duy, duz, b));
+    count_event(cnt, mcc_event<true>(P, id, step, dux, duy, duz, b));
     float ur = (float)(dux / P.c), ut = (float)(duy / P.c), uz = (float)(duz / P.c);
     if (b.born) {
       const unsigned long long k = atomicAdd(&cnt->n_births, 1ull);
@@ -1127,8 +1193,8 @@ int launch_pass(gasatt_sim *s, cudaStream_t st, int mode, int jb, cudaEvent_t mi
     if (e != cudaSuccess) return cuda_fail(s->ctx, e, "event");
   }
   if (mode == 0) {
-    if (s->form == 0) k_mcc64<<<s->mcc_grid, 128, 0, st>>>(P, s->s64[b], s->cnt, s->queue);
-    else k_mcc32<<<s->mcc_grid, 128, 0, st>>>(P, s->s32[b], s->cnt, s->queue);
+    if (s->form == 0) k_mcc64<<<s->mcc_grid, kMccBlock, 0, st>>>(P, s->s64[b], s->cnt, s->queue);
+    else k_mcc32<<<s->mcc_grid, kMccBlock, 0, st>>>(P, s->s32[b], s->cnt, s->queue);
     s->ctx->launches++;
   }
   cudaError_t e = cudaGetLastError();
@@ -1353,7 +1419,11 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   if (s->form == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass64, kBlock, 0);
   else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass32, kBlock, 0);
   s->pass_grid = (unsigned)(nsm * (occ > 0 ? occ : 1));
-  s->mcc_grid = (unsigned)nsm;
+  // as many collision warps as fit on the device at once
+  int occ_mcc = 1;
+  if (s->form == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mcc, k_mcc64, kMccBlock, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mcc, k_mcc32, kMccBlock, 0);
+  s->mcc_grid = (unsigned)(nsm * (occ_mcc > 0 ? occ_mcc : 1));
   // zero state
   SimCounters z{};
   z.step = -1;
