@@ -98,9 +98,9 @@ namespace gasatt {
 // writes back its tile.  A warp covers one 32-cell row of the patch.  The
 // current it reads (Jr, Jz, fixed point) was deposited by the previous
 // particle pass; the block clears its tile of the other buffer (Jr_next,
-// Jz_next) for the next pass.  Storage in T, arithmetic in double (float
-// arithmetic here costs the FP32 form two orders of magnitude in field
-// accuracy).
+// Jz_next) for the next pass.  Storage in T; the patch stays in shared
+// memory in double for the whole sub-cycle, so the FP32 form rounds its
+// fields to float once per step and converts once each way.
 constexpr int kFdtdPatch = 32;
 constexpr int kFdtdRows = 16;                          // blockDim = (32, kFdtdRows)
 
@@ -116,7 +116,7 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
                                            int nz, const FdtdCoef &c, const double *__restrict__ invV,
                                            double mu, double dt, int R, unsigned flags) {
   constexpr int TW = kFdtdPatch;
-  __shared__ T sEr[TW * TW], sEz[TW * TW], sH[TW * TW], sJr[TW * TW], sJz[TW * TW];
+  __shared__ double sEr[TW * TW], sEz[TW * TW], sH[TW * TW], sJr[TW * TW], sJz[TW * TW];
   const int tile = fdtd_tile(R), hl = 2 * R, hh = 2 * R + 1;
   const int i0 = blockIdx.x * tile, j0 = blockIdx.y * tile;
   const int I0 = max(i0 - hl, 0), J0 = max(j0 - hl, 0);
@@ -127,13 +127,13 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
   for (int lj = threadIdx.y; lj < Hn; lj += kFdtdRows) {
     const int j = J0 + lj, s = li + lj * TW;
     if (!col) continue;
-    if (i < nr && j <= nz) sEr[s] = Er[i + (int64_t)j * nr];
-    if (i <= nr && j < nz) sEz[s] = Ez[i + (int64_t)j * (nr + 1)];
+    if (i < nr && j <= nz) sEr[s] = (double)Er[i + (int64_t)j * nr];
+    if (i <= nr && j < nz) sEz[s] = (double)Ez[i + (int64_t)j * (nr + 1)];
     if (i < nr && j < nz) {
       const int64_t g = i + (int64_t)j * nr;
-      sH[s] = H[g];
-      sJr[s] = (T)((double)(long long)Jr[g] * invV[i]);
-      sJz[s] = (T)((double)(long long)Jz[g] * invV[i]);
+      sH[s] = (double)H[g];
+      sJr[s] = (double)(long long)Jr[g] * invV[i];
+      sJz[s] = (double)(long long)Jz[g] * invV[i];
     }
   }
   __syncthreads();
@@ -151,8 +151,7 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
         for (int lj = threadIdx.y; lj < Hn; lj += kFdtdRows) {
           const int j = J0 + lj, s = li + lj * TW;
           if (j < nz && j + 1 < J1)
-            sH[s] = (T)((double)sH[s] + (chr * ((double)sEz[s + 1] - (double)sEz[s]) -
-                                         chz * ((double)sEr[s + TW] - (double)sEr[s])));
+            sH[s] = sH[s] + (chr * (sEz[s + 1] - sEz[s]) - chz * (sEr[s + TW] - sEr[s]));
         }
       }
     } else if (col) {                                  // E update (dt/2)
@@ -161,26 +160,24 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
         if (i < nr) {
           if (j >= 1 && j < nz) {
             if (j - 1 >= J0) {
-              const T old = sEr[s];
-              sEr[s] = (T)((double)old - dt_eps * ((double)sJr[s - TW] + (double)sJr[s]) / 2 -
-                           dt_eps_dz * ((double)sH[s] - (double)sH[s - TW]));
+              const double old = sEr[s];
+              sEr[s] = old - dt_eps * (sJr[s - TW] + sJr[s]) / 2 - dt_eps_dz * (sH[s] - sH[s - TW]);
               if (endcopy) {
                 if (j == 1 && J0 == 0) sEr[s - TW] = old;
                 if (j == nz - 1 && J1 == nz + 1) sEr[s + TW] = old;
               }
             }
           } else if (!endcopy && j <= nz) {
-            sEr[s] = (T)0;
+            sEr[s] = 0.0;
           }
         }
         if (j < nz) {
           if (i == 0) {
-            const double jz0 = (double)sJz[s];
+            const double jz0 = sJz[s];
             const double jterm = (flags & GASATT_Q_EZ_AXIS_JSIGN) ? dt_eps * jz0 : -(dt_eps * jz0);
-            sEz[s] = (T)((double)sEz[s] + jterm + axis * (double)sH[s]);
+            sEz[s] = sEz[s] + jterm + axis * sH[s];
           } else if (i < nr && i - 1 >= I0) {
-            sEz[s] = (T)((double)sEz[s] - dt_eps * ((double)sJz[s - 1] + (double)sJz[s]) / 2 +
-                         ezp * (double)sH[s] + ezm * (double)sH[s - 1]);
+            sEz[s] = sEz[s] - dt_eps * (sJz[s - 1] + sJz[s]) / 2 + ezp * sH[s] + ezm * sH[s - 1];
           }
         }
       }
@@ -192,11 +189,11 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
     for (int j = J0 + threadIdx.y; j < je; j += kFdtdRows) {
       if (j < j0) continue;
       const int s = li + (j - J0) * TW;
-      if (i < nr && j <= nz) Er[i + (int64_t)j * nr] = sEr[s];
-      if (i <= nr && j < nz) Ez[i + (int64_t)j * (nr + 1)] = sEz[s];
+      if (i < nr && j <= nz) Er[i + (int64_t)j * nr] = (T)sEr[s];
+      if (i <= nr && j < nz) Ez[i + (int64_t)j * (nr + 1)] = (T)sEz[s];
       if (i < nr && j < nz) {
         const int64_t g = i + (int64_t)j * nr;
-        H[g] = sH[s];
+        H[g] = (T)sH[s];
         Jr_next[g] = 0;
         Jz_next[g] = 0;
       }

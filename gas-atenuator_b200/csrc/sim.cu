@@ -644,22 +644,26 @@ __device__ __forceinline__ void deposit_values32(const SimParams &P, int ir, int
 
 // FP32-form deposit window: int32 sums of one chunk of particles on the grid
 // rows [row0, row0 + rows) in shared memory.  A chunk holds at most kChunk
-// particles, so a node's window sum stays below kChunk * 2^20 < 2^31.  Nodes
-// outside the window go straight to the grid with 64-bit atomics; the window
-// is added to the grid with one 64-bit atomic per touched node.
+// particles, so a node's window sum stays below kChunk * 2^20 < 2^31.  Rows
+// are ws >= nr words apart with ws = 3 (mod 32), so the 3 x 3 nodes around a
+// warp's particles sit in 9 different banks.  Nodes outside the window go
+// straight to the grid with 64-bit atomics; the window is added to the grid
+// with one 64-bit atomic per touched node.
 constexpr int kWinNodes = 4096;           // per component
 constexpr int kChunk = 7 * kBlock;        // 1792 particles
 
 struct Win32 {
   int *r, *z;
-  int row0, rows;
+  int row0, rows, ws;
 };
+
+__host__ __device__ inline int win_stride(int nr) { return nr + ((3 - nr % 32) + 32) % 32; }
 
 __device__ __forceinline__ void win_node(const Win32 &w, const SimParams &P, int col, int row,
                                          int vr, int vz) {
   const unsigned lr = (unsigned)(row - w.row0);
   if (lr < (unsigned)w.rows) {
-    const int k = (int)lr * P.nr + col;
+    const int k = (int)lr * w.ws + col;
     atomicAdd(w.r + k, vr);
     atomicAdd(w.z + k, vz);
   } else {
@@ -681,7 +685,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
   const long long n0 = (long long)cnt->n_total;
   const long long step = cnt->step;
   const int lane = threadIdx.x & 31;
-  const int maxrows = min(kWinNodes / P.nr, P.nz);
+  const int ws = win_stride(P.nr);
+  const int maxrows = min(kWinNodes / ws, P.nz);
   // every block takes the same number of consecutive chunks of the
   // (cell-sorted) particles, each chunk at most kChunk long
   const long long per = (n0 + (long long)gridDim.x * kChunk - 1) / ((long long)gridDim.x * kChunk);
@@ -707,8 +712,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
       win_rows = rows;
     }
     __syncthreads();
-    const Win32 w{win_r, win_z, win_row0, win_rows};
-    const int nwin = w.rows * P.nr;
+    const Win32 w{win_r, win_z, win_row0, win_rows, ws};
+    const int nwin = w.rows * ws;
     for (int i = threadIdx.x; i < nwin; i += kBlock) { win_r[i] = 0; win_z[i] = 0; }
     __syncthreads();
     for (long long base = beg + (threadIdx.x & ~31); base < end; base += blockDim.x) {
@@ -776,7 +781,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
         deposit_nodes32(P, ir, iz, fr, fz, ur, ut, uz, ca, cb, ra, rb, vr, vz);
         const unsigned la = (unsigned)(ra - w.row0), lb = (unsigned)(rb - w.row0);
         if (la < (unsigned)w.rows && lb < (unsigned)w.rows) {
-          const int ka = (int)la * P.nr, kb = (int)lb * P.nr;
+          const int ka = (int)la * ws, kb = (int)lb * ws;
           atomicAdd(win_r + ka + ca, vr[0]); atomicAdd(win_z + ka + ca, vz[0]);
           atomicAdd(win_r + ka + cb, vr[1]); atomicAdd(win_z + ka + cb, vz[1]);
           atomicAdd(win_r + kb + ca, vr[2]); atomicAdd(win_z + kb + ca, vz[2]);
@@ -790,12 +795,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
       }
     }
     __syncthreads();
-    {
-      const int64_t off = (int64_t)w.row0 * P.nr;
-      for (int i = threadIdx.x; i < nwin; i += kBlock) {
-        const int vr = win_r[i], vz = win_z[i];
-        if (vr) atomicAdd(P.Jr + off + i, (unsigned long long)(long long)vr);
-        if (vz) atomicAdd(P.Jz + off + i, (unsigned long long)(long long)vz);
+    for (int i = threadIdx.x; i < nwin; i += kBlock) {
+      const int vr = win_r[i], vz = win_z[i];
+      if (vr | vz) {                 // the padding words stay zero
+        const int row = i / ws;
+        const int64_t g = (int64_t)(w.row0 + row) * P.nr + (i - row * ws);
+        if (vr) atomicAdd(P.Jr + g, (unsigned long long)(long long)vr);
+        if (vz) atomicAdd(P.Jz + g, (unsigned long long)(long long)vz);
       }
     }
     __syncthreads();
