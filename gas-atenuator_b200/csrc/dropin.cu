@@ -6,6 +6,8 @@
 #include <cub/device/device_scan.cuh>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include "fdtd.cuh"
 #include "gasatt_internal.h"
 
@@ -118,6 +120,33 @@ __global__ void k_density_finish(const unsigned long long *count, int64_t ncell,
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncell;
        c += (int64_t)gridDim.x * blockDim.x)
     density[c] = FN * (double)count[c] / VC[c % cellnumxy];
+}
+
+// Per-cell counters of gasatt_particle_density_noalloc: a fixed array in the
+// library's device image, so that call needs no device allocation.  In host
+// code the name g_density_counts stands for a host-side shadow, not a device
+// address; the device address comes from cudaGetSymbolAddress, once per
+// device, with that device current.
+static __device__ __align__(256) unsigned long long
+    g_density_counts[GASATT_DENSITY_NOALLOC_MAX_CELLS];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_density_mu;
+unsigned long long *g_density_addr[kMaxDevices] = {};
+
+// device address of g_density_counts on ctx->device (current device)
+int density_counts_on_device(gasatt_ctx *ctx, unsigned long long **out) {
+  if (ctx->device < 0 || ctx->device >= kMaxDevices)
+    return fail(ctx, GASATT_E_ARG, "particle_density_noalloc: device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_density_mu);
+  if (!g_density_addr[ctx->device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_density_counts);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(g_density_counts)");
+    g_density_addr[ctx->device] = static_cast<unsigned long long *>(p);
+  }
+  *out = g_density_addr[ctx->device];
+  return GASATT_OK;
 }
 
 // -------------------------------------------- electricmagneticfield6 path
@@ -556,6 +585,34 @@ int gasatt_particle_density(gasatt_ctx *ctx, double dr, double dz, const double 
   int st = scratch(ctx, (size_t)ncell * 8, &buf);
   if (st) return st;
   unsigned long long *cnt = (unsigned long long *)buf;
+  GASATT_CUDA(ctx, cudaMemsetAsync(cnt, 0, (size_t)ncell * 8, ctx->stream));
+  if (n > 0) {
+    k_density_count<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(dr, dz, dphi, rmax, r, phi, z, n,
+                                                                     cellnumxy, sum_cell, ncell, cnt);
+    GASATT_LAUNCHED(ctx);
+  }
+  k_density_finish<<<grid_for(ncell, kBlock), kBlock, 0, ctx->stream>>>(cnt, ncell, cellnumxy, VC, FN, density);
+  GASATT_LAUNCHED(ctx);
+  return GASATT_OK;
+}
+
+int gasatt_particle_density_noalloc(gasatt_ctx *ctx, double dr, double dz, const double *dphi,
+                                    int rmax, const double *r, const double *phi, const double *z,
+                                    int64_t n, int cellnumxy, const double *sum_cell,
+                                    const double *VC, int64_t ncell, double FN, double *density) {
+  if (!ctx || n < 0 || ncell <= 0 || rmax <= 0 || cellnumxy <= 0)
+    return fail(ctx, GASATT_E_ARG, "particle_density_noalloc: bad sizes");
+  if (ncell > (int64_t)GASATT_DENSITY_NOALLOC_MAX_CELLS)
+    return fail(ctx, GASATT_E_CAPACITY,
+                "particle_density_noalloc: ncell = " + std::to_string(ncell) +
+                    " exceeds its fixed scratch of " +
+                    std::to_string((long long)GASATT_DENSITY_NOALLOC_MAX_CELLS) +
+                    " cells (use gasatt_particle_density)");
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  unsigned long long *cnt = nullptr;
+  int st = density_counts_on_device(ctx, &cnt);
+  if (st) return st;
+  // the array keeps the previous call's counts: clear the cells used now
   GASATT_CUDA(ctx, cudaMemsetAsync(cnt, 0, (size_t)ncell * 8, ctx->stream));
   if (n > 0) {
     k_density_count<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(dr, dz, dphi, rmax, r, phi, z, n,

@@ -75,6 +75,8 @@ _SIGS = {
                                  c_p, c_p, c_p, c_p, c_p]),
     "gasatt_particle_density": (c_i, [c_p, c_d, c_d, c_p, c_i, c_p, c_p, c_p, c_i64, c_i,
                                       c_p, c_p, c_i64, c_d, c_p]),
+    "gasatt_particle_density_noalloc": (c_i, [c_p, c_d, c_d, c_p, c_i, c_p, c_p, c_p, c_i64,
+                                              c_i, c_p, c_p, c_i64, c_d, c_p]),
     "gasatt_electricmagneticfield6": (c_i, [c_p, c_p, c_p, c_i64, c_p, c_p, c_i64, c_p, c_p,
                                             c_i64, c_p, c_p, c_p, c_i, c_i, c_d, c_d, c_d,
                                             c_d, c_d, c_d, c_i, c_p,

@@ -156,6 +156,33 @@ int gasatt_particle_density(gasatt_ctx *ctx, double dr, double dz,
                             const double *VC, int64_t ncell, double FN,
                             double *density);
 
+/* gasatt_particle_density without any device allocation.  It has no
+ * counterpart in the reference: it exists for callers that must not call
+ * cudaMalloc/cudaFree themselves or through this library -- above all a MEX
+ * gateway running inside MATLAB, whose gpuArray memory pool owns the device
+ * memory (a private allocation competes with that pool, and cudaFree stalls
+ * the whole device).  gasatt_particle_density takes its per-cell counts from
+ * the context's scratch buffer, which it may grow with cudaMalloc; this call
+ * counts instead into a fixed array compiled into the library, of
+ * GASATT_DENSITY_NOALLOC_MAX_CELLS 64-bit counters (8 MiB, held by every
+ * device that loads the library until the process exits).
+ *  - Arguments and result are those of gasatt_particle_density.
+ *  - ncell > GASATT_DENSITY_NOALLOC_MAX_CELLS is rejected with
+ *    GASATT_E_CAPACITY (nothing is launched).
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - The counters are zeroed on the context's stream at the start of every
+ *    call.  All calls on a device share the one array, so calls whose work
+ *    overlaps on the GPU (other streams, other contexts, other host threads)
+ *    race and give wrong densities; keep them ordered. */
+#define GASATT_DENSITY_NOALLOC_MAX_CELLS (1 << 20)
+int gasatt_particle_density_noalloc(gasatt_ctx *ctx, double dr, double dz,
+                                    const double *dphi, int rmax,
+                                    const double *r, const double *phi, const double *z,
+                                    int64_t n, int cellnumxy, const double *sum_cell,
+                                    const double *VC, int64_t ncell, double FN,
+                                    double *density);
+
 /* electricmagneticfield6.m:1-188.  Species arrays are device, column-major
  * with leading dimension equal to their count (n x 3).  Positions arrive as
  * (r,phi,z) when GASATT_POS_IN_CYL is set (the reference convention) else
