@@ -63,7 +63,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                 "-lms", "50", "-i", str(self.device)], stdout=subprocess.PIPE,
                 stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -110,8 +110,8 @@ def make_sim(precision, device, rank, torch):
     w = WORKLOAD
     prec = _lib.FP32_SPLIT if precision == "fp32_split" else _lib.FP64
     cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=prec,
-                 capacity=4_000_000, seed=w["seed"] + 1000 * rank, sort_period=20)
-    parts = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=w["seed"] + 1000 * rank,
+                 capacity=4_000_000, seed=replica_seed(rank), sort_period=20)
+    parts = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=replica_seed(rank),
                    Rp=w["n_r"] * w["delta"])
     sim = Sim(cfg, device=device)
     sim.bind_stream()
@@ -241,6 +241,42 @@ def cpu_baseline(target_s=12.0):
                       f"(plain C FP64 oracle, OpenMP {threads} threads, FDTD included)"}
 
 
+class Ranks:
+    """The ranks of one run: independent replicas, one process per GPU.  Work
+    adds up over ranks; time is the slowest rank's.  Reductions go through the
+    process group on `device` ("cuda" with NCCL, "cpu" with gloo)."""
+
+    def __init__(self, dist=None, world=1, rank=0, device="cpu"):
+        self.dist, self.world, self.rank, self.device = dist, world, rank, device
+
+    def _reduce(self, x, op):
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x):
+        return self._reduce(x, self.dist.ReduceOp.MAX if self.world > 1 else None)
+
+    def sum(self, x):
+        return self._reduce(x, self.dist.ReduceOp.SUM if self.world > 1 else None)
+
+    def rate(self, units_local, ms_local):
+        """Whole-job rate: all ranks' units over the slowest rank's time."""
+        return self.sum(units_local) / (self.max(ms_local) / 1e3)
+
+
+def replica_seed(rank):
+    """Each rank simulates its own gas cell: the workload's seed offset by rank."""
+    return WORKLOAD["seed"] + 1000 * rank
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -252,24 +288,8 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    ranks = Ranks(dist, world, rank, "cuda")
+    barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
 
     flush_buf = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
@@ -325,11 +345,15 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
+    # DRAM bytes (read + write) of one k_pass32 launch from an ncu capture of
+    # this workload, scaled from the captured launch's electron count to this
+    # run's mean count (the traffic is per particle: state and id)
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "pass32_c2_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "k_pass32_c2_traffic.json")
     if os.path.exists(tp):
         try:
-            traffic = json.load(open(tp)).get("bytes_per_launch")
+            t = json.load(open(tp))
+            traffic = t["bytes_per_launch"] * f32["alive"] / t["particles"]
         except Exception:
             traffic = None
     line = {
