@@ -716,24 +716,34 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
     const int nwin = w.rows * ws;
     for (int i = threadIdx.x; i < nwin; i += kBlock) { win_r[i] = 0; win_z[i] = 0; }
     __syncthreads();
-    for (long long base = beg + (threadIdx.x & ~31); base < end; base += blockDim.x) {
+    // the next iteration's particle is loaded one iteration ahead, so its
+    // HBM latency overlaps the current particle's arithmetic
+    long long base = beg + (threadIdx.x & ~31);
+    uint4 An = make_uint4(kDead, 0, 0, 0);
+    float2 Bn = make_float2(0.f, 0.f);
+    uint64_t idn = 0;
+    if (base + lane < end) { An = S.a[base + lane]; Bn = S.b[base + lane]; idn = S.id[base + lane]; }
+    for (; base < end; base += blockDim.x) {
       const long long p = base + lane;
       bool act = p < end;
-      uint4 A = make_uint4(kDead, 0, 0, 0);
-      if (act) {
-        A = S.a[p];
-        act = A.x != kDead;
+      uint4 A = An;
+      const float2 Bc = Bn;
+      const uint64_t idc = idn;
+      {
+        const long long pn = p + blockDim.x;
+        An = make_uint4(kDead, 0, 0, 0);
+        if (pn < end) { An = S.a[pn]; Bn = S.b[pn]; idn = S.id[pn]; }
       }
+      if (!act) A = make_uint4(kDead, 0, 0, 0);
+      act = act && A.x != kDead;
       int ir = (int)(A.x & 0xFFFFu), iz = (int)(A.x >> 16);
       float fr = __uint_as_float(A.y), fz = __uint_as_float(A.z), ur = __uint_as_float(A.w);
       float ut = 0.f, uz = 0.f;
       bool cand = false;
       if (act) {
-        const float2 B = S.b[p];
+        const float2 B = Bc;
         ut = B.x; uz = B.y;
-        // block 0 of this particle's stream: words 0-1 decide the null-collision
-        // candidate, words 2-3 (mixed) drive the stochastic rounding
-        const uint64_t id = S.id[p];
+        const uint64_t id = idc;
         uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
         bool alive = true;
         if (mode == 1) {
