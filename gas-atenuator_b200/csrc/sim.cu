@@ -1,12 +1,18 @@
 // sim.cu - the resident PIC-MCC simulation (the hot path).
 //
-// One step = FDTD sub-cycle (fields t^s -> t^{s+1}) followed by one fused
+// One step s = FDTD sub-cycle (fields t^s -> t^{s+1}) followed by one fused
 // particle pass:
-//   gather (EM4.cu:41-122) -> relativistic Boris kick -> half drift with the
-//   wall / end rules (EM4.cu:146-177) -> null-collision MCC against the
-//   tabulated N2 cross-sections (electron_transport.cu:64-227, corrected) with
-//   secondary birth -> half drift (EM2.cu:26-57) -> current deposit
-//   (EM7.cu:56-202) into 64-bit fixed point.
+//   gather (EM4.cu:41-122) -> relativistic Boris kick -> drift over the step
+//   with the wall / end rules (EM2.cu:26-57, EM4.cu:146-177) -> current
+//   deposit (EM7.cu:56-202) into 64-bit fixed point -> null-collision
+//   candidate test,
+// and then the null-collision MCC of the candidates against the tabulated N2
+// cross-sections (electron_transport.cu:64-227, corrected) with secondary
+// birth, at the end of the step (operator splitting: push, then collide, as
+// the reference's driver alternates its push and electron_collision calls).
+// That collision kernel touches neither fields nor current, so the step graph
+// runs it beside the next field update; observations of the state (read,
+// diagnostics, sort, end of a run) first apply any collisions still queued.
 // Particles never leave HBM; the per-step sequence is replayed from CUDA graphs.
 //
 // Two state forms:
@@ -17,13 +23,13 @@
 // subtraction run in FP64 in both forms.
 //
 // Deposit: each particle's four node contributions (q FN v w) are rounded to
-// integers first, so the grid sum is exact and independent of order; lanes of
-// a warp that hit the same four nodes (equal sort key) are summed with
+// integers first, so the grid sum is exact and independent of order.  FP32:
+// a shared-memory window per chunk of sorted particles; FP64: lanes of a warp
+// that hit the same four nodes (equal sort key) are summed with
 // __reduce_add_sync before one 64-bit atomic per node.
 //
-// The FP32 form drifts a particle that is not a collision candidate by the
-// whole step at once (the two half drifts of the reference joined); a
-// candidate stops at integer time and the collision kernel finishes it.
+// The FP32 form drifts the whole step at once (the reference's two half
+// drifts joined).
 #include <cub/device/device_scan.cuh>
 #include <cmath>
 #include <cstring>
@@ -41,14 +47,17 @@ constexpr int kMccBlock = 64;             // collision kernels: two warps per bl
 
 struct SimCounters {
   unsigned long long n_total;    // committed slots
-  unsigned long long n_births;   // slots claimed by births in the current pass
+  unsigned long long n_births;   // slots claimed by births since the last pass
   unsigned long long ion, ela, exc, nul, lost, cap_overflow;
-  long long step;                // index of the current particle pass
+  long long step;                // index of the next particle pass
   unsigned long long sorted_total;
   unsigned long long kin_fx;     // diagnostic: sum E_kin * 2^16 [eV]
   unsigned long long alive;      // diagnostic
   unsigned long long cap;        // slot capacity
-  unsigned long long n_cand;     // collision candidates queued by the current pass
+  unsigned long long n_cand[2];  // collision candidates queued, per queue parity
+  long long cand_step[2];        // the pass that queued them
+  int uncommitted;               // a pass ran since the last commit (k_commit)
+  int pad_;
 };
 
 // slots holding particles, including births of the last pass not yet committed
@@ -279,14 +288,33 @@ __device__ __forceinline__ void count_event(SimCounters *cnt, int ev) {
 }
 
 // warp-aggregated append of candidate slots to the collision queue
-__device__ __forceinline__ void queue_push(bool want, long long p, SimCounters *cnt, int *queue) {
+__device__ __forceinline__ void queue_push(bool want, long long p, unsigned long long *n_cand,
+                                           int *queue) {
   const unsigned m = __ballot_sync(0xFFFFFFFFu, want);
   if (!m) return;
   const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
   unsigned long long base = 0;
-  if (lane == leader) base = atomicAdd(&cnt->n_cand, (unsigned long long)__popc(m));
+  if (lane == leader) base = atomicAdd(n_cand, (unsigned long long)__popc(m));
   base = __shfl_sync(0xFFFFFFFFu, base, leader);
   if (want) queue[base + __popc(m & ((1u << lane) - 1))] = (int)p;
+}
+
+// Commit of a particle pass (parity q), run as its own one-thread kernel after
+// the pass: the births of the collision kernel that ran before the pass join
+// the committed slots, the queue of the pass is labelled with its step, the
+// other queue (consumed by that collision kernel) is emptied, and the step
+// advances.  Idempotent: only the first commit after a pass does anything.
+// (Done at the end of the pass itself, by its last block, the atomics of 592
+// blocks on the counters' cache line slowed the pass by a tenth.)
+__global__ void k_commit(SimCounters *cnt, int q) {
+  if (!cnt->uncommitted) return;
+  const unsigned long long nt = cnt->n_total + cnt->n_births;
+  cnt->n_total = nt < cnt->cap ? nt : cnt->cap;
+  cnt->n_births = 0;
+  cnt->cand_step[q] = cnt->step;
+  cnt->n_cand[1 - q] = 0;
+  cnt->step += 1;
+  cnt->uncommitted = 0;
 }
 
 // ------------------------------------------------------ deposit
@@ -383,14 +411,17 @@ __device__ __forceinline__ void deposit_values64(const SimParams &P, double r, d
   }
 }
 
-// mode 0: full pass (collision candidates go to the queue and are finished by
-// k_mcc64); mode 1: half drift + deposit only (start of a run); mode 2: kick
-// + half drift only, ending at integer time (end of a run)
+// mode 0: full step - kick, drift (two half drifts), deposit; collision
+// candidates go to queue q for k_mcc64; mode 1: half drift + deposit only
+// (start of a run); mode 2: kick + half drift only, ending at integer time
+// (end of a run)
 __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fields<double> F,
-                                                      SimCounters *cnt, int *queue, int mode) {
-  const long long n0 = (long long)cnt->n_total;
+                                                      SimCounters *cnt, int *queue, int mode,
+                                                      int q) {
+  const long long n0 = slots_in_use(cnt);
   const long long step = cnt->step;
   const int lane = threadIdx.x & 31;
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->uncommitted = 1;
   // each block takes a contiguous chunk of the (cell-sorted) particles, so its
   // field reads stay in a narrow band of grid rows
   const long long chunk = (n0 + gridDim.x - 1) / gridDim.x;
@@ -416,15 +447,15 @@ __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fi
         const double B = P.mu0 * Hp;
         boris(ur, ut, uz, E_r, 0.0, E_z, 0.0, B, 0.0, P.qm_dt2, P.c);
         halfdrift64(r, z, ur, ut, uz, alive, P);
-        if (alive && mode == 0) cand = null_candidate(P, S.id[p], step);
       }
-      if (alive && mode != 2 && !cand) halfdrift64(r, z, ur, ut, uz, alive, P);
+      if (alive && mode != 2) halfdrift64(r, z, ur, ut, uz, alive, P);
+      if (alive && mode == 0) cand = null_candidate(P, S.id[p], step);
       if (!alive) { lost++; r = -1.0; }
       rz = make_double2(r, z); urt = make_double2(ur, ut);
       S.rz[p] = rz; S.urt[p] = urt; S.uz[p] = uz;
-      act = alive && mode != 2 && !cand;
+      act = alive && mode != 2;
     }
-    queue_push(cand, p, cnt, queue);
+    queue_push(cand, p, &cnt->n_cand[q], queue + (long long)q * P.cap);
     int64_t a[4] = {0, 0, 0, 0};
     long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
     unsigned key = 0;
@@ -435,56 +466,41 @@ __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fi
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
 }
 
-// collision candidates of this step: MCC, births, second half drift, deposit
+// The collisions of the pass that filled queue q, at the end of its step
+// (after the drift and the deposit): the MCC changes the velocity, and an
+// ionization appends its secondary at the parent's position.  Nothing here
+// reads or writes the fields or the current, so it can run beside the next
+// field update.
 __global__ void __launch_bounds__(kMccBlock) k_mcc64(SimParams P, State64 S, SimCounters *cnt,
-                                                     const int *queue) {
+                                                     const int *queue, int q) {
   // one candidate per warp (lane 0): the collision branches differ a lot in
   // length, and lanes on different branches would run them one after another
   if ((threadIdx.x & 31) != 0) return;
   const long long n0 = (long long)cnt->n_total;
-  const long long step = cnt->step;
-  const long long nq = (long long)cnt->n_cand;
+  const long long step = cnt->cand_step[q];
+  const long long nq = (long long)cnt->n_cand[q];
+  const int *qu = queue + (long long)q * P.cap;
   const long long nwarps = (long long)gridDim.x * (kMccBlock / 32);
-  for (long long q = (blockIdx.x * (long long)kMccBlock + threadIdx.x) >> 5; q < nq; q += nwarps) {
-    const long long p = queue[q];
-    double2 rz = S.rz[p], urt = S.urt[p];
-    double r = rz.x, z = rz.y, ur = urt.x, ut = urt.y, uz = S.uz[p];
+  for (long long k = (blockIdx.x * (long long)kMccBlock + threadIdx.x) >> 5; k < nq; k += nwarps) {
+    const long long p = qu[k];
+    const double2 rz = S.rz[p], urt = S.urt[p];
+    double ur = urt.x, ut = urt.y, uz = S.uz[p];
     const uint64_t id = S.id[p];
     Birth b;
     count_event(cnt, mcc_event<false>(P, id, step, ur, ut, uz, b));
     if (b.born) {
-      const unsigned long long k = atomicAdd(&cnt->n_births, 1ull);
-      const long long slot = n0 + (long long)k;
+      const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
+      const long long slot = n0 + (long long)kb;
       if (slot < P.cap) {
-        double cr = r, cz = z, cur = b.ux, cut = b.uy, cuz = b.uz;
-        bool calive = true;
-        halfdrift64(cr, cz, cur, cut, cuz, calive, P);
-        if (calive) {
-          int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
-          deposit_values64(P, cr, cz, cur, cut, cuz, a, vr, vz, kk);
-          deposit_direct(a, vr, vz, P);
-        } else {
-          atomicAdd(&cnt->lost, 1ull);
-        }
-        S.rz[slot] = make_double2(calive ? cr : -1.0, cz);
-        S.urt[slot] = make_double2(cur, cut);
-        S.uz[slot] = cuz;
+        S.rz[slot] = rz;
+        S.urt[slot] = make_double2(b.ux, b.uy);
+        S.uz[slot] = b.uz;
         S.id[slot] = child_id(id, step);
       } else {
         atomicAdd(&cnt->cap_overflow, 1ull);
       }
     }
-    bool alive = true;
-    halfdrift64(r, z, ur, ut, uz, alive, P);
-    if (alive) {
-      int64_t a[4]; long long vr[4], vz[4]; unsigned kk;
-      deposit_values64(P, r, z, ur, ut, uz, a, vr, vz, kk);
-      deposit_direct(a, vr, vz, P);
-    } else {
-      atomicAdd(&cnt->lost, 1ull);
-      r = -1.0;
-    }
-    S.rz[p] = make_double2(r, z); S.urt[p] = make_double2(ur, ut); S.uz[p] = uz;
+    S.urt[p] = make_double2(ur, ut); S.uz[p] = uz;
   }
 }
 
@@ -631,17 +647,6 @@ __device__ __forceinline__ void deposit_nodes32(const SimParams &P, int ir, int 
   }
 }
 
-__device__ __forceinline__ void deposit_values32(const SimParams &P, int ir, int iz, float fr,
-                                                 float fz, float ur, float ut, float uz,
-                                                 int64_t a[4], int vr[4], int vz[4],
-                                                 unsigned &key) {
-  int ca, cb, ra, rb;
-  deposit_nodes32(P, ir, iz, fr, fz, ur, ut, uz, ca, cb, ra, rb, vr, vz);
-  a[0] = ca + (int64_t)ra * P.nr; a[1] = cb + (int64_t)ra * P.nr;
-  a[2] = ca + (int64_t)rb * P.nr; a[3] = cb + (int64_t)rb * P.nr;
-  key = 0;
-}
-
 // FP32-form deposit window: int32 sums of one chunk of particles on the grid
 // rows [row0, row0 + rows) in shared memory.  A chunk holds at most kChunk
 // particles, so a node's window sum stays below kChunk * 2^20 < 2^31.  Rows
@@ -678,13 +683,16 @@ __device__ __forceinline__ uint4 pack32(int ir, int iz, float fr, float fz, floa
                     __float_as_uint(fz), __float_as_uint(ur));
 }
 
+// FP32 particle pass; modes as k_pass64 (mode 0 drifts the whole step at once)
 __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fields<float> F,
-                                                      SimCounters *cnt, int *queue, int mode) {
+                                                      SimCounters *cnt, int *queue, int mode,
+                                                      int q) {
   __shared__ int win_r[kWinNodes], win_z[kWinNodes];
   __shared__ int win_row0, win_rows;
-  const long long n0 = (long long)cnt->n_total;
+  const long long n0 = slots_in_use(cnt);
   const long long step = cnt->step;
   const int lane = threadIdx.x & 31;
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->uncommitted = 1;
   const int ws = win_stride(P.nr);
   const int maxrows = min(kWinNodes / ws, P.nz);
   // every block takes the same number of consecutive chunks of the
@@ -773,19 +781,19 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
           const float upr = fmaf(-umz, t, umr), upz = fmaf(umr, t, umz);
           ur = sround_add(ur, fmaf(-upz, s, 2.f * her), rb0);
           uz = sround_add(uz, fmaf(upr, s, 2.f * hez), rb0 >> 16);
-          // a collision candidate stops at integer time (k_mcc32 finishes it);
-          // the others drift the whole step
-          const bool c0 = mode == 0 && (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
-          const float h = (mode == 0 && !c0) ? 2.f : 1.f;
+          // the whole step (mode 0) or a half step to integer time (mode 2);
+          // a collision candidate is queued for k_mcc32 at the end of the step
+          const float h = mode == 0 ? 2.f : 1.f;
           drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, h * P.hdr, h * P.hdz);
-          cand = alive && c0;
+          cand = alive && mode == 0 &&
+                 (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
         }
         if (!alive) lost++;
         S.a[p] = pack32(ir, iz, fr, fz, ur, alive);
         S.b[p] = make_float2(ut, uz);
-        act = alive && mode != 2 && !cand;
+        act = alive && mode != 2;
       }
-      queue_push(cand, p, cnt, queue);
+      queue_push(cand, p, &cnt->n_cand[q], queue + (long long)q * P.cap);
       if (act) {
         int ca, cb, ra, rb, vr[4], vz[4];
         deposit_nodes32(P, ir, iz, fr, fz, ur, ut, uz, ca, cb, ra, rb, vr, vz);
@@ -820,84 +828,48 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
 }
 
+// FP32 form of k_mcc64
 __global__ void __launch_bounds__(kMccBlock) k_mcc32(SimParams P, State32 S, SimCounters *cnt,
-                                                     const int *queue) {
-  // one candidate per warp (lane 0): the collision branches differ a lot in
-  // length, and lanes on different branches would run them one after another
+                                                     const int *queue, int q) {
   if ((threadIdx.x & 31) != 0) return;
   const long long n0 = (long long)cnt->n_total;
-  const long long step = cnt->step;
-  const long long nq = (long long)cnt->n_cand;
+  const long long step = cnt->cand_step[q];
+  const long long nq = (long long)cnt->n_cand[q];
+  const int *qu = queue + (long long)q * P.cap;
   const long long nwarps = (long long)gridDim.x * (kMccBlock / 32);
-  for (long long q = (blockIdx.x * (long long)kMccBlock + threadIdx.x) >> 5; q < nq; q += nwarps) {
-    const long long p = queue[q];
+  for (long long k = (blockIdx.x * (long long)kMccBlock + threadIdx.x) >> 5; k < nq; k += nwarps) {
+    const long long p = qu[k];
     const uint4 A = S.a[p];
     const float2 B = S.b[p];
-    int ir = (int)(A.x & 0xFFFFu), iz = (int)(A.x >> 16);
-    float fr = __uint_as_float(A.y), fz = __uint_as_float(A.z);
     double dux = (double)__uint_as_float(A.w) * P.c, duy = (double)B.x * P.c, duz = (double)B.y * P.c;
     const uint64_t id = S.id[p];
     Birth b;
     count_event(cnt, mcc_event<true>(P, id, step, dux, duy, duz, b));
-    float ur = (float)(dux / P.c), ut = (float)(duy / P.c), uz = (float)(duz / P.c);
     if (b.born) {
-      const unsigned long long k = atomicAdd(&cnt->n_births, 1ull);
-      const long long slot = n0 + (long long)k;
+      const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
+      const long long slot = n0 + (long long)kb;
       if (slot < P.cap) {
-        int cir = ir, ciz = iz;
-        float cfr = fr, cfz = fz;
-        float cur = (float)(b.ux / P.c), cut = (float)(b.uy / P.c), cuz = (float)(b.uz / P.c);
-        bool calive = true;
-        drift32(cir, ciz, cfr, cfz, cur, cut, cuz, calive, P,
-                mix32((uint32_t)(id ^ (id >> 32)) ^ 0xA5A5A5A5u ^ (uint32_t)step), P.hdr, P.hdz);
-        if (calive) {
-          int64_t a[4]; int vr[4], vz[4]; unsigned kk;
-          deposit_values32(P, cir, ciz, cfr, cfz, cur, cut, cuz, a, vr, vz, kk);
-          deposit_direct(a, vr, vz, P);
-        } else {
-          atomicAdd(&cnt->lost, 1ull);
-        }
-        S.a[slot] = pack32(cir, ciz, cfr, cfz, cur, calive);
-        S.b[slot] = make_float2(cut, cuz);
+        S.a[slot] = make_uint4(A.x, A.y, A.z, __float_as_uint((float)(b.ux / P.c)));
+        S.b[slot] = make_float2((float)(b.uy / P.c), (float)(b.uz / P.c));
         S.id[slot] = child_id(id, step);
       } else {
         atomicAdd(&cnt->cap_overflow, 1ull);
       }
     }
-    bool alive = true;
-    drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, mix32((uint32_t)(id ^ (id >> 32)) ^ (uint32_t)step),
-            P.hdr, P.hdz);
-    if (alive) {
-      int64_t a[4]; int vr[4], vz[4]; unsigned kk;
-      deposit_values32(P, ir, iz, fr, fz, ur, ut, uz, a, vr, vz, kk);
-      deposit_direct(a, vr, vz, P);
-    } else {
-      atomicAdd(&cnt->lost, 1ull);
-    }
-    S.a[p] = pack32(ir, iz, fr, fz, ur, alive);
-    S.b[p] = make_float2(ut, uz);
+    S.a[p] = make_uint4(A.x, A.y, A.z, __float_as_uint((float)(dux / P.c)));
+    S.b[p] = make_float2((float)(duy / P.c), (float)(duz / P.c));
   }
 }
 
 // ------------------------------------------------------------- FDTD
-// One fused field sub-cycle per step (fdtd_tiled).  Block (0,0) also commits
-// the births of the previous particle pass, empties the collision queue and
-// advances the step index; no other block of this kernel reads them.
+// One fused field sub-cycle per step (fdtd_tiled).
 template <typename T>
 __global__ void __launch_bounds__(32 * kFdtdRows) k_sim_fdtd(T *Er, T *Ez, T *H, const unsigned long long *Jr,
                                                   const unsigned long long *Jz,
                                                   unsigned long long *Jr_next,
                                                   unsigned long long *Jz_next, int nr, int nz,
                                                   FdtdCoef c, const double *invV, double mu,
-                                                  double dt, int R, unsigned flags,
-                                                  SimCounters *cnt) {
-  if (cnt && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
-    const unsigned long long nt = cnt->n_total + cnt->n_births;
-    cnt->n_total = nt < cnt->cap ? nt : cnt->cap;
-    cnt->n_births = 0;
-    cnt->n_cand = 0;
-    cnt->step += 1;
-  }
+                                                  double dt, int R, unsigned flags) {
   fdtd_tiled<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, c, invV, mu, dt, R, flags);
 }
 
@@ -1136,9 +1108,12 @@ struct gasatt_sim {
   cudaGraphExec_t g_sort[2] = {nullptr, nullptr};
   double scale = 1.0;
   unsigned pass_grid = 0, mcc_grid = 0;
-  int *queue = nullptr;           // collision candidates of the current pass
+  int *queue = nullptr;           // collision candidates, two queues of capacity slots
+  bool mcc_pending = false;       // the last pass's collisions are not applied yet
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;   // graph capture fork/join
   bool timing = false;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // before FDTD, pass, collision kernel, end
+  // field update start/end, particle pass start/end, collision kernel start/end
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -1177,20 +1152,20 @@ int launch_fdtd(gasatt_sim *s, cudaStream_t st, int q) {
   if (s->form == 0)
     k_sim_fdtd<double><<<grid, block, 0, st>>>(
         (double *)s->Er, (double *)s->Ez, (double *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
-        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt);
+        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags);
   else
     k_sim_fdtd<float><<<grid, block, 0, st>>>(
         (float *)s->Er, (float *)s->Ez, (float *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
-        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt);
+        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags);
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "fdtd launch");
   return GASATT_OK;
 }
 
-// particle pass; a full pass (mode 0) is followed by the collision kernel
-// that finishes the queued candidates
-int launch_pass(gasatt_sim *s, cudaStream_t st, int mode, int jb, cudaEvent_t mid = nullptr) {
+// particle pass; its collision candidates (mode 0) go to queue q, its
+// current to buffer jb
+int launch_pass(gasatt_sim *s, cudaStream_t st, int mode, int jb, int q) {
   SimParams P = s->P;
   P.Jr = s->Jr[jb];
   P.Jz = s->Jz[jb];
@@ -1198,23 +1173,51 @@ int launch_pass(gasatt_sim *s, cudaStream_t st, int mode, int jb, cudaEvent_t mi
   if (s->form == 0)
     k_pass64<<<s->pass_grid, kBlock, 0, st>>>(P, s->s64[b],
                                               Fields<double>{(double *)s->Er, (double *)s->Ez, (double *)s->H},
-                                              s->cnt, s->queue, mode);
+                                              s->cnt, s->queue, mode, q);
   else
     k_pass32<<<s->pass_grid, kBlock, 0, st>>>(P, s->s32[b],
                                               Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H},
-                                              s->cnt, s->queue, mode);
+                                              s->cnt, s->queue, mode, q);
   s->ctx->launches++;
-  if (mid) {
-    cudaError_t e = cudaEventRecordWithFlags(mid, st, cudaEventRecordExternal);
-    if (e != cudaSuccess) return cuda_fail(s->ctx, e, "event");
-  }
-  if (mode == 0) {
-    if (s->form == 0) k_mcc64<<<s->mcc_grid, kMccBlock, 0, st>>>(P, s->s64[b], s->cnt, s->queue);
-    else k_mcc32<<<s->mcc_grid, kMccBlock, 0, st>>>(P, s->s32[b], s->cnt, s->queue);
-    s->ctx->launches++;
-  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "particle pass launch");
+  return GASATT_OK;
+}
+
+// the commit of the last pass (its parity q)
+int launch_commit(gasatt_sim *s, cudaStream_t st, int q) {
+  k_commit<<<1, 1, 0, st>>>(s->cnt, q);
+  s->ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(s->ctx, e, "commit launch");
+  return GASATT_OK;
+}
+
+// the collisions queued (parity q) by the last pass that used that parity
+int launch_mcc(gasatt_sim *s, cudaStream_t st, int q) {
+  const int b = s->cur;
+  if (s->form == 0)
+    k_mcc64<<<s->mcc_grid, kMccBlock, 0, st>>>(s->P, s->s64[b], s->cnt, s->queue, q);
+  else
+    k_mcc32<<<s->mcc_grid, kMccBlock, 0, st>>>(s->P, s->s32[b], s->cnt, s->queue, q);
+  s->ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(s->ctx, e, "collision launch");
+  return GASATT_OK;
+}
+
+// Apply the collisions still queued by the last pass, so that the particle
+// state and the counters are complete (before a sort, a read, diagnostics or
+// the end of a run).  The queue is emptied afterwards, so the collision kernel
+// of the next step graph finds nothing to redo.
+int flush_collisions(gasatt_sim *s) {
+  if (!s->mcc_pending) return GASATT_OK;
+  const int q = (int)((s->host_step - 1) & 1);
+  cudaStream_t st = s->ctx->stream;
+  SIM_TRY(launch_commit(s, st, q));
+  SIM_TRY(launch_mcc(s, st, q));
+  GASATT_CUDA(s->ctx, cudaMemsetAsync(&s->cnt->n_cand[q], 0, sizeof(unsigned long long), st));
+  s->mcc_pending = false;
   return GASATT_OK;
 }
 
@@ -1258,40 +1261,70 @@ void drop_graphs(gasatt_sim *s) {
   }
 }
 
-// capture one step (FDTD + pass) for state buffer b, and one sort b -> 1-b
+// Capture one step for state buffer b and step parity q:
+//
+//    [field update of step s]  ||  [collisions queued by pass s-1 (parity 1-q)]
+//                      \\               /
+//                   [particle pass s: kick, drift, deposit, queue q]
+//
+// The field update needs only the current of pass s-1 and the collisions only
+// the particles, so the two run side by side.  Also one sort b -> 1-b.
 int build_graphs(gasatt_sim *s) {
-  cudaStream_t cs;
-  GASATT_CUDA(s->ctx, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  // the field update goes on a higher-priority stream than the collision
+  // branch, so its blocks are placed first when both are ready
+  int lo_prio = 0, hi_prio = 0;
+  cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+  cudaStream_t cs, side;
+  GASATT_CUDA(s->ctx, cudaStreamCreateWithPriority(&cs, cudaStreamNonBlocking, hi_prio));
+  GASATT_CUDA(s->ctx, cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, lo_prio));
   const int save = s->cur;
   const int64_t save_launch = s->ctx->launches;
-  for (int b = 0; b < 2; ++b) {
+  int rc = GASATT_OK;
+  for (int b = 0; b < 2 && !rc; ++b) {
     cudaGraph_t g;
     s->cur = b;
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < 2 && !rc; ++q) {
       GASATT_CUDA(s->ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-      if (s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[0], cs, cudaEventRecordExternal));
-      int rc = launch_fdtd(s, cs, q);
-      if (!rc && s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[1], cs, cudaEventRecordExternal));
-      if (!rc) rc = launch_pass(s, cs, 0, 1 - q, s->timing ? s->ev[2] : nullptr);
-      if (!rc && s->timing) GASATT_CUDA(s->ctx, cudaEventRecordWithFlags(s->ev[3], cs, cudaEventRecordExternal));
-      cudaError_t e = cudaStreamEndCapture(cs, &g);
-      if (rc) return rc;
-      if (e != cudaSuccess) return cuda_fail(s->ctx, e, "capture step");
-      GASATT_CUDA(s->ctx, cudaGraphInstantiate(&s->g_step[b][q], g, 0));
-      cudaGraphDestroy(g);
+      cudaError_t e = cudaEventRecord(s->fork_ev, cs);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(side, s->fork_ev, 0);
+      if (e == cudaSuccess && s->timing) e = cudaEventRecordWithFlags(s->ev[4], side, cudaEventRecordExternal);
+      if (e == cudaSuccess) rc = launch_commit(s, side, 1 - q);
+      if (e == cudaSuccess && !rc) rc = launch_mcc(s, side, 1 - q);
+      if (e == cudaSuccess && !rc && s->timing) e = cudaEventRecordWithFlags(s->ev[5], side, cudaEventRecordExternal);
+      if (e == cudaSuccess && !rc) e = cudaEventRecord(s->join_ev, side);
+      if (e == cudaSuccess && !rc && s->timing) e = cudaEventRecordWithFlags(s->ev[0], cs, cudaEventRecordExternal);
+      if (e == cudaSuccess && !rc) rc = launch_fdtd(s, cs, q);
+      if (e == cudaSuccess && !rc && s->timing) e = cudaEventRecordWithFlags(s->ev[1], cs, cudaEventRecordExternal);
+      if (e == cudaSuccess && !rc) e = cudaStreamWaitEvent(cs, s->join_ev, 0);
+      if (e == cudaSuccess && !rc && s->timing) e = cudaEventRecordWithFlags(s->ev[2], cs, cudaEventRecordExternal);
+      if (e == cudaSuccess && !rc) rc = launch_pass(s, cs, 0, 1 - q, q);
+      if (e == cudaSuccess && !rc && s->timing) e = cudaEventRecordWithFlags(s->ev[3], cs, cudaEventRecordExternal);
+      cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+      if (!rc && e != cudaSuccess) rc = cuda_fail(s->ctx, e, "capture step");
+      if (!rc && e2 != cudaSuccess) rc = cuda_fail(s->ctx, e2, "capture step");
+      if (!rc) {
+        e = cudaGraphInstantiate(&s->g_step[b][q], g, 0);
+        if (e != cudaSuccess) rc = cuda_fail(s->ctx, e, "instantiate step");
+      }
+      if (e2 == cudaSuccess) cudaGraphDestroy(g);
     }
+    if (rc) break;
     GASATT_CUDA(s->ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    int rc = launch_sort(s, cs, b);
+    rc = launch_sort(s, cs, b);
     cudaError_t e = cudaStreamEndCapture(cs, &g);
-    if (rc) return rc;
-    if (e != cudaSuccess) return cuda_fail(s->ctx, e, "capture sort");
-    GASATT_CUDA(s->ctx, cudaGraphInstantiate(&s->g_sort[b], g, 0));
-    cudaGraphDestroy(g);
+    const bool captured = e == cudaSuccess;
+    if (!rc && !captured) rc = cuda_fail(s->ctx, e, "capture sort");
+    if (!rc) {
+      e = cudaGraphInstantiate(&s->g_sort[b], g, 0);
+      if (e != cudaSuccess) rc = cuda_fail(s->ctx, e, "instantiate sort");
+    }
+    if (captured) cudaGraphDestroy(g);
   }
   s->cur = save;
   s->ctx->launches = save_launch;
+  cudaStreamDestroy(side);
   cudaStreamDestroy(cs);
-  return GASATT_OK;
+  return rc;
 }
 
 }  // namespace
@@ -1358,7 +1391,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
         return cleanup(rc);
     }
   }
-  if ((rc = sim_alloc(s, &s->queue, cap))) return cleanup(rc);
+  if ((rc = sim_alloc(s, &s->queue, 2 * (size_t)cap))) return cleanup(rc);
   const size_t esz = s->form == 0 ? 8 : 4;
   double *tmpd;
   if ((rc = sim_alloc(s, (char **)&s->Er, (size_t)nr * (nz + 1) * esz)) ||
@@ -1453,8 +1486,11 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
     cudaMemset(s->Jr[q], 0, (size_t)ncell * 8);
     cudaMemset(s->Jz[q], 0, (size_t)ncell * 8);
   }
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 6; ++i)
     if (cudaEventCreate(&s->ev[i]) != cudaSuccess) return cleanup(fail(ctx, GASATT_E_CUDA, "event"));
+  if (cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming) != cudaSuccess)
+    return cleanup(fail(ctx, GASATT_E_CUDA, "event"));
   rc = build_graphs(s);
   if (rc) return cleanup(rc);
   if (cudaDeviceSynchronize() != cudaSuccess) return cleanup(fail(ctx, GASATT_E_CUDA, "sim init"));
@@ -1467,8 +1503,10 @@ int gasatt_sim_destroy(gasatt_sim *s) {
   cudaSetDevice(s->ctx->device);
   cudaDeviceSynchronize();
   drop_graphs(s);
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 6; ++i)
     if (s->ev[i]) cudaEventDestroy(s->ev[i]);
+  if (s->fork_ev) cudaEventDestroy(s->fork_ev);
+  if (s->join_ev) cudaEventDestroy(s->join_ev);
   for (void *p : s->allocs) cudaFree(p);
   if (s->h_cnt) cudaFreeHost(s->h_cnt);
   delete s;
@@ -1519,6 +1557,7 @@ int gasatt_sim_load(gasatt_sim *s, const double *r, const double *z, const doubl
   }
   GASATT_CUDA(ctx, cudaStreamSynchronize(st));
   s->primed = false;
+  s->mcc_pending = false;
   s->host_step = 0;
   s->since_sort = 0;
   return GASATT_OK;
@@ -1530,6 +1569,7 @@ int gasatt_sim_read(gasatt_sim *s, double *r, double *z, double *ur, double *ut,
   gasatt_ctx *ctx = s->ctx;
   GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
+  SIM_TRY(flush_collisions(s));
   GASATT_CUDA(ctx, cudaMemcpyAsync(s->h_cnt, s->cnt, sizeof(SimCounters), cudaMemcpyDeviceToHost, st));
   GASATT_CUDA(ctx, cudaStreamSynchronize(st));
   const unsigned long long nt = s->h_cnt->n_total + s->h_cnt->n_births;
@@ -1656,6 +1696,7 @@ int gasatt_sim_sort(gasatt_sim *s) {
   if (!s) return GASATT_E_ARG;
   gasatt_ctx *ctx = s->ctx;
   GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  SIM_TRY(flush_collisions(s));            // the queue holds slot indices
   GASATT_CUDA(ctx, cudaGraphLaunch(s->g_sort[s->cur], ctx->stream));
   ctx->launches += 4;
   s->cur = 1 - s->cur;
@@ -1670,17 +1711,20 @@ int gasatt_sim_step(gasatt_sim *s, int nsteps) {
   cudaStream_t st = ctx->stream;
   if (!s->primed) {
     // start of a run: particles at x^0 move to x^{1/2} and deposit j^{1/2}
+    // (no collision candidates; queue parity 1 is the one step 0 reads)
     if (s->cfg.sort_period > 0) SIM_TRY(gasatt_sim_sort(s));
-    SIM_TRY(launch_pass(s, st, 1, 0));
+    SIM_TRY(launch_pass(s, st, 1, 0, 1));
+    SIM_TRY(launch_commit(s, st, 1));
     s->primed = true;
   }
-  const int per_step = 3;   // field update, particle pass, collision kernel
+  const int per_step = 4;   // field update, commit, collision kernel, particle pass
   for (int k = 0; k < nsteps; ++k) {
     if (s->cfg.sort_period > 0 && s->since_sort >= s->cfg.sort_period) SIM_TRY(gasatt_sim_sort(s));
     GASATT_CUDA(ctx, cudaGraphLaunch(s->g_step[s->cur][s->host_step & 1], st));
     ctx->launches += per_step;
     s->host_step++;
     s->since_sort++;
+    s->mcc_pending = true;
   }
   return GASATT_OK;
 }
@@ -1690,6 +1734,7 @@ int gasatt_sim_diag(gasatt_sim *s, gasatt_diag *d) {
   gasatt_ctx *ctx = s->ctx;
   GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
+  SIM_TRY(flush_collisions(s));
   GASATT_CUDA(ctx, cudaMemsetAsync((char *)s->cnt + offsetof(SimCounters, kin_fx), 0, 16, st));
   if (s->form == 0) k_diag<0><<<s->pass_grid, kBlock, 0, st>>>(s->s64[s->cur], s->s32[s->cur], s->cnt, s->cfg.c, s->cfg.m_e, s->cfg.q_e);
   else k_diag<1><<<s->pass_grid, kBlock, 0, st>>>(s->s64[s->cur], s->s32[s->cur], s->cnt, s->cfg.c, s->cfg.m_e, s->cfg.q_e);
@@ -1726,6 +1771,7 @@ int gasatt_sim_counts(gasatt_sim *s, int64_t *n_slots, int64_t *n_ion, int64_t *
   if (!s) return GASATT_E_ARG;
   gasatt_ctx *ctx = s->ctx;
   GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  SIM_TRY(flush_collisions(s));
   GASATT_CUDA(ctx, cudaMemcpyAsync(s->h_cnt, s->cnt, sizeof(SimCounters), cudaMemcpyDeviceToHost, ctx->stream));
   GASATT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const SimCounters &h = *s->h_cnt;
@@ -1752,8 +1798,8 @@ int gasatt_sim_last_timing(gasatt_sim *s, float *fdtd_ms, float *pass_ms, float 
   GASATT_CUDA(s->ctx, cudaEventSynchronize(s->ev[3]));
   float a = 0, b = 0, m = 0;
   GASATT_CUDA(s->ctx, cudaEventElapsedTime(&a, s->ev[0], s->ev[1]));
-  GASATT_CUDA(s->ctx, cudaEventElapsedTime(&b, s->ev[1], s->ev[2]));
-  GASATT_CUDA(s->ctx, cudaEventElapsedTime(&m, s->ev[2], s->ev[3]));
+  GASATT_CUDA(s->ctx, cudaEventElapsedTime(&b, s->ev[2], s->ev[3]));
+  GASATT_CUDA(s->ctx, cudaEventElapsedTime(&m, s->ev[4], s->ev[5]));
   if (fdtd_ms) *fdtd_ms = a;
   if (pass_ms) *pass_ms = b;
   if (mcc_ms) *mcc_ms = m;
@@ -1833,18 +1879,24 @@ int gasatt_sim_run_host(gasatt_sim *s, double *pos, double *vel, int64_t *n_io, 
   SimCounters h = *s->h_cnt;
   h.n_total = (unsigned long long)n;
   h.n_births = 0;
+  h.n_cand[0] = h.n_cand[1] = 0;
+  h.uncommitted = 0;
   GASATT_CUDA(ctx, cudaMemcpyAsync(s->cnt, &h, sizeof(h), cudaMemcpyHostToDevice, st));
   for (int q = 0; q < 2; ++q) {
     GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
     GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
   }
   s->primed = false;
+  s->mcc_pending = false;
   s->host_step = 0;                          // the prologue deposits into buffer 0
   s->since_sort = s->cfg.sort_period;       // sort the fresh population first
   SIM_TRY(gasatt_sim_step(s, nsteps - 1));
-  // last step: fields, then a push that ends at integer time
+  // last step: the pending collisions, the fields, then a push that ends at
+  // integer time
+  SIM_TRY(flush_collisions(s));
   SIM_TRY(launch_fdtd(s, st, (int)(s->host_step & 1)));
-  SIM_TRY(launch_pass(s, st, 2, (int)((s->host_step + 1) & 1)));
+  SIM_TRY(launch_pass(s, st, 2, (int)((s->host_step + 1) & 1), (int)(s->host_step & 1)));
+  SIM_TRY(launch_commit(s, st, (int)(s->host_step & 1)));
   SIM_TRY(gasatt_sim_sort(s));               // compacts away the dead
   s->host_step++;
   s->primed = false;

@@ -287,7 +287,10 @@ int gasatt_sim_get_fields(gasatt_sim *sim, double *Er, double *Ez, double *Hphi,
                           int on_device);
 /* current density [A/m^2] deposited by the last particle pass (n_r x n_z each) */
 int gasatt_sim_get_current(gasatt_sim *sim, double *jr, double *jz, int on_device);
-/* advance nsteps steps of push + MCC + deposit + FDTD (captured in a CUDA graph) */
+/* advance nsteps steps of FDTD + push + deposit + MCC (replayed from CUDA
+ * graphs).  The collisions of a step are applied at its end; the library may
+ * defer them into the next step's graph, and every call that observes the
+ * particles (read, diag, counts, sort, run_host) applies them first. */
 int gasatt_sim_step(gasatt_sim *sim, int nsteps);
 /* cell re-sort + compaction of dead slots now */
 int gasatt_sim_sort(gasatt_sim *sim);
@@ -310,7 +313,8 @@ int gasatt_sim_counts(gasatt_sim *sim, int64_t *n_slots, int64_t *n_ionizations,
                       int64_t *n_lost);
 /* device-side phase timing: with timing enabled the step graphs record CUDA
  * events around the field sub-cycle, the particle pass and the collision
- * kernel; last_timing gives their durations in the most recent step (ms) */
+ * branch (commit + collision kernel, which runs beside the field sub-cycle);
+ * last_timing gives their durations in the most recent step (ms) */
 int gasatt_sim_enable_timing(gasatt_sim *sim, int enable);
 int gasatt_sim_last_timing(gasatt_sim *sim, float *fdtd_ms, float *pass_ms, float *mcc_ms);
 

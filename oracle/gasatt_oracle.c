@@ -1022,6 +1022,9 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
         halfdrift_u(&x[p], &y[p], &z[p], &ux[p], &uy[p], &uz[p], &alive[p], cfg, Rp, Lp);
         if (!alive[p]) { C->lost++; continue; }
       }
+      halfdrift_u(&x[p], &y[p], &z[p], &ux[p], &uy[p], &uz[p], &alive[p], cfg, Rp, Lp);
+      if (!alive[p]) { C->lost++; continue; }
+      deposit_u(x[p], y[p], z[p], ux[p], uy[p], uz[p], cfg, tjr, tjz);
       if (do_mcc) {
         double U1, U2;
         draw_block(cfg->seed, id[p], step, 0, &U1, &U2);
@@ -1066,11 +1069,7 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
             if (cfg->secondaries) {
               double s[6] = {x[p], y[p], z[p], ix * us, iy * us, iz_ * us};
               rotate_v(&s[3], &s[4], &s[5], th_s, phi_s, 0);
-              uint8_t ca = 1;
-              halfdrift_u(&s[0], &s[1], &s[2], &s[3], &s[4], &s[5], &ca, cfg, Rp, Lp);
-              if (ca) deposit_u(s[0], s[1], s[2], s[3], s[4], s[5], cfg, tjr, tjz);
-              else C->lost++;
-              births_push(B, s, orc_child_id(id[p], step), ca);
+              births_push(B, s, orc_child_id(id[p], step), 1);
             }
           } else if (X < nu_el + nu_io + nu_ex) {
             int ok;
@@ -1085,9 +1084,6 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
           }
         }
       }
-      halfdrift_u(&x[p], &y[p], &z[p], &ux[p], &uy[p], &uz[p], &alive[p], cfg, Rp, Lp);
-      if (!alive[p]) { C->lost++; continue; }
-      deposit_u(x[p], y[p], z[p], ux[p], uy[p], uz[p], cfg, tjr, tjz);
     }
     /* reduce the per-thread currents in thread order */
 #pragma omp for schedule(static)

@@ -115,9 +115,11 @@ typedef struct orc_counters {
   int64_t ion, ela, exc, nul, lost, cap_overflow;
 } orc_counters;
 
-/* one particle pass of step s: gather + kick + half drift + MCC + half drift +
- * deposit.  Arrays x..alive have capacity cap; *n grows with births.
- * jr/jz receive the current density [A/m^2] (overwritten). */
+/* one particle pass of step s: gather + kick + half drift + half drift +
+ * deposit, then the null-collision MCC at the end of the step (an ionization
+ * appends its secondary at the parent's position).  Arrays x..alive have
+ * capacity cap; *n grows with births.  jr/jz receive the current density
+ * [A/m^2] (overwritten). */
 int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step,
                  double *x, double *y, double *z, double *ux, double *uy, double *uz,
                  uint64_t *id, uint8_t *alive, int64_t *n, int64_t cap,
