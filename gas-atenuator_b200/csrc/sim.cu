@@ -45,19 +45,27 @@ constexpr uint32_t kDead = 0xFFFFFFFFu;
 constexpr int kBlock = 256;
 constexpr int kMccBlock = 64;             // collision kernels: two warps per block
 
+// Device counters.  Fields that every thread reads when a kernel starts share
+// the first 128-byte line; the counters that take atomics during a pass get
+// lines of their own, so those atomics do not hold up the reads.
 struct SimCounters {
   unsigned long long n_total;    // committed slots
-  unsigned long long n_births;   // slots claimed by births since the last pass
-  unsigned long long ion, ela, exc, nul, lost, cap_overflow;
-  long long step;                // index of the next particle pass
+  long long step;                // FP64: index of the next particle pass; FP32: of the current one
+  unsigned long long cap;        // slot capacity
   unsigned long long sorted_total;
+  long long cand_step[2];        // FP64: the pass that queued each queue
+  int uncommitted;               // FP64: a pass ran since the last commit (k_commit)
+  int pad0_;
+  unsigned long long pad1_[9];
+  unsigned long long n_births;   // slots claimed by births since the last commit
+  unsigned long long pad2_[15];
+  unsigned long long n_cand[2];  // collision candidates queued, per queue parity
+  unsigned long long pad3_[14];
+  unsigned long long chunk_next; // FP32 pass: next chunk to hand out
+  unsigned long long pad4_[15];
+  unsigned long long ion, ela, exc, nul, lost, cap_overflow;
   unsigned long long kin_fx;     // diagnostic: sum E_kin * 2^16 [eV]
   unsigned long long alive;      // diagnostic
-  unsigned long long cap;        // slot capacity
-  unsigned long long n_cand[2];  // collision candidates queued, per queue parity
-  long long cand_step[2];        // the pass that queued them
-  int uncommitted;               // a pass ran since the last commit (k_commit)
-  int pad_;
 };
 
 // slots holding particles, including births of the last pass not yet committed
@@ -678,48 +686,200 @@ __device__ __forceinline__ void win_node(const Win32 &w, const SimParams &P, int
   }
 }
 
-__device__ __forceinline__ uint4 pack32(int ir, int iz, float fr, float fz, float ur, bool alive) {
-  return make_uint4(alive ? (((uint32_t)iz << 16) | (uint32_t)ir) : kDead, __float_as_uint(fr),
-                    __float_as_uint(fz), __float_as_uint(ur));
+// FP32 state flags.  The in-cell offsets fr, fz are >= 0, so their sign bits
+// are free: the sign of fr marks a pending collision (the particle sits in the
+// collision queue of the pass that pushed it last), the sign of fz is the
+// parity of the step in which the particle was pushed last.
+constexpr uint32_t kSign = 0x80000000u;
+
+__device__ __forceinline__ uint4 pack32(int ir, int iz, float fr, float fz, float ur, bool alive,
+                                        bool pending = false, int par = 0) {
+  return make_uint4(alive ? (((uint32_t)iz << 16) | (uint32_t)ir) : kDead,
+                    __float_as_uint(fr) | (pending ? kSign : 0u),
+                    __float_as_uint(fz) | (par ? kSign : 0u), __float_as_uint(ur));
 }
 
-// FP32 particle pass; modes as k_pass64 (mode 0 drifts the whole step at once)
+// One particle's push in step `step`.  mode 0: gather, Boris kick, drift of
+// the whole step, null-collision candidate test; mode 1: half drift (start of
+// a run); mode 2: gather, kick, half drift to integer time (end of a run).
+// Returns whether the particle is a collision candidate (alive, mode 0).
+__device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &F, uint64_t id,
+                                       long long step, int mode, int &ir, int &iz, float &fr,
+                                       float &fz, float &ur, float &ut, float &uz, bool &alive) {
+  // block 0 of this particle's stream: words 0-1 decide the null-collision
+  // candidate, words 2-3 (mixed) drive the stochastic rounding
+  uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
+  if (mode == 1) {
+    philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+    drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, mix32(c[3]), P.hdr, P.hdz);
+    return false;
+  }
+  int ar, az;
+  float wr, wz;
+  half_shift(ir, fr, ar, wr);
+  half_shift(iz, fz, az, wz);
+  // the field loads go out first; their latency hides behind Philox
+  const Quad4 qEr = bilin_load(F.Er, P.nr, P.nz + 1, ar, iz);
+  const Quad4 qEz = bilin_load(F.Ez, P.nr + 1, P.nz, ir, az);
+  const Quad4 qH = bilin_load(F.H, P.nr, P.nz, ar, az);
+  philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+  const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]);
+  const float Er = bilin_mix(qEr, wr, fz);
+  const float Ez = bilin_mix(qEz, fr, wz);
+  const float H = bilin_mix(qH, wr, wz);
+  // Boris in gamma*beta units: E = (Er, 0, Ez), B = (0, mu0 H, 0); the
+  // increment u+ - u is formed first, then added with stochastic rounding
+  const float her = P.aE * Er, hez = P.aE * Ez;
+  const float umr = ur + her, umz = uz + hez;
+  const float igm = rsqrt_nr(fmaf(umr, umr, fmaf(ut, ut, fmaf(umz, umz, 1.0f))));
+  const float t = P.aB * H * igm;
+  const float s = __fdividef(2.f * t, fmaf(t, t, 1.f));
+  const float upr = fmaf(-umz, t, umr), upz = fmaf(umr, t, umz);
+  ur = sround_add(ur, fmaf(-upz, s, 2.f * her), rb0);
+  uz = sround_add(uz, fmaf(upr, s, 2.f * hez), rb0 >> 16);
+  const float h = mode == 0 ? 2.f : 1.f;
+  drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, h * P.hdr, h * P.hdz);
+  return alive && mode == 0 && (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
+}
+
+__device__ __forceinline__ void deposit_global32(const SimParams &P, int ir, int iz, float fr,
+                                                 float fz, float ur, float ut, float uz) {
+  int ca, cb, ra, rb, vr[4], vz[4];
+  deposit_nodes32(P, ir, iz, fr, fz, ur, ut, uz, ca, cb, ra, rb, vr, vz);
+  const int64_t a[4] = {ca + (int64_t)ra * P.nr, cb + (int64_t)ra * P.nr,
+                        ca + (int64_t)rb * P.nr, cb + (int64_t)rb * P.nr};
+  deposit_atomic<int>(a, vr, vz, P.Jr, P.Jz);
+}
+
+__device__ __forceinline__ void queue_one(SimCounters *cnt, int *queue, const SimParams &P,
+                                          int par, long long p) {
+  const unsigned long long k = atomicAdd(&cnt->n_cand[par], 1ull);
+  queue[(long long)par * P.cap + (long long)k] = (int)p;
+}
+
+// A collision candidate of the previous step (FP32 form), taken by one lane:
+// the MCC at the end of step `step` - 1 (FP64 test, branch, energy sharing;
+// float turn), the secondary's birth at the parent's position, then the push
+// of step `step` for both (push == true) with their current deposited by
+// global atomics and their own candidate test, or (push == false) nothing
+// more.  The chunk loop of the pass skips these particles (pending flag set,
+// or pushed-parity = this step's).
+// P: the launch's parameters in global memory (a reference to the kernel's
+// own parameter block would make every thread copy it to its stack).
+__device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Fields<float> F,
+                                         State32 S, SimCounters *cnt, int *queue, long long p,
+                                         long long step, int mode, bool push, long long n0,
+                                         unsigned &lost) {
+  const SimParams &P = *Pg;
+  const int par = (int)(step & 1);
+  const long long cstep = push ? step - 1 : step;      // step whose collision this is
+  const uint4 A = S.a[p];
+  const float2 B = S.b[p];
+  const uint64_t id = S.id[p];
+  int ir = (int)(A.x & 0xFFFFu), iz = (int)(A.x >> 16);
+  float fr = __uint_as_float(A.y & ~kSign), fz = __uint_as_float(A.z & ~kSign);
+  double dux = (double)__uint_as_float(A.w) * P.c, duy = (double)B.x * P.c, duz = (double)B.y * P.c;
+  Birth b;
+  count_event(cnt, mcc_event<true>(P, id, cstep, dux, duy, duz, b));
+  const int mark = push ? par : (int)(cstep & 1);
+  if (b.born) {
+    const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
+    const long long slot = n0 + (long long)kb;
+    if (slot < P.cap) {
+      int cir = ir, ciz = iz;
+      float cfr = fr, cfz = fz;
+      float cur = (float)(b.ux / P.c), cut = (float)(b.uy / P.c), cuz = (float)(b.uz / P.c);
+      bool calive = true, cc = false;
+      const uint64_t cid = child_id(id, cstep);
+      if (push) {
+        cc = push32(P, F, cid, step, mode, cir, ciz, cfr, cfz, cur, cut, cuz, calive);
+        if (calive && mode != 2) deposit_global32(P, cir, ciz, cfr, cfz, cur, cut, cuz);
+        if (!calive) lost++;
+        if (cc) queue_one(cnt, queue, P, par, slot);
+      }
+      S.a[slot] = pack32(cir, ciz, cfr, cfz, cur, calive, cc, mark);
+      S.b[slot] = make_float2(cut, cuz);
+      S.id[slot] = cid;
+    } else {
+      atomicAdd(&cnt->cap_overflow, 1ull);
+    }
+  }
+  float ur = (float)(dux / P.c), ut = (float)(duy / P.c), uz = (float)(duz / P.c);
+  bool alive = true, pc = false;
+  if (push) {
+    pc = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive);
+    if (alive && mode != 2) deposit_global32(P, ir, iz, fr, fz, ur, ut, uz);
+    if (!alive) lost++;
+    if (pc) queue_one(cnt, queue, P, par, p);
+  }
+  S.a[p] = pack32(ir, iz, fr, fz, ur, alive, pc, mark);
+  S.b[p] = make_float2(ut, uz);
+}
+
+// FP32 particle pass of step `step` (modes as push32).  Its blocks first take
+// the collision candidates queued by the previous pass, one per warp (a long
+// serial chain each, so blocks in order take eight at a time), then all other
+// particles in chunks of at most kChunk handed out in order, so the blocks
+// that ran a candidate simply take fewer chunks.  Counters are committed by
+// the field kernel of the next step.
 __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fields<float> F,
                                                       SimCounters *cnt, int *queue, int mode,
-                                                      int q) {
+                                                      const SimParams *__restrict__ Pg) {
   __shared__ int win_r[kWinNodes], win_z[kWinNodes];
   __shared__ int win_row0, win_rows;
-  const long long n0 = slots_in_use(cnt);
+  __shared__ long long chunk_at;
+  const long long n0 = (long long)cnt->n_total;   // births of this pass land beyond
   const long long step = cnt->step;
-  const int lane = threadIdx.x & 31;
-  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->uncommitted = 1;
+  const int par = (int)(step & 1);
+  const uint32_t parbit = par ? kSign : 0u;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned lost = 0;
+  if (mode != 1) {
+    const long long nq = (long long)cnt->n_cand[par ^ 1];
+    const int *qin = queue + (long long)(par ^ 1) * P.cap;
+    for (long long k = (long long)blockIdx.x * (kBlock / 32) + warp; k < nq;
+         k += (long long)gridDim.x * (kBlock / 32)) {
+      if (lane == 0) candidate32(Pg, F, S, cnt, queue, qin[k], step, mode, true, n0, lost);
+      __syncwarp();
+    }
+  }
   const int ws = win_stride(P.nr);
   const int maxrows = min(kWinNodes / ws, P.nz);
-  // every block takes the same number of consecutive chunks of the
-  // (cell-sorted) particles, each chunk at most kChunk long
-  const long long per = (n0 + (long long)gridDim.x * kChunk - 1) / ((long long)gridDim.x * kChunk);
-  const long long csize = per > 0 ? (n0 + per * gridDim.x - 1) / (per * gridDim.x) : 0;
-  unsigned lost = 0;
-  for (long long ch = (long long)blockIdx.x * per; ch < (long long)(blockIdx.x + 1) * per; ++ch) {
-    const long long beg = ch * csize, end = min(beg + csize, n0);
-    if (beg >= end) break;
+  const long long nchunk = (n0 + kChunk - 1) / kChunk;
+  // window rows of a chunk: the node rows of its first and last particles,
+  // with a margin for the drift since the last sort
+  auto chunk_rows = [&](long long ch, int &row0, int &rows) {
+    const long long beg = ch * kChunk, end = min(beg + kChunk, n0);
+    const uint32_t k0 = reinterpret_cast<const uint32_t *>(S.a + beg)[0];
+    const uint32_t k1 = reinterpret_cast<const uint32_t *>(S.a + end - 1)[0];
+    int lo = P.nz, hi = -1;
+    if (k0 != kDead) { lo = min(lo, (int)(k0 >> 16)); hi = max(hi, (int)(k0 >> 16)); }
+    if (k1 != kDead) { lo = min(lo, (int)(k1 >> 16)); hi = max(hi, (int)(k1 >> 16)); }
+    row0 = 0; rows = maxrows;
+    if (hi >= 0) {
+      row0 = min(max(0, lo - 3), P.nz - maxrows);
+      rows = min(maxrows, hi + 4 - row0);
+    }
+  };
+  // thread 0 fetches the next chunk (index and window rows) while the block
+  // works on the current one
+  long long next_ch = 0;
+  int next_row0 = 0, next_rows = 0;
+  if (threadIdx.x == 0) {
+    next_ch = (long long)atomicAdd(&cnt->chunk_next, 1ull);
+    if (next_ch < nchunk) chunk_rows(next_ch, next_row0, next_rows);
+  }
+  for (;;) {
     if (threadIdx.x == 0) {
-      // window rows: the node rows of the chunk's first and last particles, with
-      // a margin for the drift since the last sort
-      const uint32_t k0 = reinterpret_cast<const uint32_t *>(S.a + beg)[0];
-      const uint32_t k1 = reinterpret_cast<const uint32_t *>(S.a + end - 1)[0];
-      int lo = P.nz, hi = -1;
-      if (k0 != kDead) { lo = min(lo, (int)(k0 >> 16)); hi = max(hi, (int)(k0 >> 16)); }
-      if (k1 != kDead) { lo = min(lo, (int)(k1 >> 16)); hi = max(hi, (int)(k1 >> 16)); }
-      int row0 = 0, rows = maxrows;
-      if (hi >= 0) {
-        row0 = min(max(0, lo - 3), P.nz - maxrows);
-        rows = min(maxrows, hi + 4 - row0);
-      }
-      win_row0 = row0;
-      win_rows = rows;
+      chunk_at = next_ch;
+      win_row0 = next_row0;
+      win_rows = next_rows;
+      if (next_ch < nchunk) next_ch = (long long)atomicAdd(&cnt->chunk_next, 1ull);
     }
     __syncthreads();
+    const long long ch = chunk_at;
+    if (ch >= nchunk) break;
+    const long long beg = ch * kChunk, end = min(beg + kChunk, n0);
     const Win32 w{win_r, win_z, win_row0, win_rows, ws};
     const int nwin = w.rows * ws;
     for (int i = threadIdx.x; i < nwin; i += kBlock) { win_r[i] = 0; win_z[i] = 0; }
@@ -733,67 +893,30 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
     if (base + lane < end) { An = S.a[base + lane]; Bn = S.b[base + lane]; idn = S.id[base + lane]; }
     for (; base < end; base += blockDim.x) {
       const long long p = base + lane;
-      bool act = p < end;
       uint4 A = An;
-      const float2 Bc = Bn;
-      const uint64_t idc = idn;
+      const float2 B = Bn;
+      const uint64_t id = idn;
       {
         const long long pn = p + blockDim.x;
         An = make_uint4(kDead, 0, 0, 0);
         if (pn < end) { An = S.a[pn]; Bn = S.b[pn]; idn = S.id[pn]; }
       }
-      if (!act) A = make_uint4(kDead, 0, 0, 0);
-      act = act && A.x != kDead;
+      // skip the dead, the pending collisions and those already pushed in
+      // this step (the candidates the pass has taken)
+      bool act = p < end && A.x != kDead && !(A.y & kSign) && (A.z & kSign) != parbit;
       int ir = (int)(A.x & 0xFFFFu), iz = (int)(A.x >> 16);
-      float fr = __uint_as_float(A.y), fz = __uint_as_float(A.z), ur = __uint_as_float(A.w);
-      float ut = 0.f, uz = 0.f;
+      float fr = __uint_as_float(A.y & ~kSign), fz = __uint_as_float(A.z & ~kSign);
+      float ur = __uint_as_float(A.w), ut = B.x, uz = B.y;
       bool cand = false;
       if (act) {
-        const float2 B = Bc;
-        ut = B.x; uz = B.y;
-        const uint64_t id = idc;
-        uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
         bool alive = true;
-        if (mode == 1) {
-          philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
-          drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, mix32(c[3]), P.hdr, P.hdz);
-        } else {
-          int ar, az;
-          float wr, wz;
-          half_shift(ir, fr, ar, wr);
-          half_shift(iz, fz, az, wz);
-          // the field loads go out first; their latency hides behind Philox
-          const Quad4 qEr = bilin_load(F.Er, P.nr, P.nz + 1, ar, iz);
-          const Quad4 qEz = bilin_load(F.Ez, P.nr + 1, P.nz, ir, az);
-          const Quad4 qH = bilin_load(F.H, P.nr, P.nz, ar, az);
-          philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
-          const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]);
-          const float Er = bilin_mix(qEr, wr, fz);
-          const float Ez = bilin_mix(qEz, fr, wz);
-          const float H = bilin_mix(qH, wr, wz);
-          // Boris in gamma*beta units: E = (Er, 0, Ez), B = (0, mu0 H, 0); the
-          // increment u+ - u is formed first, then added with stochastic rounding
-          const float her = P.aE * Er, hez = P.aE * Ez;
-          const float umr = ur + her, umz = uz + hez;
-          const float igm = rsqrt_nr(fmaf(umr, umr, fmaf(ut, ut, fmaf(umz, umz, 1.0f))));
-          const float t = P.aB * H * igm;
-          const float s = __fdividef(2.f * t, fmaf(t, t, 1.f));
-          const float upr = fmaf(-umz, t, umr), upz = fmaf(umr, t, umz);
-          ur = sround_add(ur, fmaf(-upz, s, 2.f * her), rb0);
-          uz = sround_add(uz, fmaf(upr, s, 2.f * hez), rb0 >> 16);
-          // the whole step (mode 0) or a half step to integer time (mode 2);
-          // a collision candidate is queued for k_mcc32 at the end of the step
-          const float h = mode == 0 ? 2.f : 1.f;
-          drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, h * P.hdr, h * P.hdz);
-          cand = alive && mode == 0 &&
-                 (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
-        }
+        cand = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive);
         if (!alive) lost++;
-        S.a[p] = pack32(ir, iz, fr, fz, ur, alive);
+        S.a[p] = pack32(ir, iz, fr, fz, ur, alive, cand, par);
         S.b[p] = make_float2(ut, uz);
         act = alive && mode != 2;
       }
-      queue_push(cand, p, &cnt->n_cand[q], queue + (long long)q * P.cap);
+      queue_push(cand, p, &cnt->n_cand[par], queue + (long long)par * P.cap);
       if (act) {
         int ca, cb, ra, rb, vr[4], vz[4];
         deposit_nodes32(P, ir, iz, fr, fz, ur, ut, uz, ca, cb, ra, rb, vr, vz);
@@ -812,6 +935,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
         }
       }
     }
+    if (threadIdx.x == 0 && next_ch < nchunk) chunk_rows(next_ch, next_row0, next_rows);
     __syncthreads();
     for (int i = threadIdx.x; i < nwin; i += kBlock) {
       const int vr = win_r[i], vz = win_z[i];
@@ -828,37 +952,22 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
 }
 
-// FP32 form of k_mcc64
-__global__ void __launch_bounds__(kMccBlock) k_mcc32(SimParams P, State32 S, SimCounters *cnt,
-                                                     const int *queue, int q) {
-  if ((threadIdx.x & 31) != 0) return;
+// The collisions still queued by the last FP32 pass, without the next push
+// (before an observation of the state): MCC at the end of that step and the
+// secondaries' birth; the pending flags are cleared.
+__global__ void __launch_bounds__(kMccBlock) k_collide32(const SimParams *__restrict__ Pg,
+                                                         State32 S, Fields<float> F,
+                                                         SimCounters *cnt, int *queue) {
+  const SimParams &P = *Pg;
   const long long n0 = (long long)cnt->n_total;
-  const long long step = cnt->cand_step[q];
-  const long long nq = (long long)cnt->n_cand[q];
-  const int *qu = queue + (long long)q * P.cap;
+  const long long step = cnt->step;
+  const int par = (int)(step & 1);
+  const long long nq = (long long)cnt->n_cand[par];
+  const int *qu = queue + (long long)par * P.cap;
   const long long nwarps = (long long)gridDim.x * (kMccBlock / 32);
-  for (long long k = (blockIdx.x * (long long)kMccBlock + threadIdx.x) >> 5; k < nq; k += nwarps) {
-    const long long p = qu[k];
-    const uint4 A = S.a[p];
-    const float2 B = S.b[p];
-    double dux = (double)__uint_as_float(A.w) * P.c, duy = (double)B.x * P.c, duz = (double)B.y * P.c;
-    const uint64_t id = S.id[p];
-    Birth b;
-    count_event(cnt, mcc_event<true>(P, id, step, dux, duy, duz, b));
-    if (b.born) {
-      const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
-      const long long slot = n0 + (long long)kb;
-      if (slot < P.cap) {
-        S.a[slot] = make_uint4(A.x, A.y, A.z, __float_as_uint((float)(b.ux / P.c)));
-        S.b[slot] = make_float2((float)(b.uy / P.c), (float)(b.uz / P.c));
-        S.id[slot] = child_id(id, step);
-      } else {
-        atomicAdd(&cnt->cap_overflow, 1ull);
-      }
-    }
-    S.a[p] = make_uint4(A.x, A.y, A.z, __float_as_uint((float)(dux / P.c)));
-    S.b[p] = make_float2((float)(duy / P.c), (float)(duz / P.c));
-  }
+  unsigned lost = 0;
+  for (long long k = (blockIdx.x * (long long)kMccBlock + threadIdx.x) >> 5; k < nq; k += nwarps)
+    if ((threadIdx.x & 31) == 0) candidate32(Pg, F, S, cnt, queue, qu[k], step, 0, false, n0, lost);
 }
 
 // ------------------------------------------------------------- FDTD
@@ -869,7 +978,20 @@ __global__ void __launch_bounds__(32 * kFdtdRows) k_sim_fdtd(T *Er, T *Ez, T *H,
                                                   unsigned long long *Jr_next,
                                                   unsigned long long *Jz_next, int nr, int nz,
                                                   FdtdCoef c, const double *invV, double mu,
-                                                  double dt, int R, unsigned flags) {
+                                                  double dt, int R, unsigned flags,
+                                                  SimCounters *cnt) {
+  // FP32 form (cnt given): commit the previous pass and open step s - the
+  // births of the last pass join the slots, the queue that pass consumed is
+  // emptied, the chunk counter rewinds; no other kernel runs meanwhile
+  if (cnt && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+    const long long ns = cnt->step + 1;
+    const unsigned long long nt = cnt->n_total + cnt->n_births;
+    cnt->n_total = nt < cnt->cap ? nt : cnt->cap;
+    cnt->n_births = 0;
+    cnt->n_cand[ns & 1] = 0;
+    cnt->chunk_next = 0;
+    cnt->step = ns;
+  }
   fdtd_tiled<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, c, invV, mu, dt, R, flags);
 }
 
@@ -885,9 +1007,11 @@ __global__ void k_load64(State64 S, const double *r, const double *z, const doub
   }
 }
 
+// mark: the pushed-parity flag of the loaded particles (the opposite of the
+// parity of the pass that will push them first)
 __global__ void k_load32(State32 S, const double *r, const double *z, const double *ur,
                          const double *ut, const double *uz, const uint64_t *id, long long n,
-                         int nr, int nz, double dr, double dz, double c) {
+                         int nr, int nz, double dr, double dz, double c, int mark) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
        p += (long long)gridDim.x * blockDim.x) {
     const double R = r[p] / dr, Z = z[p] / dz;
@@ -897,7 +1021,7 @@ __global__ void k_load32(State32 S, const double *r, const double *z, const doub
     if (fz >= 1.f) { fz = 0.f; iz++; }
     if (iz >= nz) { iz = nz - 1; fz = 0.99999994f; }
     const bool alive = r[p] >= 0 && ir < nr && iz >= 0;
-    S.a[p] = pack32(ir, iz, fr, fz, (float)(ur[p] / c), alive);
+    S.a[p] = pack32(ir, iz, fr, fz, (float)(ur[p] / c), alive, false, mark);
     S.b[p] = make_float2((float)(ut[p] / c), (float)(uz[p] / c));
     S.id[p] = id[p];
   }
@@ -921,8 +1045,8 @@ __global__ void k_read32(State32 S, double *r, double *z, double *ur, double *ut
     const float2 B = S.b[p];
     if (A.x == kDead) { r[p] = -1.0; z[p] = 0; }
     else {
-      r[p] = ((double)(A.x & 0xFFFFu) + (double)__uint_as_float(A.y)) * dr;
-      z[p] = ((double)(A.x >> 16) + (double)__uint_as_float(A.z)) * dz;
+      r[p] = ((double)(A.x & 0xFFFFu) + (double)__uint_as_float(A.y & ~kSign)) * dr;
+      z[p] = ((double)(A.x >> 16) + (double)__uint_as_float(A.z & ~kSign)) * dz;
     }
     ur[p] = (double)__uint_as_float(A.w) * c; ut[p] = (double)B.x * c; uz[p] = (double)B.y * c;
     id[p] = S.id[p];
@@ -948,8 +1072,8 @@ __device__ __forceinline__ int cell_of64(const State64 &S, long long p, int nr, 
 __device__ __forceinline__ int cell_of32(const State32 &S, long long p, int nr) {
   const uint4 A = S.a[p];
   if (A.x == kDead) return -1;
-  const int ar = (int)(A.x & 0xFFFFu) + (__uint_as_float(A.y) >= 0.5f ? 1 : 0);
-  const int az = (int)(A.x >> 16) + (__uint_as_float(A.z) >= 0.5f ? 1 : 0);
+  const int ar = (int)(A.x & 0xFFFFu) + (__uint_as_float(A.y & ~kSign) >= 0.5f ? 1 : 0);
+  const int az = (int)(A.x >> 16) + (__uint_as_float(A.z & ~kSign) >= 0.5f ? 1 : 0);
   return ar + az * (nr + 1);
 }
 
@@ -1109,6 +1233,7 @@ struct gasatt_sim {
   double scale = 1.0;
   unsigned pass_grid = 0, mcc_grid = 0;
   int *queue = nullptr;           // collision candidates, two queues of capacity slots
+  SimParams *d_P = nullptr;       // device copies of P with the current of buffer 0 / 1
   bool mcc_pending = false;       // the last pass's collisions are not applied yet
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;   // graph capture fork/join
   bool timing = false;
@@ -1152,11 +1277,11 @@ int launch_fdtd(gasatt_sim *s, cudaStream_t st, int q) {
   if (s->form == 0)
     k_sim_fdtd<double><<<grid, block, 0, st>>>(
         (double *)s->Er, (double *)s->Ez, (double *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
-        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags);
+        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, nullptr);
   else
     k_sim_fdtd<float><<<grid, block, 0, st>>>(
         (float *)s->Er, (float *)s->Ez, (float *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
-        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags);
+        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt);
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "fdtd launch");
@@ -1177,7 +1302,7 @@ int launch_pass(gasatt_sim *s, cudaStream_t st, int mode, int jb, int q) {
   else
     k_pass32<<<s->pass_grid, kBlock, 0, st>>>(P, s->s32[b],
                                               Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H},
-                                              s->cnt, s->queue, mode, q);
+                                              s->cnt, s->queue, mode, s->d_P + jb);
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "particle pass launch");
@@ -1199,7 +1324,9 @@ int launch_mcc(gasatt_sim *s, cudaStream_t st, int q) {
   if (s->form == 0)
     k_mcc64<<<s->mcc_grid, kMccBlock, 0, st>>>(s->P, s->s64[b], s->cnt, s->queue, q);
   else
-    k_mcc32<<<s->mcc_grid, kMccBlock, 0, st>>>(s->P, s->s32[b], s->cnt, s->queue, q);
+    k_collide32<<<s->mcc_grid, kMccBlock, 0, st>>>(
+        s->d_P, s->s32[b], Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H}, s->cnt,
+        s->queue);
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "collision launch");
@@ -1214,7 +1341,7 @@ int flush_collisions(gasatt_sim *s) {
   if (!s->mcc_pending) return GASATT_OK;
   const int q = (int)((s->host_step - 1) & 1);
   cudaStream_t st = s->ctx->stream;
-  SIM_TRY(launch_commit(s, st, q));
+  if (s->form == 0) SIM_TRY(launch_commit(s, st, q));
   SIM_TRY(launch_mcc(s, st, q));
   GASATT_CUDA(s->ctx, cudaMemsetAsync(&s->cnt->n_cand[q], 0, sizeof(unsigned long long), st));
   s->mcc_pending = false;
@@ -1285,6 +1412,32 @@ int build_graphs(gasatt_sim *s) {
     s->cur = b;
     for (int q = 0; q < 2 && !rc; ++q) {
       GASATT_CUDA(s->ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      if (s->form == 1) {
+        // FP32: the field kernel commits the previous pass, the pass runs the
+        // previous step's collisions itself
+        cudaError_t e = cudaSuccess;
+        if (s->timing) e = cudaEventRecordWithFlags(s->ev[0], cs, cudaEventRecordExternal);
+        if (e == cudaSuccess) rc = launch_fdtd(s, cs, q);
+        if (e == cudaSuccess && !rc && s->timing) {
+          e = cudaEventRecordWithFlags(s->ev[1], cs, cudaEventRecordExternal);
+          if (e == cudaSuccess) e = cudaEventRecordWithFlags(s->ev[2], cs, cudaEventRecordExternal);
+        }
+        if (e == cudaSuccess && !rc) rc = launch_pass(s, cs, 0, 1 - q, q);
+        if (e == cudaSuccess && !rc && s->timing) {
+          e = cudaEventRecordWithFlags(s->ev[3], cs, cudaEventRecordExternal);
+          if (e == cudaSuccess) e = cudaEventRecordWithFlags(s->ev[4], cs, cudaEventRecordExternal);
+          if (e == cudaSuccess) e = cudaEventRecordWithFlags(s->ev[5], cs, cudaEventRecordExternal);
+        }
+        cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+        if (!rc && e != cudaSuccess) rc = cuda_fail(s->ctx, e, "capture step");
+        if (!rc && e2 != cudaSuccess) rc = cuda_fail(s->ctx, e2, "capture step");
+        if (!rc) {
+          e = cudaGraphInstantiate(&s->g_step[b][q], g, 0);
+          if (e != cudaSuccess) rc = cuda_fail(s->ctx, e, "instantiate step");
+        }
+        if (e2 == cudaSuccess) cudaGraphDestroy(g);
+        continue;
+      }
       cudaError_t e = cudaEventRecord(s->fork_ev, cs);
       if (e == cudaSuccess) e = cudaStreamWaitEvent(side, s->fork_ev, 0);
       if (e == cudaSuccess && s->timing) e = cudaEventRecordWithFlags(s->ev[4], side, cudaEventRecordExternal);
@@ -1460,6 +1613,13 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
     if (cudaMemcpy(s->invV, iv.data(), (size_t)nr * 8, cudaMemcpyHostToDevice) != cudaSuccess)
       return cleanup(fail(ctx, GASATT_E_CUDA, "volume table upload"));
   }
+  {
+    SimParams Pq[2] = {P, P};
+    Pq[1].Jr = s->Jr[1]; Pq[1].Jz = s->Jz[1];
+    if ((rc = sim_alloc(s, &s->d_P, 2))) return cleanup(rc);
+    if (cudaMemcpy(s->d_P, Pq, sizeof(Pq), cudaMemcpyHostToDevice) != cudaSuccess)
+      return cleanup(fail(ctx, GASATT_E_CUDA, "parameter upload"));
+  }
   if (fdtd_tile(c.fdtd_ratio) < 4)
     return cleanup(fail(ctx, GASATT_E_ARG, "fdtd_ratio too large for the fused field update (max 6)"));
   int dev = ctx->device, nsm = 148;
@@ -1471,7 +1631,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   // as many collision warps as fit on the device at once
   int occ_mcc = 1;
   if (s->form == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mcc, k_mcc64, kMccBlock, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mcc, k_mcc32, kMccBlock, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mcc, k_collide32, kMccBlock, 0);
   s->mcc_grid = (unsigned)(nsm * (occ_mcc > 0 ? occ_mcc : 1));
   // zero state
   SimCounters z{};
@@ -1543,7 +1703,8 @@ int gasatt_sim_load(gasatt_sim *s, const double *r, const double *z, const doubl
       k_load64<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->s64[0], d[0], d[1], d[2], d[3], d[4], did, n);
     else
       k_load32<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->s32[0], d[0], d[1], d[2], d[3], d[4], did, n,
-                                                       s->cfg.n_r, s->cfg.n_z, s->cfg.dr, s->cfg.dz, s->cfg.c);
+                                                       s->cfg.n_r, s->cfg.n_z, s->cfg.dr, s->cfg.dz, s->cfg.c,
+                                                       0);   // the first pass runs at step -1
     GASATT_LAUNCHED(ctx);
   }
   SimCounters zc{};
@@ -1714,10 +1875,11 @@ int gasatt_sim_step(gasatt_sim *s, int nsteps) {
     // (no collision candidates; queue parity 1 is the one step 0 reads)
     if (s->cfg.sort_period > 0) SIM_TRY(gasatt_sim_sort(s));
     SIM_TRY(launch_pass(s, st, 1, 0, 1));
-    SIM_TRY(launch_commit(s, st, 1));
+    if (s->form == 0) SIM_TRY(launch_commit(s, st, 1));
     s->primed = true;
   }
-  const int per_step = 4;   // field update, commit, collision kernel, particle pass
+  // field update, (FP64: commit, collision kernel,) particle pass
+  const int per_step = s->form == 0 ? 4 : 2;
   for (int k = 0; k < nsteps; ++k) {
     if (s->cfg.sort_period > 0 && s->since_sort >= s->cfg.sort_period) SIM_TRY(gasatt_sim_sort(s));
     GASATT_CUDA(ctx, cudaGraphLaunch(s->g_step[s->cur][s->host_step & 1], st));
@@ -1873,7 +2035,8 @@ int gasatt_sim_run_host(gasatt_sim *s, double *pos, double *vel, int64_t *n_io, 
       k_load64<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->s64[s->cur], sr, sz, sur, sut, suz, sid, n);
     else
       k_load32<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->s32[s->cur], sr, sz, sur, sut, suz, sid, n,
-                                                       s->cfg.n_r, s->cfg.n_z, s->cfg.dr, s->cfg.dz, s->cfg.c);
+                                                       s->cfg.n_r, s->cfg.n_z, s->cfg.dr, s->cfg.dz, s->cfg.c,
+                                                       (int)(((s->h_cnt->step + 1) & 1) ^ 1));
     GASATT_LAUNCHED(ctx);
   }
   SimCounters h = *s->h_cnt;
@@ -1881,6 +2044,8 @@ int gasatt_sim_run_host(gasatt_sim *s, double *pos, double *vel, int64_t *n_io, 
   h.n_births = 0;
   h.n_cand[0] = h.n_cand[1] = 0;
   h.uncommitted = 0;
+  h.chunk_next = 0;
+  h.step += 1;                               // never reuse the last pass's step
   GASATT_CUDA(ctx, cudaMemcpyAsync(s->cnt, &h, sizeof(h), cudaMemcpyHostToDevice, st));
   for (int q = 0; q < 2; ++q) {
     GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
@@ -1896,7 +2061,7 @@ int gasatt_sim_run_host(gasatt_sim *s, double *pos, double *vel, int64_t *n_io, 
   SIM_TRY(flush_collisions(s));
   SIM_TRY(launch_fdtd(s, st, (int)(s->host_step & 1)));
   SIM_TRY(launch_pass(s, st, 2, (int)((s->host_step + 1) & 1), (int)(s->host_step & 1)));
-  SIM_TRY(launch_commit(s, st, (int)(s->host_step & 1)));
+  if (s->form == 0) SIM_TRY(launch_commit(s, st, (int)(s->host_step & 1)));
   SIM_TRY(gasatt_sim_sort(s));               // compacts away the dead
   s->host_step++;
   s->primed = false;
