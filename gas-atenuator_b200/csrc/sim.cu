@@ -605,8 +605,8 @@ __device__ __forceinline__ void reflect_z(int &iz, float &fz, float &uz, int nz)
 // numbers).
 __device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, float &ur,
                                         float &ut, float &uz, bool &alive, const SimParams &P,
-                                        uint32_t rb, float hr, float hz) {
-  const float ig = rsqrt_nr(fmaf(ur, ur, fmaf(ut, ut, fmaf(uz, uz, 1.0f))));
+                                        uint32_t rb, float hr, float hz, float &ig) {
+  ig = rsqrt_nr(fmaf(ur, ur, fmaf(ut, ut, fmaf(uz, uz, 1.0f))));   // 1/gamma, kept by the turn
   const float dx = ur * ig * hr, dy = ut * ig * hr, dzz = uz * ig * hz;
   const float rc = (float)ir + fr;
   const float X = rc + dx;
@@ -636,10 +636,10 @@ __device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, 
 // the edges as EM7.cu:56-202) and the fixed-point contributions, node order
 // (ca,ra), (cb,ra), (ca,rb), (cb,rb).  The weights sum to 1, so one particle
 // adds at most 2^20 in magnitude to any node, even where clamped nodes merge.
+// ig: 1/gamma of u (the drift's, which turns u without changing |u|)
 __device__ __forceinline__ void deposit_nodes32(const SimParams &P, int ir, int iz, float fr,
-                                                float fz, float ur, float ut, float uz, int &ca,
+                                                float fz, float ur, float uz, float ig, int &ca,
                                                 int &cb, int &ra, int &rb, int vr[4], int vz[4]) {
-  const float ig = rsqrt_nr(fmaf(ur, ur, fmaf(ut, ut, fmaf(uz, uz, 1.0f))));
   int ar, az;
   float wr, wz;
   half_shift(ir, fr, ar, wr);
@@ -705,13 +705,14 @@ __device__ __forceinline__ uint4 pack32(int ir, int iz, float fr, float fz, floa
 // Returns whether the particle is a collision candidate (alive, mode 0).
 __device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &F, uint64_t id,
                                        long long step, int mode, int &ir, int &iz, float &fr,
-                                       float &fz, float &ur, float &ut, float &uz, bool &alive) {
+                                       float &fz, float &ur, float &ut, float &uz, bool &alive,
+                                       float &ig) {
   // block 0 of this particle's stream: words 0-1 decide the null-collision
   // candidate, words 2-3 (mixed) drive the stochastic rounding
   uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
   if (mode == 1) {
     philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
-    drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, mix32(c[3]), P.hdr, P.hdz);
+    drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, mix32(c[3]), P.hdr, P.hdz, ig);
     return false;
   }
   int ar, az;
@@ -738,14 +739,16 @@ __device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &
   ur = sround_add(ur, fmaf(-upz, s, 2.f * her), rb0);
   uz = sround_add(uz, fmaf(upr, s, 2.f * hez), rb0 >> 16);
   const float h = mode == 0 ? 2.f : 1.f;
-  drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, h * P.hdr, h * P.hdz);
+  drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, h * P.hdr, h * P.hdz, ig);
   return alive && mode == 0 && (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
 }
 
+// ig: the drift's 1/gamma, as in the chunk loop, so that a particle deposits
+// the same integers whichever path pushed it
 __device__ __forceinline__ void deposit_global32(const SimParams &P, int ir, int iz, float fr,
-                                                 float fz, float ur, float ut, float uz) {
+                                                 float fz, float ur, float uz, float ig) {
   int ca, cb, ra, rb, vr[4], vz[4];
-  deposit_nodes32(P, ir, iz, fr, fz, ur, ut, uz, ca, cb, ra, rb, vr, vz);
+  deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, ca, cb, ra, rb, vr, vz);
   const int64_t a[4] = {ca + (int64_t)ra * P.nr, cb + (int64_t)ra * P.nr,
                         ca + (int64_t)rb * P.nr, cb + (int64_t)rb * P.nr};
   deposit_atomic<int>(a, vr, vz, P.Jr, P.Jz);
@@ -792,8 +795,9 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
       bool calive = true, cc = false;
       const uint64_t cid = child_id(id, cstep);
       if (push) {
-        cc = push32(P, F, cid, step, mode, cir, ciz, cfr, cfz, cur, cut, cuz, calive);
-        if (calive && mode != 2) deposit_global32(P, cir, ciz, cfr, cfz, cur, cut, cuz);
+        float cig;
+        cc = push32(P, F, cid, step, mode, cir, ciz, cfr, cfz, cur, cut, cuz, calive, cig);
+        if (calive && mode != 2) deposit_global32(P, cir, ciz, cfr, cfz, cur, cuz, cig);
         if (!calive) lost++;
         if (cc) queue_one(cnt, queue, P, par, slot);
       }
@@ -807,8 +811,9 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
   float ur = (float)(dux / P.c), ut = (float)(duy / P.c), uz = (float)(duz / P.c);
   bool alive = true, pc = false;
   if (push) {
-    pc = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive);
-    if (alive && mode != 2) deposit_global32(P, ir, iz, fr, fz, ur, ut, uz);
+    float pig;
+    pc = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive, pig);
+    if (alive && mode != 2) deposit_global32(P, ir, iz, fr, fz, ur, uz, pig);
     if (!alive) lost++;
     if (pc) queue_one(cnt, queue, P, par, p);
   }
@@ -906,11 +911,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
       bool act = p < end && A.x != kDead && !(A.y & kSign) && (A.z & kSign) != parbit;
       int ir = (int)(A.x & 0xFFFFu), iz = (int)(A.x >> 16);
       float fr = __uint_as_float(A.y & ~kSign), fz = __uint_as_float(A.z & ~kSign);
-      float ur = __uint_as_float(A.w), ut = B.x, uz = B.y;
+      float ur = __uint_as_float(A.w), ut = B.x, uz = B.y, ig = 1.f;
       bool cand = false;
       if (act) {
         bool alive = true;
-        cand = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive);
+        cand = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive, ig);
         if (!alive) lost++;
         S.a[p] = pack32(ir, iz, fr, fz, ur, alive, cand, par);
         S.b[p] = make_float2(ut, uz);
@@ -919,7 +924,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
       queue_push(cand, p, &cnt->n_cand[par], queue + (long long)par * P.cap);
       if (act) {
         int ca, cb, ra, rb, vr[4], vz[4];
-        deposit_nodes32(P, ir, iz, fr, fz, ur, ut, uz, ca, cb, ra, rb, vr, vz);
+        deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, ca, cb, ra, rb, vr, vz);
         const unsigned la = (unsigned)(ra - w.row0), lb = (unsigned)(rb - w.row0);
         if (la < (unsigned)w.rows && lb < (unsigned)w.rows) {
           const int ka = (int)la * ws, kb = (int)lb * ws;
