@@ -104,19 +104,36 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ ours (GPU)
-def make_sim(precision, device, rank, torch):
+SORT_PERIODS = (20, 30, 40, 60)     # candidates of the sort-period autotuner
+
+
+def workload_setup(precision, rank, sort_period=20):
     from gasatt import _lib
-    from gasatt.sim import Sim, births, config
+    from gasatt.sim import births, config
     w = WORKLOAD
     prec = _lib.FP32_SPLIT if precision == "fp32_split" else _lib.FP64
     cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=prec,
-                 capacity=4_000_000, seed=replica_seed(rank), sort_period=20)
+                 capacity=4_000_000, seed=replica_seed(rank), sort_period=sort_period)
     parts = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=replica_seed(rank),
                    Rp=w["n_r"] * w["delta"])
+    return cfg, parts
+
+
+def make_sim(precision, device, rank, torch, sort_period=20):
+    from gasatt.sim import Sim
+    cfg, parts = workload_setup(precision, rank, sort_period)
     sim = Sim(cfg, device=device)
     sim.bind_stream()
     sim.load(*parts)
     return sim, parts
+
+
+def tuned_sort_period(precision, device, rank):
+    """The sort period the autotuner picks for this workload (results do not
+    depend on it; see gasatt.tune)."""
+    from gasatt.tune import tune_sort_period
+    cfg, parts = workload_setup(precision, rank)
+    return tune_sort_period(cfg, parts, candidates=SORT_PERIODS, steps=200, device=device)
 
 
 def counts(sim):
@@ -167,11 +184,11 @@ def timed_run(sim, steps, warmup, torch, flush, dist_barrier, phase_steps=50):
                 launches=launches)
 
 
-def e2e_run(precision, device, rank, torch, steps_per_call=200):
+def e2e_run(precision, device, rank, torch, steps_per_call=200, sort_period=20):
     """Through the public C ABI with pinned HOST buffers: H2D of the electrons,
     steps_per_call steps, D2H of the result, all inside the timed region."""
     from gasatt._lib import lib
-    sim, parts = make_sim(precision, device, rank, torch)
+    sim, parts = make_sim(precision, device, rank, torch, sort_period)
     r, z, ur, ut, uz, ids = parts
     n = len(r)
     cap = int(n * 1.1)
@@ -298,8 +315,12 @@ def run_ours(args):
 
     results = {}
     clocks = None
+    tuned = {}
     for prec in ("fp32_split", "fp64"):
-        sim, _ = make_sim(prec, local, rank, torch)
+        sp, table = tuned_sort_period(prec, local, rank)
+        sp = int(max_over_ranks(sp))                 # every rank uses the same period
+        tuned[prec] = (sp, table)
+        sim, _ = make_sim(prec, local, rank, torch, sp)
         if prec == "fp32_split":
             with ClockSampler(local) as cs:
                 res = timed_run(sim, args.steps, args.warmup, torch, flush, barrier)
@@ -309,7 +330,8 @@ def run_ours(args):
         res["fields"] = sim.fields()
         results[prec] = res
         sim.close()
-    e2e = e2e_run("fp32_split", local, rank, torch, steps_per_call=200)
+    e2e = e2e_run("fp32_split", local, rank, torch, steps_per_call=200,
+                  sort_period=tuned["fp32_split"][0])
 
     pk, pk_src = peaks()
     hbm = float(pk.get("hbm_gbs", 6650.0))
@@ -366,7 +388,12 @@ def run_ours(args):
                    "global_electrons": int(sum_over_ranks(f32["alive"])),
                    "per_rank": "independent replica", "parallelism": f"replicas x{world}",
                    "l2": "flushed before every timed step (256 MiB write, outside the events)",
-                   "sort_period": 20, "fdtd_ratio": 1, "timed": "whole step: FDTD + particle pass (+ periodic sort)"},
+                   "sort_period": tuned["fp32_split"][0],
+                   "sort_period_autotuned": {"candidates": list(SORT_PERIODS),
+                                             "ms_per_step": {str(k): round(v, 5) for k, v in
+                                                             tuned["fp32_split"][1].items()},
+                                             "fp64_choice": tuned["fp64"][0]},
+                   "fdtd_ratio": 1, "timed": "whole step: FDTD + particle pass (+ periodic sort)"},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"] / e2e["steps"],
                 "d2h_bytes_per_step": e2e["d2h"] / e2e["steps"],
                 "call": f"gasatt_sim_run_host, {e2e['steps']} steps per call, pinned host x,y,z,vx,vy,vz in/out"},
