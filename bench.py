@@ -469,6 +469,77 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+C3_GRIDS = ((64, 256), (128, 512), (256, 1024), (512, 2048))
+
+
+def c3_cells(n=48, seed=2):
+    """The batched workload: n gas cells with pressure log-uniform in 0.1-10
+    Torr, grid drawn from C3_GRIDS at 10 um, photon energy uniform in 2-20 keV,
+    photoionizations log-uniform in 1e4-1e6 (seeded)."""
+    rng = np.random.default_rng(seed)
+    cells = []
+    for i in range(n):
+        nr, nz = C3_GRIDS[rng.integers(len(C3_GRIDS))]
+        cells.append(dict(n_r=int(nr), n_z=int(nz), delta=10e-6, dt=2e-14,
+                          torr=float(10 ** rng.uniform(-1, 1)), e_keV=float(rng.uniform(2, 20)),
+                          photo=int(round(10 ** rng.uniform(4, 6))), seed=seed * 1000 + i))
+    return cells
+
+
+def run_c3(args):
+    """Batched instances (one graph launch per step for all cells) against the
+    same instances stepped one after another; FP32 split form."""
+    import torch
+    from gasatt import _lib
+    from gasatt.dropin import Context
+    from gasatt.sim import Batch, Sim, births, config
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    ctx.bind_stream()
+    sims = []
+    for c in c3_cells():
+        cfg = config(c["n_r"], c["n_z"], c["delta"], c["dt"], c["torr"], precision=_lib.FP32_SPLIT,
+                     capacity=6 * c["photo"], seed=c["seed"], sort_period=30)
+        sim = Sim(cfg, ctx=ctx)
+        sim.load(*births(c["photo"], c["e_keV"], c["n_z"] * c["delta"], seed=c["seed"],
+                         Rp=c["n_r"] * c["delta"]))
+        sims.append(sim)
+    batch = Batch(sims, sort_period=30)
+    stream = torch.cuda.current_stream()
+
+    def alive():
+        return sum(s.diag()["n_alive"] for s in sims)
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        a0 = alive()
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        return 0.5 * (a0 + alive()) * k / (ms / 1e3), ms / k
+
+    batch.step(args.warmup)
+    v_batch, ms_batch = timed(lambda: batch.step(1), args.steps)
+    v_seq, ms_seq = timed(lambda: [s.step(1) for s in sims], args.steps)
+    line = {"mode": "c3", "metric": METRIC, "unit": UNIT, "instances": len(sims),
+            "steps": args.steps, "warmup": args.warmup, "electrons": alive(),
+            "batched": {"value": v_batch, "ms_per_step": ms_batch},
+            "one_after_another": {"value": v_seq, "ms_per_step": ms_seq},
+            "batched_over_one_after_another": v_batch / v_seq,
+            "config": {"workload": "48 cells: p log-U(0.1, 10) Torr, grid from "
+                       "{64x256, 128x512, 256x1024, 512x2048} at 10 um, dt 2e-14 s, photon "
+                       "U(2, 20) keV, photoionizations log-U(1e4, 1e6), seed 2",
+                       "precision": "fp32_split", "sort_period": 30, "l2": "not flushed"}}
+    print(json.dumps(line), flush=True)
+    batch.close()
+    for s in sims:
+        s.close()
+
+
 def run_profile(args):
     """The step loop alone (warm-up then timed steps, no flush/e2e/baseline),
     for kernel profilers."""
@@ -491,13 +562,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="bench", choices=["bench", "profile"],
-                    help="profile: only the step loop of one precision (for ncu)")
+    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "c3"],
+                    help="profile: only the step loop of one precision (for ncu); "
+                         "c3: 48 batched gas cells")
     ap.add_argument("--precision", default="fp32_split", choices=["fp32_split", "fp64"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.mode == "profile":
         run_profile(args)
+    elif args.mode == "c3":
+        run_c3(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -1234,6 +1234,7 @@ struct gasatt_sim {
   int64_t host_step = 0;          // particle passes completed
   int64_t since_sort = 0;
   cudaGraphExec_t g_step[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [state buffer][step parity]
+  cudaGraph_t gr_step[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};     // the same, not instantiated
   cudaGraphExec_t g_sort[2] = {nullptr, nullptr};
   double scale = 1.0;
   unsigned pass_grid = 0, mcc_grid = 0;
@@ -1387,10 +1388,24 @@ void drop_graphs(gasatt_sim *s) {
     for (int q = 0; q < 2; ++q) {
       if (s->g_step[i][q]) cudaGraphExecDestroy(s->g_step[i][q]);
       s->g_step[i][q] = nullptr;
+      if (s->gr_step[i][q]) cudaGraphDestroy(s->gr_step[i][q]);
+      s->gr_step[i][q] = nullptr;
     }
     if (s->g_sort[i]) cudaGraphExecDestroy(s->g_sort[i]);
     s->g_sort[i] = nullptr;
   }
+}
+
+// Start of a run: the particles at x^0 move to x^{1/2} and deposit j^{1/2}
+// (no collision candidates; queue parity 1 is the one step 0 reads).
+int sim_prime(gasatt_sim *s) {
+  if (s->primed) return GASATT_OK;
+  cudaStream_t st = s->ctx->stream;
+  if (s->cfg.sort_period > 0) SIM_TRY(gasatt_sim_sort(s));
+  SIM_TRY(launch_pass(s, st, 1, 0, 1));
+  if (s->form == 0) SIM_TRY(launch_commit(s, st, 1));
+  s->primed = true;
+  return GASATT_OK;
 }
 
 // Capture one step for state buffer b and step parity q:
@@ -1440,7 +1455,9 @@ int build_graphs(gasatt_sim *s) {
           e = cudaGraphInstantiate(&s->g_step[b][q], g, 0);
           if (e != cudaSuccess) rc = cuda_fail(s->ctx, e, "instantiate step");
         }
-        if (e2 == cudaSuccess) cudaGraphDestroy(g);
+        if (e2 == cudaSuccess) {
+          if (!rc) s->gr_step[b][q] = g; else cudaGraphDestroy(g);
+        }
         continue;
       }
       cudaError_t e = cudaEventRecord(s->fork_ev, cs);
@@ -1464,7 +1481,9 @@ int build_graphs(gasatt_sim *s) {
         e = cudaGraphInstantiate(&s->g_step[b][q], g, 0);
         if (e != cudaSuccess) rc = cuda_fail(s->ctx, e, "instantiate step");
       }
-      if (e2 == cudaSuccess) cudaGraphDestroy(g);
+      if (e2 == cudaSuccess) {
+        if (!rc) s->gr_step[b][q] = g; else cudaGraphDestroy(g);
+      }
     }
     if (rc) break;
     GASATT_CUDA(s->ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
@@ -1633,6 +1652,12 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   if (s->form == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass64, kBlock, 0);
   else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass32, kBlock, 0);
   s->pass_grid = (unsigned)(nsm * (occ > 0 ? occ : 1));
+  if (s->form == 1) {
+    // FP32 blocks take chunks from a counter: no more blocks than chunks the
+    // capacity can hold (small instances then leave the GPU to others)
+    const long long chunks = (cap + kChunk - 1) / kChunk;
+    if ((long long)s->pass_grid > chunks) s->pass_grid = (unsigned)(chunks > 0 ? chunks : 1);
+  }
   // as many collision warps as fit on the device at once
   int occ_mcc = 1;
   if (s->form == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_mcc, k_mcc64, kMccBlock, 0);
@@ -1875,14 +1900,7 @@ int gasatt_sim_step(gasatt_sim *s, int nsteps) {
   gasatt_ctx *ctx = s->ctx;
   GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
-  if (!s->primed) {
-    // start of a run: particles at x^0 move to x^{1/2} and deposit j^{1/2}
-    // (no collision candidates; queue parity 1 is the one step 0 reads)
-    if (s->cfg.sort_period > 0) SIM_TRY(gasatt_sim_sort(s));
-    SIM_TRY(launch_pass(s, st, 1, 0, 1));
-    if (s->form == 0) SIM_TRY(launch_commit(s, st, 1));
-    s->primed = true;
-  }
+  SIM_TRY(sim_prime(s));
   // field update, (FP64: commit, collision kernel,) particle pass
   const int per_step = s->form == 0 ? 4 : 2;
   for (int k = 0; k < nsteps; ++k) {
@@ -2091,6 +2109,98 @@ int gasatt_sim_run_host(gasatt_sim *s, double *pos, double *vel, int64_t *n_io, 
   GASATT_CUDA(ctx, cudaStreamSynchronize(st));
   *n_io = nw;
   if (nout > cap) return fail(ctx, GASATT_E_CAPACITY, "run_host: more electrons than cap rows");
+  return GASATT_OK;
+}
+
+// ================================================================ batches
+// Many independent gas cells stepped together: one CUDA graph holds the step
+// graphs of all instances side by side (no dependencies between them), so
+// small cells fill the GPU together and one launch advances them all.  The
+// instances share a sort period, so they swap state buffers in lockstep; if
+// one is ever out of step (stepped on its own in between), the batch steps
+// each instance with its own graph.
+struct gasatt_batch {
+  gasatt_ctx *ctx = nullptr;
+  std::vector<gasatt_sim *> sims;
+  int sort_period = 0;
+  cudaGraphExec_t g[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [state buffer][parity]
+};
+
+int gasatt_batch_destroy(gasatt_batch *b) {
+  if (!b) return GASATT_OK;
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->stream);
+  for (int i = 0; i < 2; ++i)
+    for (int q = 0; q < 2; ++q)
+      if (b->g[i][q]) cudaGraphExecDestroy(b->g[i][q]);
+  delete b;
+  return GASATT_OK;
+}
+
+int gasatt_batch_create(gasatt_ctx *ctx, gasatt_sim *const *sims, int n, int sort_period,
+                        gasatt_batch **out) {
+  if (!ctx || !sims || n < 1 || !out || sort_period < 0)
+    return fail(ctx, GASATT_E_ARG, "batch: bad arguments");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!sims[i] || sims[i]->ctx != ctx)
+      return fail(ctx, GASATT_E_ARG, "batch: every instance must belong to this context");
+    if (sims[i]->timing) return fail(ctx, GASATT_E_STATE, "batch: disable phase timing first");
+    for (int j = 0; j < i; ++j)
+      if (sims[j] == sims[i]) return fail(ctx, GASATT_E_ARG, "batch: an instance appears twice");
+  }
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  gasatt_batch *b = new gasatt_batch();
+  b->ctx = ctx;
+  b->sims.assign(sims, sims + n);
+  b->sort_period = sort_period;
+  for (gasatt_sim *s : b->sims) s->cfg.sort_period = sort_period;
+  for (int bi = 0; bi < 2; ++bi)
+    for (int q = 0; q < 2; ++q) {
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaGraphCreate(&g, 0);
+      for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        cudaGraphNode_t node;
+        e = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, b->sims[i]->gr_step[bi][q]);
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&b->g[bi][q], g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        gasatt_batch_destroy(b);
+        return cuda_fail(ctx, e, "batch graph");
+      }
+    }
+  *out = b;
+  return GASATT_OK;
+}
+
+int gasatt_batch_step(gasatt_batch *b, int nsteps) {
+  if (!b || nsteps < 0) return GASATT_E_ARG;
+  gasatt_ctx *ctx = b->ctx;
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  for (int k = 0; k < nsteps; ++k) {
+    for (gasatt_sim *s : b->sims) SIM_TRY(sim_prime(s));
+    for (gasatt_sim *s : b->sims)
+      if (b->sort_period > 0 && s->since_sort >= b->sort_period) SIM_TRY(gasatt_sim_sort(s));
+    const gasatt_sim *s0 = b->sims[0];
+    bool lockstep = true;
+    for (const gasatt_sim *s : b->sims)
+      lockstep = lockstep && s->cur == s0->cur && (s->host_step & 1) == (s0->host_step & 1) &&
+                 !s->timing;
+    if (lockstep) {
+      GASATT_CUDA(ctx, cudaGraphLaunch(b->g[s0->cur][s0->host_step & 1], st));
+    } else {
+      for (gasatt_sim *s : b->sims)
+        GASATT_CUDA(ctx, cudaGraphLaunch(s->g_step[s->cur][s->host_step & 1], st));
+    }
+    for (gasatt_sim *s : b->sims) {
+      ctx->launches += s->form == 0 ? 4 : 2;
+      s->host_step++;
+      s->since_sort++;
+      s->mcc_pending = true;
+    }
+  }
   return GASATT_OK;
 }
 

@@ -192,3 +192,35 @@ class Sim:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Independent gas-cell instances (Sim objects on one context) advanced
+    together: one graph launch per step runs all their step graphs side by
+    side.  The instances share `sort_period`; each stays observable on its
+    own (read, diag, fields)."""
+
+    def __init__(self, sims, sort_period=20):
+        self.sims = list(sims)
+        ctx = self.sims[0].ctx
+        if any(s.ctx is not ctx for s in self.sims):
+            raise ValueError("all instances of a batch must share one Context")
+        self.ctx = ctx
+        arr = (ctypes.c_void_p * len(self.sims))(*[s.h.value for s in self.sims])
+        self.h = ctypes.c_void_p()
+        check(ctx.handle, lib.gasatt_batch_create(ctx.handle, arr, len(self.sims), int(sort_period),
+                                                  ctypes.byref(self.h)))
+
+    def step(self, n=1):
+        check(self.ctx.handle, lib.gasatt_batch_step(self.h, int(n)))
+
+    def close(self):
+        if self.h:
+            lib.gasatt_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

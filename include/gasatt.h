@@ -318,6 +318,21 @@ int gasatt_sim_counts(gasatt_sim *sim, int64_t *n_slots, int64_t *n_ionizations,
 int gasatt_sim_enable_timing(gasatt_sim *sim, int enable);
 int gasatt_sim_last_timing(gasatt_sim *sim, float *fdtd_ms, float *pass_ms, float *mcc_ms);
 
+/* ------------------------------------------------------------------ batches
+ * Many independent gas cells (instances of uneven size, pressure, photon
+ * energy) stepped together.  The reference's driver runs one cell at a time,
+ * so this has no single counterpart there; it batches gasatt_sim_step.  All
+ * instances belong to ctx and get the batch's sort period; each batch step
+ * advances every instance by one step with one graph launch (their step
+ * graphs side by side).  Each instance stays observable on its own
+ * (gasatt_sim_read, gasatt_sim_diag, ...).  Destroy the batch before its
+ * instances. */
+typedef struct gasatt_batch gasatt_batch;
+int gasatt_batch_create(gasatt_ctx *ctx, gasatt_sim *const *sims, int n, int sort_period,
+                        gasatt_batch **batch);
+int gasatt_batch_step(gasatt_batch *batch, int nsteps);
+int gasatt_batch_destroy(gasatt_batch *batch);
+
 #ifdef __cplusplus
 }
 #endif
