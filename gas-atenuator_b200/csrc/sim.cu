@@ -1001,34 +1001,94 @@ __global__ void __launch_bounds__(32 * kFdtdRows) k_sim_fdtd(T *Er, T *Ez, T *H,
 }
 
 // ---------------------------------------------------------- load/read
+
+// one particle in SI (r, z [m], u = gamma v [m/s]) into the FP32 state; mark:
+// the pushed-parity flag (the opposite of the parity of the pass that will
+// push it first)
+__device__ __forceinline__ void store32(State32 S, long long p, double r, double z, double ur,
+                                        double ut, double uz, uint64_t id, int nr, int nz,
+                                        double dr, double dz, double c, int mark) {
+  const double R = r / dr, Z = z / dz;
+  int ir = (int)floor(R), iz = (int)floor(Z);
+  float fr = (float)(R - ir), fz = (float)(Z - iz);
+  if (fr >= 1.f) { fr = 0.f; ir++; }
+  if (fz >= 1.f) { fz = 0.f; iz++; }
+  if (iz >= nz) { iz = nz - 1; fz = 0.99999994f; }
+  const bool alive = r >= 0 && ir < nr && iz >= 0;
+  S.a[p] = pack32(ir, iz, fr, fz, (float)(ur / c), alive, false, mark);
+  S.b[p] = make_float2((float)(ut / c), (float)(uz / c));
+  S.id[p] = id;
+}
+
+__device__ __forceinline__ void store64(State64 S, long long p, double r, double z, double ur,
+                                        double ut, double uz, uint64_t id) {
+  S.rz[p] = make_double2(r, z);
+  S.urt[p] = make_double2(ur, ut);
+  S.uz[p] = uz;
+  S.id[p] = id;
+}
+
 __global__ void k_load64(State64 S, const double *r, const double *z, const double *ur,
                          const double *ut, const double *uz, const uint64_t *id, long long n) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
-       p += (long long)gridDim.x * blockDim.x) {
-    S.rz[p] = make_double2(r[p], z[p]);
-    S.urt[p] = make_double2(ur[p], ut[p]);
-    S.uz[p] = uz[p];
-    S.id[p] = id[p];
-  }
+       p += (long long)gridDim.x * blockDim.x)
+    store64(S, p, r[p], z[p], ur[p], ut[p], uz[p], id[p]);
 }
 
-// mark: the pushed-parity flag of the loaded particles (the opposite of the
-// parity of the pass that will push them first)
 __global__ void k_load32(State32 S, const double *r, const double *z, const double *ur,
                          const double *ut, const double *uz, const uint64_t *id, long long n,
                          int nr, int nz, double dr, double dz, double c, int mark) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
-       p += (long long)gridDim.x * blockDim.x) {
-    const double R = r[p] / dr, Z = z[p] / dz;
-    int ir = (int)floor(R), iz = (int)floor(Z);
-    float fr = (float)(R - ir), fz = (float)(Z - iz);
-    if (fr >= 1.f) { fr = 0.f; ir++; }
-    if (fz >= 1.f) { fz = 0.f; iz++; }
-    if (iz >= nz) { iz = nz - 1; fz = 0.99999994f; }
-    const bool alive = r[p] >= 0 && ir < nr && iz >= 0;
-    S.a[p] = pack32(ir, iz, fr, fz, (float)(ur[p] / c), alive, false, mark);
-    S.b[p] = make_float2((float)(ut[p] / c), (float)(uz[p] / c));
-    S.id[p] = id[p];
+       p += (long long)gridDim.x * blockDim.x)
+    store32(S, p, r[p], z[p], ur[p], ut[p], uz[p], id[p], nr, nz, dr, dz, c, mark);
+}
+
+// ------------------------------------------------------------ births
+// Photoionization births on the device: per photon a photoelectron (photon
+// energy minus the N K-shell binding, 410 eV as EB_14.csv's 409.9; direction
+// density ~ (d . x)^2 about the polarisation x) and an isotropic 360 eV Auger
+// electron, both at a Rayleigh(sigma_r) radius (inside the wall), uniform
+// azimuth and uniform z; the state keeps the local (r, theta, z) frame of that
+// azimuth.  The reference draws its births on the host (INCIDENCE1.m:51-158,
+// with a Sauter photoelectron and a 383 eV Auger line); these are the
+// workload's laws.  Draws: Philox keyed on (seed, photon index) with the
+// reserved step word kBirthStream, apart from every simulation draw.
+constexpr long long kBirthStream = -2;
+constexpr double kKShellEv = 410.0, kAugerEv = 360.0;
+
+template <int FORM>
+__global__ void k_birth_photo(State64 S64, State32 S32, long long n_photo, double u_pe,
+                              double u_au, double sigma_r, double r_max, double Lp,
+                              uint64_t seed, uint64_t id_base, int nr, int nz, double dr,
+                              double dz, double c) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n_photo;
+       k += (long long)gridDim.x * blockDim.x) {
+    const U2 d0 = draw2(seed, (uint64_t)k, kBirthStream, 0), d1 = draw2(seed, (uint64_t)k, kBirthStream, 1);
+    const U2 d2 = draw2(seed, (uint64_t)k, kBirthStream, 2), d3 = draw2(seed, (uint64_t)k, kBirthStream, 3);
+    const double r = fmin(sigma_r * sqrt(-2.0 * log1p(-d0.a)), r_max);
+    const double z = d0.b * Lp;
+    double sp, cp;
+    sincos(2 * GASATT_PI * d1.a, &sp, &cp);                // azimuth of the birth point
+    // photoelectron: mu = cos(angle to x), p(mu) ~ mu^2 -> mu = cbrt(2U - 1)
+    const double mu = cbrt(2 * d1.b - 1), s = sqrt(fmax(0.0, 1 - mu * mu));
+    double sps, cps;
+    sincos(2 * GASATT_PI * d2.a, &sps, &cps);
+    const double px = mu, py = s * cps, pz = s * sps;
+    // Auger: isotropic
+    const double ct = 2 * d2.b - 1, st = sqrt(fmax(0.0, 1 - ct * ct));
+    double spa, cpa;
+    sincos(2 * GASATT_PI * d3.a, &spa, &cpa);
+    const double ax = st * cpa, ay = st * spa, az = ct;
+    const double pr = u_pe * (px * cp + py * sp), pt = u_pe * (-px * sp + py * cp), pzz = u_pe * pz;
+    const double ar = u_au * (ax * cp + ay * sp), at = u_au * (-ax * sp + ay * cp), azz = u_au * az;
+    const long long p = 2 * k;
+    if (FORM == 0) {
+      store64(S64, p, r, z, pr, pt, pzz, id_base + (uint64_t)p);
+      store64(S64, p + 1, r, z, ar, at, azz, id_base + (uint64_t)p + 1);
+    } else {
+      store32(S32, p, r, z, pr, pt, pzz, id_base + (uint64_t)p, nr, nz, dr, dz, c, 0);
+      store32(S32, p + 1, r, z, ar, at, azz, id_base + (uint64_t)p + 1, nr, nz, dr, dz, c, 0);
+    }
   }
 }
 
@@ -1396,6 +1456,28 @@ void drop_graphs(gasatt_sim *s) {
   }
 }
 
+// A fresh population of n particles sits in state buffer 0: counters, current
+// buffers and the step bookkeeping start over.
+int sim_reset(gasatt_sim *s, int64_t n) {
+  gasatt_ctx *ctx = s->ctx;
+  cudaStream_t st = ctx->stream;
+  SimCounters zc{};
+  zc.n_total = (unsigned long long)n;
+  zc.step = -1;
+  zc.cap = (unsigned long long)s->cfg.capacity;
+  GASATT_CUDA(ctx, cudaMemcpyAsync(s->cnt, &zc, sizeof(zc), cudaMemcpyHostToDevice, st));
+  for (int q = 0; q < 2; ++q) {
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+  }
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  s->primed = false;
+  s->mcc_pending = false;
+  s->host_step = 0;
+  s->since_sort = 0;
+  return GASATT_OK;
+}
+
 // Start of a run: the particles at x^0 move to x^{1/2} and deposit j^{1/2}
 // (no collision candidates; queue parity 1 is the one step 0 reads).
 int sim_prime(gasatt_sim *s) {
@@ -1737,21 +1819,41 @@ int gasatt_sim_load(gasatt_sim *s, const double *r, const double *z, const doubl
                                                        0);   // the first pass runs at step -1
     GASATT_LAUNCHED(ctx);
   }
-  SimCounters zc{};
-  zc.n_total = (unsigned long long)n;
-  zc.step = -1;
-  zc.cap = (unsigned long long)s->cfg.capacity;
-  GASATT_CUDA(ctx, cudaMemcpyAsync(s->cnt, &zc, sizeof(zc), cudaMemcpyHostToDevice, st));
-  for (int q = 0; q < 2; ++q) {
-    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
-    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+  return sim_reset(s, n);
+}
+
+int gasatt_sim_birth_photo(gasatt_sim *s, int64_t n_photo, double photon_keV, double sigma_r,
+                           uint64_t seed, uint64_t id_base) {
+  if (!s) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  if (n_photo < 0 || !(sigma_r > 0) || !(photon_keV * 1000 > kKShellEv))
+    return fail(ctx, GASATT_E_ARG, "birth_photo: bad arguments");
+  if (2 * n_photo > s->cfg.capacity) return fail(ctx, GASATT_E_CAPACITY, "birth_photo exceeds capacity");
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const auto &c = s->cfg;
+  auto speed = [&](double E_ev) {                      // u = gamma v of kinetic energy E
+    const double e = E_ev * c.q_e / (c.m_e * c.c * c.c);
+    return c.c * std::sqrt(e * (2 + e));
+  };
+  const double Rp = c.n_r * c.dr, Lp = c.n_z * c.dz;
+  const double r_max = std::nextafter(Rp, 0.0);
+  s->cur = 0;
+  if (n_photo > 0) {
+    const unsigned g = grid_for(n_photo, kBlock);
+    if (s->form == 0)
+      k_birth_photo<0><<<g, kBlock, 0, st>>>(s->s64[0], s->s32[0], n_photo,
+                                             speed(photon_keV * 1000 - kKShellEv), speed(kAugerEv),
+                                             sigma_r, r_max, Lp, seed, id_base, c.n_r, c.n_z,
+                                             c.dr, c.dz, c.c);
+    else
+      k_birth_photo<1><<<g, kBlock, 0, st>>>(s->s64[0], s->s32[0], n_photo,
+                                             speed(photon_keV * 1000 - kKShellEv), speed(kAugerEv),
+                                             sigma_r, r_max, Lp, seed, id_base, c.n_r, c.n_z,
+                                             c.dr, c.dz, c.c);
+    GASATT_LAUNCHED(ctx);
   }
-  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
-  s->primed = false;
-  s->mcc_pending = false;
-  s->host_step = 0;
-  s->since_sort = 0;
-  return GASATT_OK;
+  return sim_reset(s, 2 * n_photo);
 }
 
 int gasatt_sim_read(gasatt_sim *s, double *r, double *z, double *ur, double *ut, double *uz,

@@ -134,6 +134,12 @@ class Sim:
         ptrs = [a.ctypes.data_as(ctypes.c_void_p) for a in arrs] + [idn.ctypes.data_as(ctypes.c_void_p)]
         check(self.ctx.handle, lib.gasatt_sim_load(self.h, *ptrs, len(arrs[0]), 0))
 
+    def birth_photo(self, n_photo, photon_keV, *, seed, sigma_r=50e-6, id_base=0):
+        """Replace the particles by 2 n_photo photoionization births drawn on the
+        GPU (the laws of births(); Philox draws keyed on seed and photon)."""
+        check(self.ctx.handle, lib.gasatt_sim_birth_photo(self.h, int(n_photo), float(photon_keV),
+                                                          float(sigma_r), int(seed), int(id_base)))
+
     def step(self, n=1):
         check(self.ctx.handle, lib.gasatt_sim_step(self.h, int(n)))
 

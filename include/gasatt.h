@@ -277,6 +277,16 @@ int gasatt_sim_destroy(gasatt_sim *sim);
 int gasatt_sim_load(gasatt_sim *sim, const double *r, const double *z,
                     const double *ur, const double *ut, const double *uz,
                     const uint64_t *id, int64_t n, int on_device);
+/* Photoionization births generated on the device, replacing the particles
+ * like gasatt_sim_load (INCIDENCE1.m:51-158 draws the reference's births on
+ * the host): each of n_photo photons of photon_keV gives a photoelectron
+ * (photon energy minus the N K-shell binding, 410 eV; direction density
+ * ~ (d . x)^2 about the polarisation x) and an isotropic 360 eV Auger
+ * electron, both at a Rayleigh(sigma_r) radius (clipped inside the wall),
+ * uniform azimuth and uniform z.  Philox draws keyed on (seed, photon index).
+ * Ids: id_base + 2k (photoelectron of photon k), id_base + 2k + 1 (Auger). */
+int gasatt_sim_birth_photo(gasatt_sim *sim, int64_t n_photo, double photon_keV, double sigma_r,
+                           uint64_t seed, uint64_t id_base);
 int gasatt_sim_read(gasatt_sim *sim, double *r, double *z,
                     double *ur, double *ut, double *uz, uint64_t *id,
                     int64_t cap, int64_t *n, int on_device);
