@@ -927,11 +927,25 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
         deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, ca, cb, ra, rb, vr, vz);
         const unsigned la = (unsigned)(ra - w.row0), lb = (unsigned)(rb - w.row0);
         if (la < (unsigned)w.rows && lb < (unsigned)w.rows) {
-          const int ka = (int)la * ws, kb = (int)lb * ws;
-          atomicAdd(win_r + ka + ca, vr[0]); atomicAdd(win_z + ka + ca, vz[0]);
-          atomicAdd(win_r + ka + cb, vr[1]); atomicAdd(win_z + ka + cb, vz[1]);
-          atomicAdd(win_r + kb + ca, vr[2]); atomicAdd(win_z + kb + ca, vz[2]);
-          atomicAdd(win_r + kb + cb, vr[3]); atomicAdd(win_z + kb + cb, vz[3]);
+          // each lane visits its four nodes in an order permuted by lane & 3
+          // (swap the columns on bit 0, the rows on bit 1), so lanes on the
+          // same node quad hit four different nodes in each atomic
+          const bool sc = lane & 1, sr = lane & 2;
+          int k0 = (int)la * ws, k1 = (int)lb * ws, c0 = ca, c1 = cb;
+          int r0 = sc ? vr[1] : vr[0], r1 = sc ? vr[0] : vr[1];
+          int r2 = sc ? vr[3] : vr[2], r3 = sc ? vr[2] : vr[3];
+          int z0 = sc ? vz[1] : vz[0], z1 = sc ? vz[0] : vz[1];
+          int z2 = sc ? vz[3] : vz[2], z3 = sc ? vz[2] : vz[3];
+          if (sc) { c0 = cb; c1 = ca; }
+          if (sr) {
+            const int tk = k0; k0 = k1; k1 = tk;
+            int t = r0; r0 = r2; r2 = t; t = r1; r1 = r3; r3 = t;
+            t = z0; z0 = z2; z2 = t; t = z1; z1 = z3; z3 = t;
+          }
+          atomicAdd(win_r + k0 + c0, r0); atomicAdd(win_z + k0 + c0, z0);
+          atomicAdd(win_r + k0 + c1, r1); atomicAdd(win_z + k0 + c1, z1);
+          atomicAdd(win_r + k1 + c0, r2); atomicAdd(win_z + k1 + c0, z2);
+          atomicAdd(win_r + k1 + c1, r3); atomicAdd(win_z + k1 + c1, z3);
         } else {
           win_node(w, P, ca, ra, vr[0], vz[0]);
           win_node(w, P, cb, ra, vr[1], vz[1]);
