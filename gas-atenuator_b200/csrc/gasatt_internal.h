@@ -67,6 +67,7 @@ struct SimTables {
   std::vector<double> edep;                            // G: mean excitation loss [eV]
   double exc_kmin = 0;                                 // lowest excitation threshold [eV]
   double nu_max = 0;
+  double sigv_max = 0;   // max over the table of sigma_tot(E) v(E) [m^3/s]
   int n_exc = 0;
   double exc[5][16] = {};   // k, A, omega, nu, gamma
 };

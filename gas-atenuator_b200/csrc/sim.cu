@@ -77,6 +77,7 @@ __device__ __forceinline__ long long slots_in_use(const SimCounters *cnt) {
 struct SimParams {
   int nr, nz;
   double dr, dz, dt, c, qe, me, mu0, FN, PHIp, n_gas, nu_max, P_null, Rp, Lp, kb, m_ion, T_gas;
+  const double *gas;        // per-cell N2 density [m^-3] (n_r x n_z), or null: n_gas everywhere
   uint64_t seed;
   int secondaries;
   long long cap;
@@ -211,9 +212,17 @@ __device__ __forceinline__ void turn(double &ux, double &uy, double &uz, double 
 // subtractions are FP64 in both forms; FAST (the FP32 form) turns the
 // velocity in float.  The code is kept short: one candidate runs it alone,
 // mostly from a cold instruction cache.
+// gas density of cell (ir, iz), the neutral background of the collisions
+__device__ __forceinline__ double gas_density(const SimParams &P, int ir, int iz) {
+  if (!P.gas) return P.n_gas;
+  ir = min(max(ir, 0), P.nr - 1);
+  iz = min(max(iz, 0), P.nz - 1);
+  return P.gas[ir + (int64_t)iz * P.nr];
+}
+
 template <bool FAST>
 __device__ __forceinline__ int mcc_event(const SimParams &P, uint64_t id, long long step, double &ux,
-                                      double &uy, double &uz, Birth &b) {
+                                      double &uy, double &uz, Birth &b, double n_gas) {
   b.born = false;
   const U2 d0 = draw2(P.seed, id, step, 0);
   const double c = P.c, me = P.me, qe = P.qe, I = GASATT_ION_I_EV;
@@ -224,7 +233,7 @@ __device__ __forceinline__ int mcc_event(const SimParams &P, uint64_t id, long l
   const double um = sqrt(u2), v = um / g;
   double se, si, sx, L;
   xs_lookup(P, Eev, se, si, sx, L);
-  const double nu_el = P.n_gas * se * v, nu_io = P.n_gas * si * v, nu_ex = P.n_gas * sx * v;
+  const double nu_el = n_gas * se * v, nu_io = n_gas * si * v, nu_ex = n_gas * sx * v;
   const double X = d0.b * P.nu_max;
   if (X < nu_el) {
     const U2 d1 = draw2(P.seed, id, step, 1);
@@ -495,7 +504,8 @@ __global__ void __launch_bounds__(kMccBlock) k_mcc64(SimParams P, State64 S, Sim
     double ur = urt.x, ut = urt.y, uz = S.uz[p];
     const uint64_t id = S.id[p];
     Birth b;
-    count_event(cnt, mcc_event<false>(P, id, step, ur, ut, uz, b));
+    const double ng = gas_density(P, (int)floor(rz.x / P.dr), (int)floor(rz.y / P.dz));
+    count_event(cnt, mcc_event<false>(P, id, step, ur, ut, uz, b, ng));
     if (b.born) {
       const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
       const long long slot = n0 + (long long)kb;
@@ -783,7 +793,7 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
   float fr = __uint_as_float(A.y & ~kSign), fz = __uint_as_float(A.z & ~kSign);
   double dux = (double)__uint_as_float(A.w) * P.c, duy = (double)B.x * P.c, duz = (double)B.y * P.c;
   Birth b;
-  count_event(cnt, mcc_event<true>(P, id, cstep, dux, duy, duz, b));
+  count_event(cnt, mcc_event<true>(P, id, cstep, dux, duy, duz, b, gas_density(P, ir, iz)));
   const int mark = push ? par : (int)(cstep & 1);
   if (b.born) {
     const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
@@ -1314,6 +1324,7 @@ struct gasatt_sim {
   unsigned pass_grid = 0, mcc_grid = 0;
   int *queue = nullptr;           // collision candidates, two queues of capacity slots
   SimParams *d_P = nullptr;       // device copies of P with the current of buffer 0 / 1
+  double *d_gas = nullptr;        // per-cell gas density (gasatt_sim_set_gas_density)
   bool mcc_pending = false;       // the last pass's collisions are not applied yet
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;   // graph capture fork/join
   bool timing = false;
@@ -1489,6 +1500,30 @@ int sim_reset(gasatt_sim *s, int64_t n) {
   s->mcc_pending = false;
   s->host_step = 0;
   s->since_sort = 0;
+  return GASATT_OK;
+}
+
+// Null-collision bound for a peak gas density n_max: nu_max = n_max *
+// max(sigma_tot v), P_null = 1 - exp(-nu_max dt), and the integer threshold
+// of the candidate test on the 52-bit draw.
+void set_collision_bound(gasatt_sim *s, double n_max) {
+  SimParams &P = s->P;
+  P.nu_max = n_max * s->tabs.sigv_max;
+  P.P_null = -std::expm1(-P.nu_max * s->cfg.dt);
+  // largest count of 52-bit draws b with (2b+1) 2^-53 < P_null (exact in double)
+  uint64_t t = (uint64_t)std::floor(P.P_null * 0x1.0p52);
+  while ((2.0 * (double)t + 1.0) * 0x1.0p-53 < P.P_null) ++t;
+  while (t > 0 && !((2.0 * (double)(t - 1) + 1.0) * 0x1.0p-53 < P.P_null)) --t;
+  P.cand_below = t;
+}
+
+// device copies of P (current buffers 0 and 1) for the kernels that read it
+// from global memory
+int upload_params(gasatt_sim *s) {
+  SimParams Pq[2] = {s->P, s->P};
+  Pq[0].Jr = s->Jr[0]; Pq[0].Jz = s->Jz[0];
+  Pq[1].Jr = s->Jr[1]; Pq[1].Jz = s->Jz[1];
+  GASATT_CUDA(s->ctx, cudaMemcpy(s->d_P, Pq, sizeof(Pq), cudaMemcpyHostToDevice));
   return GASATT_OK;
 }
 
@@ -1698,7 +1733,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   SimParams &P = s->P;
   P.nr = nr; P.nz = nz; P.dr = c.dr; P.dz = c.dz; P.dt = c.dt; P.c = c.c; P.qe = c.q_e;
   P.me = c.m_e; P.mu0 = c.mu0; P.FN = c.FN; P.PHIp = c.PHIp; P.n_gas = c.gas_density;
-  P.nu_max = s->tabs.nu_max; P.P_null = -std::expm1(-s->tabs.nu_max * c.dt);
+  P.gas = nullptr;
   P.Rp = nr * c.dr; P.Lp = nz * c.dz; P.kb = c.kb; P.m_ion = c.m_ion; P.T_gas = c.gas_temperature;
   P.seed = c.seed; P.secondaries = c.secondaries; P.cap = cap;
   P.qm_dt2 = -c.q_e / c.m_e * c.dt / 2;
@@ -1712,13 +1747,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   s->scale = s->form == 0 ? std::ldexp(1.0, 48) / qfc : std::ldexp(1.0, 20) / qfc;
   P.dep = s->scale;
   P.depf = (float)(-c.q_e * c.FN * c.c * s->scale);
-  {
-    // largest count of 52-bit draws b with (2b+1) 2^-53 < P_null (exact in double)
-    uint64_t t = (uint64_t)std::floor(P.P_null * 0x1.0p52);
-    while ((2.0 * (double)t + 1.0) * 0x1.0p-53 < P.P_null) ++t;
-    while (t > 0 && !((2.0 * (double)(t - 1) + 1.0) * 0x1.0p-53 < P.P_null)) --t;
-    P.cand_below = t;
-  }
+  set_collision_bound(s, c.gas_density);
   P.sig = s->d_tab;
   P.edep = s->d_tab + 3 * c.table_n;
   P.cdf = s->d_tab + 4 * c.table_n;
@@ -1733,13 +1762,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
     if (cudaMemcpy(s->invV, iv.data(), (size_t)nr * 8, cudaMemcpyHostToDevice) != cudaSuccess)
       return cleanup(fail(ctx, GASATT_E_CUDA, "volume table upload"));
   }
-  {
-    SimParams Pq[2] = {P, P};
-    Pq[1].Jr = s->Jr[1]; Pq[1].Jz = s->Jz[1];
-    if ((rc = sim_alloc(s, &s->d_P, 2))) return cleanup(rc);
-    if (cudaMemcpy(s->d_P, Pq, sizeof(Pq), cudaMemcpyHostToDevice) != cudaSuccess)
-      return cleanup(fail(ctx, GASATT_E_CUDA, "parameter upload"));
-  }
+  if ((rc = sim_alloc(s, &s->d_P, 2)) || (rc = upload_params(s))) return cleanup(rc);
   if (fdtd_tile(c.fdtd_ratio) < 4)
     return cleanup(fail(ctx, GASATT_E_ARG, "fdtd_ratio too large for the fused field update (max 6)"));
   int dev = ctx->device, nsm = 148;
@@ -1834,6 +1857,41 @@ int gasatt_sim_load(gasatt_sim *s, const double *r, const double *z, const doubl
     GASATT_LAUNCHED(ctx);
   }
   return sim_reset(s, n);
+}
+
+int gasatt_sim_set_gas_density(gasatt_sim *s, const double *density, int on_device) {
+  if (!s) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t ncell = (size_t)s->cfg.n_r * s->cfg.n_z;
+  std::vector<double> h;
+  if (density) {
+    h.resize(ncell);
+    GASATT_CUDA(ctx, cudaMemcpy(h.data(), density, ncell * 8,
+                                on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost));
+    for (double v : h)
+      if (!(v >= 0) || !std::isfinite(v)) return fail(ctx, GASATT_E_ARG, "gas density: negative or not finite");
+  }
+  // collisions still queued were drawn against the old bound: apply them first
+  SIM_TRY(flush_collisions(s));
+  GASATT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  double n_max = s->cfg.gas_density;
+  if (density) {
+    if (!s->d_gas) {
+      int rc = sim_alloc(s, &s->d_gas, ncell);
+      if (rc) return rc;
+    }
+    GASATT_CUDA(ctx, cudaMemcpy(s->d_gas, h.data(), ncell * 8, cudaMemcpyHostToDevice));
+    n_max = 0;
+    for (double v : h) n_max = v > n_max ? v : n_max;
+    s->P.gas = s->d_gas;
+  } else {
+    s->P.gas = nullptr;
+  }
+  set_collision_bound(s, n_max);
+  SIM_TRY(upload_params(s));
+  drop_graphs(s);                  // the step graphs hold the launch parameters
+  return build_graphs(s);
 }
 
 int gasatt_sim_birth_photo(gasatt_sim *s, int64_t n_photo, double photon_keV, double sigma_r,

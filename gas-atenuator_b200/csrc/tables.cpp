@@ -181,6 +181,7 @@ int build_sim_tables(const gasatt_tables *t, int G, double emin_ev, double emax_
     }
     if (sg * vg > vmax) vmax = sg * vg;
   }
+  o.sigv_max = vmax;
   o.nu_max = n_gas * vmax;
   // mean excitation energy loss sum_j k_j s_j / sum_j s_j over the terms above
   // threshold (electron_transport.cu:207-219, get_ImpExc2.m; q0 cancels)

@@ -107,6 +107,7 @@ _SIGS = {
                                      ctypes.POINTER(ctypes.c_float),
                                      ctypes.POINTER(ctypes.c_float)]),
     "gasatt_sim_birth_photo": (c_i, [c_p, c_i64, c_d, c_d, c_u64, c_u64]),
+    "gasatt_sim_set_gas_density": (c_i, [c_p, c_p, c_i]),
     "gasatt_batch_create": (c_i, [c_p, c_p, c_i, c_i, c_p]),
     "gasatt_batch_step": (c_i, [c_p, c_i]),
     "gasatt_batch_destroy": (c_i, [c_p]),

@@ -175,6 +175,18 @@ class Sim:
         check(self.ctx.handle, lib.gasatt_sim_set_fields(self.h, *[a.ctypes.data_as(ctypes.c_void_p)
                                                                    for a in arrs], 0))
 
+    def set_gas_density(self, density):
+        """Per-cell N2 density [m^-3] of shape (n_r, n_z) for the collisions, or
+        None to go back to the uniform cfg.gas_density.  Step graphs are rebuilt;
+        a Batch must be created after this call."""
+        if density is None:
+            check(self.ctx.handle, lib.gasatt_sim_set_gas_density(self.h, None, 0))
+            return
+        a = np.asfortranarray(density, dtype=np.float64)
+        if a.shape != (self.cfg.n_r, self.cfg.n_z):
+            raise ValueError(f"gas density must have shape ({self.cfg.n_r}, {self.cfg.n_z})")
+        check(self.ctx.handle, lib.gasatt_sim_set_gas_density(self.h, a.ctypes.data_as(ctypes.c_void_p), 0))
+
     def current(self):
         nr, nz = self.cfg.n_r, self.cfg.n_z
         jr = np.zeros((nr, nz), order="F")

@@ -287,6 +287,18 @@ int gasatt_sim_load(gasatt_sim *sim, const double *r, const double *z,
  * Ids: id_base + 2k (photoelectron of photon k), id_base + 2k + 1 (Auger). */
 int gasatt_sim_birth_photo(gasatt_sim *sim, int64_t n_photo, double photon_keV, double sigma_r,
                            uint64_t seed, uint64_t id_base);
+/* Per-cell N2 density [m^-3] for the collisions: n_r x n_z values, column-major
+ * (cell ir + n_r iz covers [ir dr, (ir+1) dr) x [iz dz, (iz+1) dz)); NULL goes
+ * back to the uniform cfg->gas_density.  Replaces the density lookup by cell
+ * of electron_transport.cu:64-76 (the reference's density_cells array, which
+ * its DSMC neutral solver could fill) for the resident simulation: an electron
+ * collides against the density of the cell it ends the step in, and the
+ * null-collision bound becomes max(density) x max(sigma_tot v).  Values must be
+ * finite and >= 0 (GASATT_E_ARG otherwise).  Collisions still queued are
+ * applied first, with the old density; the step graphs are rebuilt, so a
+ * batch (gasatt_batch_create) holding this simulation must be created after
+ * the call.  on_device: 1 = device pointer, 0 = host pointer. */
+int gasatt_sim_set_gas_density(gasatt_sim *sim, const double *density, int on_device);
 int gasatt_sim_read(gasatt_sim *sim, double *r, double *z,
                     double *ur, double *ut, double *uz, uint64_t *id,
                     int64_t cap, int64_t *n, int on_device);

@@ -974,7 +974,7 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
                  double *y, double *z, double *ux, double *uy, double *uz, uint64_t *id,
                  uint8_t *alive, int64_t *n_io, int64_t cap, const double *Er, const double *Ez,
                  const double *H, double *jr, double *jz, int do_kick, int do_mcc,
-                 orc_counters *cnt) {
+                 const double *gas, orc_counters *cnt) {
   const int nr = cfg->n_r, nz = cfg->n_z;
   const double Rp = nr * cfg->dr, Lp = nz * cfg->dz, c = cfg->c, me = cfg->m_e, qe = cfg->q_e;
   const double qm_dt2 = -qe / me * cfg->dt / 2;
@@ -1036,8 +1036,17 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
           double um = sqrt(u2), v = um / g;
           double se, si, sx, L;
           xs_lookup(xs, Eev, &se, &si, &sx, &L);
-          double nu_el = cfg->gas_density * se * v, nu_io = cfg->gas_density * si * v;
-          double nu_ex = cfg->gas_density * sx * v;
+          double ng = cfg->gas_density;
+          if (gas) {
+            /* density of the cell the electron ends the step in */
+            double r = sqrt(x[p] * x[p] + y[p] * y[p]);
+            int ir = (int)floor(r / cfg->dr), iz = (int)floor(z[p] / cfg->dz);
+            ir = ir < 0 ? 0 : ir > nr - 1 ? nr - 1 : ir;
+            iz = iz < 0 ? 0 : iz > nz - 1 ? nz - 1 : iz;
+            ng = gas[ir + (int64_t)iz * nr];
+          }
+          double nu_el = ng * se * v, nu_io = ng * si * v;
+          double nu_ex = ng * sx * v;
           double X = U2 * xs->nu_max;
           if (X < nu_el) {
             double U3, U4;

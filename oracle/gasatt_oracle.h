@@ -119,12 +119,15 @@ typedef struct orc_counters {
  * deposit, then the null-collision MCC at the end of the step (an ionization
  * appends its secondary at the parent's position).  Arrays x..alive have
  * capacity cap; *n grows with births.  jr/jz receive the current density
- * [A/m^2] (overwritten). */
+ * [A/m^2] (overwritten).  gas: per-cell N2 density (n_r x n_z, column-major,
+ * cell ir = floor(r/dr), iz = floor(z/dz), both clamped to the grid) or NULL
+ * for cfg->gas_density everywhere; xs->nu_max must bound the largest density. */
 int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step,
                  double *x, double *y, double *z, double *ux, double *uy, double *uz,
                  uint64_t *id, uint8_t *alive, int64_t *n, int64_t cap,
                  const double *Er, const double *Ez, const double *H,
-                 double *jr, double *jz, int do_kick, int do_mcc, orc_counters *cnt);
+                 double *jr, double *jz, int do_kick, int do_mcc, const double *gas,
+                 orc_counters *cnt);
 /* field sub-cycle: H(-dt/4), [H(dt/2), E(dt/2)] x 2 ratio, H(dt/4), dt = cfg->dt/ratio */
 void orc_sim_fdtd(const gasatt_sim_config *cfg, double *Er, double *Ez, double *H,
                   const double *jr, const double *jz);

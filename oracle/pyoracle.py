@@ -200,8 +200,10 @@ class Sim:
 
     def __init__(self, cfg, tab, cap):
         self.cfg = cfg                      # gasatt SimConfig (ctypes structure)
+        self.tab = tab
         self.xs = XS(tab, cfg.table_n, cfg.table_emin_ev, cfg.table_emax_ev, cfg.gas_density,
                      cfg.c, cfg.m_e, cfg.q_e)
+        self.gas = None
         self.cap = cap
         self.x = np.zeros(cap); self.y = np.zeros(cap); self.z = np.zeros(cap)
         self.ux = np.zeros(cap); self.uy = np.zeros(cap); self.uz = np.zeros(cap)
@@ -225,13 +227,26 @@ class Sim:
         self.alive[:n] = 1
         self.n = n
 
+    def set_gas_density(self, density):
+        """Per-cell gas density (n_r x n_z) or None for the uniform density; the
+        null-collision bound follows the largest cell."""
+        cfg = self.cfg
+        if density is None:
+            self.gas, n_max = None, cfg.gas_density
+        else:
+            self.gas = np.asfortranarray(np.asarray(density, dtype=np.float64)
+                                         .reshape(cfg.n_r, cfg.n_z, order="F"))
+            n_max = float(self.gas.max())
+        self.xs = XS(self.tab, cfg.table_n, cfg.table_emin_ev, cfg.table_emax_ev, n_max,
+                     cfg.c, cfg.m_e, cfg.q_e)
+
     def _pass(self, step, kick, mcc):
         n = c_i64(self.n)
         rc = lib.orc_sim_pass(ctypes.byref(self.cfg), c_p(self.xs.h), c_i64(step), P(self.x),
                               P(self.y), P(self.z), P(self.ux), P(self.uy), P(self.uz), P(self.id),
                               P(self.alive), ctypes.byref(n), c_i64(self.cap), P(self.Er),
                               P(self.Ez), P(self.H), P(self.jr), P(self.jz), c_i(kick), c_i(mcc),
-                              P(self.counters))
+                              None if self.gas is None else P(self.gas), P(self.counters))
         assert rc == 0
         self.n = n.value
 

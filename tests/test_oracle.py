@@ -189,3 +189,31 @@ def test_emf6_oracle_wall_deletion_and_counts():
     assert len(e_pos) <= 295 and len(kin) == len(e_pos)
     assert np.all(np.hypot(e_pos[:, 0], e_pos[:, 1]) <= nr * d)
     assert np.all((e_pos[:, 2] >= 0) & (e_pos[:, 2] <= nz * d))
+
+
+def _oracle_sim(tables, gas=None, steps=3):
+    from gasatt.sim import births, config
+    nr, nz, d = 16, 32, 5e-6
+    cfg = config(nr, nz, d, 1e-14, 300.0, precision=_lib.FP64, capacity=8000, seed=7)
+    orc = O.Sim(cfg, tables, cap=cfg.capacity)
+    orc.load(*births(600, 8.0, nz * d, seed=3, sigma_r=30e-6, Rp=nr * d))
+    if gas is not None:
+        orc.set_gas_density(gas(cfg, nr, nz))
+    orc.prologue()
+    for _ in range(steps):
+        orc.step()
+    return orc
+
+
+def test_oracle_uniform_gas_map_equals_scalar_density(tables):
+    a = _oracle_sim(tables)
+    b = _oracle_sim(tables, lambda cfg, nr, nz: np.full((nr, nz), cfg.gas_density))
+    assert a.counters[0] > 0 and np.array_equal(a.counters, b.counters)
+    for u, v in zip(a.state_rz(), b.state_rz()):
+        assert np.array_equal(u, v)
+    assert np.array_equal(a.jr, b.jr) and np.array_equal(a.jz, b.jz)
+
+
+def test_oracle_vacuum_gas_map_has_no_collisions(tables):
+    o = _oracle_sim(tables, lambda cfg, nr, nz: np.zeros((nr, nz)))
+    assert list(o.counters[:4]) == [0, 0, 0, 0]
