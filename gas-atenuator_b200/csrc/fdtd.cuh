@@ -106,6 +106,13 @@ constexpr int kFdtdRows = 16;                          // blockDim = (32, kFdtdR
 
 __host__ __device__ inline int fdtd_tile(int R) { return kFdtdPatch - 4 * R - 1; }
 
+// A second fixed-point current added to the first (the held ion current of
+// the resident simulation), in units of rel x the first one's; Jr null: none.
+struct ExtraCurrent {
+  const unsigned long long *Jr, *Jz;
+  double rel;
+};
+
 template <typename T>
 __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ Ez,
                                            T *__restrict__ H,
@@ -114,7 +121,8 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
                                            unsigned long long *__restrict__ Jr_next,
                                            unsigned long long *__restrict__ Jz_next, int nr,
                                            int nz, const FdtdCoef &c, const double *__restrict__ invV,
-                                           double mu, double dt, int R, unsigned flags) {
+                                           double mu, double dt, int R, unsigned flags,
+                                           ExtraCurrent xj) {
   constexpr int TW = kFdtdPatch;
   __shared__ double sEr[TW * TW], sEz[TW * TW], sH[TW * TW], sJr[TW * TW], sJz[TW * TW];
   const int tile = fdtd_tile(R), hl = 2 * R, hh = 2 * R + 1;
@@ -132,8 +140,13 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
     if (i < nr && j < nz) {
       const int64_t g = i + (int64_t)j * nr;
       sH[s] = (double)H[g];
-      sJr[s] = (double)(long long)Jr[g] * invV[i];
-      sJz[s] = (double)(long long)Jz[g] * invV[i];
+      if (xj.Jr) {
+        sJr[s] = ((double)(long long)Jr[g] + (double)(long long)xj.Jr[g] * xj.rel) * invV[i];
+        sJz[s] = ((double)(long long)Jz[g] + (double)(long long)xj.Jz[g] * xj.rel) * invV[i];
+      } else {
+        sJr[s] = (double)(long long)Jr[g] * invV[i];
+        sJz[s] = (double)(long long)Jz[g] * invV[i];
+      }
     }
   }
   __syncthreads();

@@ -66,6 +66,10 @@ struct SimCounters {
   unsigned long long ion, ela, exc, nul, lost, cap_overflow;
   unsigned long long kin_fx;     // diagnostic: sum E_kin * 2^16 [eV]
   unsigned long long alive;      // diagnostic
+  unsigned long long pad5_[8];
+  unsigned long long n_ions;     // ion slots claimed (loads and births; may pass the capacity)
+  unsigned long long ion_overflow, ion_lost;
+  unsigned long long ion_alive, ion_charge, ion_kin_fx;   // diagnostics; kinetic: E * 2^32 [eV]
 };
 
 // slots holding particles, including births of the last pass not yet committed
@@ -73,6 +77,9 @@ __device__ __forceinline__ long long slots_in_use(const SimCounters *cnt) {
   const unsigned long long nt = cnt->n_total + cnt->n_births;
   return (long long)(nt < cnt->cap ? nt : cnt->cap);
 }
+
+// N2+ ions (FP64 in both forms): (r, z), (u_r, u_theta), u_z, id, charge number
+struct IonState { double2 *rz; double2 *urt; double *uz; uint64_t *id; int8_t *q; };
 
 struct SimParams {
   int nr, nz;
@@ -96,6 +103,9 @@ struct SimParams {
   int n_exc;
   double exc[5][16];
   unsigned long long *Jr, *Jz;
+  IonState ion;             // ion store (ion_cap > 0)
+  long long ion_cap;        // ions stored at most; 0: no ion species
+  double ion_sigma;         // spread of a newborn ion's velocity components sqrt(kT/m) [m/s]
 };
 
 template <typename Real>
@@ -304,6 +314,30 @@ __device__ __forceinline__ void count_event(SimCounters *cnt, int ev) {
   else if (ev == 4) atomicAdd(&cnt->nul, 1ull);
 }
 
+// The N2+ ion of an ionization of electron `id` at step `step`, at the
+// parent's position (r, z), singly charged, with a Maxwellian velocity at the
+// gas temperature: each component normal with spread sqrt(kT/m)
+// (electron_transport.cu:202-204).  The three normals are the Box-Muller
+// transforms of the Philox draws (id, step) blocks 2 and 3; the ion takes the
+// id of the secondary electron.  Takes no SimParams: a reference to a kernel
+// parameter handed to a call would copy the whole block to the stack.
+__device__ __noinline__ void ion_birth(IonState I, long long cap, double sigma, uint64_t seed,
+                                       SimCounters *cnt, uint64_t id, long long step, double r,
+                                       double z) {
+  const unsigned long long k = atomicAdd(&cnt->n_ions, 1ull);
+  if (k >= (unsigned long long)cap) { atomicAdd(&cnt->ion_overflow, 1ull); return; }
+  const U2 a = draw2(seed, id, step, 2), b = draw2(seed, id, step, 3);
+  double sa, ca, sb, cb;
+  sincos(2 * GASATT_PI * a.b, &sa, &ca);
+  sincos(2 * GASATT_PI * b.b, &sb, &cb);
+  const double ra = sigma * sqrt(-2 * log(a.a)), rb = sigma * sqrt(-2 * log(b.a));
+  I.rz[k] = make_double2(r, z);
+  I.urt[k] = make_double2(ra * ca, ra * sa);
+  I.uz[k] = rb * cb;
+  I.id[k] = child_id(id, step);
+  I.q[k] = 1;
+}
+
 // warp-aggregated append of candidate slots to the collision queue
 __device__ __forceinline__ void queue_push(bool want, long long p, unsigned long long *n_cand,
                                            int *queue) {
@@ -411,8 +445,8 @@ __device__ __forceinline__ void halfdrift64(double &r, double &z, double &ur, do
 }
 
 __device__ __forceinline__ void deposit_values64(const SimParams &P, double r, double z,
-                                                 double ur, double ut, double uz, int64_t a[4],
-                                                 long long vr[4], long long vz[4],
+                                                 double ur, double ut, double uz, double q,
+                                                 int64_t a[4], long long vr[4], long long vz[4],
                                                  unsigned &key) {
   const double g = sqrt(1 + (ur * ur + ut * ut + uz * uz) / (P.c * P.c));
   const double vrr = ur / g, vzz = uz / g;
@@ -420,7 +454,6 @@ __device__ __forceinline__ void deposit_values64(const SimParams &P, double r, d
   const int ar = em7_weights(r, z, P.nr, P.nz, P.dr, P.dz, a, b);
   const int az = (int)floor(z / P.dz - 0.5);
   key = (unsigned)((ar + 1) + (az + 1) * (P.nr + 1));
-  const double q = -P.qe;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     vr[k] = __double2ll_rn(P.FN * b[k] * q * vrr * P.dep);
@@ -476,7 +509,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fi
     int64_t a[4] = {0, 0, 0, 0};
     long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
     unsigned key = 0;
-    if (act) deposit_values64(P, rz.x, rz.y, urt.x, urt.y, uz, a, vr, vz, key);
+    if (act) deposit_values64(P, rz.x, rz.y, urt.x, urt.y, uz, -P.qe, a, vr, vz, key);
     warp_deposit<long long>(act, key, a, vr, vz, P.Jr, P.Jz);
   }
   lost = __reduce_add_sync(0xFFFFFFFFu, lost);
@@ -505,7 +538,9 @@ __global__ void __launch_bounds__(kMccBlock) k_mcc64(SimParams P, State64 S, Sim
     const uint64_t id = S.id[p];
     Birth b;
     const double ng = gas_density(P, (int)floor(rz.x / P.dr), (int)floor(rz.y / P.dz));
-    count_event(cnt, mcc_event<false>(P, id, step, ur, ut, uz, b, ng));
+    const int ev = mcc_event<false>(P, id, step, ur, ut, uz, b, ng);
+    count_event(cnt, ev);
+    if (ev == 2 && P.ion_cap > 0) ion_birth(P.ion, P.ion_cap, P.ion_sigma, P.seed, cnt, id, step, rz.x, rz.y);
     if (b.born) {
       const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
       const long long slot = n0 + (long long)kb;
@@ -519,6 +554,109 @@ __global__ void __launch_bounds__(kMccBlock) k_mcc64(SimParams P, State64 S, Sim
       }
     }
     S.urt[p] = make_double2(ur, ut); S.uz[p] = uz;
+  }
+}
+
+// ----------------------------------------------------------- ions
+// Ion push, once every ion_subcycle electron steps: P is the simulation's
+// parameter block with dt = the ion step, qm_dt2 = q_e/m_ion dt/2 and the
+// ion current buffers as Jr/Jz (cleared before the launch), dep = the
+// fixed-point factor of the ion current.  Per ion: gather, Boris kick with
+// charge Z q_e, two half drifts (the electrons' walls: absorbed beyond Rp,
+// reflected at z = 0 and Lp), deposit of Z q_e FN v at the new position.  The
+// field update adds the ion current to the electrons' until the next push
+// (charge moved over the ion step = the held current x the ion step).
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_ion_push(SimParams P, Fields<T> F, SimCounters *cnt) {
+  const unsigned long long nc = cnt->n_ions;
+  const long long n = (long long)(nc < (unsigned long long)P.ion_cap ? nc : P.ion_cap);
+  const IonState I = P.ion;
+  unsigned lost = 0;
+  for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
+       base += (long long)gridDim.x * blockDim.x) {
+    const long long p = base + (threadIdx.x & 31);
+    bool act = p < n;
+    double2 rz = make_double2(-1.0, 0.0), urt = make_double2(0.0, 0.0);
+    double uz = 0, Zq = 0;
+    if (act) {
+      rz = I.rz[p];
+      act = rz.x >= 0;
+    }
+    if (act) {
+      urt = I.urt[p]; uz = I.uz[p];
+      Zq = (double)I.q[p];
+      double r = rz.x, z = rz.y, ur = urt.x, ut = urt.y;
+      bool alive = true;
+      double E_r, E_z, Hp;
+      gather3<T>(F.Er, F.Ez, F.H, P.nr, P.nz, P.dr, P.dz, r, z, E_r, E_z, Hp);
+      boris(ur, ut, uz, E_r, 0.0, E_z, 0.0, P.mu0 * Hp, 0.0, Zq * P.qm_dt2, P.c);
+      halfdrift64(r, z, ur, ut, uz, alive, P);
+      if (alive) halfdrift64(r, z, ur, ut, uz, alive, P);
+      if (!alive) { lost++; r = -1.0; }
+      rz = make_double2(r, z); urt = make_double2(ur, ut);
+      I.rz[p] = rz; I.urt[p] = urt; I.uz[p] = uz;
+      act = alive;
+    }
+    int64_t a[4] = {0, 0, 0, 0};
+    long long vr[4] = {0, 0, 0, 0}, vz[4] = {0, 0, 0, 0};
+    unsigned key = 0;
+    if (act) deposit_values64(P, rz.x, rz.y, urt.x, urt.y, uz, Zq * P.qe, a, vr, vz, key);
+    warp_deposit<long long>(act, key, a, vr, vz, P.Jr, P.Jz);
+  }
+  lost = __reduce_add_sync(0xFFFFFFFFu, lost);
+  if ((threadIdx.x & 31) == 0 && lost) atomicAdd(&cnt->ion_lost, (unsigned long long)lost);
+}
+
+// ion diagnostics: alive, sum of charge numbers, kinetic energy (fixed point)
+__global__ void k_ion_diag(IonState I, long long cap, SimCounters *cnt, double c, double m_ion,
+                           double qe) {
+  const unsigned long long nc = cnt->n_ions;
+  const long long n = (long long)(nc < (unsigned long long)cap ? nc : cap);
+  unsigned long long kin = 0, alive = 0, charge = 0;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    if (I.rz[p].x < 0) continue;
+    const double2 a = I.urt[p];
+    const double w = I.uz[p];
+    const double u2 = (a.x * a.x + a.y * a.y + w * w) / (c * c);
+    const double g = sqrt(1 + u2);
+    kin += (unsigned long long)__double2ll_rn(m_ion * c * c * (u2 / (g + 1)) / qe * 4294967296.0);
+    alive++;
+    charge += (unsigned long long)I.q[p];
+  }
+  for (int o = 16; o; o >>= 1) {
+    kin += __shfl_down_sync(0xFFFFFFFFu, kin, o);
+    alive += __shfl_down_sync(0xFFFFFFFFu, alive, o);
+    charge += __shfl_down_sync(0xFFFFFFFFu, charge, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&cnt->ion_kin_fx, kin);
+    atomicAdd(&cnt->ion_alive, alive);
+    atomicAdd(&cnt->ion_charge, charge);
+  }
+}
+
+__global__ void k_ion_load(IonState I, const double *r, const double *z, const double *ur,
+                           const double *ut, const double *uz, const uint64_t *id,
+                           const int8_t *q, long long n) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    I.rz[p] = make_double2(r[p], z[p]);
+    I.urt[p] = make_double2(ur[p], ut[p]);
+    I.uz[p] = uz[p];
+    I.id[p] = id[p];
+    I.q[p] = q ? q[p] : (int8_t)1;
+  }
+}
+
+__global__ void k_ion_read(IonState I, double *r, double *z, double *ur, double *ut, double *uz,
+                           uint64_t *id, int8_t *q, long long n) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double2 a = I.rz[p], b = I.urt[p];
+    r[p] = a.x; z[p] = a.y; ur[p] = b.x; ut[p] = b.y; uz[p] = I.uz[p];
+    id[p] = I.id[p];
+    q[p] = I.q[p];
   }
 }
 
@@ -793,7 +931,11 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
   float fr = __uint_as_float(A.y & ~kSign), fz = __uint_as_float(A.z & ~kSign);
   double dux = (double)__uint_as_float(A.w) * P.c, duy = (double)B.x * P.c, duz = (double)B.y * P.c;
   Birth b;
-  count_event(cnt, mcc_event<true>(P, id, cstep, dux, duy, duz, b, gas_density(P, ir, iz)));
+  const int ev = mcc_event<true>(P, id, cstep, dux, duy, duz, b, gas_density(P, ir, iz));
+  count_event(cnt, ev);
+  if (ev == 2 && P.ion_cap > 0)
+    ion_birth(P.ion, P.ion_cap, P.ion_sigma, P.seed, cnt, id, cstep, ((double)ir + (double)fr) * P.dr,
+              ((double)iz + (double)fz) * P.dz);
   const int mark = push ? par : (int)(cstep & 1);
   if (b.born) {
     const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
@@ -1008,7 +1150,7 @@ __global__ void __launch_bounds__(32 * kFdtdRows) k_sim_fdtd(T *Er, T *Ez, T *H,
                                                   unsigned long long *Jz_next, int nr, int nz,
                                                   FdtdCoef c, const double *invV, double mu,
                                                   double dt, int R, unsigned flags,
-                                                  SimCounters *cnt) {
+                                                  SimCounters *cnt, ExtraCurrent ion) {
   // FP32 form (cnt given): commit the previous pass and open step s - the
   // births of the last pass join the slots, the queue that pass consumed is
   // emptied, the chunk counter rewinds; no other kernel runs meanwhile
@@ -1021,7 +1163,7 @@ __global__ void __launch_bounds__(32 * kFdtdRows) k_sim_fdtd(T *Er, T *Ez, T *H,
     cnt->chunk_next = 0;
     cnt->step = ns;
   }
-  fdtd_tiled<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, c, invV, mu, dt, R, flags);
+  fdtd_tiled<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, c, invV, mu, dt, R, flags, ion);
 }
 
 // ---------------------------------------------------------- load/read
@@ -1325,6 +1467,11 @@ struct gasatt_sim {
   int *queue = nullptr;           // collision candidates, two queues of capacity slots
   SimParams *d_P = nullptr;       // device copies of P with the current of buffer 0 / 1
   double *d_gas = nullptr;        // per-cell gas density (gasatt_sim_set_gas_density)
+  // ions (cfg.ion_capacity > 0): the store lives in P.ion; the ion current,
+  // deposited by each ion push and held until the next, in fixed point with
+  // the factor ion_scale (2^48 per q_e FN c, in both forms)
+  unsigned long long *Jir = nullptr, *Jiz = nullptr;
+  double ion_scale = 1.0;
   bool mcc_pending = false;       // the last pass's collisions are not applied yet
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;   // graph capture fork/join
   bool timing = false;
@@ -1365,14 +1512,16 @@ int launch_fdtd(gasatt_sim *s, cudaStream_t st, int q) {
   const dim3 grid((nr + 1 + tile - 1) / tile, (nz + 1 + tile - 1) / tile);
   const dim3 block(32, kFdtdRows);
   const double dt = c.dt / R;
+  // the held ion current, in the electron current's fixed-point units
+  const ExtraCurrent ion{s->Jir, s->Jiz, s->scale / s->ion_scale};
   if (s->form == 0)
     k_sim_fdtd<double><<<grid, block, 0, st>>>(
         (double *)s->Er, (double *)s->Ez, (double *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
-        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, nullptr);
+        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, nullptr, ion);
   else
     k_sim_fdtd<float><<<grid, block, 0, st>>>(
         (float *)s->Er, (float *)s->Ez, (float *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
-        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt);
+        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt, ion);
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "fdtd launch");
@@ -1439,6 +1588,35 @@ int flush_collisions(gasatt_sim *s) {
   return GASATT_OK;
 }
 
+// Ion push after step host_step when it completes a sub-cycle.  Collisions
+// still queued are applied first, so that the ions born in the step just
+// taken are pushed with the others.
+int launch_ion_push(gasatt_sim *s, cudaStream_t st) {
+  SIM_TRY(flush_collisions(s));
+  const size_t nc = (size_t)s->cfg.n_r * s->cfg.n_z;
+  GASATT_CUDA(s->ctx, cudaMemsetAsync(s->Jir, 0, nc * 8, st));
+  GASATT_CUDA(s->ctx, cudaMemsetAsync(s->Jiz, 0, nc * 8, st));
+  const auto &c = s->cfg;
+  SimParams PI = s->P;
+  PI.dt = c.dt * c.ion_subcycle;
+  PI.qm_dt2 = c.q_e / c.m_ion * PI.dt / 2;
+  PI.dep = s->ion_scale;
+  PI.Jr = s->Jir; PI.Jz = s->Jiz;
+  const unsigned g = grid_for(c.ion_capacity, kBlock) < s->pass_grid ? grid_for(c.ion_capacity, kBlock) : s->pass_grid;
+  if (s->form == 0)
+    k_ion_push<double><<<g, kBlock, 0, st>>>(PI, Fields<double>{(double *)s->Er, (double *)s->Ez, (double *)s->H}, s->cnt);
+  else
+    k_ion_push<float><<<g, kBlock, 0, st>>>(PI, Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H}, s->cnt);
+  s->ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(s->ctx, e, "ion push launch");
+  return GASATT_OK;
+}
+
+bool ion_push_due(const gasatt_sim *s) {
+  return s->cfg.ion_capacity > 0 && s->host_step % s->cfg.ion_subcycle == 0;
+}
+
 // sort from buffer `from` into 1 - from
 int launch_sort(gasatt_sim *s, cudaStream_t st, int from) {
   const auto &c = s->cfg;
@@ -1494,6 +1672,10 @@ int sim_reset(gasatt_sim *s, int64_t n) {
   for (int q = 0; q < 2; ++q) {
     GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
     GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+  }
+  if (s->Jir) {                    // a new run: no ions, no ion current
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jir, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jiz, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
   }
   GASATT_CUDA(ctx, cudaStreamSynchronize(st));
   s->primed = false;
@@ -1655,6 +1837,7 @@ int gasatt_sim_default_config(gasatt_sim_config *c) {
   c->precision = GASATT_FP32_SPLIT;
   c->capacity = 1 << 20;
   c->ion_capacity = 0;
+  c->ion_subcycle = 50;
   c->seed = 0;
   c->flags = 0;
   c->sort_period = 20;
@@ -1675,6 +1858,9 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
     return fail(ctx, GASATT_E_ARG, "sim config out of range");
   if (c.flags & ~(unsigned)(GASATT_Q_ER_END_COPY | GASATT_Q_EZ_AXIS_JSIGN | GASATT_Q_EZ_RSHIFT))
     return fail(ctx, GASATT_E_ARG, "the resident simulation accepts only the field quirk flags");
+  if (c.ion_capacity < 0 || (c.ion_capacity > 0 && (c.ion_subcycle < 1 || !(c.m_ion > 0) ||
+                                                     !(c.gas_temperature >= 0))))
+    return fail(ctx, GASATT_E_ARG, "ion species: ion_capacity >= 0, ion_subcycle >= 1, m_ion > 0");
   GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
   gasatt_sim *s = new gasatt_sim();
   s->ctx = ctx;
@@ -1700,6 +1886,15 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
     }
   }
   if ((rc = sim_alloc(s, &s->queue, 2 * (size_t)cap))) return cleanup(rc);
+  if (c.ion_capacity > 0) {
+    IonState &I = s->P.ion;
+    const size_t ic = (size_t)c.ion_capacity;
+    if ((rc = sim_alloc(s, &I.rz, ic)) || (rc = sim_alloc(s, &I.urt, ic)) ||
+        (rc = sim_alloc(s, &I.uz, ic)) || (rc = sim_alloc(s, &I.id, ic)) ||
+        (rc = sim_alloc(s, &I.q, ic)) || (rc = sim_alloc(s, &s->Jir, (size_t)c.n_r * c.n_z)) ||
+        (rc = sim_alloc(s, &s->Jiz, (size_t)c.n_r * c.n_z)))
+      return cleanup(rc);
+  }
   const size_t esz = s->form == 0 ? 8 : 4;
   double *tmpd;
   if ((rc = sim_alloc(s, (char **)&s->Er, (size_t)nr * (nz + 1) * esz)) ||
@@ -1736,6 +1931,8 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   P.gas = nullptr;
   P.Rp = nr * c.dr; P.Lp = nz * c.dz; P.kb = c.kb; P.m_ion = c.m_ion; P.T_gas = c.gas_temperature;
   P.seed = c.seed; P.secondaries = c.secondaries; P.cap = cap;
+  P.ion_cap = c.ion_capacity;
+  P.ion_sigma = c.ion_capacity > 0 ? std::sqrt(c.kb * c.gas_temperature / c.m_ion) : 0.0;
   P.qm_dt2 = -c.q_e / c.m_e * c.dt / 2;
   P.aE = (float)(-c.q_e * c.dt / (2 * c.m_e * c.c));
   P.aB = (float)(-c.q_e * c.dt * c.mu0 / (2 * c.m_e));
@@ -1747,6 +1944,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   s->scale = s->form == 0 ? std::ldexp(1.0, 48) / qfc : std::ldexp(1.0, 20) / qfc;
   P.dep = s->scale;
   P.depf = (float)(-c.q_e * c.FN * c.c * s->scale);
+  s->ion_scale = std::ldexp(1.0, 48) / qfc;
   set_collision_bound(s, c.gas_density);
   P.sig = s->d_tab;
   P.edep = s->d_tab + 3 * c.table_n;
@@ -1794,6 +1992,10 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   for (int q = 0; q < 2; ++q) {
     cudaMemset(s->Jr[q], 0, (size_t)ncell * 8);
     cudaMemset(s->Jz[q], 0, (size_t)ncell * 8);
+  }
+  if (s->Jir) {
+    cudaMemset(s->Jir, 0, (size_t)ncell * 8);
+    cudaMemset(s->Jiz, 0, (size_t)ncell * 8);
   }
   for (int i = 0; i < 6; ++i)
     if (cudaEventCreate(&s->ev[i]) != cudaSuccess) return cleanup(fail(ctx, GASATT_E_CUDA, "event"));
@@ -1967,6 +2169,93 @@ int gasatt_sim_read(gasatt_sim *s, double *r, double *z, double *ur, double *ut,
   return GASATT_OK;
 }
 
+int gasatt_sim_load_ions(gasatt_sim *s, const double *r, const double *z, const double *ur,
+                         const double *ut, const double *uz, const uint64_t *id,
+                         const int8_t *charge, int64_t n, int on_device) {
+  if (!s) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  if (s->cfg.ion_capacity <= 0) return fail(ctx, GASATT_E_STATE, "load_ions: no ion species (ion_capacity 0)");
+  if (n < 0 || n > s->cfg.ion_capacity) return fail(ctx, GASATT_E_CAPACITY, "load_ions exceeds ion_capacity");
+  if (n > 0 && (!r || !z || !ur || !ut || !uz || !id)) return fail(ctx, GASATT_E_ARG, "load_ions: null array");
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  SIM_TRY(flush_collisions(s));
+  const double *src[5] = {r, z, ur, ut, uz};
+  const double *d[5] = {r, z, ur, ut, uz};
+  const uint64_t *did = id;
+  const int8_t *dq = charge;
+  if (!on_device && n > 0) {
+    void *buf = nullptr;
+    int rc = scratch(ctx, (size_t)n * 49, &buf);
+    if (rc) return rc;
+    for (int i = 0; i < 5; ++i) {
+      d[i] = (double *)buf + (size_t)i * n;
+      GASATT_CUDA(ctx, cudaMemcpyAsync((void *)d[i], src[i], (size_t)n * 8, cudaMemcpyHostToDevice, st));
+    }
+    did = (uint64_t *)((double *)buf + 5 * (size_t)n);
+    GASATT_CUDA(ctx, cudaMemcpyAsync((void *)did, id, (size_t)n * 8, cudaMemcpyHostToDevice, st));
+    if (charge) {
+      dq = (int8_t *)(did + n);
+      GASATT_CUDA(ctx, cudaMemcpyAsync((void *)dq, charge, (size_t)n, cudaMemcpyHostToDevice, st));
+    }
+  }
+  if (n > 0) {
+    k_ion_load<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->P.ion, d[0], d[1], d[2], d[3], d[4], did, dq, n);
+    GASATT_LAUNCHED(ctx);
+  }
+  const unsigned long long zc[3] = {(unsigned long long)n, 0ull, 0ull};   // n_ions, overflow, lost
+  GASATT_CUDA(ctx, cudaMemcpyAsync((char *)s->cnt + offsetof(SimCounters, n_ions), zc, sizeof(zc),
+                                   cudaMemcpyHostToDevice, st));
+  const size_t nc = (size_t)s->cfg.n_r * s->cfg.n_z;
+  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jir, 0, nc * 8, st));
+  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jiz, 0, nc * 8, st));
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));    // the host arrays zc and charge go out of scope
+  return GASATT_OK;
+}
+
+int gasatt_sim_read_ions(gasatt_sim *s, double *r, double *z, double *ur, double *ut, double *uz,
+                         uint64_t *id, int8_t *charge, int64_t cap, int64_t *n_out, int on_device) {
+  if (!s) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  if (s->cfg.ion_capacity <= 0) {
+    if (n_out) *n_out = 0;
+    return GASATT_OK;
+  }
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  SIM_TRY(flush_collisions(s));
+  GASATT_CUDA(ctx, cudaMemcpyAsync(s->h_cnt, s->cnt, sizeof(SimCounters), cudaMemcpyDeviceToHost, st));
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  const unsigned long long nc = s->h_cnt->n_ions;
+  const int64_t n = (int64_t)(nc < (unsigned long long)s->cfg.ion_capacity ? nc : s->cfg.ion_capacity);
+  if (n_out) *n_out = n;
+  if (n > cap) return fail(ctx, GASATT_E_CAPACITY, "read_ions buffer too small");
+  if (n == 0) return GASATT_OK;
+  if (!r || !z || !ur || !ut || !uz || !id || !charge) return fail(ctx, GASATT_E_ARG, "read_ions: null array");
+  double *d[5] = {r, z, ur, ut, uz};
+  uint64_t *did = id;
+  int8_t *dq = charge;
+  if (!on_device) {
+    void *buf = nullptr;
+    int rc = scratch(ctx, (size_t)n * 49, &buf);
+    if (rc) return rc;
+    for (int i = 0; i < 5; ++i) d[i] = (double *)buf + (size_t)i * n;
+    did = (uint64_t *)((double *)buf + 5 * (size_t)n);
+    dq = (int8_t *)(did + n);
+  }
+  k_ion_read<<<grid_for(n, kBlock), kBlock, 0, st>>>(s->P.ion, d[0], d[1], d[2], d[3], d[4], did, dq, n);
+  GASATT_LAUNCHED(ctx);
+  if (!on_device) {
+    double *h[5] = {r, z, ur, ut, uz};
+    for (int i = 0; i < 5; ++i)
+      GASATT_CUDA(ctx, cudaMemcpyAsync(h[i], d[i], (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    GASATT_CUDA(ctx, cudaMemcpyAsync(id, did, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    GASATT_CUDA(ctx, cudaMemcpyAsync(charge, dq, (size_t)n, cudaMemcpyDeviceToHost, st));
+  }
+  GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+  return GASATT_OK;
+}
+
 namespace {
 __global__ void k_f64_to_f32(const double *a, float *b, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -2084,6 +2373,7 @@ int gasatt_sim_step(gasatt_sim *s, int nsteps) {
     s->host_step++;
     s->since_sort++;
     s->mcc_pending = true;
+    if (ion_push_due(s)) SIM_TRY(launch_ion_push(s, st));
   }
   return GASATT_OK;
 }
@@ -2098,6 +2388,12 @@ int gasatt_sim_diag(gasatt_sim *s, gasatt_diag *d) {
   if (s->form == 0) k_diag<0><<<s->pass_grid, kBlock, 0, st>>>(s->s64[s->cur], s->s32[s->cur], s->cnt, s->cfg.c, s->cfg.m_e, s->cfg.q_e);
   else k_diag<1><<<s->pass_grid, kBlock, 0, st>>>(s->s64[s->cur], s->s32[s->cur], s->cnt, s->cfg.c, s->cfg.m_e, s->cfg.q_e);
   GASATT_LAUNCHED(ctx);
+  if (s->cfg.ion_capacity > 0) {
+    GASATT_CUDA(ctx, cudaMemsetAsync((char *)s->cnt + offsetof(SimCounters, ion_alive), 0, 24, st));
+    k_ion_diag<<<s->pass_grid, kBlock, 0, st>>>(s->P.ion, s->cfg.ion_capacity, s->cnt, s->cfg.c,
+                                                  s->cfg.m_ion, s->cfg.q_e);
+    GASATT_LAUNCHED(ctx);
+  }
   const int nr = s->cfg.n_r, nz = s->cfg.n_z;
   if (s->form == 0)
     k_field_energy<double><<<s->partial_blocks, kBlock, 0, st>>>((double *)s->Er, (double *)s->Ez, (double *)s->H, nr, nz, s->cfg.dr, s->cfg.dz, s->partial);
@@ -2118,11 +2414,14 @@ int gasatt_sim_diag(gasatt_sim *s, gasatt_diag *d) {
   d->n_excitation = (int64_t)h.exc;
   d->n_null = (int64_t)h.nul;
   d->n_lost_wall = (int64_t)h.lost;
-  d->n_ions = 0;
+  d->n_ions = (int64_t)h.ion_alive;
   d->kinetic_ev = (double)h.kin_fx / 65536.0;
   d->field_energy_j = s->cfg.PHIp * 0.5 * s->cfg.eps0 * we + s->cfg.PHIp * 0.5 * s->cfg.mu0 * wm;
   d->steps = s->host_step;
-  d->status_flags = (h.cap_overflow ? 2 : 0);
+  d->status_flags = (h.cap_overflow ? 2 : 0) | (h.ion_overflow ? 4 : 0);
+  d->n_ion_lost_wall = (int64_t)h.ion_lost;
+  d->ion_kinetic_ev = (double)h.ion_kin_fx / 4294967296.0;
+  d->net_charge_c = s->cfg.q_e * s->cfg.FN * ((double)h.ion_charge - (double)h.alive);
   return GASATT_OK;
 }
 
@@ -2373,6 +2672,7 @@ int gasatt_batch_step(gasatt_batch *b, int nsteps) {
       s->host_step++;
       s->since_sort++;
       s->mcc_pending = true;
+      if (ion_push_due(s)) SIM_TRY(launch_ion_push(s, st));
     }
   }
   return GASATT_OK;

@@ -52,14 +52,16 @@ class SimConfig(ctypes.Structure):
                 ("eps0", c_d), ("mu0", c_d), ("kb", c_d), ("m_ion", c_d),
                 ("precision", c_i), ("capacity", c_i64), ("ion_capacity", c_i64),
                 ("seed", c_u64), ("flags", c_u), ("sort_period", c_i), ("secondaries", c_i),
-                ("table_n", c_i), ("table_emin_ev", c_d), ("table_emax_ev", c_d)]
+                ("table_n", c_i), ("table_emin_ev", c_d), ("table_emax_ev", c_d),
+                ("ion_subcycle", c_i)]
 
 
 class Diag(ctypes.Structure):
     _fields_ = [("n_alive", c_i64), ("n_total", c_i64), ("n_ionizations", c_i64),
                 ("n_elastic", c_i64), ("n_excitation", c_i64), ("n_null", c_i64),
                 ("n_lost_wall", c_i64), ("n_ions", c_i64), ("kinetic_ev", c_d),
-                ("field_energy_j", c_d), ("steps", c_i64), ("status_flags", ctypes.c_int32)]
+                ("field_energy_j", c_d), ("steps", c_i64), ("status_flags", ctypes.c_int32),
+                ("n_ion_lost_wall", c_i64), ("ion_kinetic_ev", c_d), ("net_charge_c", c_d)]
 
 
 _SIGS = {
@@ -108,6 +110,8 @@ _SIGS = {
                                      ctypes.POINTER(ctypes.c_float)]),
     "gasatt_sim_birth_photo": (c_i, [c_p, c_i64, c_d, c_d, c_u64, c_u64]),
     "gasatt_sim_set_gas_density": (c_i, [c_p, c_p, c_i]),
+    "gasatt_sim_load_ions": (c_i, [c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_i64, c_i]),
+    "gasatt_sim_read_ions": (c_i, [c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_i64, c_p, c_i]),
     "gasatt_batch_create": (c_i, [c_p, c_p, c_i, c_i, c_p]),
     "gasatt_batch_step": (c_i, [c_p, c_i]),
     "gasatt_batch_destroy": (c_i, [c_p]),

@@ -25,7 +25,8 @@ def gas_density(torr, T=300.0):
 
 
 def config(n_r, n_z, delta, dt, torr, *, precision=_lib.FP32_SPLIT, capacity=1 << 20, seed=0,
-           sort_period=20, secondaries=1, FN=1.0, fdtd_ratio=1, flags=0):
+           sort_period=20, secondaries=1, FN=1.0, fdtd_ratio=1, flags=0, ion_capacity=0,
+           ion_subcycle=50):
     cfg = SimConfig()
     check(None, lib.gasatt_sim_default_config(ctypes.byref(cfg)))
     cfg.n_r, cfg.n_z, cfg.dr, cfg.dz, cfg.dt = n_r, n_z, delta, delta, dt
@@ -38,6 +39,8 @@ def config(n_r, n_z, delta, dt, torr, *, precision=_lib.FP32_SPLIT, capacity=1 <
     cfg.FN = FN
     cfg.fdtd_ratio = fdtd_ratio
     cfg.flags = flags
+    cfg.ion_capacity = int(ion_capacity)
+    cfg.ion_subcycle = int(ion_subcycle)
     return cfg
 
 
@@ -160,6 +163,35 @@ class Sim:
         k = n.value
         return dict(r=out[0][:k], z=out[1][:k], ur=out[2][:k], ut=out[3][:k], uz=out[4][:k],
                     id=ids[:k])
+
+    def load_ions(self, r, z, ur, ut, uz, ids, charge=None):
+        """Replace the ions (host arrays; charge numbers 1 or 2, default all 1).
+        Needs cfg.ion_capacity > 0; call after load / birth_photo."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (r, z, ur, ut, uz)]
+        idn = np.ascontiguousarray(ids, dtype=np.uint64)
+        q = None if charge is None else np.ascontiguousarray(charge, dtype=np.int8)
+        ptrs = [a.ctypes.data_as(ctypes.c_void_p) for a in arrs] + [idn.ctypes.data_as(ctypes.c_void_p)]
+        qp = None if q is None else q.ctypes.data_as(ctypes.c_void_p)
+        check(self.ctx.handle, lib.gasatt_sim_load_ions(self.h, *ptrs, qp, len(arrs[0]), 0))
+
+    def read_ions(self):
+        """Ion slots in use as a dict like read(), plus the charge numbers
+        (dead ions have r = -1)."""
+        n = ctypes.c_int64()
+        # a first call with no room only reports the count
+        lib.gasatt_sim_read_ions(self.h, None, None, None, None, None, None, None, 0,
+                                 ctypes.byref(n), 0)
+        cap = max(n.value, 1)
+        out = [np.zeros(cap) for _ in range(5)]
+        ids = np.zeros(cap, np.uint64)
+        q = np.zeros(cap, np.int8)
+        ptrs = [a.ctypes.data_as(ctypes.c_void_p) for a in out] + [
+            ids.ctypes.data_as(ctypes.c_void_p), q.ctypes.data_as(ctypes.c_void_p)]
+        if n.value:
+            check(self.ctx.handle, lib.gasatt_sim_read_ions(self.h, *ptrs, cap, ctypes.byref(n), 0))
+        k = n.value
+        return dict(r=out[0][:k], z=out[1][:k], ur=out[2][:k], ut=out[3][:k], uz=out[4][:k],
+                    id=ids[:k], charge=q[:k])
 
     def fields(self):
         nr, nz = self.cfg.n_r, self.cfg.n_z

@@ -243,13 +243,18 @@ typedef struct gasatt_sim_config {
   double   q_e, m_e, c, eps0, mu0, kb, m_ion;  /* constants (SI); q_e > 0 */
   int      precision;       /* GASATT_FP64 / GASATT_FP32_SPLIT */
   int64_t  capacity;        /* max electrons */
-  int64_t  ion_capacity;    /* max ions (0: ions are counted, not stored) */
+  int64_t  ion_capacity;    /* N2+ ions stored at most (0: no ion species; ionizations are
+                               only counted).  One ion per ionization, born at the parent's
+                               position with a Maxwellian velocity at gas_temperature
+                               (electron_transport.cu:202-204), pushed in the same fields
+                               every ion_subcycle steps, its current added to the electrons' */
   uint64_t seed;
   unsigned flags;           /* quirk flags (0 for the product) */
   int      sort_period;     /* steps between cell re-sorts (0 = never) */
   int      secondaries;     /* 1: ionization births enabled */
   int      table_n;         /* log-energy grid points (2048) */
   double   table_emin_ev, table_emax_ev;  /* 0.1 eV, 30 keV */
+  int      ion_subcycle;    /* electron steps per ion push (50); the ion step is ion_subcycle*dt */
 } gasatt_sim_config;
 
 typedef struct gasatt_diag {
@@ -258,11 +263,15 @@ typedef struct gasatt_diag {
   int64_t n_ionizations;    /* cumulative ionization events (= secondaries born) */
   int64_t n_elastic, n_excitation, n_null;   /* cumulative collision branches */
   int64_t n_lost_wall;      /* cumulative electrons absorbed at r = Rp */
-  int64_t n_ions;           /* ions stored (ion_capacity > 0) */
+  int64_t n_ions;           /* ions alive in the store (ion_capacity > 0) */
   double  kinetic_ev;       /* sum of electron kinetic energy [eV] (x FN not applied) */
   double  field_energy_j;   /* electromagnetic field energy [J] */
   int64_t steps;            /* steps taken */
-  int32_t status_flags;     /* bit0 NaN seen, bit1 capacity overflow */
+  int32_t status_flags;     /* bit0 NaN seen, bit1 capacity overflow, bit2 ion capacity overflow */
+  int64_t n_ion_lost_wall;  /* cumulative ions absorbed at r = Rp */
+  double  ion_kinetic_ev;   /* sum of ion kinetic energy [eV] (x FN not applied) */
+  double  net_charge_c;     /* charge of the macro-particles in the domain [C]:
+                               q_e FN (sum of ion charge numbers - electrons alive) */
 } gasatt_diag;
 
 typedef struct gasatt_sim gasatt_sim;
@@ -287,6 +296,19 @@ int gasatt_sim_load(gasatt_sim *sim, const double *r, const double *z,
  * Ids: id_base + 2k (photoelectron of photon k), id_base + 2k + 1 (Auger). */
 int gasatt_sim_birth_photo(gasatt_sim *sim, int64_t n_photo, double photon_keV, double sigma_r,
                            uint64_t seed, uint64_t id_base);
+/* Ion species (cfg->ion_capacity > 0).  load_ions replaces the ions (the
+ * reference's ion1 and ion2 arrays of electricmagneticfield6.m:1, charge
+ * numbers 1 and 2, mass cfg->m_ion, electricmagneticfield6.m:6-7,68-69); charge
+ * NULL means all singly charged.  gasatt_sim_load and gasatt_sim_birth_photo
+ * start a new run and clear the ions, so load ions after them.  read_ions
+ * returns the ion slots in use (dead ions: r = -1), the same layout as
+ * gasatt_sim_read.  Ions are FP64 in both precision forms. */
+int gasatt_sim_load_ions(gasatt_sim *sim, const double *r, const double *z,
+                         const double *ur, const double *ut, const double *uz,
+                         const uint64_t *id, const int8_t *charge, int64_t n, int on_device);
+int gasatt_sim_read_ions(gasatt_sim *sim, double *r, double *z, double *ur, double *ut,
+                         double *uz, uint64_t *id, int8_t *charge, int64_t cap, int64_t *n,
+                         int on_device);
 /* Per-cell N2 density [m^-3] for the collisions: n_r x n_z values, column-major
  * (cell ir + n_r iz covers [ir dr, (ir+1) dr) x [iz dz, (iz+1) dz)); NULL goes
  * back to the uniform cfg->gas_density.  Replaces the density lookup by cell

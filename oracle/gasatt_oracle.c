@@ -974,7 +974,7 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
                  double *y, double *z, double *ux, double *uy, double *uz, uint64_t *id,
                  uint8_t *alive, int64_t *n_io, int64_t cap, const double *Er, const double *Ez,
                  const double *H, double *jr, double *jz, int do_kick, int do_mcc,
-                 const double *gas, orc_counters *cnt) {
+                 const double *gas, orc_ions *ions, orc_counters *cnt) {
   const int nr = cfg->n_r, nz = cfg->n_z;
   const double Rp = nr * cfg->dr, Lp = nz * cfg->dz, c = cfg->c, me = cfg->m_e, qe = cfg->q_e;
   const double qm_dt2 = -qe / me * cfg->dt / 2;
@@ -989,6 +989,8 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
     g_tj_len = need;
   }
   births_t *bt = (births_t *)calloc((size_t)nt, sizeof(births_t));
+  births_t *it = (births_t *)calloc((size_t)nt, sizeof(births_t));   /* ion births */
+  const double ion_sigma = ions ? sqrt(cfg->kb * cfg->gas_temperature / cfg->m_ion) : 0.0;
   orc_counters *ct = (orc_counters *)calloc((size_t)nt, sizeof(orc_counters));
   const int64_t n0 = *n_io;
 #pragma omp parallel num_threads(nt)
@@ -1001,6 +1003,7 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
     double *tjr = g_tj + (size_t)tid * 2 * ncel, *tjz = tjr + ncel;
     memset(tjr, 0, 2 * (size_t)ncel * sizeof(double));
     births_t *B = &bt[tid];
+    births_t *IB = &it[tid];
     orc_counters *C = &ct[tid];
 #pragma omp for schedule(static)
     for (int64_t p = 0; p < n0; ++p) {
@@ -1075,6 +1078,20 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
             ux[p] = ix * up; uy[p] = iy * up; uz[p] = iz_ * up;
             rotate_v(&ux[p], &uy[p], &uz[p], th_p, phi_p, 0);
             C->ion++;
+            if (ions) {
+              /* Maxwellian ion: three normals by Box-Muller from draw blocks
+               * 2 and 3, in the parent's local (r, theta, z) frame */
+              double a1, a2, b1, b2;
+              draw_block(cfg->seed, id[p], step, 2, &a1, &a2);
+              draw_block(cfg->seed, id[p], step, 3, &b1, &b2);
+              double ra = ion_sigma * sqrt(-2 * log(a1)), rb = ion_sigma * sqrt(-2 * log(b1));
+              double wr = ra * cos(2 * GASATT_PI * a2), wt = ra * sin(2 * GASATT_PI * a2);
+              double rr = sqrt(x[p] * x[p] + y[p] * y[p]);
+              double cq = rr > 0 ? x[p] / rr : 1.0, sq = rr > 0 ? y[p] / rr : 0.0;
+              double s[6] = {x[p], y[p], z[p], wr * cq - wt * sq, wr * sq + wt * cq,
+                             rb * cos(2 * GASATT_PI * b2)};
+              births_push(IB, s, orc_child_id(id[p], step), 1);
+            }
             if (cfg->secondaries) {
               double s[6] = {x[p], y[p], z[p], ix * us, iy * us, iz_ * us};
               rotate_v(&s[3], &s[4], &s[5], th_s, phi_s, 0);
@@ -1106,6 +1123,22 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
       jz[k] = b;
     }
   }
+  if (ions) {
+    for (int t = 0; t < nt; ++t) {
+      for (int64_t k = 0; k < it[t].n; ++k) {
+        if (ions->n >= ions->cap) { ions->overflow++; continue; }
+        const double *s = it[t].st + 6 * k;
+        const int64_t m = ions->n++;
+        ions->x[m] = s[0]; ions->y[m] = s[1]; ions->z[m] = s[2];
+        ions->ux[m] = s[3]; ions->uy[m] = s[4]; ions->uz[m] = s[5];
+        ions->id[m] = it[t].id[k];
+        ions->alive[m] = 1;
+        ions->q[m] = 1;
+      }
+    }
+  }
+  for (int t = 0; t < nt; ++t) { free(it[t].st); free(it[t].id); free(it[t].alive); }
+  free(it);
   int64_t n = n0;
   for (int t = 0; t < nt; ++t) {
     cnt->ion += ct[t].ion; cnt->ela += ct[t].ela; cnt->exc += ct[t].exc;
@@ -1123,6 +1156,45 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
   free(bt); free(ct);
   *n_io = n;
   return 0;
+}
+
+/* The push of the resident step (kick, two half drifts, deposit) applied to
+ * the ions over the ion step; electricmagneticfield6.m:68-69 pushes ion1 and
+ * ion2 in the electrons' kernel with their own charge and mass. */
+void orc_ion_push(const gasatt_sim_config *cfg, orc_ions *ions, const double *Er,
+                  const double *Ez, const double *H, double *jr, double *jz) {
+  const int nr = cfg->n_r, nz = cfg->n_z;
+  const double Rp = nr * cfg->dr, Lp = nz * cfg->dz, c = cfg->c;
+  const double dti = cfg->dt * cfg->ion_subcycle;
+  memset(jr, 0, (size_t)nr * nz * sizeof(double));
+  memset(jz, 0, (size_t)nr * nz * sizeof(double));
+  for (int64_t p = 0; p < ions->n; ++p) {
+    if (!ions->alive[p]) continue;
+    double *x = &ions->x[p], *y = &ions->y[p], *z = &ions->z[p];
+    double *ux = &ions->ux[p], *uy = &ions->uy[p], *uz = &ions->uz[p];
+    const double Zq = ions->q[p];
+    double r0 = sqrt(*x * *x + *y * *y);
+    double cp = r0 > 0 ? *x / r0 : 1.0, sp = r0 > 0 ? *y / r0 : 0.0;
+    double E_r, E_z, Hp;
+    gather(Er, Ez, H, nr, nz, cfg->dr, cfg->dz, r0, *z, &E_r, &E_z, &Hp);
+    double B_ = cfg->mu0 * Hp;
+    boris(ux, uy, uz, E_r * cp, E_r * sp, E_z, -B_ * sp, B_ * cp, 0.0,
+          Zq * cfg->q_e / cfg->m_ion * dti / 2, c);
+    for (int h = 0; h < 2 && ions->alive[p]; ++h) {
+      double g = sqrt(1 + (*ux * *ux + *uy * *uy + *uz * *uz) / (c * c));
+      double r, ph;
+      int del = 0;
+      halfdrift_cart(x, y, z, ux, uy, uz, *ux / g, *uy / g, *uz / g, &r, &ph, &del, Rp, Lp,
+                     cfg->PHIp, dti, cfg->flags);
+      if (del) ions->alive[p] = 0;
+    }
+    if (!ions->alive[p]) { ions->lost++; continue; }
+    double g = sqrt(1 + (*ux * *ux + *uy * *uy + *uz * *uz) / (c * c));
+    double r = sqrt(*x * *x + *y * *y);
+    double cq = r > 0 ? *x / r : 1.0, sq = r > 0 ? *y / r : 0.0;
+    em7_one(r, *z, Zq * cfg->q_e, (*ux * cq + *uy * sq) / g, *uz / g, jr, jz, nr, nz, cfg->dr,
+            cfg->dz, cfg->FN, cfg->PHIp);
+  }
 }
 
 void orc_sim_fdtd(const gasatt_sim_config *cfg, double *Er, double *Ez, double *H,

@@ -115,6 +115,19 @@ typedef struct orc_counters {
   int64_t ion, ela, exc, nul, lost, cap_overflow;
 } orc_counters;
 
+/* N2+ ion store of the resident step (Cartesian u = gamma v form).  Ions are
+ * born one per ionization (electron_transport.cu:202-204) when the store is
+ * given, at the parent's position with a Maxwellian velocity at
+ * cfg->gas_temperature, id = the secondary electron's id, charge number 1. */
+typedef struct orc_ions {
+  double *x, *y, *z, *ux, *uy, *uz;
+  uint64_t *id;
+  uint8_t *alive;
+  int8_t *q;
+  int64_t n, cap;
+  int64_t overflow, lost;
+} orc_ions;
+
 /* one particle pass of step s: gather + kick + half drift + half drift +
  * deposit, then the null-collision MCC at the end of the step (an ionization
  * appends its secondary at the parent's position).  Arrays x..alive have
@@ -127,7 +140,14 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step,
                  uint64_t *id, uint8_t *alive, int64_t *n, int64_t cap,
                  const double *Er, const double *Ez, const double *H,
                  double *jr, double *jz, int do_kick, int do_mcc, const double *gas,
-                 orc_counters *cnt);
+                 orc_ions *ions, orc_counters *cnt);
+/* ion push over dt_i = cfg->ion_subcycle * cfg->dt: gather, Boris kick with
+ * charge q e and mass cfg->m_ion, two half drifts (absorbed beyond Rp,
+ * reflected at the z ends), deposit of the ion current density [A/m^2] into
+ * jr/jz (overwritten); the field update adds it to the electrons' until the
+ * next ion push. */
+void orc_ion_push(const gasatt_sim_config *cfg, orc_ions *ions, const double *Er,
+                  const double *Ez, const double *H, double *jr, double *jz);
 /* field sub-cycle: H(-dt/4), [H(dt/2), E(dt/2)] x 2 ratio, H(dt/4), dt = cfg->dt/ratio */
 void orc_sim_fdtd(const gasatt_sim_config *cfg, double *Er, double *Ez, double *H,
                   const double *jr, const double *jz);

@@ -195,6 +195,12 @@ def electron_collision(e_pos, e_vel, i1_pos, i1_vel, tab, kin, sum_cell, cellnum
 
 
 # ------------------------------------------------------------ resident step
+class OrcIons(ctypes.Structure):
+    _fields_ = [("x", c_p), ("y", c_p), ("z", c_p), ("ux", c_p), ("uy", c_p), ("uz", c_p),
+                ("id", c_p), ("alive", c_p), ("q", c_p), ("n", c_i64), ("cap", c_i64),
+                ("overflow", c_i64), ("lost", c_i64)]
+
+
 class Sim:
     """Oracle of the resident simulation (Cartesian u = gamma v form)."""
 
@@ -218,6 +224,19 @@ class Sim:
         self.jz = np.zeros((nr, nz), order="F")
         self.counters = np.zeros(6, np.int64)   # ion, ela, exc, nul, lost, cap_overflow
         self.step_index = 0
+        # ions (cfg.ion_capacity > 0): store, held ion current
+        ic = int(cfg.ion_capacity)
+        self.ions = None
+        self.jri = np.zeros((nr, nz), order="F")
+        self.jzi = np.zeros((nr, nz), order="F")
+        if ic > 0:
+            self.ix = np.zeros(ic); self.iy = np.zeros(ic); self.iz = np.zeros(ic)
+            self.iux = np.zeros(ic); self.iuy = np.zeros(ic); self.iuz = np.zeros(ic)
+            self.iid = np.zeros(ic, np.uint64)
+            self.ialive = np.zeros(ic, np.uint8)
+            self.iq = np.zeros(ic, np.int8)
+            self.ions = OrcIons(P(self.ix), P(self.iy), P(self.iz), P(self.iux), P(self.iuy),
+                                P(self.iuz), P(self.iid), P(self.ialive), P(self.iq), 0, ic, 0, 0)
 
     def load(self, r, z, ur, ut, uz, ids):
         n = len(r)
@@ -226,6 +245,9 @@ class Sim:
         self.id[:n] = ids
         self.alive[:n] = 1
         self.n = n
+        if self.ions is not None:           # a new run starts without ions
+            self.ions.n, self.ions.overflow, self.ions.lost = 0, 0, 0
+            self.jri[:] = 0; self.jzi[:] = 0
 
     def set_gas_density(self, density):
         """Per-cell gas density (n_r x n_z) or None for the uniform density; the
@@ -246,7 +268,9 @@ class Sim:
                               P(self.y), P(self.z), P(self.ux), P(self.uy), P(self.uz), P(self.id),
                               P(self.alive), ctypes.byref(n), c_i64(self.cap), P(self.Er),
                               P(self.Ez), P(self.H), P(self.jr), P(self.jz), c_i(kick), c_i(mcc),
-                              None if self.gas is None else P(self.gas), P(self.counters))
+                              None if self.gas is None else P(self.gas),
+                              None if self.ions is None else ctypes.byref(self.ions),
+                              P(self.counters))
         assert rc == 0
         self.n = n.value
 
@@ -254,13 +278,40 @@ class Sim:
         self._pass(-1, 0, 0)
 
     def fdtd(self):
-        lib.orc_sim_fdtd(ctypes.byref(self.cfg), P(self.Er), P(self.Ez), P(self.H), P(self.jr),
-                         P(self.jz))
+        jr, jz = self.jr, self.jz
+        if self.ions is not None:
+            jr, jz = np.asfortranarray(jr + self.jri), np.asfortranarray(jz + self.jzi)
+        lib.orc_sim_fdtd(ctypes.byref(self.cfg), P(self.Er), P(self.Ez), P(self.H), P(jr), P(jz))
 
     def step(self):
         self.fdtd()
         self._pass(self.step_index, 1, 1)
         self.step_index += 1
+        if self.ions is not None and self.step_index % self.cfg.ion_subcycle == 0:
+            lib.orc_ion_push(ctypes.byref(self.cfg), ctypes.byref(self.ions), P(self.Er),
+                             P(self.Ez), P(self.H), P(self.jri), P(self.jzi))
+
+    def load_ions(self, r, z, ur, ut, uz, ids, charge=None):
+        n = len(r)
+        self.ix[:n] = r; self.iy[:n] = 0; self.iz[:n] = z
+        self.iux[:n] = ur; self.iuy[:n] = ut; self.iuz[:n] = uz
+        self.iid[:n] = ids
+        self.ialive[:n] = 1
+        self.iq[:n] = 1 if charge is None else charge
+        self.ions.n, self.ions.overflow, self.ions.lost = n, 0, 0
+        self.jri[:] = 0; self.jzi[:] = 0
+
+    def ion_state_rz(self):
+        """(r, z, u_r, u_theta, u_z, id, alive, charge) of the ions."""
+        n = self.ions.n
+        x, y = self.ix[:n], self.iy[:n]
+        r = np.hypot(x, y)
+        ph = np.arctan2(y, x)
+        cp, sp = np.cos(ph), np.sin(ph)
+        ux, uy = self.iux[:n], self.iuy[:n]
+        return (r, self.iz[:n].copy(), ux * cp + uy * sp, -ux * sp + uy * cp,
+                self.iuz[:n].copy(), self.iid[:n].copy(), self.ialive[:n].copy(),
+                self.iq[:n].copy())
 
     def field_energy(self):
         return lib.orc_field_energy(ctypes.byref(self.cfg), P(self.Er), P(self.Ez), P(self.H))
