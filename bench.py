@@ -540,12 +540,148 @@ def run_c3(args):
         s.close()
 
 
+C5 = dict(n_r=256, n_z=1024, delta=10e-6, dt=2e-14, torr=5.0, photo=2_000_000, e_keV=8.0,
+          seed=4, ion_subcycle=50)
+
+
+def run_c5(args):
+    """Electrons plus N2+ ions (one per ionization, Maxwellian at 300 K,
+    pushed every 50 steps), 4,000,000 initial electrons at 5 Torr, both
+    forms for the whole run: throughput, the growth of both species, exact
+    charge conservation, the energy budget, and the FP32 form's drift from
+    the FP64 form at the end."""
+    import torch
+    from gasatt import _lib
+    from gasatt.sim import Sim, births, config
+    torch.cuda.set_device(0)
+    w = C5
+    steps, chunk = args.c5_steps, 1000
+    parts = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=w["seed"],
+                   Rp=w["n_r"] * w["delta"])
+    n0 = len(parts[0])
+    out = {}
+    for prec, code in (("fp32_split", _lib.FP32_SPLIT), ("fp64", _lib.FP64)):
+        cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=code,
+                     capacity=args.c5_capacity, seed=w["seed"], sort_period=30,
+                     ion_capacity=args.c5_capacity, ion_subcycle=w["ion_subcycle"])
+        sim = Sim(cfg)
+        sim.bind_stream()
+        sim.load(*parts)
+        stream = torch.cuda.current_stream()
+        d_start = sim.diag()
+        work, ms_total, trace = 0.0, 0.0, []
+        done = 0
+        while done < steps:
+            k = min(chunk, steps - done)
+            a0 = sim.diag()["n_alive"]
+            e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            sim.step(k)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            d = sim.diag()
+            work += 0.5 * (a0 + d["n_alive"]) * k
+            ms_total += ms
+            done += k
+            trace.append(dict(step=done, electrons=d["n_alive"], ions=d["n_ions"],
+                              ms_per_step=ms / k))
+        d = sim.diag()
+        # per-step cost of the ion sub-cycle: 100 steps with an event pair each
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(100)]
+        torch.cuda.synchronize()
+        for e0, e1 in evs:
+            e0.record(stream); sim.step(1); e1.record(stream)
+        torch.cuda.synchronize()
+        per = [e0.elapsed_time(e1) for e0, e1 in evs]
+        base = steps + 1                              # step index of the first of the 100
+        push = [t for i, t in enumerate(per) if (base + i) % w["ion_subcycle"] == 0]
+        plain = [t for i, t in enumerate(per) if (base + i) % w["ion_subcycle"] != 0]
+        out[prec] = dict(value=work / (ms_total / 1e3), ms_total=ms_total, trace=trace,
+                         start=d_start, end=d, fields=sim.fields(),
+                         step_ms_plain=float(np.median(plain)),
+                         step_ms_with_ion_push=float(np.median(push)) if push else None)
+        sim.close()
+    f32, f64 = out["fp32_split"], out["fp64"]
+
+    def charge_ok(d):
+        return d["n_ions"] - d["n_alive"] == -n0 + d["n_lost_wall"] - d["n_ion_lost_wall"]
+
+    def energy(d):
+        ev = 6.241509074e18 * d["field_energy_j"]
+        return dict(electron_kinetic_ev=d["kinetic_ev"], ion_kinetic_ev=d["ion_kinetic_ev"],
+                    field_energy_j=d["field_energy_j"], collision_loss_ev=d["collision_loss_ev"],
+                    sum_ev=d["kinetic_ev"] + d["ion_kinetic_ev"] + ev + d["collision_loss_ev"])
+
+    ferr = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+               for a, b in zip(f32["fields"], f64["fields"]))
+    e32, e64 = f32["end"], f64["end"]
+    line = {"mode": "c5", "metric": METRIC, "unit": UNIT, "steps": steps,
+            "value": f32["value"], "fp64_value": f64["value"],
+            "fp32_over_fp64": f32["value"] / f64["value"],
+            "ms_per_step": f32["ms_total"] / steps, "fp64_ms_per_step": f64["ms_total"] / steps,
+            "step_ms_plain": f32["step_ms_plain"], "step_ms_with_ion_push": f32["step_ms_with_ion_push"],
+            "electrons": {"initial": n0, "final_fp32": e32["n_alive"], "final_fp64": e64["n_alive"]},
+            "ions": {"final_fp32": e32["n_ions"], "final_fp64": e64["n_ions"],
+                     "lost_wall_fp32": e32["n_ion_lost_wall"], "overflow": bool((e32["status_flags"] | e64["status_flags"]) & 6)},
+            "ionizations": {"fp32": e32["n_ionizations"], "fp64": e64["n_ionizations"],
+                            "rel_diff": (e32["n_ionizations"] - e64["n_ionizations"]) / max(e64["n_ionizations"], 1)},
+            "charge_conserved": {"fp32": charge_ok(e32), "fp64": charge_ok(e64),
+                                 "net_charge_c_fp64": e64["net_charge_c"],
+                                 "identity": "ions - electrons = -N0 + electrons lost - ions lost"},
+            "energy_fp64": {"start": energy(f64["start"]), "end": energy(e64),
+                            "sum_rel_change": energy(e64)["sum_ev"] / energy(f64["start"])["sum_ev"] - 1,
+                            "note": "sum = electron + ion kinetic + field + given to the gas; "
+                                    "electrons and ions absorbed at the wall take theirs away"},
+            "drift_fp32_vs_fp64": {"field_rel_err_l2": ferr,
+                                   "electron_kinetic_rel": e32["kinetic_ev"] / e64["kinetic_ev"] - 1,
+                                   "ion_kinetic_rel": (e32["ion_kinetic_ev"] / e64["ion_kinetic_ev"] - 1)
+                                   if e64["ion_kinetic_ev"] else None,
+                                   "ions_rel": (e32["n_ions"] - e64["n_ions"]) / max(e64["n_ions"], 1)},
+            "trace_fp32": f32["trace"][::max(1, len(f32["trace"]) // 10)],
+            "config": {"workload": "4,000,000 e- from 2,000,000 photoionizations at 8 keV, N2 5 Torr "
+                       "300 K, 256x1024 cells at 10 um, dt 2e-14 s, one N2+ ion (28 amu) per "
+                       "ionization, Maxwellian 300 K, ion push every 50 steps, seed 4",
+                       "capacity": args.c5_capacity, "sort_period": 30, "l2": "not flushed",
+                       "timed": "whole steps incl. ion pushes, 1000-step chunks"}}
+    print(json.dumps(line), flush=True)
+
+
+def c5_profile_sim(precision, torch):
+    """The C5 cell with its ions already grown: the 4,000,000 birth electrons
+    plus 4,000,000 ions at their positions (Maxwellian 300 K), so that the
+    first ion push (step 50) handles a grown ion population."""
+    from gasatt import _lib
+    from gasatt.sim import Sim, births, config
+    w = C5
+    code = _lib.FP32_SPLIT if precision == "fp32_split" else _lib.FP64
+    cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=code,
+                 capacity=16_000_000, seed=w["seed"], sort_period=30, ion_capacity=16_000_000,
+                 ion_subcycle=w["ion_subcycle"])
+    parts = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=w["seed"],
+                   Rp=w["n_r"] * w["delta"])
+    sim = Sim(cfg)
+    sim.bind_stream()
+    sim.load(*parts)
+    n = len(parts[0])
+    rng = np.random.default_rng(w["seed"])
+    sig = np.sqrt(cfg.kb * cfg.gas_temperature / cfg.m_ion)
+    sim.load_ions(parts[0], parts[1], *(rng.normal(0, sig, n) for _ in range(3)),
+                  np.arange(n, dtype=np.uint64))
+    return sim
+
+
 def run_profile(args):
     """The step loop alone (warm-up then timed steps, no flush/e2e/baseline),
-    for kernel profilers."""
+    for kernel profilers; --workload c5 adds the ion species."""
     import torch
     torch.cuda.set_device(0)
-    sim, _ = make_sim(args.precision, 0, 0, torch)
+    if args.workload == "c5":
+        sim = c5_profile_sim(args.precision, torch)
+    else:
+        sim, _ = make_sim(args.precision, 0, 0, torch)
     sim.step(args.warmup + args.steps)
     torch.cuda.synchronize()
     d = sim.diag()
@@ -562,9 +698,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "c3"],
+    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "c3", "c5"],
                     help="profile: only the step loop of one precision (for ncu); "
-                         "c3: 48 batched gas cells")
+                         "c3: 48 batched gas cells; c5: electrons plus ions, long run")
+    ap.add_argument("--c5-steps", type=int, default=20_000)
+    ap.add_argument("--workload", default="c2", choices=["c2", "c5"],
+                    help="workload of --mode profile")
+    ap.add_argument("--c5-capacity", type=int, default=80_000_000)
     ap.add_argument("--precision", default="fp32_split", choices=["fp32_split", "fp64"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -572,6 +712,8 @@ def main():
         run_profile(args)
     elif args.mode == "c3":
         run_c3(args)
+    elif args.mode == "c5":
+        run_c5(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

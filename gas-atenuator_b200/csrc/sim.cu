@@ -66,7 +66,8 @@ struct SimCounters {
   unsigned long long ion, ela, exc, nul, lost, cap_overflow;
   unsigned long long kin_fx;     // diagnostic: sum E_kin * 2^16 [eV]
   unsigned long long alive;      // diagnostic
-  unsigned long long pad5_[8];
+  unsigned long long exc_loss_fx; // diagnostic: excitation energy losses * 2^16 [eV]
+  unsigned long long pad5_[7];
   unsigned long long n_ions;     // ion slots claimed (loads and births; may pass the capacity)
   unsigned long long ion_overflow, ion_lost;
   unsigned long long ion_alive, ion_charge, ion_kin_fx;   // diagnostics; kinetic: E * 2^32 [eV]
@@ -116,7 +117,7 @@ struct State64 { double2 *rz; double2 *urt; double *uz; uint64_t *id; };
 struct State32 { uint4 *a; float2 *b; uint64_t *id; };
 
 // ------------------------------------------------------------------- MCC
-struct Birth { bool born; double ux, uy, uz; };
+struct Birth { bool born; double ux, uy, uz; double eloss; };   // eloss: excitation loss [eV]
 
 __device__ __forceinline__ void xs_lookup(const SimParams &P, double Eev, double &se, double &si,
                                           double &sx, double &L) {
@@ -234,6 +235,7 @@ template <bool FAST>
 __device__ __forceinline__ int mcc_event(const SimParams &P, uint64_t id, long long step, double &ux,
                                       double &uy, double &uz, Birth &b, double n_gas) {
   b.born = false;
+  b.eloss = 0;
   const U2 d0 = draw2(P.seed, id, step, 0);
   const double c = P.c, me = P.me, qe = P.qe, I = GASATT_ION_I_EV;
   const double u2 = ux * ux + uy * uy + uz * uz;
@@ -302,16 +304,19 @@ __device__ __forceinline__ int mcc_event(const SimParams &P, uint64_t id, long l
     if (!(E_dep > 0) || !(E_dep < Eev)) return 4;
     const double up = u_of_energy((Eev - E_dep) * qe, me, c);
     ux = ux / um * up; uy = uy / um * up; uz = uz / um * up;
+    b.eloss = E_dep;
     return 3;
   }
   return 4;
 }
 
-__device__ __forceinline__ void count_event(SimCounters *cnt, int ev) {
+__device__ __forceinline__ void count_event(SimCounters *cnt, int ev, const Birth &b) {
   if (ev == 1) atomicAdd(&cnt->ela, 1ull);
   else if (ev == 2) atomicAdd(&cnt->ion, 1ull);
-  else if (ev == 3) atomicAdd(&cnt->exc, 1ull);
-  else if (ev == 4) atomicAdd(&cnt->nul, 1ull);
+  else if (ev == 3) {
+    atomicAdd(&cnt->exc, 1ull);
+    atomicAdd(&cnt->exc_loss_fx, (unsigned long long)__double2ll_rn(b.eloss * 65536.0));
+  } else if (ev == 4) atomicAdd(&cnt->nul, 1ull);
 }
 
 // The N2+ ion of an ionization of electron `id` at step `step`, at the
@@ -539,7 +544,7 @@ __global__ void __launch_bounds__(kMccBlock) k_mcc64(SimParams P, State64 S, Sim
     Birth b;
     const double ng = gas_density(P, (int)floor(rz.x / P.dr), (int)floor(rz.y / P.dz));
     const int ev = mcc_event<false>(P, id, step, ur, ut, uz, b, ng);
-    count_event(cnt, ev);
+    count_event(cnt, ev, b);
     if (ev == 2 && P.ion_cap > 0) ion_birth(P.ion, P.ion_cap, P.ion_sigma, P.seed, cnt, id, step, rz.x, rz.y);
     if (b.born) {
       const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
@@ -558,18 +563,82 @@ __global__ void __launch_bounds__(kMccBlock) k_mcc64(SimParams P, State64 S, Sim
 }
 
 // ----------------------------------------------------------- ions
+// Before each push the ions are sorted by deposit node quad (the electrons'
+// sort key) from the store into a scratch store, dropping the dead; the push
+// reads the scratch and writes the store back in that order.  Ions hardly
+// move between pushes, so only those born since the last push are out of
+// place, and the lanes of a warp then share their deposit nodes (the warp
+// sums replace most of the atomics on the crowded cells near the axis).
+__device__ __forceinline__ int ion_cell(const IonState &I, long long p, int nr, int nz, double dr,
+                                        double dz) {
+  const double2 rz = I.rz[p];
+  if (rz.x < 0) return -1;
+  int ar = (int)floor(rz.x / dr - 0.5) + 1, az = (int)floor(rz.y / dz - 0.5) + 1;
+  ar = min(max(ar, 0), nr);
+  az = min(max(az, 0), nz);
+  return ar + az * (nr + 1);
+}
+
+__device__ __forceinline__ long long ions_in_use(const SimCounters *cnt, long long cap) {
+  const unsigned long long nc = cnt->n_ions;
+  return (long long)(nc < (unsigned long long)cap ? nc : cap);
+}
+
+__global__ void k_ion_hist(IonState I, const SimCounters *cnt, long long cap, int nr, int nz,
+                           double dr, double dz, int *count) {
+  const long long n = ions_in_use(cnt, cap);
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+       base += (long long)gridDim.x * blockDim.x) {
+    const long long p = base + (threadIdx.x & 31);
+    const int c = p < n ? ion_cell(I, p, nr, nz, dr, dz) : -1;
+    const unsigned live = __ballot_sync(0xFFFFFFFFu, c >= 0);
+    if (c < 0) continue;
+    const unsigned mask = __match_any_sync(live, c);
+    if ((__ffs(mask) - 1) == (int)(threadIdx.x & 31)) atomicAdd(count + c, __popc(mask));
+  }
+}
+
+__global__ void k_ion_scatter(IonState A, IonState B, const SimCounters *cnt, long long cap,
+                              int nr, int nz, double dr, double dz, const int *offset,
+                              int *cursor) {
+  const long long n = ions_in_use(cnt, cap);
+  const int lane = threadIdx.x & 31;
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+       base += (long long)gridDim.x * blockDim.x) {
+    const long long p = base + lane;
+    const int c = p < n ? ion_cell(A, p, nr, nz, dr, dz) : -1;
+    const unsigned live = __ballot_sync(0xFFFFFFFFu, c >= 0);
+    if (c < 0) continue;
+    const unsigned mask = __match_any_sync(live, c);
+    const int leader = __ffs(mask) - 1;
+    int basepos = 0;
+    if (lane == leader) basepos = atomicAdd(cursor + c, __popc(mask));
+    basepos = __shfl_sync(mask, basepos, leader);
+    const long long dst = (long long)offset[c] + basepos + __popc(mask & ((1u << lane) - 1));
+    B.rz[dst] = A.rz[p]; B.urt[dst] = A.urt[p]; B.uz[dst] = A.uz[p];
+    B.id[dst] = A.id[p]; B.q[dst] = A.q[p];
+  }
+}
+
+// the live ions are now the first offset[nbin] slots
+__global__ void k_ion_sort_finish(SimCounters *cnt, const int *offset, int nbin) {
+  cnt->n_ions = (unsigned long long)offset[nbin];
+}
+
 // Ion push, once every ion_subcycle electron steps: P is the simulation's
 // parameter block with dt = the ion step, qm_dt2 = q_e/m_ion dt/2 and the
 // ion current buffers as Jr/Jz (cleared before the launch), dep = the
-// fixed-point factor of the ion current.  Per ion: gather, Boris kick with
-// charge Z q_e, two half drifts (the electrons' walls: absorbed beyond Rp,
-// reflected at z = 0 and Lp), deposit of Z q_e FN v at the new position.  The
-// field update adds the ion current to the electrons' until the next push
-// (charge moved over the ion step = the held current x the ion step).
+// fixed-point factor of the ion current.  Per ion of the sorted scratch
+// store src: gather, Boris kick with charge Z q_e, two half drifts (the
+// electrons' walls: absorbed beyond Rp, reflected at z = 0 and Lp), deposit
+// of Z q_e FN v at the new position; the ion goes back to the store P.ion at
+// the same index.  The field update adds the ion current to the electrons'
+// until the next push (charge moved over the ion step = the held current x
+// the ion step).
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_ion_push(SimParams P, Fields<T> F, SimCounters *cnt) {
-  const unsigned long long nc = cnt->n_ions;
-  const long long n = (long long)(nc < (unsigned long long)P.ion_cap ? nc : P.ion_cap);
+__global__ void __launch_bounds__(kBlock) k_ion_push(SimParams P, Fields<T> F, SimCounters *cnt,
+                                                     IonState src) {
+  const long long n = ions_in_use(cnt, P.ion_cap);
   const IonState I = P.ion;
   unsigned lost = 0;
   for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
@@ -579,12 +648,14 @@ __global__ void __launch_bounds__(kBlock) k_ion_push(SimParams P, Fields<T> F, S
     double2 rz = make_double2(-1.0, 0.0), urt = make_double2(0.0, 0.0);
     double uz = 0, Zq = 0;
     if (act) {
-      rz = I.rz[p];
+      rz = src.rz[p];
       act = rz.x >= 0;
     }
     if (act) {
-      urt = I.urt[p]; uz = I.uz[p];
-      Zq = (double)I.q[p];
+      urt = src.urt[p]; uz = src.uz[p];
+      const int8_t q = src.q[p];
+      Zq = (double)q;
+      I.id[p] = src.id[p]; I.q[p] = q;
       double r = rz.x, z = rz.y, ur = urt.x, ut = urt.y;
       bool alive = true;
       double E_r, E_z, Hp;
@@ -932,7 +1003,7 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
   double dux = (double)__uint_as_float(A.w) * P.c, duy = (double)B.x * P.c, duz = (double)B.y * P.c;
   Birth b;
   const int ev = mcc_event<true>(P, id, cstep, dux, duy, duz, b, gas_density(P, ir, iz));
-  count_event(cnt, ev);
+  count_event(cnt, ev, b);
   if (ev == 2 && P.ion_cap > 0)
     ion_birth(P.ion, P.ion_cap, P.ion_sigma, P.seed, cnt, id, cstep, ((double)ir + (double)fr) * P.dr,
               ((double)iz + (double)fz) * P.dz);
@@ -1472,6 +1543,7 @@ struct gasatt_sim {
   // the factor ion_scale (2^48 per q_e FN c, in both forms)
   unsigned long long *Jir = nullptr, *Jiz = nullptr;
   double ion_scale = 1.0;
+  IonState ion_tmp{};             // scratch store the ions are sorted into before a push
   bool mcc_pending = false;       // the last pass's collisions are not applied yet
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;   // graph capture fork/join
   bool timing = false;
@@ -1593,20 +1665,31 @@ int flush_collisions(gasatt_sim *s) {
 // taken are pushed with the others.
 int launch_ion_push(gasatt_sim *s, cudaStream_t st) {
   SIM_TRY(flush_collisions(s));
-  const size_t nc = (size_t)s->cfg.n_r * s->cfg.n_z;
+  const auto &c = s->cfg;
+  const size_t nc = (size_t)c.n_r * c.n_z;
+  const int nbin = (c.n_r + 1) * (c.n_z + 1);
+  const unsigned g = grid_for(c.ion_capacity, kBlock) < s->pass_grid ? grid_for(c.ion_capacity, kBlock) : s->pass_grid;
+  // sort the store into the scratch store (the electrons' sort buffers are free here)
+  GASATT_CUDA(s->ctx, cudaMemsetAsync(s->cell_count, 0, (size_t)(nbin + 1) * 4, st));
+  GASATT_CUDA(s->ctx, cudaMemsetAsync(s->cell_cursor, 0, (size_t)nbin * 4, st));
+  k_ion_hist<<<g, kBlock, 0, st>>>(s->P.ion, s->cnt, c.ion_capacity, c.n_r, c.n_z, c.dr, c.dz, s->cell_count);
+  size_t nb = s->scan_bytes;
+  GASATT_CUDA(s->ctx, cub::DeviceScan::ExclusiveSum(s->scan_tmp, nb, s->cell_count, s->cell_offset, nbin + 1, st));
+  k_ion_scatter<<<g, kBlock, 0, st>>>(s->P.ion, s->ion_tmp, s->cnt, c.ion_capacity, c.n_r, c.n_z, c.dr,
+                                      c.dz, s->cell_offset, s->cell_cursor);
+  k_ion_sort_finish<<<1, 1, 0, st>>>(s->cnt, s->cell_offset, nbin);
+  s->ctx->launches += 4;
   GASATT_CUDA(s->ctx, cudaMemsetAsync(s->Jir, 0, nc * 8, st));
   GASATT_CUDA(s->ctx, cudaMemsetAsync(s->Jiz, 0, nc * 8, st));
-  const auto &c = s->cfg;
   SimParams PI = s->P;
   PI.dt = c.dt * c.ion_subcycle;
   PI.qm_dt2 = c.q_e / c.m_ion * PI.dt / 2;
   PI.dep = s->ion_scale;
   PI.Jr = s->Jir; PI.Jz = s->Jiz;
-  const unsigned g = grid_for(c.ion_capacity, kBlock) < s->pass_grid ? grid_for(c.ion_capacity, kBlock) : s->pass_grid;
   if (s->form == 0)
-    k_ion_push<double><<<g, kBlock, 0, st>>>(PI, Fields<double>{(double *)s->Er, (double *)s->Ez, (double *)s->H}, s->cnt);
+    k_ion_push<double><<<g, kBlock, 0, st>>>(PI, Fields<double>{(double *)s->Er, (double *)s->Ez, (double *)s->H}, s->cnt, s->ion_tmp);
   else
-    k_ion_push<float><<<g, kBlock, 0, st>>>(PI, Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H}, s->cnt);
+    k_ion_push<float><<<g, kBlock, 0, st>>>(PI, Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H}, s->cnt, s->ion_tmp);
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "ion push launch");
@@ -1891,7 +1974,10 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
     const size_t ic = (size_t)c.ion_capacity;
     if ((rc = sim_alloc(s, &I.rz, ic)) || (rc = sim_alloc(s, &I.urt, ic)) ||
         (rc = sim_alloc(s, &I.uz, ic)) || (rc = sim_alloc(s, &I.id, ic)) ||
-        (rc = sim_alloc(s, &I.q, ic)) || (rc = sim_alloc(s, &s->Jir, (size_t)c.n_r * c.n_z)) ||
+        (rc = sim_alloc(s, &I.q, ic)) || (rc = sim_alloc(s, &s->ion_tmp.rz, ic)) ||
+        (rc = sim_alloc(s, &s->ion_tmp.urt, ic)) || (rc = sim_alloc(s, &s->ion_tmp.uz, ic)) ||
+        (rc = sim_alloc(s, &s->ion_tmp.id, ic)) || (rc = sim_alloc(s, &s->ion_tmp.q, ic)) ||
+        (rc = sim_alloc(s, &s->Jir, (size_t)c.n_r * c.n_z)) ||
         (rc = sim_alloc(s, &s->Jiz, (size_t)c.n_r * c.n_z)))
       return cleanup(rc);
   }
@@ -2422,6 +2508,7 @@ int gasatt_sim_diag(gasatt_sim *s, gasatt_diag *d) {
   d->n_ion_lost_wall = (int64_t)h.ion_lost;
   d->ion_kinetic_ev = (double)h.ion_kin_fx / 4294967296.0;
   d->net_charge_c = s->cfg.q_e * s->cfg.FN * ((double)h.ion_charge - (double)h.alive);
+  d->collision_loss_ev = GASATT_ION_I_EV * (double)h.ion + (double)h.exc_loss_fx / 65536.0;
   return GASATT_OK;
 }
 

@@ -61,7 +61,8 @@ class Diag(ctypes.Structure):
                 ("n_elastic", c_i64), ("n_excitation", c_i64), ("n_null", c_i64),
                 ("n_lost_wall", c_i64), ("n_ions", c_i64), ("kinetic_ev", c_d),
                 ("field_energy_j", c_d), ("steps", c_i64), ("status_flags", ctypes.c_int32),
-                ("n_ion_lost_wall", c_i64), ("ion_kinetic_ev", c_d), ("net_charge_c", c_d)]
+                ("n_ion_lost_wall", c_i64), ("ion_kinetic_ev", c_d), ("net_charge_c", c_d),
+                ("collision_loss_ev", c_d)]
 
 
 _SIGS = {

@@ -272,6 +272,8 @@ typedef struct gasatt_diag {
   double  ion_kinetic_ev;   /* sum of ion kinetic energy [eV] (x FN not applied) */
   double  net_charge_c;     /* charge of the macro-particles in the domain [C]:
                                q_e FN (sum of ion charge numbers - electrons alive) */
+  double  collision_loss_ev;/* cumulative electron energy given to the gas [eV] (x FN not
+                               applied): 15.6 eV per ionization + the excitation losses */
 } gasatt_diag;
 
 typedef struct gasatt_sim gasatt_sim;

@@ -1104,6 +1104,7 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
               double up = u_of_energy((Eev - E_dep) * qe, me, c);
               ux[p] = ux[p] / um * up; uy[p] = uy[p] / um * up; uz[p] = uz[p] / um * up;
               C->exc++;
+              C->exc_loss_fx += llrint(E_dep * 65536.0);
             } else C->nul++;
           } else {
             C->nul++;
@@ -1143,6 +1144,7 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
   for (int t = 0; t < nt; ++t) {
     cnt->ion += ct[t].ion; cnt->ela += ct[t].ela; cnt->exc += ct[t].exc;
     cnt->nul += ct[t].nul; cnt->lost += ct[t].lost;
+    cnt->exc_loss_fx += ct[t].exc_loss_fx;
     for (int64_t k = 0; k < bt[t].n; ++k) {
       if (n >= cap) { cnt->cap_overflow++; continue; }
       const double *s = bt[t].st + 6 * k;

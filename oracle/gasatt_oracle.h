@@ -113,6 +113,7 @@ const double *orc_xs_array(const orc_xs *xs, int which);
 
 typedef struct orc_counters {
   int64_t ion, ela, exc, nul, lost, cap_overflow;
+  int64_t exc_loss_fx;                /* excitation losses, sum of llrint(E_dep * 2^16) [eV] */
 } orc_counters;
 
 /* N2+ ion store of the resident step (Cartesian u = gamma v form).  Ions are

@@ -222,7 +222,9 @@ class Sim:
         self.H = np.zeros((nr, nz), order="F")
         self.jr = np.zeros((nr, nz), order="F")
         self.jz = np.zeros((nr, nz), order="F")
-        self.counters = np.zeros(6, np.int64)   # ion, ela, exc, nul, lost, cap_overflow
+        # ion, ela, exc, nul, lost, cap_overflow, then the excitation losses x 2^16 [eV]
+        self._cnt = np.zeros(7, np.int64)
+        self.counters = self._cnt[:6]
         self.step_index = 0
         # ions (cfg.ion_capacity > 0): store, held ion current
         ic = int(cfg.ion_capacity)
@@ -270,7 +272,7 @@ class Sim:
                               P(self.Ez), P(self.H), P(self.jr), P(self.jz), c_i(kick), c_i(mcc),
                               None if self.gas is None else P(self.gas),
                               None if self.ions is None else ctypes.byref(self.ions),
-                              P(self.counters))
+                              P(self._cnt))
         assert rc == 0
         self.n = n.value
 
@@ -290,6 +292,11 @@ class Sim:
         if self.ions is not None and self.step_index % self.cfg.ion_subcycle == 0:
             lib.orc_ion_push(ctypes.byref(self.cfg), ctypes.byref(self.ions), P(self.Er),
                              P(self.Ez), P(self.H), P(self.jri), P(self.jzi))
+
+    @property
+    def collision_loss_ev(self):
+        """15.6 eV per ionization plus the excitation losses [eV]."""
+        return 15.6 * float(self._cnt[0]) + float(self._cnt[6]) / 65536.0
 
     def load_ions(self, r, z, ur, ut, uz, ids, charge=None):
         n = len(r)

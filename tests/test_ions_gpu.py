@@ -58,6 +58,7 @@ def test_fp64_ions_match_oracle(tables):
     ion, ela, exc, nul, lost, ovf = orc.counters
     assert (d["n_ionizations"], d["n_elastic"], d["n_excitation"], d["n_null"]) == (ion, ela, exc, nul)
     assert ion > 10
+    assert d["collision_loss_ev"] == pytest.approx(orc.collision_loss_ev, rel=1e-12)
     # one ion per ionization, ids of the secondary electrons
     gi = sim.read_ions()
     r, z, ur, ut, uz, ids, alive, q = orc.ion_state_rz()
@@ -222,3 +223,21 @@ def test_ion_arguments_are_checked():
     sim2 = Sim(ion_cfg(_lib.FP64, 5, ion_cap=4))
     with pytest.raises(RuntimeError):                    # beyond the ion capacity
         sim2.load_ions(*[np.ones(5) * D] * 2, *[np.zeros(5)] * 3, np.zeros(5, np.uint64))
+
+
+@pytest.mark.parametrize("precision,tol", [(_lib.FP64, 1e-6), (_lib.FP32_SPLIT, 1e-4)])
+def test_energy_budget_closes(precision, tol):
+    """No applied field, no wall losses: the electrons' kinetic energy drops by
+    what the collisions give to the gas (15.6 eV per ionization plus the
+    excitation losses) and what the self-field takes."""
+    cfg = ion_cfg(precision, 10)
+    sim = Sim(cfg)
+    sim.load(*births(4000, 8.0, NZ * D, seed=3, sigma_r=30e-6, Rp=NR * D))
+    d0 = sim.diag()
+    sim.step(20)
+    d = sim.diag()
+    assert d["n_lost_wall"] == 0 and d["n_ionizations"] > 100 and d["n_excitation"] > 100
+    e_c = 6.241509074e18                          # eV per joule
+    lhs = d0["kinetic_ev"] + d0["field_energy_j"] * e_c
+    rhs = d["kinetic_ev"] + d["field_energy_j"] * e_c + d["collision_loss_ev"]
+    assert abs(rhs - lhs) < tol * lhs, (lhs, rhs, d["collision_loss_ev"])
