@@ -87,6 +87,58 @@ __global__ void k_fdtd_e(T *__restrict__ Er, T *__restrict__ Ez, const T *__rest
 
 namespace gasatt {
 
+// Packed gather quads of the FP32 form: for each interpolation cell of a
+// field, its four (edge-clamped) corner values as one float4, so the particle
+// pass reads one 16-byte vector per field instead of four scalars and needs no
+// clamping.  Indices (ar, az: the half-cell shifted column and row of a
+// particle, from -1; ir, iz: its cell):
+//   Er: (ar + 1) + iz (n_r + 1)        corners (max(ar,0) | min(ar+1,n_r-1)) x (iz | iz+1)
+//   Ez: ir + (az + 1) n_r              corners (ir | ir+1) x (max(az,0) | min(az+1,n_z-1))
+//   H:  (ar + 1) + (az + 1) (n_r + 1)  corners as Er's columns x Ez's rows
+// in the order (c0,r0), (c1,r0), (c0,r1), (c1,r1).
+struct FieldQuads {
+  float4 *er, *ez, *h;
+};
+
+// The quad slots that read field value (i, j) along one axis: a "shifted"
+// axis (quads 0..n, corners max(q-1,0) and min(q,n-1)) or a "plain" one
+// (quads 0..n-1, corners q and q+1).  Four fixed (quad, corner) slots, m the
+// mask of those that apply (fixed slots keep the arrays in registers).
+struct QuadAxis {
+  int q[4], d[4];
+  unsigned m;
+};
+__device__ __forceinline__ QuadAxis quad_axis_shifted(int i, int n) {
+  QuadAxis a;
+  a.q[0] = i + 1; a.d[0] = 0;
+  a.q[1] = i;     a.d[1] = 1;
+  a.q[2] = 0;     a.d[2] = 0;        // the clamped low edge reads value 0 twice
+  a.q[3] = n;     a.d[3] = 1;        // the clamped high edge reads value n-1 twice
+  a.m = 3u | (i == 0 ? 4u : 0u) | (i == n - 1 ? 8u : 0u);
+  return a;
+}
+__device__ __forceinline__ QuadAxis quad_axis_plain(int i, int n) {
+  QuadAxis a;
+  a.q[0] = i;     a.d[0] = 0;
+  a.q[1] = i - 1; a.d[1] = 1;
+  a.q[2] = 0;     a.d[2] = 0;
+  a.q[3] = 0;     a.d[3] = 0;
+  a.m = (i < n ? 1u : 0u) | (i > 0 ? 2u : 0u);
+  return a;
+}
+__device__ __forceinline__ void quad_put(float4 *Q, int ncq, const QuadAxis &cx,
+                                         const QuadAxis &ry, float v) {
+  float *f = reinterpret_cast<float *>(Q);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      if (((cx.m >> a) & 1u) && ((ry.m >> b) & 1u))
+        f[(((int64_t)cx.q[a] + (int64_t)ry.q[b] * ncq) << 2) + cx.d[a] + 2 * ry.d[b]] = v;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Fused field sub-cycle for the resident simulation: one launch advances the
 // fields by one particle step, H(dt/4), [E(dt/2), H(dt/2)] x (2R - 1), E(dt/2),
@@ -122,7 +174,7 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
                                            unsigned long long *__restrict__ Jz_next, int nr,
                                            int nz, const FdtdCoef &c, const double *__restrict__ invV,
                                            double mu, double dt, int R, unsigned flags,
-                                           ExtraCurrent xj) {
+                                           ExtraCurrent xj, FieldQuads q) {
   constexpr int TW = kFdtdPatch;
   __shared__ double sEr[TW * TW], sEz[TW * TW], sH[TW * TW], sJr[TW * TW], sJz[TW * TW];
   const int tile = fdtd_tile(R), hl = 2 * R, hh = 2 * R + 1;
@@ -202,11 +254,169 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
     for (int j = J0 + threadIdx.y; j < je; j += kFdtdRows) {
       if (j < j0) continue;
       const int s = li + (j - J0) * TW;
-      if (i < nr && j <= nz) Er[i + (int64_t)j * nr] = (T)sEr[s];
-      if (i <= nr && j < nz) Ez[i + (int64_t)j * (nr + 1)] = (T)sEz[s];
+      if (i < nr && j <= nz) {
+        const T v = (T)sEr[s];
+        Er[i + (int64_t)j * nr] = v;
+        if (q.er) quad_put(q.er, nr + 1, quad_axis_shifted(i, nr), quad_axis_plain(j, nz), (float)v);
+      }
+      if (i <= nr && j < nz) {
+        const T v = (T)sEz[s];
+        Ez[i + (int64_t)j * (nr + 1)] = v;
+        if (q.ez) quad_put(q.ez, nr, quad_axis_plain(i, nr), quad_axis_shifted(j, nz), (float)v);
+      }
       if (i < nr && j < nz) {
         const int64_t g = i + (int64_t)j * nr;
-        H[g] = (T)sH[s];
+        const T v = (T)sH[s];
+        H[g] = v;
+        if (q.h) quad_put(q.h, nr + 1, quad_axis_shifted(i, nr), quad_axis_shifted(j, nz), (float)v);
+        Jr_next[g] = 0;
+        Jz_next[g] = 0;
+      }
+    }
+  }
+}
+
+// The fused sub-cycle for fdtd_ratio 1 (the product's): H(dt/4), E(dt/2),
+// H(dt/2), E(dt/2), H(dt/4) on a 32 x 32 patch with a 27 x 27 tile, the same
+// arithmetic as fdtd_tiled, unrolled: each thread owns one column and two rows
+// of the patch, and the boundary tests of its cells are taken once.  FP32 form
+// (q.er non-null): also writes the gather quads of the tile's values.
+template <typename T>
+__device__ __forceinline__ void fdtd_tiled1(T *__restrict__ Er, T *__restrict__ Ez,
+                                            T *__restrict__ H,
+                                            const unsigned long long *__restrict__ Jr,
+                                            const unsigned long long *__restrict__ Jz,
+                                            unsigned long long *__restrict__ Jr_next,
+                                            unsigned long long *__restrict__ Jz_next, int nr,
+                                            int nz, const FdtdCoef &c,
+                                            const double *__restrict__ invV, double mu, double dt,
+                                            unsigned flags, ExtraCurrent xj, FieldQuads q) {
+  constexpr int TW = kFdtdPatch, RW = kFdtdRows;
+  static_assert(TW == 2 * RW, "two patch rows per thread");
+  __shared__ double sEr[TW * TW], sEz[TW * TW], sH[TW * TW], sJr[TW * TW], sJz[TW * TW];
+  const int tile = fdtd_tile(1);
+  const int i0 = blockIdx.x * tile, j0 = blockIdx.y * tile;
+  const int I0 = max(i0 - 2, 0), J0 = max(j0 - 2, 0);
+  const int I1 = min(i0 + tile + 3, nr + 1), J1 = min(j0 + tile + 3, nz + 1);
+  const int W = I1 - I0, Hn = J1 - J0;
+  const int li = threadIdx.x, i = I0 + li;
+  const bool col = li < W;
+  const bool endcopy = (flags & GASATT_Q_ER_END_COPY) != 0;
+  // the thread's two patch rows
+  int lj[2], j[2], sidx[2];
+  bool row[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    lj[k] = threadIdx.y + RW * k;
+    j[k] = J0 + lj[k];
+    sidx[k] = li + lj[k] * TW;
+    row[k] = col && lj[k] < Hn;
+  }
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    if (!row[k]) continue;
+    const int jj = j[k], s = sidx[k];
+    if (i < nr && jj <= nz) sEr[s] = (double)Er[i + jj * nr];
+    if (i <= nr && jj < nz) sEz[s] = (double)Ez[i + jj * (nr + 1)];
+    if (i < nr && jj < nz) {
+      const int g = i + jj * nr;
+      sH[s] = (double)H[g];
+      if (xj.Jr) {
+        sJr[s] = ((double)(long long)Jr[g] + (double)(long long)xj.Jr[g] * xj.rel) * invV[i];
+        sJz[s] = ((double)(long long)Jz[g] + (double)(long long)xj.Jz[g] * xj.rel) * invV[i];
+      } else {
+        sJr[s] = (double)(long long)Jr[g] * invV[i];
+        sJz[s] = (double)(long long)Jz[g] * invV[i];
+      }
+    }
+  }
+  // which update each of the two cells takes
+  bool upH[2], upEr[2], zeroEr[2], upEzAxis[2], upEz[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int jj = j[k];
+    upH[k] = row[k] && i < nr && i + 1 < I1 && jj < nz && jj + 1 < J1;
+    const bool erin = jj >= 1 && jj < nz;
+    upEr[k] = row[k] && i < nr && erin && jj - 1 >= J0;
+    zeroEr[k] = row[k] && i < nr && !erin && !endcopy && jj <= nz;
+    upEzAxis[k] = row[k] && jj < nz && i == 0;
+    upEz[k] = row[k] && jj < nz && i > 0 && i < nr && i - 1 >= I0;
+  }
+  const double dt_eps = c.dt_eps, dt_eps_dz = c.dt_eps_dz, axis = c.axis, inv_dr = 1 / c.dr;
+  const double ri = ((flags & GASATT_Q_EZ_RSHIFT) ? (i + 1) : i) * c.dr;
+  const double ezp = i > 0 ? dt_eps * (1 / (2 * ri) + inv_dr) : 0.0;   // coefficient of H(i)
+  const double ezm = i > 0 ? dt_eps * (1 / (2 * ri) - inv_dr) : 0.0;   // coefficient of H(i-1)
+  const bool jsign = (flags & GASATT_Q_EZ_AXIS_JSIGN) != 0;
+  __syncthreads();
+  auto h_update = [&](double h) {
+    const double chr = h / (mu * c.dr), chz = h / (mu * c.dz);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int s = sidx[k];
+      if (upH[k]) sH[s] = sH[s] + (chr * (sEz[s + 1] - sEz[s]) - chz * (sEr[s + TW] - sEr[s]));
+    }
+  };
+  auto e_update = [&]() {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int s = sidx[k], jj = j[k];
+      if (upEr[k]) {
+        const double old = sEr[s];
+        sEr[s] = old - dt_eps * (sJr[s - TW] + sJr[s]) / 2 - dt_eps_dz * (sH[s] - sH[s - TW]);
+        if (endcopy) {
+          if (jj == 1 && J0 == 0) sEr[s - TW] = old;
+          if (jj == nz - 1 && J1 == nz + 1) sEr[s + TW] = old;
+        }
+      } else if (zeroEr[k]) {
+        sEr[s] = 0.0;
+      }
+      if (upEzAxis[k]) {
+        const double jz0 = sJz[s];
+        const double jterm = jsign ? dt_eps * jz0 : -(dt_eps * jz0);
+        sEz[s] = sEz[s] + jterm + axis * sH[s];
+      } else if (upEz[k]) {
+        sEz[s] = sEz[s] - dt_eps * (sJz[s - 1] + sJz[s]) / 2 + ezp * sH[s] + ezm * sH[s - 1];
+      }
+    }
+  };
+  h_update(dt / 4);
+  __syncthreads();
+  e_update();
+  __syncthreads();
+  h_update(dt / 2);
+  __syncthreads();
+  e_update();
+  __syncthreads();
+  h_update(dt / 4);
+  __syncthreads();
+  const int ie = min(i0 + tile, nr + 1), je = min(j0 + tile, nz + 1);
+  if (i >= i0 && i < ie) {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int jj = j[k], s = sidx[k];
+      if (!row[k] || jj < j0 || jj >= je) continue;
+      if (i < nr && jj <= nz) Er[i + jj * nr] = (T)sEr[s];
+      if (i <= nr && jj < nz) Ez[i + jj * (nr + 1)] = (T)sEz[s];
+      // whole Er and Ez quads of the tile's quad indices: after the sub-cycle
+      // E is correct one cell beyond the tile (Er one column below it, Ez one
+      // row below it, both one above), which covers their corners
+      if (q.er && jj < nz) {
+        const int sa = (max(i - 1, 0) - I0) + (jj - J0) * TW, sb = (min(i, nr - 1) - I0) + (jj - J0) * TW;
+        q.er[i + jj * (nr + 1)] = make_float4((float)sEr[sa], (float)sEr[sb], (float)sEr[sa + TW],
+                                              (float)sEr[sb + TW]);
+      }
+      if (q.ez && i < nr) {
+        const int s0 = (i - I0) + (max(jj - 1, 0) - J0) * TW, s1 = (i - I0) + (min(jj, nz - 1) - J0) * TW;
+        q.ez[i + jj * nr] = make_float4((float)sEz[s0], (float)sEz[s0 + 1], (float)sEz[s1],
+                                        (float)sEz[s1 + 1]);
+      }
+      if (i < nr && jj < nz) {
+        const int g = i + jj * nr;
+        const T v = (T)sH[s];
+        H[g] = v;
+        // H is correct only on the tile, one short of its quads' corners:
+        // each value goes to the quad slots that read it instead
+        if (q.h) quad_put(q.h, nr + 1, quad_axis_shifted(i, nr), quad_axis_shifted(jj, nz), (float)v);
         Jr_next[g] = 0;
         Jz_next[g] = 0;
       }

@@ -104,6 +104,7 @@ struct SimParams {
   int n_exc;
   double exc[5][16];
   unsigned long long *Jr, *Jz;
+  const float4 *qEr, *qEz, *qH;   // FP32 form: packed gather quads (FieldQuads)
   IonState ion;             // ion store (ion_cap > 0)
   long long ion_cap;        // ions stored at most; 0: no ion species
   double ion_sigma;         // spread of a newborn ion's velocity components sqrt(kT/m) [m/s]
@@ -732,17 +733,9 @@ __global__ void k_ion_read(IonState I, double *r, double *z, double *ur, double 
 }
 
 // ----------------------------------------------------------- FP32 form
-// clamped bilinear interpolation on a (ncol x nrow) column-major grid, split
-// into the four loads and the blend so that the loads can be issued early
+// bilinear interpolation from the four corners (c0,r0), (c1,r0), (c0,r1),
+// (c1,r1) of a packed gather quad (FieldQuads)
 struct Quad4 { float f00, f10, f01, f11; };
-
-__device__ __forceinline__ Quad4 bilin_load(const float *__restrict__ F, int ncol, int nrow,
-                                            int c0, int r0) {
-  const int ca = max(c0, 0), cb = min(c0 + 1, ncol - 1);
-  const int ra = max(r0, 0), rb = min(r0 + 1, nrow - 1);
-  const float *pa = F + ra * ncol, *pb = F + rb * ncol;
-  return Quad4{__ldg(pa + ca), __ldg(pa + cb), __ldg(pb + ca), __ldg(pb + cb)};
-}
 
 __device__ __forceinline__ float bilin_mix(const Quad4 &q, float wc, float wr) {
   const float lo = fmaf(wc, q.f10 - q.f00, q.f00), hi = fmaf(wc, q.f11 - q.f01, q.f01);
@@ -759,18 +752,20 @@ __device__ __forceinline__ float rsqrt_nr(float x) {
 // a + d with stochastic rounding.  The per-step velocity changes of the FP32
 // form (a drift rotation by a small angle, a kick in a weak field) are often
 // below one float ulp of u; rounding them to nearest would bias |u| steadily.
-// The exact residual e of a + d (TwoSum) moves the rounded sum s to its
-// neighbour nb on the side of e with probability |e| / |nb - s|.  The uniform
-// u = (k + 1/2) 2^-16 (k: the low 16 bits of r) is built as a float in [1, 2)
-// minus 1, so no conversion or division is issued; e = 0 keeps s.
+// With h the spacing of the floats in a's binade and U uniform in [0, 1), the
+// sum a + d + sign(a) U h rounded toward zero is a + d rounded to one of its
+// two neighbours on that grid, the far one with probability equal to the
+// distance from the near one in units of h: unbiased as long as a + d stays
+// in a's binade (within |d| of a power of two the grid changes and the split
+// is off by up to a factor 2; there |d| << |a| makes that a rare, tiny
+// error).  a + d + U h is formed exactly enough in one FMA (d and U h are
+// both small against a) and rounded once.  U = (k + 1/2) 2^-16 (k: the low 16
+// bits of r) is built as a float in [1, 2) minus 1; a = 0 gives h = 0 and the
+// exact d.
 __device__ __forceinline__ float sround_add(float a, float d, uint32_t r) {
-  const float s = a + d;
-  const float bb = s - a;
-  const float e = (a - (s - bb)) + (d - bb);
-  const int dir = ((__float_as_int(e) ^ __float_as_int(s)) >> 31) | 1;   // +1: away from 0
-  const float nb = __int_as_float(__float_as_int(s) + dir);
+  const float h = __int_as_float(__float_as_int(a) & 0x7F800000) * 1.1920928955078125e-07f;   // 2^-23
   const float u = __uint_as_float(0x3F800040u | ((r & 0xFFFFu) << 7)) - 1.0f;
-  return fabsf(e) > u * fabsf(nb - s) ? nb : s;
+  return __fadd_rz(a, fmaf(copysignf(u, a), h, d));
 }
 
 // floor(x) for |x| < 2^22, subtracted from x and returned as an int: x + 1.5
@@ -938,10 +933,12 @@ __device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &
   float wr, wz;
   half_shift(ir, fr, ar, wr);
   half_shift(iz, fz, az, wz);
-  // the field loads go out first; their latency hides behind Philox
-  const Quad4 qEr = bilin_load(F.Er, P.nr, P.nz + 1, ar, iz);
-  const Quad4 qEz = bilin_load(F.Ez, P.nr + 1, P.nz, ir, az);
-  const Quad4 qH = bilin_load(F.H, P.nr, P.nz, ar, az);
+  // the field loads go out first (one packed quad per field, corners already
+  // clamped at the edges); their latency hides behind Philox
+  const float4 a4 = __ldg(P.qEr + ((ar + 1) + iz * (P.nr + 1)));
+  const float4 b4 = __ldg(P.qEz + (ir + (az + 1) * P.nr));
+  const float4 c4 = __ldg(P.qH + ((ar + 1) + (az + 1) * (P.nr + 1)));
+  const Quad4 qEr{a4.x, a4.y, a4.z, a4.w}, qEz{b4.x, b4.y, b4.z, b4.w}, qH{c4.x, c4.y, c4.z, c4.w};
   philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
   const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]);
   const float Er = bilin_mix(qEr, wr, fz);
@@ -1214,14 +1211,17 @@ __global__ void __launch_bounds__(kMccBlock) k_collide32(const SimParams *__rest
 
 // ------------------------------------------------------------- FDTD
 // One fused field sub-cycle per step (fdtd_tiled).
-template <typename T>
-__global__ void __launch_bounds__(32 * kFdtdRows) k_sim_fdtd(T *Er, T *Ez, T *H, const unsigned long long *Jr,
+// R1: the fdtd_ratio 1 specialisation (the two variants need their own
+// kernels: each declares a 40 KB patch)
+template <typename T, bool R1>
+__global__ void __launch_bounds__(32 * kFdtdRows, 3) k_sim_fdtd(T *Er, T *Ez, T *H, const unsigned long long *Jr,
                                                   const unsigned long long *Jz,
                                                   unsigned long long *Jr_next,
                                                   unsigned long long *Jz_next, int nr, int nz,
                                                   FdtdCoef c, const double *invV, double mu,
                                                   double dt, int R, unsigned flags,
-                                                  SimCounters *cnt, ExtraCurrent ion) {
+                                                  SimCounters *cnt, ExtraCurrent ion,
+                                                  FieldQuads quads) {
   // FP32 form (cnt given): commit the previous pass and open step s - the
   // births of the last pass join the slots, the queue that pass consumed is
   // emptied, the chunk counter rewinds; no other kernel runs meanwhile
@@ -1234,7 +1234,10 @@ __global__ void __launch_bounds__(32 * kFdtdRows) k_sim_fdtd(T *Er, T *Ez, T *H,
     cnt->chunk_next = 0;
     cnt->step = ns;
   }
-  fdtd_tiled<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, c, invV, mu, dt, R, flags, ion);
+  if (R1)
+    fdtd_tiled1<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, c, invV, mu, dt, flags, ion, quads);
+  else
+    fdtd_tiled<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, c, invV, mu, dt, R, flags, ion, quads);
 }
 
 // ---------------------------------------------------------- load/read
@@ -1544,6 +1547,7 @@ struct gasatt_sim {
   unsigned long long *Jir = nullptr, *Jiz = nullptr;
   double ion_scale = 1.0;
   IonState ion_tmp{};             // scratch store the ions are sorted into before a push
+  FieldQuads quads{};             // FP32 form: gather quads, written with the fields
   bool mcc_pending = false;       // the last pass's collisions are not applied yet
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;   // graph capture fork/join
   bool timing = false;
@@ -1586,14 +1590,16 @@ int launch_fdtd(gasatt_sim *s, cudaStream_t st, int q) {
   const double dt = c.dt / R;
   // the held ion current, in the electron current's fixed-point units
   const ExtraCurrent ion{s->Jir, s->Jiz, s->scale / s->ion_scale};
+  auto k64 = R == 1 ? k_sim_fdtd<double, true> : k_sim_fdtd<double, false>;
+  auto k32 = R == 1 ? k_sim_fdtd<float, true> : k_sim_fdtd<float, false>;
   if (s->form == 0)
-    k_sim_fdtd<double><<<grid, block, 0, st>>>(
+    k64<<<grid, block, 0, st>>>(
         (double *)s->Er, (double *)s->Ez, (double *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
-        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, nullptr, ion);
+        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, nullptr, ion, FieldQuads{});
   else
-    k_sim_fdtd<float><<<grid, block, 0, st>>>(
+    k32<<<grid, block, 0, st>>>(
         (float *)s->Er, (float *)s->Ez, (float *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
-        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt, ion);
+        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt, ion, s->quads);
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "fdtd launch");
@@ -1995,6 +2001,15 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
     return cleanup(rc);
   s->d_tab = tmpd;
   if ((rc = sim_alloc(s, &s->invV, (size_t)nr))) return cleanup(rc);
+  if (s->form == 1) {
+    if ((rc = sim_alloc(s, &s->quads.er, (size_t)(nr + 1) * nz)) ||
+        (rc = sim_alloc(s, &s->quads.ez, (size_t)nr * (nz + 1))) ||
+        (rc = sim_alloc(s, &s->quads.h, (size_t)(nr + 1) * (nz + 1))))
+      return cleanup(rc);
+    cudaMemset(s->quads.er, 0, (size_t)(nr + 1) * nz * 16);
+    cudaMemset(s->quads.ez, 0, (size_t)nr * (nz + 1) * 16);
+    cudaMemset(s->quads.h, 0, (size_t)(nr + 1) * (nz + 1) * 16);
+  }
   cub::DeviceScan::ExclusiveSum(nullptr, s->scan_bytes, s->cell_count, s->cell_offset, nbin + 1);
   if ((rc = sim_alloc(s, (char **)&s->scan_tmp, s->scan_bytes))) return cleanup(rc);
   s->partial_blocks = 296;
@@ -2040,6 +2055,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   P.n_exc = s->tabs.n_exc;
   std::memcpy(P.exc, s->tabs.exc, sizeof(P.exc));
   P.Jr = s->Jr[0]; P.Jz = s->Jz[0];
+  P.qEr = s->quads.er; P.qEz = s->quads.ez; P.qH = s->quads.h;
   {
     std::vector<double> iv(nr);
     for (int i = 0; i < nr; ++i) iv[i] = (1.0 / s->scale) / shell_volume(i, c.dr, c.dz, c.PHIp);
@@ -2343,6 +2359,27 @@ int gasatt_sim_read_ions(gasatt_sim *s, double *r, double *z, double *ur, double
 }
 
 namespace {
+// the gather quads of whole float fields (after the fields are set from outside)
+__global__ void k_build_quads(const float *Er, const float *Ez, const float *H, int nr, int nz,
+                              FieldQuads q) {
+  const int64_t nE = (int64_t)nr * (nz + 1), nZ = (int64_t)(nr + 1) * nz, nH = (int64_t)nr * nz;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nE + nZ + nH;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    if (k < nE) {
+      const int i = (int)(k % nr), j = (int)(k / nr);
+      quad_put(q.er, nr + 1, quad_axis_shifted(i, nr), quad_axis_plain(j, nz), Er[k]);
+    } else if (k < nE + nZ) {
+      const int64_t m = k - nE;
+      const int i = (int)(m % (nr + 1)), j = (int)(m / (nr + 1));
+      quad_put(q.ez, nr, quad_axis_plain(i, nr), quad_axis_shifted(j, nz), Ez[m]);
+    } else {
+      const int64_t m = k - nE - nZ;
+      const int i = (int)(m % nr), j = (int)(m / nr);
+      quad_put(q.h, nr + 1, quad_axis_shifted(i, nr), quad_axis_shifted(j, nz), H[m]);
+    }
+  }
+}
+
 __global__ void k_f64_to_f32(const double *a, float *b, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     b[i] = (float)a[i];
@@ -2386,6 +2423,11 @@ int fields_io(gasatt_sim *s, double *Er, double *Ez, double *H, int on_device, b
         GASATT_CUDA(ctx, cudaMemcpyAsync(u[f], stage, n[f] * 8, cudaMemcpyDeviceToHost, st));
     }
     off += n[f];
+  }
+  if (set && s->form == 1) {
+    k_build_quads<<<grid_for(n[0] + n[1] + n[2], kBlock), kBlock, 0, st>>>(
+        (const float *)s->Er, (const float *)s->Ez, (const float *)s->H, nr, nz, s->quads);
+    GASATT_LAUNCHED(ctx);
   }
   GASATT_CUDA(ctx, cudaStreamSynchronize(st));
   return GASATT_OK;

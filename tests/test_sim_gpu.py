@@ -176,3 +176,52 @@ def test_births_conserved(precision, sort_period):
             assert d["n_total"] == n0 + d["n_ionizations"]
         assert len(np.unique(got["id"][alive])) == int(alive.sum())
     assert d["n_ionizations"] > 50
+
+
+def test_fp32_gather_matches_fp64_in_strong_fields():
+    """One step in strong random fields: the FP32 form's packed-quad gather
+    gives the kicks of the FP64 form's scalar gather to float precision (a
+    wrong corner or edge clamp would show as an O(1) error in the kick)."""
+    got = {}
+    for prec in (_lib.FP64, _lib.FP32_SPLIT):
+        cfg, sim, parts, _ = start(prec, n_photo=4000)
+        sim.set_gas_density(np.zeros((NR, NZ)))          # no collisions: pure push
+        sim.step(1)
+        d = sim.read()
+        got[prec] = by_id(d["id"], d["r"], d["z"], d["ur"], d["ut"], d["uz"])
+        u0 = np.sqrt(parts[2]**2 + parts[3]**2 + parts[4]**2)
+        sim.close()
+    r64, z64, ur64, ut64, uz64 = got[_lib.FP64]
+    r32, z32, ur32, ut32, uz32 = got[_lib.FP32_SPLIT]
+    umax = u0.max()
+    for a, b, k in ((ur32, ur64, "ur"), (ut32, ut64, "ut"), (uz32, uz64, "uz")):
+        assert np.abs(a - b).max() < 5e-7 * umax, k     # kicks here are ~1e-4 of |u|
+    assert np.abs(r32 - r64).max() < 1e-6 * NR * D
+    assert np.abs(z32 - z64).max() < 1e-6 * NZ * D
+
+
+@pytest.mark.parametrize("precision,tol", [(_lib.FP64, 1e-8), (_lib.FP32_SPLIT, 1e-6)])
+def test_free_drift_keeps_kinetic_energy(precision, tol):
+    """2000 steps without fields or collisions (gas map all zero, FN 1e-6 so
+    the self-field does no measurable work): the drift only turns (u_r,
+    u_theta), so the kinetic energy must stay put; the FP32 form's turns are
+    far below one ulp of u each step, and stochastic rounding keeps them from
+    adding up to a drift."""
+    nr, nz = 64, 64
+    cfg = config(nr, nz, D, 1e-14, 1.0, precision=precision, capacity=8000, seed=5,
+                 sort_period=50, FN=1e-6)
+    rng = np.random.default_rng(9)
+    n = 8000
+    speed = 5.93e6                                     # about 100 eV
+    ct = rng.uniform(-1, 1, n); ph = rng.uniform(0, 2 * np.pi, n); st = np.sqrt(1 - ct**2)
+    sim = Sim(cfg)
+    # radii 20-150 um against a wall at 320 um: 2000 steps move them 119 um at most
+    sim.load(rng.uniform(20e-6, 150e-6, n), rng.uniform(5, nz - 5, n) * D,
+             speed * st * np.cos(ph), speed * st * np.sin(ph), speed * ct,
+             np.arange(n, dtype=np.uint64))
+    sim.set_gas_density(np.zeros((nr, nz)))
+    e0 = sim.diag()["kinetic_ev"]
+    sim.step(2000)
+    d = sim.diag()
+    assert d["n_lost_wall"] == 0 and d["n_alive"] == n
+    assert abs(d["kinetic_ev"] / e0 - 1) < tol, d["kinetic_ev"] / e0 - 1
