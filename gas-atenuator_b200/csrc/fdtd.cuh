@@ -276,6 +276,27 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
   }
 }
 
+// quad_put for H (shifted on both axes): the four slots every value has,
+// written directly, then the clamped edges' extra slots
+__device__ __forceinline__ void quad_put_h(float4 *Q, int nr, int nz, int i, int j, float v) {
+  const int ncq = nr + 1;
+  float *f = reinterpret_cast<float *>(Q) + 4 * ((int64_t)(i + 1) + (int64_t)(j + 1) * ncq);
+  f[0] = v;                          // quad (i+1, j+1), corner (c0, r0)
+  f[-4 + 1] = v;                     // quad (i, j+1), corner (c1, r0)
+  f[-4 * ncq + 2] = v;               // quad (i+1, j), corner (c0, r1)
+  f[-4 * ncq - 4 + 3] = v;           // quad (i, j), corner (c1, r1)
+  if (i == 0 || i == nr - 1 || j == 0 || j == nz - 1) {
+    const QuadAxis cx = quad_axis_shifted(i, nr), ry = quad_axis_shifted(j, nz);
+    float *g = reinterpret_cast<float *>(Q);
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        if ((a >= 2 || b >= 2) && ((cx.m >> a) & 1u) && ((ry.m >> b) & 1u))
+          g[(((int64_t)cx.q[a] + (int64_t)ry.q[b] * ncq) << 2) + cx.d[a] + 2 * ry.d[b]] = v;
+  }
+}
+
 // The fused sub-cycle for fdtd_ratio 1 (the product's): H(dt/4), E(dt/2),
 // H(dt/2), E(dt/2), H(dt/4) on a 32 x 32 patch with a 27 x 27 tile, the same
 // arithmetic as fdtd_tiled, unrolled: each thread owns one column and two rows
@@ -416,7 +437,7 @@ __device__ __forceinline__ void fdtd_tiled1(T *__restrict__ Er, T *__restrict__ 
         H[g] = v;
         // H is correct only on the tile, one short of its quads' corners:
         // each value goes to the quad slots that read it instead
-        if (q.h) quad_put(q.h, nr + 1, quad_axis_shifted(i, nr), quad_axis_shifted(jj, nz), (float)v);
+        if (q.h) quad_put_h(q.h, nr, nz, i, jj, (float)v);
         Jr_next[g] = 0;
         Jz_next[g] = 0;
       }
