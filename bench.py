@@ -613,7 +613,9 @@ def run_c5(args):
         ev = 6.241509074e18 * d["field_energy_j"]
         return dict(electron_kinetic_ev=d["kinetic_ev"], ion_kinetic_ev=d["ion_kinetic_ev"],
                     field_energy_j=d["field_energy_j"], collision_loss_ev=d["collision_loss_ev"],
-                    sum_ev=d["kinetic_ev"] + d["ion_kinetic_ev"] + ev + d["collision_loss_ev"])
+                    wall_loss_ev=d["wall_loss_ev"],
+                    sum_ev=d["kinetic_ev"] + d["ion_kinetic_ev"] + ev + d["collision_loss_ev"]
+                    + d["wall_loss_ev"])
 
     ferr = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
                for a, b in zip(f32["fields"], f64["fields"]))
@@ -633,8 +635,9 @@ def run_c5(args):
                                  "identity": "ions - electrons = -N0 + electrons lost - ions lost"},
             "energy_fp64": {"start": energy(f64["start"]), "end": energy(e64),
                             "sum_rel_change": energy(e64)["sum_ev"] / energy(f64["start"])["sum_ev"] - 1,
-                            "note": "sum = electron + ion kinetic + field + given to the gas; "
-                                    "electrons and ions absorbed at the wall take theirs away"},
+                            "note": "sum = electron + ion kinetic + field + given to the gas "
+                                    "+ carried out by the electrons and ions absorbed at the wall; "
+                                    "newborn ions add their thermal energy"},
             "drift_fp32_vs_fp64": {"field_rel_err_l2": ferr,
                                    "electron_kinetic_rel": e32["kinetic_ev"] / e64["kinetic_ev"] - 1,
                                    "ion_kinetic_rel": (e32["ion_kinetic_ev"] / e64["ion_kinetic_ev"] - 1)

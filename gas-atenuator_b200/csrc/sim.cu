@@ -67,7 +67,8 @@ struct SimCounters {
   unsigned long long kin_fx;     // diagnostic: sum E_kin * 2^16 [eV]
   unsigned long long alive;      // diagnostic
   unsigned long long exc_loss_fx; // diagnostic: excitation energy losses * 2^16 [eV]
-  unsigned long long pad5_[7];
+  unsigned long long wall_loss_fx;// diagnostic: kinetic energy absorbed at r = Rp * 2^16 [eV]
+  unsigned long long pad5_[6];
   unsigned long long n_ions;     // ion slots claimed (loads and births; may pass the capacity)
   unsigned long long ion_overflow, ion_lost;
   unsigned long long ion_alive, ion_charge, ion_kin_fx;   // diagnostics; kinetic: E * 2^32 [eV]
@@ -311,6 +312,13 @@ __device__ __forceinline__ int mcc_event(const SimParams &P, uint64_t id, long l
   return 4;
 }
 
+// kinetic energy of a particle absorbed at the wall, u2 = |u / c|^2 and
+// mc2 = m c^2 / q_e [eV] (rare: taken only on the step it leaves)
+__device__ __forceinline__ void count_wall_loss(SimCounters *cnt, double u2, double mc2) {
+  const double E = mc2 * (u2 / (sqrt(1 + u2) + 1));
+  atomicAdd(&cnt->wall_loss_fx, (unsigned long long)__double2ll_rn(E * 65536.0));
+}
+
 __device__ __forceinline__ void count_event(SimCounters *cnt, int ev, const Birth &b) {
   if (ev == 1) atomicAdd(&cnt->ela, 1ull);
   else if (ev == 2) atomicAdd(&cnt->ion, 1ull);
@@ -506,7 +514,11 @@ __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fi
       }
       if (alive && mode != 2) halfdrift64(r, z, ur, ut, uz, alive, P);
       if (alive && mode == 0) cand = null_candidate(P, S.id[p], step);
-      if (!alive) { lost++; r = -1.0; }
+      if (!alive) {
+        lost++;
+        r = -1.0;
+        count_wall_loss(cnt, (ur * ur + ut * ut + uz * uz) / (P.c * P.c), P.me * P.c * P.c / P.qe);
+      }
       rz = make_double2(r, z); urt = make_double2(ur, ut);
       S.rz[p] = rz; S.urt[p] = urt; S.uz[p] = uz;
       act = alive && mode != 2;
@@ -664,7 +676,11 @@ __global__ void __launch_bounds__(kBlock) k_ion_push(SimParams P, Fields<T> F, S
       boris(ur, ut, uz, E_r, 0.0, E_z, 0.0, P.mu0 * Hp, 0.0, Zq * P.qm_dt2, P.c);
       halfdrift64(r, z, ur, ut, uz, alive, P);
       if (alive) halfdrift64(r, z, ur, ut, uz, alive, P);
-      if (!alive) { lost++; r = -1.0; }
+      if (!alive) {
+        lost++;
+        r = -1.0;
+        count_wall_loss(cnt, (ur * ur + ut * ut + uz * uz) / (P.c * P.c), P.m_ion * P.c * P.c / P.qe);
+      }
       rz = make_double2(r, z); urt = make_double2(ur, ut);
       I.rz[p] = rz; I.urt[p] = urt; I.uz[p] = uz;
       act = alive;
@@ -1018,7 +1034,10 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
         float cig;
         cc = push32(P, F, cid, step, mode, cir, ciz, cfr, cfz, cur, cut, cuz, calive, cig);
         if (calive && mode != 2) deposit_global32(P, cir, ciz, cfr, cfz, cur, cuz, cig);
-        if (!calive) lost++;
+        if (!calive) {
+          lost++;
+          count_wall_loss(cnt, (double)cur * cur + (double)cut * cut + (double)cuz * cuz, P.me * P.c * P.c / P.qe);
+        }
         if (cc) queue_one(cnt, queue, P, par, slot);
       }
       S.a[slot] = pack32(cir, ciz, cfr, cfz, cur, calive, cc, mark);
@@ -1034,7 +1053,10 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
     float pig;
     pc = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive, pig);
     if (alive && mode != 2) deposit_global32(P, ir, iz, fr, fz, ur, uz, pig);
-    if (!alive) lost++;
+    if (!alive) {
+      lost++;
+      count_wall_loss(cnt, (double)ur * ur + (double)ut * ut + (double)uz * uz, P.me * P.c * P.c / P.qe);
+    }
     if (pc) queue_one(cnt, queue, P, par, p);
   }
   S.a[p] = pack32(ir, iz, fr, fz, ur, alive, pc, mark);
@@ -1136,7 +1158,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
       if (act) {
         bool alive = true;
         cand = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive, ig);
-        if (!alive) lost++;
+        if (!alive) {
+          lost++;
+          count_wall_loss(cnt, (double)ur * ur + (double)ut * ut + (double)uz * uz, P.me * P.c * P.c / P.qe);
+        }
         S.a[p] = pack32(ir, iz, fr, fz, ur, alive, cand, par);
         S.b[p] = make_float2(ut, uz);
         act = alive && mode != 2;
@@ -2551,6 +2576,7 @@ int gasatt_sim_diag(gasatt_sim *s, gasatt_diag *d) {
   d->ion_kinetic_ev = (double)h.ion_kin_fx / 4294967296.0;
   d->net_charge_c = s->cfg.q_e * s->cfg.FN * ((double)h.ion_charge - (double)h.alive);
   d->collision_loss_ev = GASATT_ION_I_EV * (double)h.ion + (double)h.exc_loss_fx / 65536.0;
+  d->wall_loss_ev = (double)h.wall_loss_fx / 65536.0;
   return GASATT_OK;
 }
 

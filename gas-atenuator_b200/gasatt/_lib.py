@@ -62,7 +62,7 @@ class Diag(ctypes.Structure):
                 ("n_lost_wall", c_i64), ("n_ions", c_i64), ("kinetic_ev", c_d),
                 ("field_energy_j", c_d), ("steps", c_i64), ("status_flags", ctypes.c_int32),
                 ("n_ion_lost_wall", c_i64), ("ion_kinetic_ev", c_d), ("net_charge_c", c_d),
-                ("collision_loss_ev", c_d)]
+                ("collision_loss_ev", c_d), ("wall_loss_ev", c_d)]
 
 
 _SIGS = {

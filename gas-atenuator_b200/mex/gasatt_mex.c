@@ -421,9 +421,9 @@ static void cmd_sim_diag(mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
                                 "n_excitation", "n_null", "n_lost_wall", "n_ions",
                                 "kinetic_ev", "field_energy_j", "steps", "status_flags",
                                 "n_ion_lost_wall", "ion_kinetic_ev", "net_charge_c",
-                                "collision_loss_ev"};
+                                "collision_loss_ev", "wall_loss_ev"};
   gasatt_diag d;
-  double w[16];
+  double w[17];
   int k;
   nargs(nrhs, 2, "sim_diag(h)");
   check(gasatt_sim_diag(sim_of(prhs[1]), &d));
@@ -432,9 +432,9 @@ static void cmd_sim_diag(mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
   w[6] = (double)d.n_lost_wall; w[7] = (double)d.n_ions; w[8] = d.kinetic_ev;
   w[9] = d.field_energy_j; w[10] = (double)d.steps; w[11] = (double)d.status_flags;
   w[12] = (double)d.n_ion_lost_wall; w[13] = d.ion_kinetic_ev; w[14] = d.net_charge_c;
-  w[15] = d.collision_loss_ev;
-  plhs[0] = mxCreateStructMatrix(1, 1, 16, names);
-  for (k = 0; k < 16; ++k) mxSetField(plhs[0], 0, names[k], mxCreateDoubleScalar(w[k]));
+  w[15] = d.collision_loss_ev; w[16] = d.wall_loss_ev;
+  plhs[0] = mxCreateStructMatrix(1, 1, 17, names);
+  for (k = 0; k < 17; ++k) mxSetField(plhs[0], 0, names[k], mxCreateDoubleScalar(w[k]));
 }
 
 static const char *const k_commands[] = {

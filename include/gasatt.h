@@ -274,6 +274,8 @@ typedef struct gasatt_diag {
                                q_e FN (sum of ion charge numbers - electrons alive) */
   double  collision_loss_ev;/* cumulative electron energy given to the gas [eV] (x FN not
                                applied): 15.6 eV per ionization + the excitation losses */
+  double  wall_loss_ev;     /* cumulative kinetic energy of the electrons and ions absorbed
+                               at r = Rp [eV] (x FN not applied) */
 } gasatt_diag;
 
 typedef struct gasatt_sim gasatt_sim;
