@@ -97,6 +97,66 @@ __global__ void k_free_motion(const double *vx, const double *vy, const double *
   }
 }
 
+// ---------------------------------------------------------------- REBOND
+// REBOND.m:6-66: an azimuth below 0 is raised by PHIp, with (v1, v2) turned
+// by +PHIp, until it is not; the wrapped particle's x, y are rebuilt from r
+// and the new azimuth; the same downwards above PHIp; then specular
+// reflection at z = Lp and at z = 0.  Each wrap or reflection is one boundary
+// event (count[0]).  The reference loops until every azimuth is inside; here a
+// particle stops after kRebondMaxWraps wraps and raises count[1] (the call
+// then fails) instead of looping without end on a wild azimuth.
+constexpr int kRebondMaxWraps = 4096;
+
+__global__ void k_rebond(double *pos, int64_t ldp, const double *r, const double *phi,
+                         double *vel, int64_t ldv, int64_t n, double Lp, double PHIp, double cP,
+                         double sP, unsigned long long *count) {
+  unsigned long long ev = 0, bad = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double ph = phi[i], v1 = vel[i], v2 = vel[ldv + i];
+    int k = 0;
+    if (ph < 0) {
+      while (ph < 0 && k < kRebondMaxWraps) {
+        ph = ph + PHIp;
+        const double w = v1 * cP - v2 * sP;
+        v2 = v1 * sP + v2 * cP;
+        v1 = w;
+        ++k;
+      }
+      pos[i] = r[i] * cos(ph);
+      pos[ldp + i] = r[i] * sin(ph);
+    }
+    if (ph > PHIp) {
+      while (ph > PHIp && k < kRebondMaxWraps) {
+        ph = ph - PHIp;
+        const double w = v1 * cP + v2 * sP;
+        v2 = -v1 * sP + v2 * cP;
+        v1 = w;
+        ++k;
+      }
+      pos[i] = r[i] * cos(ph);
+      pos[ldp + i] = r[i] * sin(ph);
+    }
+    if (ph < 0 || ph > PHIp) bad++;
+    vel[i] = v1;
+    vel[ldv + i] = v2;
+    double z = pos[2 * ldp + i], vz = vel[2 * ldv + i];
+    if (z > Lp) { z = 2 * Lp - z; vz = -vz; ++k; }
+    if (z < 0) { z = -z; vz = -vz; ++k; }
+    pos[2 * ldp + i] = z;
+    vel[2 * ldv + i] = vz;
+    ev += (unsigned long long)k;
+  }
+  for (int o = 16; o; o >>= 1) {
+    ev += __shfl_down_sync(0xFFFFFFFFu, ev, o);
+    bad += __shfl_down_sync(0xFFFFFFFFu, bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (ev) atomicAdd(count, ev);
+    if (bad) atomicAdd(count + 1, bad);
+  }
+}
+
 // ------------------------------------------------------ particle_density
 // particle_density.m:24-28: 1-based cell index via MATLAB round(x/d + 0.5)
 __global__ void k_density_count(double dr, double dz, const double *dphi, int rmax,
@@ -571,6 +631,31 @@ int gasatt_free_motion(gasatt_ctx *ctx, const double *vx, const double *vy, cons
   GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
   k_free_motion<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(vx, vy, vz, x, y, z, n, dt, xn, yn, zn, rn, phin);
   GASATT_LAUNCHED(ctx);
+  return GASATT_OK;
+}
+
+int gasatt_rebond(gasatt_ctx *ctx, double *pos, int64_t ld_pos, const double *r,
+                  const double *phi, double *vel, int64_t ld_vel, int64_t n, double Lp,
+                  double PHIp, int64_t *n_boundary) {
+  if (!ctx || n < 0 || ld_pos < n || ld_vel < n || !(PHIp > 0) || !(Lp > 0))
+    return fail(ctx, GASATT_E_ARG, "REBOND: bad sizes");
+  if (n_boundary) *n_boundary = 0;
+  if (n == 0) return GASATT_OK;
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  void *buf;
+  int st = scratch(ctx, 16, &buf);
+  if (st) return st;
+  unsigned long long *cnt = (unsigned long long *)buf, h[2] = {0, 0};
+  GASATT_CUDA(ctx, cudaMemsetAsync(cnt, 0, 16, ctx->stream));
+  // cos and sin of the wedge angle on the host, once, like the reference's
+  // cos(PHIp) and sin(PHIp) of every wrap
+  k_rebond<<<grid_for(n, kBlock), kBlock, 0, ctx->stream>>>(pos, ld_pos, r, phi, vel, ld_vel, n, Lp,
+                                                             PHIp, std::cos(PHIp), std::sin(PHIp), cnt);
+  GASATT_LAUNCHED(ctx);
+  GASATT_CUDA(ctx, cudaMemcpyAsync(h, cnt, 16, cudaMemcpyDeviceToHost, ctx->stream));
+  GASATT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h[1]) return fail(ctx, GASATT_E_ARG, "REBOND: an azimuth lies more than 4096 wedges outside");
+  if (n_boundary) *n_boundary = (int64_t)h[0];
   return GASATT_OK;
 }
 

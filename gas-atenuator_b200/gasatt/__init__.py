@@ -6,10 +6,11 @@ simulation driver.
 """
 from . import _lib
 from ._lib import FAITHFUL, FP32_SPLIT, FP64, POS_IN_CYL, GasattError
-from .dropin import (Context, default_context, electricmagneticfield6, electron_collision,
-                     find_CS0, free_motion, particle_density, particle_density0)
+from .dropin import (REBOND, Context, default_context, electricmagneticfield6,
+                     electron_collision, find_CS0, free_motion, particle_density,
+                     particle_density0)
 from .tables import N2Tables
 
 __all__ = ["Context", "default_context", "electricmagneticfield6", "electron_collision",
-           "find_CS0", "free_motion", "particle_density", "particle_density0", "N2Tables",
+           "find_CS0", "free_motion", "particle_density", "particle_density0", "REBOND", "N2Tables",
            "GasattError", "FAITHFUL", "POS_IN_CYL", "FP64", "FP32_SPLIT"]

@@ -111,6 +111,21 @@ def free_motion(vx, vy, vz, x, y, z, dt, *, device=0):
     return tuple(outs)
 
 
+def REBOND(particle_position, particle_r, particle_phi, particle_velocity, Lp, PHIp, *, device=0):
+    """[particle_position, particle_velocity, N_boundary] = REBOND(particle_position,
+    particle_r, particle_phi, particle_velocity, Lp, PHIp): azimuths wrapped
+    into the wedge [0, PHIp] (velocity turned with them), z reflected at Lp and 0."""
+    ctx = default_context(device)
+    pos, vel = _col(particle_position, device), _col(particle_velocity, device)
+    r = _dev(particle_r, device).reshape(-1).contiguous()
+    phi = _dev(particle_phi, device).reshape(-1).contiguous()
+    n = pos.shape[1]
+    nb = ctypes.c_int64()
+    check(ctx.handle, lib.gasatt_rebond(ctx.handle, _p(pos), n, _p(r), _p(phi), _p(vel), n, n,
+                                        float(Lp), float(PHIp), ctypes.byref(nb)))
+    return pos.t(), vel.t(), nb.value
+
+
 def particle_density(dr, dz, dphi, r, phi, z, cellnumxy, sum_cell, VC, FN, *, ncell=None, device=0):
     """density = particle_density(dr, dz, dphi, r, phi, z, cellnumxy, sum_cell, VC, FN).
 

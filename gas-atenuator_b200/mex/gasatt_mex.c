@@ -11,6 +11,7 @@
  *   gasatt_mex('tables', t_el, t_sel, t_sel_1, t_del, t_sdel, t_ion, t_exc)
  *   [se, si, sx] = gasatt_mex('find_CS0', t_el, t_sel, t_ion, t_exc, E_PE)        find_CS0.m:1
  *   [xn, yn, zn, rn, phin] = gasatt_mex('free_motion', vx, vy, vz, x, y, z, dt)   free_motion.m:1
+ *   [pos, vel, N_boundary] = gasatt_mex('REBOND', pos, r, phi, vel, Lp, PHIp)     REBOND.m:1
  *   d = gasatt_mex('particle_density', dr, dz, dphi, r, phi, z, cellnumxy,
  *                  sum_cell, VC, FN, ncell)                                      particle_density.m:1
  *   [e_pos, e_vel, i1_pos, i1_vel, i2_pos, i2_vel, Er, Ez, Hphi, kin] =
@@ -220,6 +221,27 @@ static void cmd_free_motion(int nlhs, mxArray *plhs[], int nrhs, const mxArray *
     if (k < (nlhs > 0 ? nlhs : 1)) plhs[k] = gpu_out(g[k]);
     else mxGPUDestroyGPUArray(g[k]);
   }
+}
+
+static void cmd_rebond(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
+  gpu_in pos, r, phi, vel;
+  int64_t nb = 0, n;
+  nargs(nrhs, 7, "REBOND(particle_position, particle_r, particle_phi, particle_velocity, Lp, PHIp)");
+  pos = gpu_copy(prhs[1], "particle_position must be a double gpuArray");
+  r = gpu_copy(prhs[2], "particle_r must be a double gpuArray");
+  phi = gpu_copy(prhs[3], "particle_phi must be a double gpuArray");
+  vel = gpu_copy(prhs[4], "particle_velocity must be a double gpuArray");
+  n = pos.rows;
+  if ((n && pos.cols != 3) || vel.rows != n || (n && vel.cols != 3) || r.rows * r.cols != n ||
+      phi.rows * phi.cols != n)
+    fail("REBOND: positions and velocities n x 3, r and phi of length n");
+  check(gasatt_rebond(g_ctx, pos.p, n, r.p, phi.p, vel.p, n, n, scalar(prhs[5], "Lp"),
+                      scalar(prhs[6], "PHIp"), &nb));
+  plhs[0] = mxGPUCreateMxArrayOnGPU(pos.g);
+  if (nlhs > 1) plhs[1] = mxGPUCreateMxArrayOnGPU(vel.g);
+  if (nlhs > 2) plhs[2] = mxCreateDoubleScalar((double)nb);
+  mxGPUDestroyGPUArray(pos.g); mxGPUDestroyGPUArray(r.g);
+  mxGPUDestroyGPUArray(phi.g); mxGPUDestroyGPUArray(vel.g);
 }
 
 static void cmd_particle_density(mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
@@ -438,7 +460,7 @@ static void cmd_sim_diag(mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
 }
 
 static const char *const k_commands[] = {
-    "init", "tables", "find_CS0", "free_motion", "particle_density", "electricmagneticfield6",
+    "init", "tables", "find_CS0", "free_motion", "REBOND", "particle_density", "electricmagneticfield6",
     "electron_collision", "sim_create", "sim_load", "sim_step", "sim_read", "sim_diag",
     "sim_destroy"};
 
@@ -465,6 +487,7 @@ void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
   ensure_ctx();
   if (!strcmp(cmd, "find_CS0")) cmd_find_cs0(nlhs, plhs, nrhs, prhs);
   else if (!strcmp(cmd, "free_motion")) cmd_free_motion(nlhs, plhs, nrhs, prhs);
+  else if (!strcmp(cmd, "REBOND")) cmd_rebond(nlhs, plhs, nrhs, prhs);
   else if (!strcmp(cmd, "particle_density")) cmd_particle_density(plhs, nrhs, prhs);
   else if (!strcmp(cmd, "electricmagneticfield6")) cmd_emf6(nlhs, plhs, nrhs, prhs);
   else if (!strcmp(cmd, "electron_collision")) cmd_collision(nlhs, plhs, nrhs, prhs);

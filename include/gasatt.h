@@ -143,6 +143,19 @@ int gasatt_free_motion(gasatt_ctx *ctx,
                        int64_t n, double dt,
                        double *xn, double *yn, double *zn, double *rn, double *phin);
 
+/* REBOND.m:1-70: the boundary rule of the reference's gpuArray drivers.
+ * pos, vel: device, n x 3 column-major with leading dimensions ld_pos, ld_vel
+ * (x, y, z and vx, vy, vz), updated in place; r, phi: device, length n (the
+ * particles' radius and azimuth).  An azimuth outside [0, PHIp] is wrapped
+ * into it one wedge at a time, turning (vx, vy) by the wedge angle each time,
+ * and x, y are rebuilt from r and the new azimuth; then z is reflected at Lp
+ * and at 0 (vz flipped).  *n_boundary: wraps plus reflections.  An azimuth
+ * more than 4096 wedges outside fails with GASATT_E_ARG (the reference would
+ * loop on). */
+int gasatt_rebond(gasatt_ctx *ctx, double *pos, int64_t ld_pos, const double *r,
+                  const double *phi, double *vel, int64_t ld_vel, int64_t n, double Lp,
+                  double PHIp, int64_t *n_boundary);
+
 /* particle_density.m:1-38 (10-argument form).
  * dphi, sum_cell: device arrays of length rmax (sum_cell(k) = cells with r index <= k).
  * r, phi, z: device, length n.  VC: device, length cellnumxy (volume of the

@@ -661,6 +661,52 @@ void orc_free_motion(const double *vx, const double *vy, const double *vz, const
   }
 }
 
+/* REBOND.m:6-66: an azimuth below 0 is raised by PHIp, and (v1, v2) turned
+ * by +PHIp, until it is not (:7-22); the wrapped particles' x, y are rebuilt
+ * from r and the new azimuth (:24-25); the same downwards above PHIp
+ * (:31-48); then specular reflection at z = Lp (:53-60) and at z = 0
+ * (:62-67).  Every wrap and reflection counts one boundary event. */
+int64_t orc_rebond(double *pos, int64_t ldp, const double *r, const double *phi, double *vel,
+                   int64_t ldv, int64_t n, double Lp, double PHIp, int max_wraps) {
+  const double cP = cos(PHIp), sP = sin(PHIp);
+  int64_t events = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    double ph = phi[i], v1 = vel[i], v2 = vel[ldv + i];
+    int k = 0;
+    if (ph < 0) {
+      while (ph < 0) {
+        if (++k > max_wraps) return -1;
+        ph = ph + PHIp;
+        const double w = v1 * cP - v2 * sP;
+        v2 = v1 * sP + v2 * cP;
+        v1 = w;
+      }
+      pos[i] = r[i] * cos(ph);
+      pos[ldp + i] = r[i] * sin(ph);
+    }
+    if (ph > PHIp) {
+      while (ph > PHIp) {
+        if (++k > max_wraps) return -1;
+        ph = ph - PHIp;
+        const double w = v1 * cP + v2 * sP;
+        v2 = -v1 * sP + v2 * cP;
+        v1 = w;
+      }
+      pos[i] = r[i] * cos(ph);
+      pos[ldp + i] = r[i] * sin(ph);
+    }
+    vel[i] = v1;
+    vel[ldv + i] = v2;
+    double z = pos[2 * ldp + i], vz = vel[2 * ldv + i];
+    if (z > Lp) { z = 2 * Lp - z; vz = -vz; ++k; }
+    if (z < 0) { z = -z; vz = -vz; ++k; }
+    pos[2 * ldp + i] = z;
+    vel[2 * ldv + i] = vz;
+    events += k;
+  }
+  return events;
+}
+
 /* particle_density.m:24-34: round(x/d + 0.5) indices (MATLAB round = half
  * away from zero), sparse histogram, FN / VC. */
 void orc_particle_density(double dr, double dz, const double *dphi, int rmax, const double *r,

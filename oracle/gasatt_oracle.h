@@ -68,6 +68,11 @@ void orc_electron_transport(double *x, double *y, double *z, double *vx, double 
                             const double *draws, unsigned flags);
 
 /* ---- MATLAB drop-ins ---- */
+/* REBOND.m:1-70.  pos, vel: n x 3 column-major (leading dimensions ldp, ldv),
+ * updated in place; returns N_boundary, or -1 when a particle needs more than
+ * max_wraps wedge wraps. */
+int64_t orc_rebond(double *pos, int64_t ldp, const double *r, const double *phi, double *vel,
+                   int64_t ldv, int64_t n, double Lp, double PHIp, int max_wraps);
 void orc_free_motion(const double *vx, const double *vy, const double *vz,
                      const double *x, const double *y, const double *z, int64_t n, double dt,
                      double *xn, double *yn, double *zn, double *rn, double *phin);

@@ -148,6 +148,18 @@ def free_motion(vx, vy, vz, x, y, z, dt):
     return out
 
 
+def rebond(pos, r, phi, vel, Lp, PHIp, max_wraps=4096):
+    """REBOND.m on (n, 3) arrays: (pos, vel, N_boundary), or N_boundary -1."""
+    pos = np.asfortranarray(np.array(pos, dtype=np.float64))
+    vel = np.asfortranarray(np.array(vel, dtype=np.float64))
+    n = pos.shape[0]
+    lib.orc_rebond.restype = c_i64
+    nb = lib.orc_rebond(P(pos), c_i64(n), P(np.ascontiguousarray(r, dtype=np.float64)),
+                        P(np.ascontiguousarray(phi, dtype=np.float64)), P(vel), c_i64(n),
+                        c_i64(n), c_d(Lp), c_d(PHIp), c_i(max_wraps))
+    return pos, vel, nb
+
+
 def particle_density(dr, dz, dphi, r, phi, z, cellnumxy, sum_cell, VC, FN, ncell):
     out = np.zeros(ncell)
     lib.orc_particle_density(c_d(dr), c_d(dz), P(f64(dphi)), c_i(dphi.size), P(f64(r)),

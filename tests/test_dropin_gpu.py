@@ -143,3 +143,25 @@ def test_electron_collision_philox_reproducible(tables):
     for a, b in zip(outs[0], outs[1]):
         assert torch.allclose(a, b, rtol=0, atol=0, equal_nan=True)
     assert outs[0][0].shape[0] > 2000
+
+
+def test_rebond():
+    """REBOND.m: azimuths up to three wedges out on either side, z beyond both
+    ends; against the oracle, and the wrap limit."""
+    rng = np.random.default_rng(13)
+    n, PHIp, Lp = 20000, 0.1, 1e-2
+    r = rng.uniform(1e-4, 5e-3, n)
+    phi = rng.uniform(-3.2 * PHIp, 4.2 * PHIp, n)
+    pos = np.stack([r * np.cos(phi), r * np.sin(phi), rng.uniform(-0.2 * Lp, 1.3 * Lp, n)], 1)
+    vel = rng.normal(size=(n, 3)) * 1e7
+    got = gasatt.REBOND(torch.tensor(pos), torch.tensor(r), torch.tensor(phi), torch.tensor(vel),
+                        Lp, PHIp)
+    want = O.rebond(pos, r, phi, vel, Lp, PHIp)
+    assert got[2] == want[2] > n // 2
+    close(np_(got[0]), want[0], 1e-14, "pos")
+    close(np_(got[1]), want[1], 1e-14, "vel")
+    assert np_(got[1])[:, 2].tolist() != vel[:, 2].tolist()       # some z reflections
+    bad = phi.copy(); bad[7] = -1e3                                # 10,000 wedges below
+    with pytest.raises(gasatt.GasattError):
+        gasatt.REBOND(torch.tensor(pos), torch.tensor(r), torch.tensor(bad), torch.tensor(vel),
+                      Lp, PHIp)

@@ -155,6 +155,17 @@ def test_mex_dropins_match_the_c_abi(mex, tables):
     want = gasatt.free_motion(*[torch.tensor(x) for x in a], 1e-12)
     for g, w in zip(got, want):
         np.testing.assert_array_equal(mex.value(g).ravel(), np_(w))
+    # REBOND
+    n, PHIp, Lp = 4000, 0.1, 1e-2
+    r = rng.uniform(1e-4, 5e-3, n); phi = rng.uniform(-2.2 * PHIp, 3.2 * PHIp, n)
+    pos = np.stack([r * np.cos(phi), r * np.sin(phi), rng.uniform(-0.2 * Lp, 1.3 * Lp, n)], 1)
+    vel = rng.normal(size=(n, 3)) * 1e7
+    got = mex.call(3, "REBOND", Gpu(pos), Gpu(r), Gpu(phi), Gpu(vel), Lp, PHIp)
+    want = gasatt.REBOND(torch.tensor(pos), torch.tensor(r), torch.tensor(phi), torch.tensor(vel),
+                         Lp, PHIp)
+    np.testing.assert_array_equal(mex.value(got[0]), np_(want[0]))
+    np.testing.assert_array_equal(mex.value(got[1]), np_(want[1]))
+    assert mex.value(got[2])[0, 0] == want[2]
     # particle_density (the gateway takes the no-allocation variant)
     PHIp, Rp, rmax, delta, zmax, dz = 0.1, 1e-2, 25, 4e-4, 6, 1e-2
     phimax, sum_cell, cellnumxy = cell_structure(PHIp, Rp, rmax, delta)

@@ -217,3 +217,21 @@ def test_oracle_uniform_gas_map_equals_scalar_density(tables):
 def test_oracle_vacuum_gas_map_has_no_collisions(tables):
     o = _oracle_sim(tables, lambda cfg, nr, nz: np.zeros((nr, nz)))
     assert list(o.counters[:4]) == [0, 0, 0, 0]
+
+
+def test_oracle_rebond_small_case():
+    """REBOND.m by hand: one particle a wedge and a half below, one above,
+    one past z = Lp."""
+    PHIp, Lp = 0.5, 1.0
+    pos = np.array([[0.0, 0.0, 0.5], [0.0, 0.0, 0.5], [1.0, 0.0, 1.25]])
+    r = np.array([2.0, 1.0, 1.0])
+    phi = np.array([-0.75, 0.8, 0.0])
+    vel = np.array([[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 3.0]])
+    p, v, nb = O.rebond(pos, r, phi, vel, Lp, PHIp)
+    assert nb == 2 + 1 + 1
+    np.testing.assert_allclose(p[0, :2], [2 * np.cos(0.25), 2 * np.sin(0.25)], rtol=1e-15)
+    np.testing.assert_allclose(v[0, :2], [np.cos(1.0), np.sin(1.0)], rtol=1e-15)   # turned by 2 PHIp
+    np.testing.assert_allclose(p[1, :2], [np.cos(0.3), np.sin(0.3)], rtol=1e-14)
+    np.testing.assert_allclose(v[1, :2], [np.sin(0.5), np.cos(0.5)], rtol=1e-15)   # turned by -PHIp
+    np.testing.assert_allclose([p[2, 2], v[2, 2]], [0.75, -3.0], rtol=1e-15)
+    assert O.rebond(pos, r, np.array([-10.0, 0.0, 0.0]), vel, Lp, PHIp, max_wraps=8)[2] == -1
