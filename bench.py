@@ -652,6 +652,62 @@ def run_c5(args):
     print(json.dumps(line), flush=True)
 
 
+C4 = dict(n_r=1024, n_z=4096, delta=5e-6, dt=1e-14, torr=10.0, photo=8_000_000, e_keV=12.0,
+          seed=3, capacity=64 << 20)
+
+
+def run_c4(args):
+    """The single large cascade: 16,000,000 electrons from 8,000,000
+    photoionizations at 12 keV (drawn on the GPU), N2 at 10 Torr, 1024 x 4096
+    cells at 5 um, capacity 64M, FP32 split form, sort period 30; the steps
+    are timed in chunks with CUDA events (whole steps, sorts included)."""
+    import torch
+    from gasatt import _lib
+    from gasatt.sim import Sim, config
+    torch.cuda.set_device(0)
+    w = C4
+    steps, chunk = args.c4_steps, 500
+    cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=_lib.FP32_SPLIT,
+                 capacity=w["capacity"], seed=w["seed"], sort_period=30)
+    sim = Sim(cfg)
+    sim.bind_stream()
+    sim.birth_photo(w["photo"], w["e_keV"], seed=w["seed"])
+    stream = torch.cuda.current_stream()
+    d0 = sim.diag()
+    work, ms_total, trace, done = 0.0, 0.0, [], 0
+    while done < steps:
+        k = min(chunk, steps - done)
+        a0 = sim.diag()["n_alive"]
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sim.step(k)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        d = sim.diag()
+        work += 0.5 * (a0 + d["n_alive"]) * k
+        ms_total += ms
+        done += k
+        trace.append(dict(step=done, electrons=d["n_alive"], ms_per_step=ms / k))
+    d = sim.diag()
+    line = {"mode": "c4", "metric": METRIC, "unit": UNIT, "steps": steps,
+            "value": work / (ms_total / 1e3), "ms_per_step": ms_total / steps,
+            "electrons": {"initial": d0["n_alive"], "final": d["n_alive"]},
+            "ionizations": d["n_ionizations"], "lost_wall": d["n_lost_wall"],
+            "capacity_overflow": bool(d["status_flags"] & 2),
+            "energy_ev": {"start": d0["kinetic_ev"],
+                          "end_sum": d["kinetic_ev"] + d["collision_loss_ev"] + d["wall_loss_ev"]
+                          + 6.241509074e18 * d["field_energy_j"]},
+            "trace": trace[::max(1, len(trace) // 10)],
+            "config": {"workload": "16,000,000 e- from 8,000,000 photoionizations at 12 keV (GPU "
+                       "births), N2 10 Torr 300 K, 1024x4096 cells at 5 um, dt 1e-14 s, seed 3",
+                       "precision": "fp32_split", "capacity": w["capacity"], "sort_period": 30,
+                       "l2": "not flushed", "timed": "whole steps, 500-step chunks"}}
+    print(json.dumps(line), flush=True)
+    sim.close()
+
+
 def c5_profile_sim(precision, torch):
     """The C5 cell with its ions already grown: the 4,000,000 birth electrons
     plus 4,000,000 ions at their positions (Maxwellian 300 K), so that the
@@ -701,9 +757,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "c3", "c5"],
+    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "c3", "c4", "c5"],
                     help="profile: only the step loop of one precision (for ncu); "
-                         "c3: 48 batched gas cells; c5: electrons plus ions, long run")
+                         "c3: 48 batched gas cells; c4: the 16M-electron cascade; "
+                         "c5: electrons plus ions, long run")
+    ap.add_argument("--c4-steps", type=int, default=5000)
     ap.add_argument("--c5-steps", type=int, default=20_000)
     ap.add_argument("--workload", default="c2", choices=["c2", "c5"],
                     help="workload of --mode profile")
@@ -715,6 +773,8 @@ def main():
         run_profile(args)
     elif args.mode == "c3":
         run_c3(args)
+    elif args.mode == "c4":
+        run_c4(args)
     elif args.mode == "c5":
         run_c5(args)
     elif args.impl == "reference":

@@ -1104,7 +1104,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
     if (k1 != kDead) { lo = min(lo, (int)(k1 >> 16)); hi = max(hi, (int)(k1 >> 16)); }
     row0 = 0; rows = maxrows;
     if (hi >= 0) {
-      row0 = min(max(0, lo - 3), P.nz - maxrows);
+      // the chunk's own deposit rows lo-1 .. hi+1 first, then up to three
+      // rows either side for the drift since the last sort (a wide grid
+      // leaves room for few rows)
+      const int core = hi - lo + 3;
+      const int below = maxrows >= core + 6 ? 3 : max(1, 1 + (maxrows - core) / 2);
+      row0 = min(max(0, lo - below), P.nz - maxrows);
       rows = min(maxrows, hi + 4 - row0);
     }
   };
