@@ -652,6 +652,87 @@ def run_c5(args):
     print(json.dumps(line), flush=True)
 
 
+C1 = dict(n_r=64, n_z=256, delta=10e-6, dt=2e-14, torr=1.0, photo=10_000, e_keV=8.0, seed=0)
+
+
+def run_c1(args):
+    """The reference's CPU-runnable case at full size: 20,000 electrons, 64 x
+    256 cells at 10 um, 1 Torr, dt 2e-14 s, 500 steps.  The FP64 form against
+    the CPU oracle of the same step (same random streams): agreement and
+    both rates; the FP32 form's rate beside them."""
+    import torch
+    from gasatt import _lib
+    from gasatt.sim import Sim, births, config
+    from gasatt.tables import N2Tables
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    torch.cuda.set_device(0)
+    w = C1
+    steps = args.c1_steps
+    parts = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=w["seed"],
+                   Rp=w["n_r"] * w["delta"])
+    out = {}
+    for prec, code in (("fp64", _lib.FP64), ("fp32_split", _lib.FP32_SPLIT)):
+        cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=code,
+                     capacity=200_000, seed=w["seed"], sort_period=30)
+        sim = Sim(cfg)
+        sim.bind_stream()
+        sim.load(*parts)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sim.step(steps)
+        e1.record(); e1.synchronize()
+        d = sim.diag()
+        out[prec] = dict(ms=e0.elapsed_time(e1), diag=d, fields=sim.fields(), read=sim.read(),
+                         cfg=cfg)
+        sim.close()
+    cfg = out["fp64"]["cfg"]
+    O.lib.orc_set_threads(os.cpu_count() or 1)
+    orc = O.Sim(cfg, N2Tables(), cap=cfg.capacity)
+    orc.load(*parts)
+    t0 = time.perf_counter()
+    orc.prologue()
+    for _ in range(steps):
+        orc.step()
+    cpu_s = time.perf_counter() - t0
+    g = out["fp64"]
+    ion, ela, exc, nul, lost, ovf = (int(x) for x in orc.counters)
+    ferr = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+               for a, b in zip(g["fields"], (orc.Er, orc.Ez, orc.H)))
+    r, z, ur, ut, uz, ids, alive = orc.state_rz()
+    a = alive.astype(bool)
+    gr = g["read"]
+    ga = gr["r"] >= 0
+    same_ids = set(gr["id"][ga].tolist()) == set(ids[a].tolist())
+    uerr = None
+    if same_ids:
+        o1, o2 = np.argsort(ids[a]), np.argsort(gr["id"][ga])
+        umag = np.sqrt(ur[a] ** 2 + ut[a] ** 2 + uz[a] ** 2)[o1]
+        du = np.sqrt((gr["ur"][ga][o2] - ur[a][o1]) ** 2 + (gr["ut"][ga][o2] - ut[a][o1]) ** 2
+                     + (gr["uz"][ga][o2] - uz[a][o1]) ** 2)
+        uerr = float((du / umag).max())
+    n_mean = len(parts[0])
+    line = {"mode": "c1", "metric": METRIC, "unit": UNIT, "steps": steps,
+            "gpu_fp64": {"value": n_mean * steps / (g["ms"] / 1e3), "ms": g["ms"]},
+            "gpu_fp32_split": {"value": n_mean * steps / (out["fp32_split"]["ms"] / 1e3),
+                               "ms": out["fp32_split"]["ms"]},
+            "cpu_oracle": {"value": n_mean * steps / cpu_s, "s": cpu_s,
+                           "cores": os.cpu_count() or 1, "kind": "port"},
+            "fp64_vs_oracle": {"counts_gpu": [g["diag"][k] for k in ("n_ionizations", "n_elastic",
+                                                                   "n_excitation", "n_null",
+                                                                   "n_lost_wall")],
+                               "counts_oracle": [ion, ela, exc, nul, lost],
+                               "same_population": same_ids,
+                               "max_rel_u_err": uerr, "field_rel_err_l2": ferr},
+            "fp32_vs_fp64_ionizations": [out["fp32_split"]["diag"]["n_ionizations"],
+                                         g["diag"]["n_ionizations"]],
+            "config": {"workload": "20,000 e- from 10,000 photoionizations at 8 keV, N2 1 Torr "
+                       "300 K, 64x256 cells at 10 um, dt 2e-14 s, seed 0",
+                       "rates": "initial electrons x steps / time (one call of all steps)"}}
+    print(json.dumps(line), flush=True)
+
+
 C4 = dict(n_r=1024, n_z=4096, delta=5e-6, dt=1e-14, torr=10.0, photo=8_000_000, e_keV=12.0,
           seed=3, capacity=64 << 20)
 
@@ -757,11 +838,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "c3", "c4", "c5"],
+    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "c1", "c3", "c4", "c5"],
                     help="profile: only the step loop of one precision (for ncu); "
                          "c3: 48 batched gas cells; c4: the 16M-electron cascade; "
                          "c5: electrons plus ions, long run")
     ap.add_argument("--c4-steps", type=int, default=5000)
+    ap.add_argument("--c1-steps", type=int, default=500)
     ap.add_argument("--c5-steps", type=int, default=20_000)
     ap.add_argument("--workload", default="c2", choices=["c2", "c5"],
                     help="workload of --mode profile")
@@ -773,6 +855,8 @@ def main():
         run_profile(args)
     elif args.mode == "c3":
         run_c3(args)
+    elif args.mode == "c1":
+        run_c1(args)
     elif args.mode == "c4":
         run_c4(args)
     elif args.mode == "c5":

@@ -225,3 +225,38 @@ def test_free_drift_keeps_kinetic_energy(precision, tol):
     d = sim.diag()
     assert d["n_lost_wall"] == 0 and d["n_alive"] == n
     assert abs(d["kinetic_ev"] / e0 - 1) < tol, d["kinetic_ev"] / e0 - 1
+
+
+def test_c1_full_size_fp64_matches_oracle(tables):
+    """The reference's CPU-runnable case at full size (20,000 electrons, 64 x
+    256 cells at 10 um, 1 Torr, dt 2e-14 s) for 500 steps: the FP64 form and
+    the oracle keep the same population and event counts, and agree to 1e-10."""
+    nr, nz, d = 64, 256, 10e-6
+    cfg = config(nr, nz, d, 2e-14, 1.0, precision=_lib.FP64, capacity=200_000, seed=0,
+                 sort_period=30)
+    parts = births(10_000, 8.0, nz * d, seed=0, Rp=nr * d)
+    sim = Sim(cfg)
+    sim.load(*parts)
+    sim.step(500)
+    got = sim.read()
+    orc = O.Sim(cfg, tables, cap=cfg.capacity)
+    orc.load(*parts)
+    orc.prologue()
+    for _ in range(500):
+        orc.step()
+    dg = sim.diag()
+    ion, ela, exc, nul, lost, ovf = orc.counters
+    assert (dg["n_ionizations"], dg["n_elastic"], dg["n_excitation"], dg["n_null"],
+            dg["n_lost_wall"]) == (ion, ela, exc, nul, lost)
+    assert ion > 500
+    r, z, ur, ut, uz, ids, alive = orc.state_rz()
+    a = alive.astype(bool)
+    ga = got["r"] >= 0
+    assert set(got["id"][ga].tolist()) == set(ids[a].tolist())
+    want = by_id(ids[a], r[a], z[a], ur[a], ut[a], uz[a])
+    have = by_id(got["id"][ga], got["r"][ga], got["z"][ga], got["ur"][ga], got["ut"][ga],
+                 got["uz"][ga])
+    for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
+        close(h, w, 1e-10, k)
+    for g, w, k in zip(sim.fields(), (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
+        close(g, w, 1e-10, k)
