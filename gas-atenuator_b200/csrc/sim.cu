@@ -2141,6 +2141,12 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   return GASATT_OK;
 }
 
+int gasatt_sim_get_config(const gasatt_sim *s, gasatt_sim_config *cfg) {
+  if (!s || !cfg) return GASATT_E_ARG;
+  *cfg = s->cfg;
+  return GASATT_OK;
+}
+
 int gasatt_sim_destroy(gasatt_sim *s) {
   if (!s) return GASATT_OK;
   cudaSetDevice(s->ctx->device);

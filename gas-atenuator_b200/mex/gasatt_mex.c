@@ -23,6 +23,11 @@
  *       sig_elastic, sig_ionization, sig_excitation, dt_transport)            electron_collision.m:1
  *   h = gasatt_mex('sim_create', cfg)        cfg: struct with gasatt_sim_config field names
  *   gasatt_mex('sim_load', h, r, z, ur, ut, uz, id)
+ *   gasatt_mex('sim_birth_photo', h, n_photo, photon_keV, seed, sigma_r)
+ *   gasatt_mex('sim_set_fields', h, Er, Ez, Hphi)     [Er, Ez, Hphi] = gasatt_mex('sim_get_fields', h)
+ *   gasatt_mex('sim_set_gas_density', h, density)     density n_r x n_z, or [] for the uniform one
+ *   gasatt_mex('sim_load_ions', h, r, z, ur, ut, uz, id, charge)
+ *   [r, z, ur, ut, uz, id, charge] = gasatt_mex('sim_read_ions', h)
  *   gasatt_mex('sim_step', h, nsteps)
  *   [r, z, ur, ut, uz, id] = gasatt_mex('sim_read', h)
  *   d = gasatt_mex('sim_diag', h)             struct with gasatt_diag field names
@@ -417,6 +422,107 @@ static void cmd_sim_load(int nrhs, const mxArray *prhs[]) {
                         (const uint64_t *)mxGetData(prhs[7]), (int64_t)n, 0));
 }
 
+static void cmd_sim_fields(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[], int set) {
+  gasatt_sim *s;
+  gasatt_sim_config cfg;
+  size_t nr, nz;
+  int k;
+  if (set) nargs(nrhs, 5, "sim_set_fields(h, Er, Ez, Hphi)");
+  else nargs(nrhs, 2, "sim_get_fields(h)");
+  s = sim_of(prhs[1]);
+  check(gasatt_sim_get_config(s, &cfg));
+  nr = (size_t)cfg.n_r; nz = (size_t)cfg.n_z;
+  if (set) {
+    const double *f[3];
+    if (mxGetM(prhs[2]) != nr || mxGetN(prhs[2]) != nz + 1 || mxGetM(prhs[3]) != nr + 1 ||
+        mxGetN(prhs[3]) != nz || mxGetM(prhs[4]) != nr || mxGetN(prhs[4]) != nz)
+      fail("sim_set_fields: Er n_r x (n_z+1), Ez (n_r+1) x n_z, Hphi n_r x n_z");
+    for (k = 0; k < 3; ++k) f[k] = host(prhs[2 + k], "fields must be double host matrices");
+    check(gasatt_sim_set_fields(s, f[0], f[1], f[2], 0));
+  } else {
+    mxArray *o[3];
+    o[0] = mxCreateDoubleMatrix(nr, nz + 1, mxREAL);
+    o[1] = mxCreateDoubleMatrix(nr + 1, nz, mxREAL);
+    o[2] = mxCreateDoubleMatrix(nr, nz, mxREAL);
+    check(gasatt_sim_get_fields(s, mxGetDoubles(o[0]), mxGetDoubles(o[1]), mxGetDoubles(o[2]), 0));
+    for (k = 0; k < 3; ++k) {
+      if (k < (nlhs > 0 ? nlhs : 1)) plhs[k] = o[k];
+      else mxDestroyArray(o[k]);
+    }
+  }
+}
+
+static void cmd_sim_gas(int nrhs, const mxArray *prhs[]) {
+  gasatt_sim *s;
+  gasatt_sim_config cfg;
+  nargs(nrhs, 3, "sim_set_gas_density(h, density)");
+  s = sim_of(prhs[1]);
+  check(gasatt_sim_get_config(s, &cfg));
+  if (mxGetNumberOfElements(prhs[2]) == 0) {               /* [] : back to uniform */
+    check(gasatt_sim_set_gas_density(s, NULL, 0));
+    return;
+  }
+  if (mxGetM(prhs[2]) != (size_t)cfg.n_r || mxGetN(prhs[2]) != (size_t)cfg.n_z)
+    fail("sim_set_gas_density: density must be n_r x n_z");
+  check(gasatt_sim_set_gas_density(s, host(prhs[2], "density must be a double host matrix"), 0));
+}
+
+static void cmd_sim_load_ions(int nrhs, const mxArray *prhs[]) {
+  const double *a[5];
+  const int8_t *q = NULL;
+  int8_t *qbuf = NULL;
+  size_t n, k;
+  nargs(nrhs, 9, "sim_load_ions(h, r, z, ur, ut, uz, id, charge)");
+  n = mxGetNumberOfElements(prhs[2]);
+  for (k = 0; k < 5; ++k) {
+    a[k] = host(prhs[2 + k], "r..uz must be double host arrays");
+    if (mxGetNumberOfElements(prhs[2 + k]) != n) fail("sim_load_ions: arrays of different lengths");
+  }
+  if (!mxIsUint64(prhs[7]) || mxGetNumberOfElements(prhs[7]) != n) fail("sim_load_ions: id must be uint64");
+  if (mxGetNumberOfElements(prhs[8]) > 0) {                /* charge numbers as doubles; [] = all 1 */
+    const double *c = host(prhs[8], "charge must be a double host array");
+    if (mxGetNumberOfElements(prhs[8]) != n) fail("sim_load_ions: charge of another length");
+    qbuf = (int8_t *)mxMalloc(n ? n : 1);
+    for (k = 0; k < n; ++k) qbuf[k] = (int8_t)c[k];
+    q = qbuf;
+  }
+  {
+    const int rc = gasatt_sim_load_ions(sim_of(prhs[1]), a[0], a[1], a[2], a[3], a[4],
+                                        (const uint64_t *)mxGetData(prhs[7]), q, (int64_t)n, 0);
+    mxFree(qbuf);
+    check(rc);
+  }
+}
+
+static void cmd_sim_read_ions(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
+  gasatt_sim *s;
+  int64_t n = 0, k;
+  double *p[5];
+  int8_t *q;
+  mxArray *o[7];
+  nargs(nrhs, 2, "sim_read_ions(h)");
+  s = sim_of(prhs[1]);
+  gasatt_sim_read_ions(s, NULL, NULL, NULL, NULL, NULL, NULL, NULL, 0, &n, 0);   /* count only */
+  for (k = 0; k < 5; ++k) {
+    o[k] = mxCreateDoubleMatrix((mwSize)n, 1, mxREAL);
+    p[k] = mxGetDoubles(o[k]);
+  }
+  o[5] = mxCreateNumericMatrix((mwSize)n, 1, mxUINT64_CLASS, mxREAL);
+  o[6] = mxCreateDoubleMatrix((mwSize)n, 1, mxREAL);
+  q = (int8_t *)mxMalloc(n ? (size_t)n : 1);
+  {
+    const int rc = gasatt_sim_read_ions(s, p[0], p[1], p[2], p[3], p[4],
+                                        (uint64_t *)mxGetData(o[5]), q, n, &n, 0);
+    for (k = 0; k < n; ++k) mxGetDoubles(o[6])[k] = (double)q[k];
+    mxFree(q);
+    check(rc);
+  }
+  for (k = 0; k < 7; ++k) {
+    if (k < (nlhs > 0 ? nlhs : 1)) plhs[k] = o[k];
+    else mxDestroyArray(o[k]);
+  }
+}
+
 static void cmd_sim_read(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
   gasatt_sim *s;
   int64_t n = 0;
@@ -462,7 +568,8 @@ static void cmd_sim_diag(mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
 static const char *const k_commands[] = {
     "init", "tables", "find_CS0", "free_motion", "REBOND", "particle_density", "electricmagneticfield6",
     "electron_collision", "sim_create", "sim_load", "sim_step", "sim_read", "sim_diag",
-    "sim_destroy"};
+    "sim_destroy", "sim_birth_photo", "sim_set_fields", "sim_get_fields", "sim_set_gas_density",
+    "sim_load_ions", "sim_read_ions"};
 
 void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
   char cmd[64];
@@ -498,6 +605,16 @@ void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
     check(gasatt_sim_step(sim_of(prhs[1]), (int)scalar(prhs[2], "nsteps")));
   } else if (!strcmp(cmd, "sim_read")) cmd_sim_read(nlhs, plhs, nrhs, prhs);
   else if (!strcmp(cmd, "sim_diag")) cmd_sim_diag(plhs, nrhs, prhs);
+  else if (!strcmp(cmd, "sim_birth_photo")) {
+    nargs(nrhs, 6, "sim_birth_photo(h, n_photo, photon_keV, seed, sigma_r)");
+    check(gasatt_sim_birth_photo(sim_of(prhs[1]), (int64_t)scalar(prhs[2], "n_photo"),
+                                 scalar(prhs[3], "photon_keV"), scalar(prhs[5], "sigma_r"),
+                                 (uint64_t)scalar(prhs[4], "seed"), 0));
+  } else if (!strcmp(cmd, "sim_set_fields")) cmd_sim_fields(nlhs, plhs, nrhs, prhs, 1);
+  else if (!strcmp(cmd, "sim_get_fields")) cmd_sim_fields(nlhs, plhs, nrhs, prhs, 0);
+  else if (!strcmp(cmd, "sim_set_gas_density")) cmd_sim_gas(nrhs, prhs);
+  else if (!strcmp(cmd, "sim_load_ions")) cmd_sim_load_ions(nrhs, prhs);
+  else if (!strcmp(cmd, "sim_read_ions")) cmd_sim_read_ions(nlhs, plhs, nrhs, prhs);
   else {
     nargs(nrhs, 2, "sim_destroy(h)");
     check(gasatt_sim_destroy(sim_of(prhs[1])));

@@ -297,6 +297,9 @@ int gasatt_sim_default_config(gasatt_sim_config *cfg);
 int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg,
                       const gasatt_tables *tab, gasatt_sim **sim);
 int gasatt_sim_destroy(gasatt_sim *sim);
+/* the configuration the simulation was created with (sizes for a caller that
+ * allocates the arrays of gasatt_sim_get_fields and the like) */
+int gasatt_sim_get_config(const gasatt_sim *sim, gasatt_sim_config *cfg);
 /* particle state in SI, axisymmetric frame: r, z [m]; u = gamma*v [m/s] in
  * (r, theta, z); id: 64-bit identity keying the random stream.
  * on_device: 1 = pointers are device memory, 0 = host memory. */

@@ -246,3 +246,49 @@ def test_mex_resident_simulation_matches_the_python_api(mex, tables):
         np.testing.assert_array_equal(g[o_g], want[k][o_w], err_msg=k)
     for k in ("n_alive", "n_ionizations", "n_elastic", "kinetic_ev", "field_energy_j"):
         assert mex.field(dg, k) == d[k], k
+
+
+@pytest.mark.gpu
+def test_mex_resident_fields_gas_ions_and_births(mex, tables):
+    """The sim_* commands for GPU births, fields, a gas map and ions give what
+    the Python API gives on the same sequence of calls."""
+    from _cases import grid_fields
+    from gasatt import _lib
+    from gasatt.sim import Sim, config
+    nr, nz, d = 32, 64, 5e-6
+    cfg = config(nr, nz, d, 1e-14, 300.0, precision=_lib.FP64, capacity=40000, seed=9,
+                 sort_period=5, ion_capacity=40000, ion_subcycle=5)
+    Er, Ez, H = grid_fields(nr, nz, np.random.default_rng(2), E0=2e6, H0=1e3)
+    Er[:, 0] = 0; Er[:, -1] = 0; Ez[-1, :] = 0
+    rho = cfg.gas_density * np.outer(np.ones(nr), np.linspace(0.5, 1.5, nz))
+    rng = np.random.default_rng(5)
+    ions = (rng.uniform(10e-6, 100e-6, 50), rng.uniform(0, nz * d, 50), rng.normal(0, 300, 50),
+            rng.normal(0, 300, 50), rng.normal(0, 300, 50), np.arange(50, dtype=np.uint64) + 7,
+            rng.integers(1, 3, 50).astype(np.int8))
+    register_tables(mex, tables)
+    (h,) = mex.call(1, "sim_create", {k: float(getattr(cfg, k)) for k, _ in type(cfg)._fields_})
+    mex.call(0, "sim_birth_photo", h, 1500.0, 8.0, 4.0, 30e-6)
+    mex.call(0, "sim_set_fields", h, Er, Ez, H)
+    mex.call(0, "sim_set_gas_density", h, rho)
+    mex.call(0, "sim_load_ions", h, *ions[:5], ions[5], ions[6].astype(np.float64))
+    mex.call(0, "sim_step", h, 12.0)
+    f_mex = [mex.value(p) for p in mex.call(3, "sim_get_fields", h)]
+    i_mex = [mex.value(p).ravel() for p in mex.call(7, "sim_read_ions", h)]
+    (dg,) = mex.call(1, "sim_diag", h)
+    mex.call(0, "sim_destroy", h)
+    sim = Sim(cfg)
+    sim.birth_photo(1500, 8.0, seed=4, sigma_r=30e-6)
+    sim.set_fields(Er, Ez, H)
+    sim.set_gas_density(rho)
+    sim.load_ions(*ions[:6], charge=ions[6])
+    sim.step(12)
+    for g, w in zip(f_mex, sim.fields()):
+        np.testing.assert_array_equal(g, w)
+    iw = sim.read_ions()
+    og, ow = np.argsort(i_mex[5]), np.argsort(iw["id"])
+    for g, k in zip(i_mex, ("r", "z", "ur", "ut", "uz", "id", "charge")):
+        np.testing.assert_array_equal(g[og], np.asarray(iw[k][ow], dtype=g.dtype), err_msg=k)
+    d = sim.diag()
+    for k in ("n_alive", "n_ionizations", "n_ions", "kinetic_ev", "wall_loss_ev"):
+        assert mex.field(dg, k) == d[k], k
+    assert d["n_ionizations"] > 0 and d["n_ions"] > 50
