@@ -260,3 +260,29 @@ def test_c1_full_size_fp64_matches_oracle(tables):
         close(h, w, 1e-10, k)
     for g, w, k in zip(sim.fields(), (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
         close(g, w, 1e-10, k)
+
+
+def test_fp32_energy_distribution_within_3_sigma_of_fp64():
+    """Free-running 60 steps at 100 Torr: the electron energy distribution of
+    the FP32 split form (40 log-spaced bins from 0.1 eV to 10 keV), its mean
+    energy and the ionization yield agree with the FP64 form's within 3 sigma
+    of the Monte Carlo error of a bin (sqrt of its count)."""
+    me, c, qe = 9.1093837015e-31, 299792458.0, 1.602176634e-19
+    res = {}
+    for prec in (_lib.FP64, _lib.FP32_SPLIT):
+        cfg, sim, _, _ = start(prec, n_photo=4000, sort_period=5, torr=100.0)
+        sim.step(60)
+        d = sim.read()
+        a = d["r"] >= 0
+        u2 = (d["ur"][a] ** 2 + d["ut"][a] ** 2 + d["uz"][a] ** 2) / c ** 2
+        E = me * c * c * (u2 / (np.sqrt(1 + u2) + 1)) / qe
+        res[prec] = (E, sim.diag()["n_ionizations"])
+        sim.close()
+    (E64, i64), (E32, i32) = res[_lib.FP64], res[_lib.FP32_SPLIT]
+    bins = np.logspace(-1, 4, 41)
+    h64, _ = np.histogram(E64, bins)
+    h32, _ = np.histogram(E32, bins)
+    assert h64.sum() > 5000
+    assert np.all(np.abs(h32 - h64) <= 3 * np.sqrt(h64 + 1) + 1)
+    assert abs(E32.mean() - E64.mean()) <= 3 * E64.std() / np.sqrt(len(E64))
+    assert abs(i32 - i64) <= 3 * np.sqrt(i64) + 1
