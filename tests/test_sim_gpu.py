@@ -286,3 +286,33 @@ def test_fp32_energy_distribution_within_3_sigma_of_fp64():
     assert np.all(np.abs(h32 - h64) <= 3 * np.sqrt(h64 + 1) + 1)
     assert abs(E32.mean() - E64.mean()) <= 3 * E64.std() / np.sqrt(len(E64))
     assert abs(i32 - i64) <= 3 * np.sqrt(i64) + 1
+
+
+@pytest.mark.parametrize("ratio", [2, 3])
+def test_field_subcycle_ratio_matches_oracle(tables, ratio):
+    """fdtd_ratio > 1 (ratio field sub-cycles of dt/ratio per particle step,
+    the general fused field kernel): the FP64 form against the oracle, and the
+    FP32 form (whose gather quads that kernel then writes value by value)
+    against the FP64 form."""
+    out = {}
+    for prec in (_lib.FP64, _lib.FP32_SPLIT):
+        cfg = config(NR, NZ, D, 1e-14, 300.0, precision=prec, capacity=40000, seed=7,
+                     sort_period=0, fdtd_ratio=ratio)
+        parts = births(2000, 8.0, NZ * D, seed=3, sigma_r=30e-6, Rp=NR * D)
+        Er, Ez, H = grid_fields(NR, NZ, np.random.default_rng(8), E0=3e6, H0=2e3)
+        Er[:, 0] = 0; Er[:, -1] = 0; Ez[-1, :] = 0
+        sim = Sim(cfg)
+        sim.load(*parts)
+        sim.set_fields(Er, Ez, H)
+        sim.step(4)
+        out[prec] = (sim.fields(), sim.diag(), cfg, parts, (Er, Ez, H))
+        sim.close()
+    f64, d64, cfg, parts, flds = out[_lib.FP64]
+    orc = oracle_run(cfg, tables, parts, flds, 4)
+    for g, w, k in zip(f64, (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
+        close(g, w, 1e-10, k)
+    assert d64["n_ionizations"] == orc.counters[0]
+    f32, d32 = out[_lib.FP32_SPLIT][:2]
+    for g, w, k in zip(f32, f64, ("Er", "Ez", "H")):
+        assert np.linalg.norm(g - w) <= 1e-4 * np.linalg.norm(w), k
+    assert abs(d32["n_ionizations"] - d64["n_ionizations"]) <= 2
