@@ -60,3 +60,46 @@ def test_batch_equals_instances_alone():
     for s in sims:
         s.close()
     ctx.close()
+
+
+def test_batch_with_ions_and_gas_maps_equals_instances_alone():
+    """Cells with the ion species (pushes every 4 steps) and per-cell gas maps
+    give in a batch what they give alone: fields, counts and the ions."""
+    ctx = Context(0)
+
+    def make_ionic(cell):
+        nr, nz, d, torr, photo, kev, prec, seed = cell
+        cfg = config(nr, nz, d, 1e-14, torr, precision=prec, capacity=8 * photo, seed=seed,
+                     sort_period=SORT_PERIOD, ion_capacity=8 * photo, ion_subcycle=4)
+        sim = Sim(cfg, ctx=ctx)
+        sim.load(*births(photo, kev, nz * d, seed=seed, sigma_r=nr * d / 4, Rp=nr * d))
+        sim.set_gas_density(cfg.gas_density * np.outer(np.linspace(1.5, 0.5, nr), np.ones(nz)))
+        return sim
+
+    def ions(sim):
+        st = sim.read_ions()
+        o = np.argsort(st["id"], kind="stable")
+        return {k: v[o] for k, v in st.items()}
+
+    cells = CELLS[:3]
+    alone = []
+    for cell in cells:
+        sim = make_ionic(cell)
+        sim.step(11)
+        alone.append((snapshot(sim), ions(sim)))
+        sim.close()
+    sims = [make_ionic(cell) for cell in cells]
+    batch = Batch(sims, sort_period=SORT_PERIOD)
+    batch.step(11)
+    for sim, (ref, ref_ions) in zip(sims, alone):
+        got = snapshot(sim)
+        for a, b in zip(got[1] + got[2], ref[1] + ref[2]):
+            np.testing.assert_array_equal(a, b)
+        assert got[3] == ref[3]
+        gi = ions(sim)
+        for k in ref_ions:
+            np.testing.assert_array_equal(gi[k], ref_ions[k], err_msg=k)
+    assert sum(len(r[1]["id"]) for r in alone) > 20
+    batch.close()
+    for s in sims:
+        s.close()
