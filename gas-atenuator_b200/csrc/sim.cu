@@ -87,6 +87,7 @@ struct SimParams {
   int nr, nz;
   double dr, dz, dt, c, qe, me, mu0, FN, PHIp, n_gas, nu_max, P_null, Rp, Lp, kb, m_ion, T_gas;
   const double *gas;        // per-cell N2 density [m^-3] (n_r x n_z), or null: n_gas everywhere
+  const double *ion_sig;    // per-cell sqrt(kT/m_ion) of newborn ions (n_r x n_z), or null: ion_sigma
   uint64_t seed;
   int secondaries;
   long long cap;
@@ -231,6 +232,16 @@ __device__ __forceinline__ double gas_density(const SimParams &P, int ir, int iz
   ir = min(max(ir, 0), P.nr - 1);
   iz = min(max(iz, 0), P.nz - 1);
   return P.gas[ir + (int64_t)iz * P.nr];
+}
+
+// velocity spread sqrt(kT/m_ion) of an ion born in cell (ir, iz): the gas
+// temperature of that cell (electron_transport.cu:202-204 reads
+// temperature[index]) or the uniform one
+__device__ __forceinline__ double ion_spread(const SimParams &P, int ir, int iz) {
+  if (!P.ion_sig) return P.ion_sigma;
+  ir = min(max(ir, 0), P.nr - 1);
+  iz = min(max(iz, 0), P.nz - 1);
+  return P.ion_sig[ir + (int64_t)iz * P.nr];
 }
 
 template <bool FAST>
@@ -558,7 +569,9 @@ __global__ void __launch_bounds__(kMccBlock) k_mcc64(SimParams P, State64 S, Sim
     const double ng = gas_density(P, (int)floor(rz.x / P.dr), (int)floor(rz.y / P.dz));
     const int ev = mcc_event<false>(P, id, step, ur, ut, uz, b, ng);
     count_event(cnt, ev, b);
-    if (ev == 2 && P.ion_cap > 0) ion_birth(P.ion, P.ion_cap, P.ion_sigma, P.seed, cnt, id, step, rz.x, rz.y);
+    if (ev == 2 && P.ion_cap > 0)
+      ion_birth(P.ion, P.ion_cap, ion_spread(P, (int)floor(rz.x / P.dr), (int)floor(rz.y / P.dz)),
+                P.seed, cnt, id, step, rz.x, rz.y);
     if (b.born) {
       const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
       const long long slot = n0 + (long long)kb;
@@ -1018,7 +1031,7 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
   const int ev = mcc_event<true>(P, id, cstep, dux, duy, duz, b, gas_density(P, ir, iz));
   count_event(cnt, ev, b);
   if (ev == 2 && P.ion_cap > 0)
-    ion_birth(P.ion, P.ion_cap, P.ion_sigma, P.seed, cnt, id, cstep, ((double)ir + (double)fr) * P.dr,
+    ion_birth(P.ion, P.ion_cap, ion_spread(P, ir, iz), P.seed, cnt, id, cstep, ((double)ir + (double)fr) * P.dr,
               ((double)iz + (double)fz) * P.dz);
   const int mark = push ? par : (int)(cstep & 1);
   if (b.born) {
@@ -1571,6 +1584,7 @@ struct gasatt_sim {
   int *queue = nullptr;           // collision candidates, two queues of capacity slots
   SimParams *d_P = nullptr;       // device copies of P with the current of buffer 0 / 1
   double *d_gas = nullptr;        // per-cell gas density (gasatt_sim_set_gas_density)
+  double *d_ion_sig = nullptr;    // per-cell newborn-ion spread (gasatt_sim_set_gas_temperature)
   // ions (cfg.ion_capacity > 0): the store lives in P.ion; the ion current,
   // deposited by each ion push and held until the next, in fixed point with
   // the factor ion_scale (2^48 per q_e FN c, in both forms)
@@ -2060,6 +2074,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   P.nr = nr; P.nz = nz; P.dr = c.dr; P.dz = c.dz; P.dt = c.dt; P.c = c.c; P.qe = c.q_e;
   P.me = c.m_e; P.mu0 = c.mu0; P.FN = c.FN; P.PHIp = c.PHIp; P.n_gas = c.gas_density;
   P.gas = nullptr;
+  P.ion_sig = nullptr;
   P.Rp = nr * c.dr; P.Lp = nz * c.dz; P.kb = c.kb; P.m_ion = c.m_ion; P.T_gas = c.gas_temperature;
   P.seed = c.seed; P.secondaries = c.secondaries; P.cap = cap;
   P.ion_cap = c.ion_capacity;
@@ -2229,6 +2244,40 @@ int gasatt_sim_set_gas_density(gasatt_sim *s, const double *density, int on_devi
     s->P.gas = nullptr;
   }
   set_collision_bound(s, n_max);
+  SIM_TRY(upload_params(s));
+  drop_graphs(s);                  // the step graphs hold the launch parameters
+  return build_graphs(s);
+}
+
+int gasatt_sim_set_gas_temperature(gasatt_sim *s, const double *temperature, int on_device) {
+  if (!s) return GASATT_E_ARG;
+  gasatt_ctx *ctx = s->ctx;
+  GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t ncell = (size_t)s->cfg.n_r * s->cfg.n_z;
+  std::vector<double> h;
+  if (temperature) {
+    h.resize(ncell);
+    GASATT_CUDA(ctx, cudaMemcpy(h.data(), temperature, ncell * 8,
+                                on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost));
+    for (double &v : h) {
+      if (!(v >= 0) || !std::isfinite(v))
+        return fail(ctx, GASATT_E_ARG, "gas temperature: negative or not finite");
+      v = std::sqrt(s->cfg.kb * v / s->cfg.m_ion);    // the spread the births use
+    }
+  }
+  // ions of the collisions still queued are born at the old temperature
+  SIM_TRY(flush_collisions(s));
+  GASATT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (temperature) {
+    if (!s->d_ion_sig) {
+      int rc = sim_alloc(s, &s->d_ion_sig, ncell);
+      if (rc) return rc;
+    }
+    GASATT_CUDA(ctx, cudaMemcpy(s->d_ion_sig, h.data(), ncell * 8, cudaMemcpyHostToDevice));
+    s->P.ion_sig = s->d_ion_sig;
+  } else {
+    s->P.ion_sig = nullptr;
+  }
   SIM_TRY(upload_params(s));
   drop_graphs(s);                  // the step graphs hold the launch parameters
   return build_graphs(s);

@@ -111,6 +111,7 @@ _SIGS = {
                                      ctypes.POINTER(ctypes.c_float)]),
     "gasatt_sim_birth_photo": (c_i, [c_p, c_i64, c_d, c_d, c_u64, c_u64]),
     "gasatt_sim_set_gas_density": (c_i, [c_p, c_p, c_i]),
+    "gasatt_sim_set_gas_temperature": (c_i, [c_p, c_p, c_i]),
     "gasatt_sim_get_config": (c_i, [c_p, c_p]),
     "gasatt_rebond": (c_i, [c_p, c_p, c_i64, c_p, c_p, c_p, c_i64, c_i64, c_d, c_d, c_p]),
     "gasatt_sim_load_ions": (c_i, [c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_i64, c_i]),

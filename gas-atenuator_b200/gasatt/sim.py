@@ -219,6 +219,17 @@ class Sim:
             raise ValueError(f"gas density must have shape ({self.cfg.n_r}, {self.cfg.n_z})")
         check(self.ctx.handle, lib.gasatt_sim_set_gas_density(self.h, a.ctypes.data_as(ctypes.c_void_p), 0))
 
+    def set_gas_temperature(self, temperature):
+        """Per-cell gas temperature [K] of shape (n_r, n_z) for the newborn
+        ions' Maxwellian, or None for the uniform cfg.gas_temperature."""
+        if temperature is None:
+            check(self.ctx.handle, lib.gasatt_sim_set_gas_temperature(self.h, None, 0))
+            return
+        a = np.asfortranarray(temperature, dtype=np.float64)
+        if a.shape != (self.cfg.n_r, self.cfg.n_z):
+            raise ValueError(f"gas temperature must have shape ({self.cfg.n_r}, {self.cfg.n_z})")
+        check(self.ctx.handle, lib.gasatt_sim_set_gas_temperature(self.h, a.ctypes.data_as(ctypes.c_void_p), 0))
+
     def current(self):
         nr, nz = self.cfg.n_r, self.cfg.n_z
         jr = np.zeros((nr, nz), order="F")

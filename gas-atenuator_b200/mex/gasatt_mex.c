@@ -26,6 +26,7 @@
  *   gasatt_mex('sim_birth_photo', h, n_photo, photon_keV, seed, sigma_r)
  *   gasatt_mex('sim_set_fields', h, Er, Ez, Hphi)     [Er, Ez, Hphi] = gasatt_mex('sim_get_fields', h)
  *   gasatt_mex('sim_set_gas_density', h, density)     density n_r x n_z, or [] for the uniform one
+ *   gasatt_mex('sim_set_gas_temperature', h, T)       T n_r x n_z [K], or [] for the uniform one
  *   gasatt_mex('sim_load_ions', h, r, z, ur, ut, uz, id, charge)
  *   [r, z, ur, ut, uz, id, charge] = gasatt_mex('sim_read_ions', h)
  *   gasatt_mex('sim_step', h, nsteps)
@@ -452,19 +453,20 @@ static void cmd_sim_fields(int nlhs, mxArray *plhs[], int nrhs, const mxArray *p
   }
 }
 
-static void cmd_sim_gas(int nrhs, const mxArray *prhs[]) {
+/* a per-cell gas map (density or temperature), n_r x n_z; [] = uniform */
+static void cmd_sim_gas(int nrhs, const mxArray *prhs[], int temperature) {
   gasatt_sim *s;
   gasatt_sim_config cfg;
-  nargs(nrhs, 3, "sim_set_gas_density(h, density)");
+  const double *m = NULL;
+  nargs(nrhs, 3, temperature ? "sim_set_gas_temperature(h, T)" : "sim_set_gas_density(h, density)");
   s = sim_of(prhs[1]);
   check(gasatt_sim_get_config(s, &cfg));
-  if (mxGetNumberOfElements(prhs[2]) == 0) {               /* [] : back to uniform */
-    check(gasatt_sim_set_gas_density(s, NULL, 0));
-    return;
+  if (mxGetNumberOfElements(prhs[2]) != 0) {
+    if (mxGetM(prhs[2]) != (size_t)cfg.n_r || mxGetN(prhs[2]) != (size_t)cfg.n_z)
+      fail("gas map must be n_r x n_z");
+    m = host(prhs[2], "gas map must be a double host matrix");
   }
-  if (mxGetM(prhs[2]) != (size_t)cfg.n_r || mxGetN(prhs[2]) != (size_t)cfg.n_z)
-    fail("sim_set_gas_density: density must be n_r x n_z");
-  check(gasatt_sim_set_gas_density(s, host(prhs[2], "density must be a double host matrix"), 0));
+  check(temperature ? gasatt_sim_set_gas_temperature(s, m, 0) : gasatt_sim_set_gas_density(s, m, 0));
 }
 
 static void cmd_sim_load_ions(int nrhs, const mxArray *prhs[]) {
@@ -569,6 +571,7 @@ static const char *const k_commands[] = {
     "init", "tables", "find_CS0", "free_motion", "REBOND", "particle_density", "electricmagneticfield6",
     "electron_collision", "sim_create", "sim_load", "sim_step", "sim_read", "sim_diag",
     "sim_destroy", "sim_birth_photo", "sim_set_fields", "sim_get_fields", "sim_set_gas_density",
+    "sim_set_gas_temperature",
     "sim_load_ions", "sim_read_ions"};
 
 void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
@@ -612,7 +615,8 @@ void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
                                  (uint64_t)scalar(prhs[4], "seed"), 0));
   } else if (!strcmp(cmd, "sim_set_fields")) cmd_sim_fields(nlhs, plhs, nrhs, prhs, 1);
   else if (!strcmp(cmd, "sim_get_fields")) cmd_sim_fields(nlhs, plhs, nrhs, prhs, 0);
-  else if (!strcmp(cmd, "sim_set_gas_density")) cmd_sim_gas(nrhs, prhs);
+  else if (!strcmp(cmd, "sim_set_gas_density")) cmd_sim_gas(nrhs, prhs, 0);
+  else if (!strcmp(cmd, "sim_set_gas_temperature")) cmd_sim_gas(nrhs, prhs, 1);
   else if (!strcmp(cmd, "sim_load_ions")) cmd_sim_load_ions(nrhs, prhs);
   else if (!strcmp(cmd, "sim_read_ions")) cmd_sim_read_ions(nlhs, plhs, nrhs, prhs);
   else {

@@ -341,6 +341,14 @@ int gasatt_sim_read_ions(gasatt_sim *sim, double *r, double *z, double *ur, doub
  * batch (gasatt_batch_create) holding this simulation must be created after
  * the call.  on_device: 1 = device pointer, 0 = host pointer. */
 int gasatt_sim_set_gas_density(gasatt_sim *sim, const double *density, int on_device);
+/* Per-cell gas temperature [K] (n_r x n_z, column-major like the density;
+ * NULL: the uniform cfg->gas_temperature): the temperature of the
+ * reference's temperature_cells array, which its collision kernel reads for
+ * the newborn ion's Maxwellian (electron_transport.cu:202-204).  An ion born
+ * in a cell gets velocity components of spread sqrt(kb T / m_ion) of that
+ * cell.  Values finite and >= 0.  Collisions still queued are applied first;
+ * the step graphs are rebuilt, so create a batch after this call. */
+int gasatt_sim_set_gas_temperature(gasatt_sim *sim, const double *temperature, int on_device);
 int gasatt_sim_read(gasatt_sim *sim, double *r, double *z,
                     double *ur, double *ut, double *uz, uint64_t *id,
                     int64_t cap, int64_t *n, int on_device);

@@ -1020,7 +1020,7 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
                  double *y, double *z, double *ux, double *uy, double *uz, uint64_t *id,
                  uint8_t *alive, int64_t *n_io, int64_t cap, const double *Er, const double *Ez,
                  const double *H, double *jr, double *jz, int do_kick, int do_mcc,
-                 const double *gas, orc_ions *ions, orc_counters *cnt) {
+                 const double *gas, const double *gas_T, orc_ions *ions, orc_counters *cnt) {
   const int nr = cfg->n_r, nz = cfg->n_z;
   const double Rp = nr * cfg->dr, Lp = nz * cfg->dz, c = cfg->c, me = cfg->m_e, qe = cfg->q_e;
   const double qm_dt2 = -qe / me * cfg->dt / 2;
@@ -1085,14 +1085,15 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
           double um = sqrt(u2), v = um / g;
           double se, si, sx, L;
           xs_lookup(xs, Eev, &se, &si, &sx, &L);
-          double ng = cfg->gas_density;
-          if (gas) {
-            /* density of the cell the electron ends the step in */
+          double ng = cfg->gas_density, isig = ion_sigma;
+          if (gas || gas_T) {
+            /* density and temperature of the cell the electron ends the step in */
             double r = sqrt(x[p] * x[p] + y[p] * y[p]);
             int ir = (int)floor(r / cfg->dr), iz = (int)floor(z[p] / cfg->dz);
             ir = ir < 0 ? 0 : ir > nr - 1 ? nr - 1 : ir;
             iz = iz < 0 ? 0 : iz > nz - 1 ? nz - 1 : iz;
-            ng = gas[ir + (int64_t)iz * nr];
+            if (gas) ng = gas[ir + (int64_t)iz * nr];
+            if (gas_T) isig = sqrt(cfg->kb * gas_T[ir + (int64_t)iz * nr] / cfg->m_ion);
           }
           double nu_el = ng * se * v, nu_io = ng * si * v;
           double nu_ex = ng * sx * v;
@@ -1130,7 +1131,7 @@ int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step, d
               double a1, a2, b1, b2;
               draw_block(cfg->seed, id[p], step, 2, &a1, &a2);
               draw_block(cfg->seed, id[p], step, 3, &b1, &b2);
-              double ra = ion_sigma * sqrt(-2 * log(a1)), rb = ion_sigma * sqrt(-2 * log(b1));
+              double ra = isig * sqrt(-2 * log(a1)), rb = isig * sqrt(-2 * log(b1));
               double wr = ra * cos(2 * GASATT_PI * a2), wt = ra * sin(2 * GASATT_PI * a2);
               double rr = sqrt(x[p] * x[p] + y[p] * y[p]);
               double cq = rr > 0 ? x[p] / rr : 1.0, sq = rr > 0 ? y[p] / rr : 0.0;

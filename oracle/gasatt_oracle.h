@@ -140,13 +140,15 @@ typedef struct orc_ions {
  * capacity cap; *n grows with births.  jr/jz receive the current density
  * [A/m^2] (overwritten).  gas: per-cell N2 density (n_r x n_z, column-major,
  * cell ir = floor(r/dr), iz = floor(z/dz), both clamped to the grid) or NULL
- * for cfg->gas_density everywhere; xs->nu_max must bound the largest density. */
+ * for cfg->gas_density everywhere; xs->nu_max must bound the largest density.
+ * gas_T: per-cell temperature [K] for the newborn ions (same layout), or NULL
+ * for cfg->gas_temperature. */
 int orc_sim_pass(const gasatt_sim_config *cfg, const orc_xs *xs, int64_t step,
                  double *x, double *y, double *z, double *ux, double *uy, double *uz,
                  uint64_t *id, uint8_t *alive, int64_t *n, int64_t cap,
                  const double *Er, const double *Ez, const double *H,
                  double *jr, double *jz, int do_kick, int do_mcc, const double *gas,
-                 orc_ions *ions, orc_counters *cnt);
+                 const double *gas_T, orc_ions *ions, orc_counters *cnt);
 /* ion push over dt_i = cfg->ion_subcycle * cfg->dt: gather, Boris kick with
  * charge q e and mass cfg->m_ion, two half drifts (absorbed beyond Rp,
  * reflected at the z ends), deposit of the ion current density [A/m^2] into

@@ -222,6 +222,7 @@ class Sim:
         self.xs = XS(tab, cfg.table_n, cfg.table_emin_ev, cfg.table_emax_ev, cfg.gas_density,
                      cfg.c, cfg.m_e, cfg.q_e)
         self.gas = None
+        self.gas_T = None
         self.cap = cap
         self.x = np.zeros(cap); self.y = np.zeros(cap); self.z = np.zeros(cap)
         self.ux = np.zeros(cap); self.uy = np.zeros(cap); self.uz = np.zeros(cap)
@@ -276,6 +277,12 @@ class Sim:
         self.xs = XS(self.tab, cfg.table_n, cfg.table_emin_ev, cfg.table_emax_ev, n_max,
                      cfg.c, cfg.m_e, cfg.q_e)
 
+    def set_gas_temperature(self, temperature):
+        """Per-cell gas temperature (n_r x n_z) for the newborn ions, or None."""
+        cfg = self.cfg
+        self.gas_T = None if temperature is None else np.asfortranarray(
+            np.asarray(temperature, dtype=np.float64).reshape(cfg.n_r, cfg.n_z, order="F"))
+
     def _pass(self, step, kick, mcc):
         n = c_i64(self.n)
         rc = lib.orc_sim_pass(ctypes.byref(self.cfg), c_p(self.xs.h), c_i64(step), P(self.x),
@@ -283,6 +290,7 @@ class Sim:
                               P(self.alive), ctypes.byref(n), c_i64(self.cap), P(self.Er),
                               P(self.Ez), P(self.H), P(self.jr), P(self.jz), c_i(kick), c_i(mcc),
                               None if self.gas is None else P(self.gas),
+                              None if self.gas_T is None else P(self.gas_T),
                               None if self.ions is None else ctypes.byref(self.ions),
                               P(self._cnt))
         assert rc == 0

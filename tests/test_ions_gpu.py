@@ -263,3 +263,45 @@ def test_energy_budget_closes_with_wall_losses(precision, tol):
     lhs = d0["kinetic_ev"] + d0["field_energy_j"] * e_c
     rhs = d["kinetic_ev"] + d["field_energy_j"] * e_c + d["collision_loss_ev"] + d["wall_loss_ev"]
     assert abs(rhs - lhs) < tol * lhs, (lhs, rhs, d["wall_loss_ev"])
+
+
+def test_gas_temperature_map_sets_the_newborn_ions_spread(tables):
+    """A per-cell gas temperature (300 K in the lower half of z, 3000 K in the
+    upper): the FP64 form's ions match the oracle's, and ions born in the hot
+    half spread sqrt(10) times wider.  A uniform 300 K map is the scalar run."""
+    steps = 20
+    cfg, sim, parts, flds = start(_lib.FP64, 1000, n_photo=3000)
+    T = np.full((NR, NZ), 300.0)
+    T[:, NZ // 2:] = 3000.0
+    sim.set_gas_temperature(T)
+    sim.step(steps)
+    gi = sim.read_ions()
+    orc = O.Sim(cfg, tables, cap=cfg.capacity)
+    orc.load(*parts)
+    orc.Er[:], orc.Ez[:], orc.H[:] = flds
+    orc.set_gas_temperature(T)
+    orc.prologue()
+    for _ in range(steps):
+        orc.step()
+    r, z, ur, ut, uz, ids, alive, q = orc.ion_state_rz()
+    assert len(gi["id"]) == len(ids) > 300
+    have, _ = alive_by_id(gi)
+    want = by_id(ids, r, z, ur, ut, uz)
+    for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
+        close(h, w, 1e-10, "ion " + k)
+    hot = gi["z"] >= NZ // 2 * D
+    s_hot, s_cold = gi["uz"][hot].std(), gi["uz"][~hot].std()
+    assert hot.sum() > 100 and (~hot).sum() > 100
+    assert abs(s_hot / s_cold / np.sqrt(10) - 1) < 0.25
+    # a uniform map at the configured temperature is the scalar run
+    runs = []
+    for use_map in (False, True):
+        cfg2, sim2, _, _ = start(_lib.FP32_SPLIT, 1000)
+        if use_map:
+            sim2.set_gas_temperature(np.full((NR, NZ), cfg2.gas_temperature))
+        sim2.step(8)
+        st = sim2.read_ions()
+        o = np.argsort(st["id"])
+        runs.append(np.stack([st[k][o] for k in ("r", "z", "ur", "ut", "uz")]))
+        sim2.close()
+    assert runs[0].shape[1] > 10 and np.array_equal(runs[0], runs[1])
