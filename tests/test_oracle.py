@@ -235,3 +235,24 @@ def test_oracle_rebond_small_case():
     np.testing.assert_allclose(v[1, :2], [np.sin(0.5), np.cos(0.5)], rtol=1e-15)   # turned by -PHIp
     np.testing.assert_allclose([p[2, 2], v[2, 2]], [0.75, -3.0], rtol=1e-15)
     assert O.rebond(pos, r, np.array([-10.0, 0.0, 0.0]), vel, Lp, PHIp, max_wraps=8)[2] == -1
+
+
+def test_oracle_ion_births_follow_the_gas_temperature_map(tables):
+    """Oracle ions born in the 3000 K half spread sqrt(10) wider than those
+    born in the 300 K half (one ion per ionization)."""
+    from gasatt.sim import births, config
+    nr, nz, d = 16, 32, 5e-6
+    cfg = config(nr, nz, d, 1e-14, 300.0, precision=_lib.FP64, capacity=20000, seed=7,
+                 ion_capacity=20000, ion_subcycle=1000)
+    orc = O.Sim(cfg, tables, cap=cfg.capacity)
+    orc.load(*births(3000, 8.0, nz * d, seed=3, sigma_r=30e-6, Rp=nr * d))
+    T = np.full((nr, nz), 300.0)
+    T[:, nz // 2:] = 3000.0
+    orc.set_gas_temperature(T)
+    orc.prologue()
+    for _ in range(15):
+        orc.step()
+    r, z, ur, ut, uz, ids, alive, q = orc.ion_state_rz()
+    assert len(ids) == orc.counters[0] > 300
+    hot = z >= nz // 2 * d
+    assert abs(uz[hot].std() / uz[~hot].std() / np.sqrt(10) - 1) < 0.25
