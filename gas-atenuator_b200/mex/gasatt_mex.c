@@ -14,6 +14,8 @@
  *   [pos, vel, N_boundary] = gasatt_mex('REBOND', pos, r, phi, vel, Lp, PHIp)     REBOND.m:1
  *   d = gasatt_mex('particle_density', dr, dz, dphi, r, phi, z, cellnumxy,
  *                  sum_cell, VC, FN, ncell)                                      particle_density.m:1
+ *   d = gasatt_mex('particle_density0', dr, dz, dphi, position, cellnumxy,
+ *                  sum_cell, VC, FN, ncell)          position n x 3 (r, z, phi)   particle_density0.m:1
  *   [e_pos, e_vel, i1_pos, i1_vel, i2_pos, i2_vel, Er, Ez, Hphi, kin] =
  *       gasatt_mex('electricmagneticfield6', e_pos, e_vel, i1_pos, i1_vel, i2_pos,
  *                  i2_vel, Er, Ez, Hphi, delta, dt, Rp, Lp, PHIp, FN, cycle_time)  electricmagneticfield6.m:1
@@ -250,31 +252,48 @@ static void cmd_rebond(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[
   mxGPUDestroyGPUArray(phi.g); mxGPUDestroyGPUArray(vel.g);
 }
 
-static void cmd_particle_density(mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
-  gpu_in dphi, r, phi, z, sum_cell, VC;
+/* the density of particles at (r, phi, z) on the sector cells; the variant
+   without device allocation leaves MATLAB's pool alone when the grid fits it */
+static mxArray *density(const mxArray *dr, const mxArray *dz, const gpu_in *dphi,
+                        const double *r, const double *phi, const double *z, int64_t n,
+                        const mxArray *cellnumxy, const mxArray *sum_cell_a, const mxArray *VC_a,
+                        const mxArray *FN, const mxArray *ncell_a) {
+  gpu_in sum_cell = gpu_copy(sum_cell_a, "sum_cell must be a double gpuArray");
+  gpu_in VC = gpu_copy(VC_a, "VC must be a double gpuArray");
+  const int64_t ncell = (int64_t)scalar(ncell_a, "ncell");
   double *d;
-  mxGPUArray *g;
-  int64_t ncell;
-  int rmax;
+  mxGPUArray *g = gpu_new(ncell, 1, &d);
+  check((ncell <= GASATT_DENSITY_NOALLOC_MAX_CELLS ? gasatt_particle_density_noalloc
+                                                    : gasatt_particle_density)(
+      g_ctx, scalar(dr, "dr"), scalar(dz, "dz"), dphi->p, (int)(dphi->rows * dphi->cols), r, phi,
+      z, n, (int)scalar(cellnumxy, "cellnumxy"), sum_cell.p, VC.p, ncell, scalar(FN, "FN"), d));
+  mxGPUDestroyGPUArray(sum_cell.g); mxGPUDestroyGPUArray(VC.g);
+  return gpu_out(g);
+}
+
+static void cmd_particle_density(mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
+  gpu_in dphi, r, phi, z;
   nargs(nrhs, 12, "particle_density(dr, dz, dphi, r, phi, z, cellnumxy, sum_cell, VC, FN, ncell)");
   dphi = gpu_copy(prhs[3], "dphi must be a double gpuArray");
   r = gpu_copy(prhs[4], "r must be a double gpuArray");
   phi = gpu_copy(prhs[5], "phi must be a double gpuArray");
   z = gpu_copy(prhs[6], "z must be a double gpuArray");
-  sum_cell = gpu_copy(prhs[8], "sum_cell must be a double gpuArray");
-  VC = gpu_copy(prhs[9], "VC must be a double gpuArray");
-  ncell = (int64_t)scalar(prhs[11], "ncell");
-  rmax = (int)(dphi.rows * dphi.cols);
-  g = gpu_new(ncell, 1, &d);
-  /* the variant without device allocation leaves MATLAB's pool alone */
-  check((ncell <= GASATT_DENSITY_NOALLOC_MAX_CELLS ? gasatt_particle_density_noalloc
-                                                    : gasatt_particle_density)(
-      g_ctx, scalar(prhs[1], "dr"), scalar(prhs[2], "dz"), dphi.p, rmax, r.p, phi.p, z.p,
-      r.rows * r.cols, (int)scalar(prhs[7], "cellnumxy"), sum_cell.p, VC.p, ncell,
-      scalar(prhs[10], "FN"), d));
+  plhs[0] = density(prhs[1], prhs[2], &dphi, r.p, phi.p, z.p, r.rows * r.cols, prhs[7], prhs[8],
+                    prhs[9], prhs[10], prhs[11]);
   mxGPUDestroyGPUArray(dphi.g); mxGPUDestroyGPUArray(r.g); mxGPUDestroyGPUArray(phi.g);
-  mxGPUDestroyGPUArray(z.g); mxGPUDestroyGPUArray(sum_cell.g); mxGPUDestroyGPUArray(VC.g);
-  plhs[0] = gpu_out(g);
+  mxGPUDestroyGPUArray(z.g);
+}
+
+/* particle_density0.m: position columns (r, z, phi) */
+static void cmd_particle_density0(mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
+  gpu_in dphi, pos;
+  nargs(nrhs, 10, "particle_density0(dr, dz, dphi, position, cellnumxy, sum_cell, VC, FN, ncell)");
+  dphi = gpu_copy(prhs[3], "dphi must be a double gpuArray");
+  pos = gpu_copy(prhs[4], "position must be an n x 3 double gpuArray");
+  if (pos.rows && pos.cols != 3) fail("particle_density0: position must be n x 3");
+  plhs[0] = density(prhs[1], prhs[2], &dphi, pos.p, pos.p + 2 * pos.rows, pos.p + pos.rows,
+                    pos.rows, prhs[5], prhs[6], prhs[7], prhs[8], prhs[9]);
+  mxGPUDestroyGPUArray(dphi.g); mxGPUDestroyGPUArray(pos.g);
 }
 
 static void cmd_emf6(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
@@ -568,7 +587,8 @@ static void cmd_sim_diag(mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
 }
 
 static const char *const k_commands[] = {
-    "init", "tables", "find_CS0", "free_motion", "REBOND", "particle_density", "electricmagneticfield6",
+    "init", "tables", "find_CS0", "free_motion", "REBOND", "particle_density", "particle_density0",
+    "electricmagneticfield6",
     "electron_collision", "sim_create", "sim_load", "sim_step", "sim_read", "sim_diag",
     "sim_destroy", "sim_birth_photo", "sim_set_fields", "sim_get_fields", "sim_set_gas_density",
     "sim_set_gas_temperature",
@@ -599,6 +619,7 @@ void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
   else if (!strcmp(cmd, "free_motion")) cmd_free_motion(nlhs, plhs, nrhs, prhs);
   else if (!strcmp(cmd, "REBOND")) cmd_rebond(nlhs, plhs, nrhs, prhs);
   else if (!strcmp(cmd, "particle_density")) cmd_particle_density(plhs, nrhs, prhs);
+  else if (!strcmp(cmd, "particle_density0")) cmd_particle_density0(plhs, nrhs, prhs);
   else if (!strcmp(cmd, "electricmagneticfield6")) cmd_emf6(nlhs, plhs, nrhs, prhs);
   else if (!strcmp(cmd, "electron_collision")) cmd_collision(nlhs, plhs, nrhs, prhs);
   else if (!strcmp(cmd, "sim_create")) cmd_sim_create(plhs, nrhs, prhs);

@@ -179,6 +179,9 @@ def test_mex_dropins_match_the_c_abi(mex, tables):
                                    torch.tensor(z), cellnumxy, sum_cell, VC, 3.0,
                                    ncell=cellnumxy * zmax)
     np.testing.assert_array_equal(mex.value(got[0]).ravel(), np_(want))
+    got0 = mex.call(1, "particle_density0", delta, dz, Gpu(dphi), Gpu(np.stack([r, z, phi], 1)),
+                    float(cellnumxy), Gpu(sum_cell), Gpu(VC), 3.0, float(cellnumxy * zmax))
+    np.testing.assert_array_equal(mex.value(got0[0]).ravel(), np_(want))
     # electricmagneticfield6 (positions (r, phi, z) in, like the reference)
     cs = emf6_inputs(5)
     d, nr, nz, PHIp = cs["d"], cs["nr"], cs["nz"], cs["PHIp"]
