@@ -316,3 +316,37 @@ def test_field_subcycle_ratio_matches_oracle(tables, ratio):
     for g, w, k in zip(f32, f64, ("Er", "Ez", "H")):
         assert np.linalg.norm(g - w) <= 1e-4 * np.linalg.norm(w), k
     assert abs(d32["n_ionizations"] - d64["n_ionizations"]) <= 2
+
+
+@pytest.mark.parametrize("precision", [_lib.FP64, _lib.FP32_SPLIT])
+def test_fields_set_between_steps(tables, precision):
+    """Fields replaced after two steps (the FP32 form must rebuild its gather
+    quads from them): the FP64 form follows the oracle, the FP32 form the
+    FP64 form."""
+    out = {}
+    for prec in (_lib.FP64, precision):
+        cfg, sim, parts, flds = start(prec)
+        sim.step(2)
+        F2 = grid_fields(NR, NZ, np.random.default_rng(21), E0=2e6, H0=3e3)
+        F2[0][:, 0] = 0; F2[0][:, -1] = 0; F2[1][-1, :] = 0
+        sim.set_fields(*F2)
+        sim.step(3)
+        out[prec] = (sim.fields(), sim.diag()["n_ionizations"])
+        sim.close()
+    orc = O.Sim(cfg, tables, cap=cfg.capacity)
+    orc.load(*parts)
+    orc.Er[:], orc.Ez[:], orc.H[:] = flds
+    orc.prologue()
+    for _ in range(2):
+        orc.step()
+    orc.Er[:], orc.Ez[:], orc.H[:] = F2
+    for _ in range(3):
+        orc.step()
+    f64, i64 = out[_lib.FP64]
+    for g, w, k in zip(f64, (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
+        close(g, w, 1e-10, k)
+    assert i64 == orc.counters[0]
+    f, i = out[precision]
+    for g, w, k in zip(f, f64, ("Er", "Ez", "H")):
+        assert np.linalg.norm(g - w) <= 1e-4 * np.linalg.norm(w), k
+    assert abs(i - i64) <= 2
