@@ -104,36 +104,44 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ ours (GPU)
-SORT_PERIODS = (20, 30, 40, 60)     # candidates of the sort-period autotuner
+SORT_PERIODS = (20, 30, 40, 60)     # candidates of the sort period for the autotuner
+KNOBS = ("fdtd_tile_rows", "pass_chunk", "sort_period")
 
 
-def workload_setup(precision, rank, sort_period=20):
-    from gasatt import _lib
-    from gasatt.sim import births, config
+def workload_setup(precision, rank, knobs=None):
+    from gasatt import abi
+    from gasatt.workload import births, config
     w = WORKLOAD
-    prec = _lib.FP32_SPLIT if precision == "fp32_split" else _lib.FP64
+    prec = abi.FP32_SPLIT if precision == "fp32_split" else abi.FP64
     cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=prec,
-                 capacity=4_000_000, seed=replica_seed(rank), sort_period=sort_period)
+                 capacity=4_000_000, seed=replica_seed(rank), sort_period=20)
+    for k, v in (knobs or {}).items():
+        setattr(cfg, k, int(v))
     parts = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=replica_seed(rank),
                    Rp=w["n_r"] * w["delta"])
     return cfg, parts
 
 
-def make_sim(precision, device, rank, torch, sort_period=20):
+def make_sim(precision, device, rank, torch, knobs=None):
     from gasatt.sim import Sim
-    cfg, parts = workload_setup(precision, rank, sort_period)
+    cfg, parts = workload_setup(precision, rank, knobs)
     sim = Sim(cfg, device=device)
     sim.bind_stream()
     sim.load(*parts)
     return sim, parts
 
 
-def tuned_sort_period(precision, device, rank):
-    """The sort period the autotuner picks for this workload (results do not
-    depend on it; see gasatt.tune)."""
-    from gasatt.tune import tune_sort_period
+def tuned_knobs(precision, device, rank):
+    """The launch-shape knobs (field patch rows, FP32 chunk size, sort period)
+    the autotuner picks for this workload by coordinate descent; results do
+    not depend on them (see gasatt.tune).  Returns ({knob: value}, {knob:
+    {candidate: ms per step}})."""
+    from gasatt.tune import knob_candidates, tune
     cfg, parts = workload_setup(precision, rank)
-    return tune_sort_period(cfg, parts, candidates=SORT_PERIODS, steps=200, device=device)
+    knobs = knob_candidates(cfg)
+    knobs["sort_period"] = SORT_PERIODS
+    best, table = tune(cfg, parts, knobs=knobs, steps=200, device=device)
+    return {k: int(getattr(best, k)) for k in knobs}, table
 
 
 def counts(sim):
@@ -143,52 +151,126 @@ def counts(sim):
     return a.value, b.value, c.value
 
 
-def timed_run(sim, steps, warmup, torch, flush, dist_barrier, phase_steps=50):
-    """K steps enqueued back to back, each preceded by an L2 flush (outside
-    its event pair); the host synchronises once at the end.  A second, short
-    loop with the library's per-kernel events on gives the field / pass /
-    collision split (those events add graph nodes, so they stay out of the
-    headline loop)."""
+def aligned_warmup(warmup, sort_period):
+    """Warm-up steps stretched to a multiple of the sort period.  A run sorts
+    at its steps 0, P, 2P, ... (counted from the load), so K timed steps that
+    start on a multiple of P contain ceil(K / P) sorts: never fewer than their
+    share of the periodic sort."""
+    if sort_period <= 0:
+        return warmup
+    return -(-warmup // sort_period) * sort_period
+
+
+def timed_run(sim, steps, warmup, torch, flush, dist_barrier, sort_period):
+    """K steps, each preceded by an L2 flush (outside its event pair), with the
+    library's phase events on: the same steps give the whole-step time (event
+    pair around the step, the periodic sort included when it falls in it), the
+    field update and the particle pass (event nodes in the step graph right
+    before and after each kernel).  The host waits for each step before
+    enqueuing the next flush; the flush (256 MiB) runs long enough for the
+    next step's launch to be queued behind it."""
     from gasatt._lib import lib
     stream = torch.cuda.current_stream()
-    for _ in range(warmup):
-        sim.step(1)
+    lib.gasatt_sim_enable_timing(sim.h, 1)
+    pre = aligned_warmup(warmup, sort_period)
+    sim.step(pre)
     torch.cuda.synchronize()
     d0 = sim.diag()
     l0 = sim.ctx.launches
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(steps)]
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    fd = ctypes.c_float(); ps = ctypes.c_float(); mc = ctypes.c_float()
+    step_ms, pass_ms, fdtd_ms, mcc_ms = [], [], [], []
     dist_barrier()
     torch.cuda.synchronize()
-    for e0, e1 in evs:
+    for _ in range(steps):
         flush()                                      # L2 cold before every timed step
         e0.record(stream)
         sim.step(1)
         e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        lib.gasatt_sim_last_timing(sim.h, ctypes.byref(fd), ctypes.byref(ps), ctypes.byref(mc))
+        fdtd_ms.append(fd.value); pass_ms.append(ps.value); mcc_ms.append(mc.value)
     torch.cuda.synchronize()
     dist_barrier()
     launches = sim.ctx.launches - l0
-    step_ms = [e0.elapsed_time(e1) for e0, e1 in evs]
     d1 = sim.diag()
-    fd = ctypes.c_float(); ps = ctypes.c_float(); mc = ctypes.c_float()
-    pass_ms, fdtd_ms, mcc_ms = [], [], []
-    lib.gasatt_sim_enable_timing(sim.h, 1)
-    for _ in range(phase_steps):
-        flush()
-        sim.step(1)
-        torch.cuda.synchronize()
-        lib.gasatt_sim_last_timing(sim.h, ctypes.byref(fd), ctypes.byref(ps), ctypes.byref(mc))
-        fdtd_ms.append(fd.value); pass_ms.append(ps.value); mcc_ms.append(mc.value)
     lib.gasatt_sim_enable_timing(sim.h, 0)
+    sorts = sum(1 for i in range(pre, pre + steps) if sort_period > 0 and i % sort_period == 0)
     return dict(step_ms=step_ms, pass_ms=pass_ms, fdtd_ms=fdtd_ms, mcc_ms=mcc_ms, d0=d0, d1=d1,
-                launches=launches)
+                launches=launches, sorts=sorts, warmup_steps=pre)
 
 
-def e2e_run(precision, device, rank, torch, steps_per_call=200, sort_period=20):
+ME_C2_EV = 510998.95                                 # m_e c^2 [eV]
+
+
+def energies_ev(p):
+    """Kinetic energies [eV] of the live electrons of a Sim.read() dict."""
+    a = p["r"] >= 0
+    u2 = (p["ur"][a] ** 2 + p["ut"][a] ** 2 + p["uz"][a] ** 2) / 299792458.0 ** 2
+    return ME_C2_EV * (u2 / (np.sqrt(1 + u2) + 1))
+
+
+def accuracy_run(precision, device, rank, torch, steps, knobs):
+    """The workload free-running for `steps` steps (its stated length): the
+    event counts, the fields and the electrons' energies at the end."""
+    sim, _ = make_sim(precision, device, rank, torch, knobs)
+    sim.step(steps)
+    torch.cuda.synchronize()
+    out = dict(diag=sim.diag(), fields=sim.fields(), E=energies_ev(sim.read()))
+    sim.close()
+    return out
+
+
+def compare_forms(a32, a64):
+    """FP32 split form against the FP64 form after the same steps: yield
+    error, field errors, the electron energy distribution (40 log bins from
+    0.1 eV to 10 keV) and the mean energy, each with its Monte Carlo error."""
+    d32, d64 = a32["diag"], a64["diag"]
+    i32, i64 = d32["n_ionizations"], d64["n_ionizations"]
+    pairs = list(zip(a32["fields"], a64["fields"]))
+    ferr = max(float(np.linalg.norm((x - y).ravel()) / max(np.linalg.norm(y.ravel()), 1e-300))
+               for x, y in pairs)
+    fmax = max(float(np.max(np.abs(x - y)) / max(np.max(np.abs(y)), 1e-300)) for x, y in pairs)
+    E32, E64 = a32["E"], a64["E"]
+    bins = np.logspace(-1, 4, 41)
+    h32, _ = np.histogram(E32, bins)
+    h64, _ = np.histogram(E64, bins)
+    used = (h32 + h64) > 0
+    chi2 = float(np.sum((h32[used] - h64[used]) ** 2 / (h32[used] + h64[used])))
+    zbin = float(np.max(np.abs(h32 - h64) / np.sqrt(h64 + 1.0)))
+    s32, s64 = np.sort(E32), np.sort(E64)
+    grid = np.concatenate([s32, s64])
+    ks = float(np.max(np.abs(np.searchsorted(s32, grid, side="right") / len(s32)
+                             - np.searchsorted(s64, grid, side="right") / len(s64))))
+    sig_mean = float(E64.std() / np.sqrt(len(E64)))
+    dmean = float(E32.mean() - E64.mean())
+    return {
+        "yield_rel_err_fp32_vs_fp64": abs(i32 - i64) / max(i64, 1),
+        "ionizations_fp32": int(i32), "ionizations_fp64": int(i64),
+        "yield_diff_in_sigma": abs(i32 - i64) / max(math.sqrt(i64), 1.0),
+        "field_rel_err_fp32_vs_fp64": ferr,
+        "field_rel_err_definition": "max over Er, Ez, H of ||F32 - F64||_2 / ||F64||_2",
+        "field_max_abs_rel_err_fp32_vs_fp64": fmax,
+        "eedf_chi2": chi2, "eedf_dof": int(used.sum()),
+        "eedf_max_bin_diff_in_sigma": zbin,
+        "eedf_ks_distance": ks,
+        "eedf_ks_critical_1pct": 1.63 * math.sqrt((len(E32) + len(E64)) / (len(E32) * len(E64))),
+        "mean_energy_ev_fp32": float(E32.mean()), "mean_energy_ev_fp64": float(E64.mean()),
+        "mean_energy_diff_in_sigma": abs(dmean) / sig_mean if sig_mean > 0 else 0.0,
+        "electrons_fp32": int(len(E32)), "electrons_fp64": int(len(E64)),
+        "kinetic_rel_fp32_vs_fp64": d32["kinetic_ev"] / d64["kinetic_ev"] - 1,
+        "gates": {"yield_rel_err_max": 0.005, "field_rel_err_max": 1e-4,
+                  "three_sigma": "eedf bins, mean energy and yield within 3 sigma"},
+    }
+
+
+def e2e_run(precision, device, rank, torch, steps_per_call=200, knobs=None):
     """Through the public C ABI with pinned HOST buffers: H2D of the electrons,
     steps_per_call steps, D2H of the result, all inside the timed region."""
     from gasatt._lib import lib
-    sim, parts = make_sim(precision, device, rank, torch, sort_period)
+    sim, parts = make_sim(precision, device, rank, torch, knobs)
     r, z, ur, ut, uz, ids = parts
     n = len(r)
     cap = int(n * 1.1)
@@ -229,20 +311,9 @@ def e2e_run(precision, device, rank, torch, steps_per_call=200, sort_period=20):
 def cpu_baseline(target_s=12.0):
     """CPU oracle (plain C FP64 restatement, OpenMP on all host cores) on the
     same workload: full population, a bounded number of steps."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as O
-    from gasatt import _lib
-    from gasatt.sim import births, config
-    from gasatt.tables import N2Tables
-    w = WORKLOAD
     threads = os.cpu_count() or 1
+    O, orc = oracle_workload(2_200_000)
     O.lib.orc_set_threads(threads)
-    cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=_lib.FP64,
-                 capacity=2_200_000, seed=w["seed"], sort_period=0)
-    parts = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=w["seed"],
-                   Rp=w["n_r"] * w["delta"])
-    orc = O.Sim(cfg, N2Tables(), cap=cfg.capacity)
-    orc.load(*parts)
     orc.prologue()
     t0 = time.perf_counter()
     orc.step()
@@ -254,8 +325,8 @@ def cpu_baseline(target_s=12.0):
     dt = time.perf_counter() - t0
     n_alive = int(orc.alive[:orc.n].sum())
     return {"value": n_alive * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"full 2,000,000-electron population, {steps} steps after 1 warm-up step "
-                      f"(plain C FP64 oracle, OpenMP {threads} threads, FDTD included)"}
+            "sample": f"full 2,000,000-electron population, {steps} steps after 1 warm-up step; "
+                      f"{ORACLE_WHAT}; OpenMP {threads} threads"}
 
 
 class Ranks:
@@ -316,22 +387,26 @@ def run_ours(args):
     results = {}
     clocks = None
     tuned = {}
+    accuracy_legs = {}
     for prec in ("fp32_split", "fp64"):
-        sp, table = tuned_sort_period(prec, local, rank)
-        sp = int(max_over_ranks(sp))                 # every rank uses the same period
-        tuned[prec] = (sp, table)
-        sim, _ = make_sim(prec, local, rank, torch, sp)
+        knobs, table = tuned_knobs(prec, local, rank)
+        # every rank uses the same launch shapes (and sorts in the same steps)
+        knobs = {k: int(max_over_ranks(v)) for k, v in knobs.items()}
+        tuned[prec] = (knobs, table)
+        sp = knobs["sort_period"]
+        sim, _ = make_sim(prec, local, rank, torch, knobs)
         if prec == "fp32_split":
             with ClockSampler(local) as cs:
-                res = timed_run(sim, args.steps, args.warmup, torch, flush, barrier)
+                res = timed_run(sim, args.steps, args.warmup, torch, flush, barrier, sp)
             clocks = cs.summary()
         else:
-            res = timed_run(sim, args.steps, args.warmup, torch, flush, barrier)
-        res["fields"] = sim.fields()
+            res = timed_run(sim, args.steps, args.warmup, torch, flush, barrier, sp)
         results[prec] = res
         sim.close()
+        # the accuracy gates at the workload's stated length (2000 steps)
+        accuracy_legs[prec] = accuracy_run(prec, local, rank, torch, args.accuracy_steps, knobs)
     e2e = e2e_run("fp32_split", local, rank, torch, steps_per_call=200,
-                  sort_period=tuned["fp32_split"][0])
+                  knobs=tuned["fp32_split"][0])
 
     pk, pk_src = peaks()
     hbm = float(pk.get("hbm_gbs", 6650.0))
@@ -354,14 +429,8 @@ def run_ours(args):
                          bytes_launch=bytes_launch,
                          cell_updates_per_s=ncell / (fdtd_avg / 1e3))
     f32, f64 = out["fp32_split"], out["fp64"]
-    yerr = abs(f32["ion_total"] - f64["ion_total"]) / max(f64["ion_total"], 1)
-    # relative field error of the FP32 form against FP64 after the same steps:
-    # norm-wise ||F32 - F64||_2 / ||F64||_2 (the gated figure), and the
-    # max-abs form max|F32 - F64| / max|F64|, both the worst of Er, Ez, H
-    pairs = list(zip(results["fp32_split"]["fields"], results["fp64"]["fields"]))
-    ferr = max(float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
-               for a, b in pairs)
-    ferr_max = max(float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)) for a, b in pairs)
+    accuracy = compare_forms(accuracy_legs["fp32_split"], accuracy_legs["fp64"])
+    accuracy["steps"] = args.accuracy_steps
     e2e_ms = max_over_ranks(e2e["ms"])
     e2e_val = sum_over_ranks(e2e["n_in"] * e2e["steps"]) / (e2e_ms / 1e3)
     cpu = None
@@ -388,12 +457,22 @@ def run_ours(args):
                    "global_electrons": int(sum_over_ranks(f32["alive"])),
                    "per_rank": "independent replica", "parallelism": f"replicas x{world}",
                    "l2": "flushed before every timed step (256 MiB write, outside the events)",
-                   "sort_period": tuned["fp32_split"][0],
-                   "sort_period_autotuned": {"candidates": list(SORT_PERIODS),
-                                             "ms_per_step": {str(k): round(v, 5) for k, v in
-                                                             tuned["fp32_split"][1].items()},
-                                             "fp64_choice": tuned["fp64"][0]},
-                   "fdtd_ratio": 1, "timed": "whole step: FDTD + particle pass (+ periodic sort)"},
+                   "sort_period": tuned["fp32_split"][0]["sort_period"],
+                   "autotuned": {"knobs": tuned["fp32_split"][0],
+                                 "ms_per_step": {k: {str(c): round(v, 5) for c, v in t.items()}
+                                                 for k, t in tuned["fp32_split"][1].items()},
+                                 "fp64_knobs": tuned["fp64"][0],
+                                 "method": "coordinate descent, 200 steps per candidate on a "
+                                           "fresh copy of the population"},
+                   "fdtd_ratio": 1,
+                   "timed": (f"{args.steps} whole steps (field update + particle pass; the periodic "
+                             f"sort inside the step it falls in); warm-up stretched to "
+                             f"{results['fp32_split']['warmup_steps']} steps so that the window "
+                             f"holds ceil(K / sort period) = {results['fp32_split']['sorts']} sorts"),
+                   "sorts_in_timed_steps": results["fp32_split"]["sorts"],
+                   "phases": "pass_ms and fdtd_ms: event nodes right before and after each kernel "
+                             "in the same step graphs as the headline (their sum is below "
+                             "ms_per_step)"},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"] / e2e["steps"],
                 "d2h_bytes_per_step": e2e["d2h"] / e2e["steps"],
                 "call": f"gasatt_sim_run_host, {e2e['steps']} steps per call, pinned host x,y,z,vx,vy,vz in/out"},
@@ -404,13 +483,11 @@ def run_ours(args):
                      "peak_source": f"{pk_src} hbm_gbs",
                      "bytes_per_launch": f32["bytes_launch"]},
         "fp64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"], "pass_ms": f64["pass_ms"],
+                 "sort_period": tuned["fp64"][0]["sort_period"], "sorts_in_timed_steps": results["fp64"]["sorts"],
                  "mcc_ms": f64["mcc_ms"], "fdtd_ms": f64["fdtd_ms"],
                  "achieved_gbs": f64["achieved_gbs"], "frac": f64["achieved_gbs"] / hbm},
         "fp32_over_fp64": f32["value"] / f64["value"],
-        "accuracy": {"yield_rel_err_fp32_vs_fp64": yerr, "field_rel_err_fp32_vs_fp64": ferr,
-                     "field_rel_err_definition": "max over Er, Ez, H of ||F32 - F64||_2 / ||F64||_2",
-                     "field_max_abs_rel_err_fp32_vs_fp64": ferr_max,
-                     "ionizations_fp32": f32["ion_total"], "ionizations_fp64": f64["ion_total"]},
+        "accuracy": accuracy,
         "fdtd": {"cell_updates_per_s": f32["cell_updates_per_s"], "ms": f32["fdtd_ms"],
                  "note": "one cell-update = one cell advanced by a full particle step (H, E, H, E, H sub-updates)"},
         "pass_ms": f32["pass_ms"], "mcc_ms": f32["mcc_ms"],
@@ -425,25 +502,39 @@ def run_ours(args):
 
 
 # ------------------------------------------------------ reference arm (CPU)
-def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
+def oracle_workload(cap):
+    """The workload's configuration, births and tables for the CPU oracle,
+    built without the CUDA library (gasatt.workload / gasatt.tables load none)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as O
-    from gasatt import _lib
-    from gasatt.sim import births, config
+    from gasatt import abi
     from gasatt.tables import N2Tables
+    from gasatt.workload import births, config
     w = WORKLOAD
-    threads = os.cpu_count() or 1
-    O.lib.orc_set_threads(threads)
-    sample_photo = w["photo"] // 4                     # 500,000 electrons per step
-    cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=_lib.FP64,
-                 capacity=2 * sample_photo + 100_000, seed=w["seed"], sort_period=0)
-    parts = births(sample_photo, w["e_keV"], w["n_z"] * w["delta"], seed=w["seed"],
+    cfg = config(w["n_r"], w["n_z"], w["delta"], w["dt"], w["torr"], precision=abi.FP64,
+                 capacity=cap, seed=w["seed"], sort_period=0)
+    parts = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=w["seed"],
                    Rp=w["n_r"] * w["delta"])
     orc = O.Sim(cfg, N2Tables(), cap=cfg.capacity)
     orc.load(*parts)
+    return O, orc
+
+
+ORACLE_WHAT = ("plain C FP64 restatement of the same corrected step (Boris push, null-collision "
+               "MCC, fixed-point deposit, FDTD); the reference's own CPU path is MATLAB, "
+               "which is not installed")
+
+
+def run_reference(args):
+    """The reference arm: the CPU oracle (the reference's algorithm restated in
+    plain C, OpenMP on every host core) on the full 2,000,000-electron
+    workload, K steps after W warm-up steps.  Rank 0 alone runs it."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    O, orc = oracle_workload(4_000_000)
+    O.lib.orc_set_threads(threads)
     orc.prologue()
     for _ in range(args.warmup):
         orc.step()
@@ -454,18 +545,18 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     alive1 = int(orc.alive[:orc.n].sum())
     value = 0.5 * (alive0 + alive1) * args.steps / dt
-    sample = (f"500,000 of the 2,000,000 electrons (the first 250,000 photoionizations) on the full "
-              f"256x1024 grid, FDTD every step; plain C FP64 oracle of the same step, OpenMP "
-              f"{threads} threads")
+    sample = (f"the full workload ({alive0:,} electrons at the first timed step, 256x1024 grid, FDTD "
+              f"every step), {args.steps} steps after {args.warmup} warm-up steps; {ORACLE_WHAT}; "
+              f"OpenMP {threads} threads")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD_NAME, "sample": sample},
+            "data": "synthetic (seeded photoionization births; N2 cross-sections from the reference CSVs)",
+            "config": {"workload": WORKLOAD_NAME, "precision": "fp64",
+                       "global_electrons": alive0, "parallelism": "host threads x%d" % threads},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference's CPU path is MATLAB (not installed); its algorithm is timed as "
-                    "the plain C restatement"}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -842,6 +933,8 @@ def main():
                     help="profile: only the step loop of one precision (for ncu); "
                          "c3: 48 batched gas cells; c4: the 16M-electron cascade; "
                          "c5: electrons plus ions, long run")
+    ap.add_argument("--accuracy-steps", type=int, default=2000,
+                    help="length of the FP32-vs-FP64 accuracy runs (the workload's 2000 steps)")
     ap.add_argument("--c4-steps", type=int, default=5000)
     ap.add_argument("--c1-steps", type=int, default=500)
     ap.add_argument("--c5-steps", type=int, default=20_000)

@@ -6,7 +6,6 @@
 #include <cub/device/device_scan.cuh>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include "fdtd.cuh"
 #include "gasatt_internal.h"
@@ -185,27 +184,21 @@ __global__ void k_density_finish(const unsigned long long *count, int64_t ncell,
 // Per-cell counters of gasatt_particle_density_noalloc: a fixed array in the
 // library's device image, so that call needs no device allocation.  In host
 // code the name g_density_counts stands for a host-side shadow, not a device
-// address; the device address comes from cudaGetSymbolAddress, once per
-// device, with that device current.
+// address; the device address comes from cudaGetSymbolAddress with the
+// device current.
 static __device__ __align__(256) unsigned long long
     g_density_counts[GASATT_DENSITY_NOALLOC_MAX_CELLS];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_density_mu;
-unsigned long long *g_density_addr[kMaxDevices] = {};
-
-// device address of g_density_counts on ctx->device (current device)
+// Device address of g_density_counts on the current device, looked up on
+// every call: a cached address would go stale when the device's primary
+// context is reset (cudaDeviceReset, or MATLAB's reset(gpuDevice)) and the
+// module is loaded again elsewhere.  Once the module is loaded the lookup is
+// a table read.
 int density_counts_on_device(gasatt_ctx *ctx, unsigned long long **out) {
-  if (ctx->device < 0 || ctx->device >= kMaxDevices)
-    return fail(ctx, GASATT_E_ARG, "particle_density_noalloc: device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_density_mu);
-  if (!g_density_addr[ctx->device]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_density_counts);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(g_density_counts)");
-    g_density_addr[ctx->device] = static_cast<unsigned long long *>(p);
-  }
-  *out = g_density_addr[ctx->device];
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_density_counts);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(g_density_counts)");
+  *out = static_cast<unsigned long long *>(p);
   return GASATT_OK;
 }
 

@@ -172,9 +172,9 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
                                            const unsigned long long *__restrict__ Jz,
                                            unsigned long long *__restrict__ Jr_next,
                                            unsigned long long *__restrict__ Jz_next, int nr,
-                                           int nz, const FdtdCoef &c, const double *__restrict__ invV,
-                                           double mu, double dt, int R, unsigned flags,
-                                           ExtraCurrent xj, FieldQuads q) {
+                                           int nz, int ldf, int ldj, const FdtdCoef &c,
+                                           const double *__restrict__ invV, double mu, double dt,
+                                           int R, unsigned flags, ExtraCurrent xj, FieldQuads q) {
   constexpr int TW = kFdtdPatch;
   __shared__ double sEr[TW * TW], sEz[TW * TW], sH[TW * TW], sJr[TW * TW], sJz[TW * TW];
   const int tile = fdtd_tile(R), hl = 2 * R, hh = 2 * R + 1;
@@ -187,11 +187,11 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
   for (int lj = threadIdx.y; lj < Hn; lj += kFdtdRows) {
     const int j = J0 + lj, s = li + lj * TW;
     if (!col) continue;
-    if (i < nr && j <= nz) sEr[s] = (double)Er[i + (int64_t)j * nr];
-    if (i <= nr && j < nz) sEz[s] = (double)Ez[i + (int64_t)j * (nr + 1)];
+    if (i < nr && j <= nz) sEr[s] = (double)Er[i + (int64_t)j * ldf];
+    if (i <= nr && j < nz) sEz[s] = (double)Ez[i + (int64_t)j * ldf];
     if (i < nr && j < nz) {
-      const int64_t g = i + (int64_t)j * nr;
-      sH[s] = (double)H[g];
+      const int64_t g = i + (int64_t)j * ldj;
+      sH[s] = (double)H[i + (int64_t)j * ldf];
       if (xj.Jr) {
         sJr[s] = ((double)(long long)Jr[g] + (double)(long long)xj.Jr[g] * xj.rel) * invV[i];
         sJz[s] = ((double)(long long)Jz[g] + (double)(long long)xj.Jz[g] * xj.rel) * invV[i];
@@ -256,18 +256,18 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
       const int s = li + (j - J0) * TW;
       if (i < nr && j <= nz) {
         const T v = (T)sEr[s];
-        Er[i + (int64_t)j * nr] = v;
+        Er[i + (int64_t)j * ldf] = v;
         if (q.er) quad_put(q.er, nr + 1, quad_axis_shifted(i, nr), quad_axis_plain(j, nz), (float)v);
       }
       if (i <= nr && j < nz) {
         const T v = (T)sEz[s];
-        Ez[i + (int64_t)j * (nr + 1)] = v;
+        Ez[i + (int64_t)j * ldf] = v;
         if (q.ez) quad_put(q.ez, nr, quad_axis_plain(i, nr), quad_axis_shifted(j, nz), (float)v);
       }
       if (i < nr && j < nz) {
-        const int64_t g = i + (int64_t)j * nr;
+        const int64_t g = i + (int64_t)j * ldj;
         const T v = (T)sH[s];
-        H[g] = v;
+        H[i + (int64_t)j * ldf] = v;
         if (q.h) quad_put(q.h, nr + 1, quad_axis_shifted(i, nr), quad_axis_shifted(j, nz), (float)v);
         Jr_next[g] = 0;
         Jz_next[g] = 0;
@@ -309,7 +309,7 @@ __device__ __forceinline__ void fdtd_tiled1(T *__restrict__ Er, T *__restrict__ 
                                             const unsigned long long *__restrict__ Jz,
                                             unsigned long long *__restrict__ Jr_next,
                                             unsigned long long *__restrict__ Jz_next, int nr,
-                                            int nz, const FdtdCoef &c,
+                                            int nz, int ldf, int ldj, const FdtdCoef &c,
                                             const double *__restrict__ invV, double mu, double dt,
                                             unsigned flags, ExtraCurrent xj, FieldQuads q) {
   constexpr int TW = kFdtdPatch, RW = kFdtdRows;
@@ -337,11 +337,11 @@ __device__ __forceinline__ void fdtd_tiled1(T *__restrict__ Er, T *__restrict__ 
   for (int k = 0; k < 2; ++k) {
     if (!row[k]) continue;
     const int jj = j[k], s = sidx[k];
-    if (i < nr && jj <= nz) sEr[s] = (double)Er[i + jj * nr];
-    if (i <= nr && jj < nz) sEz[s] = (double)Ez[i + jj * (nr + 1)];
+    if (i < nr && jj <= nz) sEr[s] = (double)Er[i + jj * ldf];
+    if (i <= nr && jj < nz) sEz[s] = (double)Ez[i + jj * ldf];
     if (i < nr && jj < nz) {
-      const int g = i + jj * nr;
-      sH[s] = (double)H[g];
+      const int g = i + jj * ldj;
+      sH[s] = (double)H[i + jj * ldf];
       if (xj.Jr) {
         sJr[s] = ((double)(long long)Jr[g] + (double)(long long)xj.Jr[g] * xj.rel) * invV[i];
         sJz[s] = ((double)(long long)Jz[g] + (double)(long long)xj.Jz[g] * xj.rel) * invV[i];
@@ -416,8 +416,8 @@ __device__ __forceinline__ void fdtd_tiled1(T *__restrict__ Er, T *__restrict__ 
     for (int k = 0; k < 2; ++k) {
       const int jj = j[k], s = sidx[k];
       if (!row[k] || jj < j0 || jj >= je) continue;
-      if (i < nr && jj <= nz) Er[i + jj * nr] = (T)sEr[s];
-      if (i <= nr && jj < nz) Ez[i + jj * (nr + 1)] = (T)sEz[s];
+      if (i < nr && jj <= nz) Er[i + jj * ldf] = (T)sEr[s];
+      if (i <= nr && jj < nz) Ez[i + jj * ldf] = (T)sEz[s];
       // whole Er and Ez quads of the tile's quad indices: after the sub-cycle
       // E is correct one cell beyond the tile (Er one column below it, Ez one
       // row below it, both one above), which covers their corners
@@ -432,9 +432,9 @@ __device__ __forceinline__ void fdtd_tiled1(T *__restrict__ Er, T *__restrict__ 
                                         (float)sEz[s1 + 1]);
       }
       if (i < nr && jj < nz) {
-        const int g = i + jj * nr;
+        const int g = i + jj * ldj;
         const T v = (T)sH[s];
-        H[g] = v;
+        H[i + jj * ldf] = v;
         // H is correct only on the tile, one short of its quads' corners:
         // each value goes to the quad slots that read it instead
         if (q.h) quad_put_h(q.h, nr, nz, i, jj, (float)v);

@@ -15,15 +15,44 @@ namespace gasatt {
 // key = 64-bit seed.  Each block yields two (0,1) doubles from 52 bits each.
 struct U2 { double a, b; };
 
+// One Philox round: the two 32 x 32 -> 64-bit products (one wide multiply
+// each) and the key mix.
+__device__ __forceinline__ void philox_round(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+  const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+  const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0, n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+  c[0] = n0; c[1] = (uint32_t)p1; c[2] = n2; c[3] = (uint32_t)p0;
+}
+
 __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
 #pragma unroll
   for (int i = 0; i < 10; ++i) {
-    const uint32_t lo0 = 0xD2511F53u * c[0], hi0 = __umulhi(0xD2511F53u, c[0]);
-    const uint32_t lo1 = 0xCD9E8D57u * c[2], hi1 = __umulhi(0xCD9E8D57u, c[2]);
-    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
-    c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+    philox_round(c, k0, k1);
     k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
   }
+}
+
+// The ten round keys of a 64-bit seed, computed once per launch on the host
+// (the Weyl sequence k + i W of the key schedule), so that a kernel's rounds
+// take their keys straight from its parameters.
+struct PhiloxKeys {
+  uint32_t k[10][2];
+};
+
+inline PhiloxKeys philox_keys(uint64_t seed) {
+  PhiloxKeys K;
+  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  for (int i = 0; i < 10; ++i) {
+    K.k[i][0] = k0; K.k[i][1] = k1;
+    k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+  }
+  return K;
+}
+
+// Philox4x32-10 with the precomputed round keys (same output as philox4x32_10)
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], const PhiloxKeys &K) {
+#pragma unroll
+  for (int i = 0; i < 10; ++i) philox_round(c, K.k[i][0], K.k[i][1]);
 }
 
 // (2b+1) 2^-53 with b the top 52 bits: exact, in (0, 1)
@@ -51,18 +80,19 @@ __host__ __device__ __forceinline__ uint64_t child_id(uint64_t parent, int64_t s
 // ((n_r+1) x n_z), Hphi (n_r x n_z) at (r0, z0) with the reference's
 // one-sided edge cases.  The row (column) index is clamped at z0 = Lp
 // (r0 = Rp) exactly, where the reference reads past the array with weight 0.
+// ldE, ldZ, ldH: row strides (elements) of Er, Ez and H.
 template <typename T>
-__device__ __forceinline__ void gather3(const T *__restrict__ Er, const T *__restrict__ Ez,
-                                        const T *__restrict__ H, int nr, int nz, double dr,
-                                        double dz, double r0, double z0, double &E_r,
-                                        double &E_z, double &Hp) {
+__device__ __forceinline__ void gather3s(const T *__restrict__ Er, const T *__restrict__ Ez,
+                                         const T *__restrict__ H, int nr, int nz, int64_t ldE,
+                                         int64_t ldZ, int64_t ldH, double dr, double dz, double r0,
+                                         double z0, double &E_r, double &E_z, double &Hp) {
   int ar, az;
   int64_t a1, a2, a3, a4;
   ar = (int)floor(r0 / dr - 0.5);
   az = (int)floor(z0 / dz);
   if (az > nz - 1) az = nz - 1;
-  a1 = ar + (int64_t)az * nr; a2 = (ar + 1) + (int64_t)az * nr;
-  a3 = ar + (int64_t)(az + 1) * nr; a4 = (ar + 1) + (int64_t)(az + 1) * nr;
+  a1 = ar + az * ldE; a2 = (ar + 1) + az * ldE;
+  a3 = ar + (az + 1) * ldE; a4 = (ar + 1) + (az + 1) * ldE;
   if (ar < 0) E_r = ((double)Er[a2] * (az * dz + dz - z0) + (double)Er[a4] * (z0 - az * dz)) / dz;
   else if (ar >= nr - 1) E_r = ((double)Er[a1] * (az * dz + dz - z0) + (double)Er[a3] * (z0 - az * dz)) / dz;
   else
@@ -73,8 +103,8 @@ __device__ __forceinline__ void gather3(const T *__restrict__ Er, const T *__res
   ar = (int)floor(r0 / dr);
   az = (int)floor(z0 / dz - 0.5);
   if (ar > nr - 1) ar = nr - 1;
-  a1 = ar + (int64_t)az * (nr + 1); a2 = (ar + 1) + (int64_t)az * (nr + 1);
-  a3 = ar + (int64_t)(az + 1) * (nr + 1); a4 = (ar + 1) + (int64_t)(az + 1) * (nr + 1);
+  a1 = ar + az * ldZ; a2 = (ar + 1) + az * ldZ;
+  a3 = ar + (az + 1) * ldZ; a4 = (ar + 1) + (az + 1) * ldZ;
   if (az < 0) E_z = ((double)Ez[a3] * (ar * dr + dr - r0) + (double)Ez[a4] * (r0 - ar * dr)) / dr;
   else if (az >= nz - 1) E_z = ((double)Ez[a1] * (ar * dr + dr - r0) + (double)Ez[a2] * (r0 - ar * dr)) / dr;
   else
@@ -84,8 +114,8 @@ __device__ __forceinline__ void gather3(const T *__restrict__ Er, const T *__res
            (double)Ez[a4] * (r0 - ar * dr) * (z0 - (az + 0.5) * dz)) / (dr * dz);
   ar = (int)floor(r0 / dr - 0.5);
   az = (int)floor(z0 / dz - 0.5);
-  a1 = ar + (int64_t)az * nr; a2 = (ar + 1) + (int64_t)az * nr;
-  a3 = ar + (int64_t)(az + 1) * nr; a4 = (ar + 1) + (int64_t)(az + 1) * nr;
+  a1 = ar + az * ldH; a2 = (ar + 1) + az * ldH;
+  a3 = ar + (az + 1) * ldH; a4 = (ar + 1) + (az + 1) * ldH;
   if (ar < 0) {
     if (az < 0) Hp = H[a4];
     else if (az >= nz - 1) Hp = H[a2];
@@ -106,43 +136,53 @@ __device__ __forceinline__ void gather3(const T *__restrict__ Er, const T *__res
   }
 }
 
+// the reference's dense column-major grids (EM4.cu:41-122)
+template <typename T>
+__device__ __forceinline__ void gather3(const T *__restrict__ Er, const T *__restrict__ Ez,
+                                        const T *__restrict__ H, int nr, int nz, double dr,
+                                        double dz, double r0, double z0, double &E_r,
+                                        double &E_z, double &Hp) {
+  gather3s<T>(Er, Ez, H, nr, nz, nr, nr + 1, nr, dr, dz, r0, z0, E_r, E_z, Hp);
+}
+
 // ------------------------------------------------------ deposit weights
 // EM7.cu:56-162: the four cell-centred nodes around (r0, z0) and their
 // bilinear weights, one-sided at the grid edges.  Returns ar (column of a1).
-__device__ __forceinline__ int em7_weights(double r0, double z0, int nr, int nz, double dr,
-                                           double dz, int64_t a[4], double b[4]) {
+// ld: row stride (elements) of the current grid the indices a[] address.
+__device__ __forceinline__ int em7_weights_ld(double r0, double z0, int nr, int nz, int64_t ld,
+                                              double dr, double dz, int64_t a[4], double b[4]) {
   const int ar = (int)floor(r0 / dr - 0.5);
   const int az = (int)floor(z0 / dz - 0.5);
   a[0] = a[1] = a[2] = a[3] = 0;
   b[0] = b[1] = b[2] = b[3] = 0;
   if (ar < 0) {
-    if (az < 0) { a[3] = (ar + 1) + (int64_t)(az + 1) * nr; b[3] = 1; }
-    else if (az >= nz - 1) { a[1] = (ar + 1) + (int64_t)az * nr; b[1] = 1; }
+    if (az < 0) { a[3] = (ar + 1) + (int64_t)(az + 1) * ld; b[3] = 1; }
+    else if (az >= nz - 1) { a[1] = (ar + 1) + (int64_t)az * ld; b[1] = 1; }
     else {
-      a[1] = (ar + 1) + (int64_t)az * nr; a[3] = (ar + 1) + (int64_t)(az + 1) * nr;
+      a[1] = (ar + 1) + (int64_t)az * ld; a[3] = (ar + 1) + (int64_t)(az + 1) * ld;
       b[1] = ((az + 1.5) * dz - z0) / (dz);
       b[3] = (z0 - (az + 0.5) * dz) / (dz);
     }
   } else if (ar >= nr - 1) {
-    if (az < 0) { a[2] = ar + (int64_t)(az + 1) * nr; b[2] = 1; }
-    else if (az >= nz - 1) { a[0] = ar + (int64_t)az * nr; b[0] = 1; }
+    if (az < 0) { a[2] = ar + (int64_t)(az + 1) * ld; b[2] = 1; }
+    else if (az >= nz - 1) { a[0] = ar + (int64_t)az * ld; b[0] = 1; }
     else {
-      a[0] = ar + (int64_t)az * nr; a[2] = ar + (int64_t)(az + 1) * nr;
+      a[0] = ar + (int64_t)az * ld; a[2] = ar + (int64_t)(az + 1) * ld;
       b[0] = ((az + 1.5) * dz - z0) / (dz);
       b[2] = (z0 - (az + 0.5) * dz) / (dz);
     }
   } else {
     if (az < 0) {
-      a[2] = ar + (int64_t)(az + 1) * nr; a[3] = (ar + 1) + (int64_t)(az + 1) * nr;
+      a[2] = ar + (int64_t)(az + 1) * ld; a[3] = (ar + 1) + (int64_t)(az + 1) * ld;
       b[2] = ((ar + 1.5) * dr - r0) / (dr);
       b[3] = (r0 - (ar + 0.5) * dr) / (dr);
     } else if (az >= nz - 1) {
-      a[0] = ar + (int64_t)az * nr; a[1] = (ar + 1) + (int64_t)az * nr;
+      a[0] = ar + (int64_t)az * ld; a[1] = (ar + 1) + (int64_t)az * ld;
       b[0] = ((ar + 1.5) * dr - r0) / (dr);
       b[1] = (r0 - (ar + 0.5) * dr) / (dr);
     } else {
-      a[0] = ar + (int64_t)az * nr; a[1] = (ar + 1) + (int64_t)az * nr;
-      a[2] = ar + (int64_t)(az + 1) * nr; a[3] = (ar + 1) + (int64_t)(az + 1) * nr;
+      a[0] = ar + (int64_t)az * ld; a[1] = (ar + 1) + (int64_t)az * ld;
+      a[2] = ar + (int64_t)(az + 1) * ld; a[3] = (ar + 1) + (int64_t)(az + 1) * ld;
       b[0] = ((ar + 1.5) * dr - r0) * ((az + 1.5) * dz - z0) / (dr * dz);
       b[1] = (r0 - (ar + 0.5) * dr) * ((az + 1.5) * dz - z0) / (dr * dz);
       b[2] = ((ar + 1.5) * dr - r0) * (z0 - (az + 0.5) * dz) / (dr * dz);
@@ -150,6 +190,12 @@ __device__ __forceinline__ int em7_weights(double r0, double z0, int nr, int nz,
     }
   }
   return ar;
+}
+
+// the reference's dense n_r x n_z grid (EM7.cu:56-162)
+__device__ __forceinline__ int em7_weights(double r0, double z0, int nr, int nz, double dr,
+                                           double dz, int64_t a[4], double b[4]) {
+  return em7_weights_ld(r0, z0, nr, nz, nr, dr, dz, a, b);
 }
 
 // fixed-point current: value * 2^S rounded to nearest, added with a 64-bit

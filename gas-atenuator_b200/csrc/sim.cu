@@ -30,11 +30,12 @@
 //
 // The FP32 form drifts the whole step at once (the reference's two half
 // drifts joined).
-#include <cub/device/device_scan.cuh>
 #include <cmath>
 #include <cstring>
 #include <vector>
+#include <cudaTypedefs.h>
 #include "fdtd.cuh"
+#include "fdtd_tma.cuh"
 #include "gasatt_internal.h"
 
 using namespace gasatt;
@@ -68,7 +69,9 @@ struct SimCounters {
   unsigned long long alive;      // diagnostic
   unsigned long long exc_loss_fx; // diagnostic: excitation energy losses * 2^16 [eV]
   unsigned long long wall_loss_fx;// diagnostic: kinetic energy absorbed at r = Rp * 2^16 [eV]
-  unsigned long long pad5_[6];
+  unsigned fdtd_err;             // a field-update block gave up waiting for its tile copy
+  unsigned scan_err;             // a sort's scan gave up waiting for a predecessor tile
+  unsigned long long pad5_[5];
   unsigned long long n_ions;     // ion slots claimed (loads and births; may pass the capacity)
   unsigned long long ion_overflow, ion_lost;
   unsigned long long ion_alive, ion_charge, ion_kin_fx;   // diagnostics; kinetic: E * 2^32 [eV]
@@ -85,10 +88,12 @@ struct IonState { double2 *rz; double2 *urt; double *uz; uint64_t *id; int8_t *q
 
 struct SimParams {
   int nr, nz;
+  int ldf, ldj;             // row strides (elements) of the field grids and of the current grids
   double dr, dz, dt, c, qe, me, mu0, FN, PHIp, n_gas, nu_max, P_null, Rp, Lp, kb, m_ion, T_gas;
   const double *gas;        // per-cell N2 density [m^-3] (n_r x n_z), or null: n_gas everywhere
   const double *ion_sig;    // per-cell sqrt(kT/m_ion) of newborn ions (n_r x n_z), or null: ion_sigma
   uint64_t seed;
+  PhiloxKeys pk;            // Philox round keys of seed
   int secondaries;
   long long cap;
   double qm_dt2;            // -q_e/m_e dt/2
@@ -96,6 +101,7 @@ struct SimParams {
   double dep;               // fixed-point factor: FP64 q FN scale (x v)
   float depf;               // FP32: q FN c scale (x beta)
   uint64_t cand_below;      // null-collision candidate iff the 52-bit draw is below this
+  int chunk;                // FP32 pass: particles per chunk (a multiple of the block, <= kChunkMax)
   // tables
   const double *sig;        // 3 x G (el, ion, exc)
   const double *cdf;        // G x 181
@@ -172,7 +178,7 @@ __device__ __forceinline__ double u_of_energy(double EJ, double m, double c) {
 // exactly b < P.cand_below.
 __device__ __forceinline__ bool null_candidate(const SimParams &P, uint64_t id, long long step) {
   uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
-  philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+  philox4x32_10(c, P.pk);
   const uint64_t b = ((((uint64_t)c[0]) << 32) | c[1]) >> 12;
   return b < P.cand_below;
 }
@@ -476,7 +482,7 @@ __device__ __forceinline__ void deposit_values64(const SimParams &P, double r, d
   const double g = sqrt(1 + (ur * ur + ut * ut + uz * uz) / (P.c * P.c));
   const double vrr = ur / g, vzz = uz / g;
   double b[4];
-  const int ar = em7_weights(r, z, P.nr, P.nz, P.dr, P.dz, a, b);
+  const int ar = em7_weights_ld(r, z, P.nr, P.nz, P.ldj, P.dr, P.dz, a, b);
   const int az = (int)floor(z / P.dz - 0.5);
   key = (unsigned)((ar + 1) + (az + 1) * (P.nr + 1));
 #pragma unroll
@@ -518,7 +524,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fi
       bool alive = true;
       if (mode != 1) {
         double E_r, E_z, Hp;
-        gather3<double>(F.Er, F.Ez, F.H, P.nr, P.nz, P.dr, P.dz, r, z, E_r, E_z, Hp);
+        gather3s<double>(F.Er, F.Ez, F.H, P.nr, P.nz, P.ldf, P.ldf, P.ldf, P.dr, P.dz, r, z, E_r,
+                         E_z, Hp);
         const double B = P.mu0 * Hp;
         boris(ur, ut, uz, E_r, 0.0, E_z, 0.0, B, 0.0, P.qm_dt2, P.c);
         halfdrift64(r, z, ur, ut, uz, alive, P);
@@ -685,7 +692,7 @@ __global__ void __launch_bounds__(kBlock) k_ion_push(SimParams P, Fields<T> F, S
       double r = rz.x, z = rz.y, ur = urt.x, ut = urt.y;
       bool alive = true;
       double E_r, E_z, Hp;
-      gather3<T>(F.Er, F.Ez, F.H, P.nr, P.nz, P.dr, P.dz, r, z, E_r, E_z, Hp);
+      gather3s<T>(F.Er, F.Ez, F.H, P.nr, P.nz, P.ldf, P.ldf, P.ldf, P.dr, P.dz, r, z, E_r, E_z, Hp);
       boris(ur, ut, uz, E_r, 0.0, E_z, 0.0, P.mu0 * Hp, 0.0, Zq * P.qm_dt2, P.c);
       halfdrift64(r, z, ur, ut, uz, alive, P);
       if (alive) halfdrift64(r, z, ur, ut, uz, alive, P);
@@ -879,16 +886,18 @@ __device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, 
 // the edges as EM7.cu:56-202) and the fixed-point contributions, node order
 // (ca,ra), (cb,ra), (ca,rb), (cb,rb).  The weights sum to 1, so one particle
 // adds at most 2^20 in magnitude to any node, even where clamped nodes merge.
-// ig: 1/gamma of u (the drift's, which turns u without changing |u|)
-__device__ __forceinline__ void deposit_nodes32(const SimParams &P, int ir, int iz, float fr,
-                                                float fz, float ur, float uz, float ig, int &ca,
-                                                int &cb, int &ra, int &rb, int vr[4], int vz[4]) {
+// ig: 1/gamma of u (the drift's, which turns u without changing |u|).
+// Returns the quad key (ar + 1) + (az + 1)(n_r + 1): equal keys, equal nodes.
+__device__ __forceinline__ unsigned deposit_nodes32(const SimParams &P, int ir, int iz, float fr,
+                                                    float fz, float ur, float uz, float ig, int &ca,
+                                                    int &cb, int &ra, int &rb, int vr[4], int vz[4]) {
   int ar, az;
   float wr, wz;
   half_shift(ir, fr, ar, wr);
   half_shift(iz, fz, az, wz);
   ca = max(ar, 0); cb = min(ar + 1, P.nr - 1);
   ra = max(az, 0); rb = min(az + 1, P.nz - 1);
+  const unsigned key = (unsigned)(ar + 1) + (unsigned)(az + 1) * (unsigned)(P.nr + 1);
   const float w[4] = {(1 - wr) * (1 - wz), wr * (1 - wz), (1 - wr) * wz, wr * wz};
   const float kr = P.depf * ur * ig, kz = P.depf * uz * ig;
 #pragma unroll
@@ -896,17 +905,18 @@ __device__ __forceinline__ void deposit_nodes32(const SimParams &P, int ir, int 
     vr[k] = fma_rint(kr, w[k]);
     vz[k] = fma_rint(kz, w[k]);
   }
+  return key;
 }
 
 // FP32-form deposit window: int32 sums of one chunk of particles on the grid
-// rows [row0, row0 + rows) in shared memory.  A chunk holds at most kChunk
-// particles, so a node's window sum stays below kChunk * 2^20 < 2^31.  Rows
+// rows [row0, row0 + rows) in shared memory.  A chunk holds at most kChunkMax
+// particles, so a node's window sum stays below kChunkMax * 2^20 < 2^31.  Rows
 // are ws >= nr words apart with ws = 3 (mod 32), so the 3 x 3 nodes around a
 // warp's particles sit in 9 different banks.  Nodes outside the window go
 // straight to the grid with 64-bit atomics; the window is added to the grid
 // with one 64-bit atomic per touched node.
 constexpr int kWinNodes = 4096;           // per component
-constexpr int kChunk = 7 * kBlock;        // 1792 particles
+constexpr int kChunkMax = 7 * kBlock;     // 1792 particles (the default chunk)
 
 struct Win32 {
   int *r, *z;
@@ -923,7 +933,7 @@ __device__ __forceinline__ void win_node(const Win32 &w, const SimParams &P, int
     atomicAdd(w.r + k, vr);
     atomicAdd(w.z + k, vz);
   } else {
-    const int64_t g = col + (int64_t)row * P.nr;
+    const int64_t g = col + (int64_t)row * P.ldj;
     if (vr) atomicAdd(P.Jr + g, (unsigned long long)(long long)vr);
     if (vz) atomicAdd(P.Jz + g, (unsigned long long)(long long)vz);
   }
@@ -954,7 +964,7 @@ __device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &
   // candidate, words 2-3 (mixed) drive the stochastic rounding
   uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
   if (mode == 1) {
-    philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+    philox4x32_10(c, P.pk);
     drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, mix32(c[3]), P.hdr, P.hdz, ig);
     return false;
   }
@@ -968,7 +978,7 @@ __device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &
   const float4 b4 = __ldg(P.qEz + (ir + (az + 1) * P.nr));
   const float4 c4 = __ldg(P.qH + ((ar + 1) + (az + 1) * (P.nr + 1)));
   const Quad4 qEr{a4.x, a4.y, a4.z, a4.w}, qEz{b4.x, b4.y, b4.z, b4.w}, qH{c4.x, c4.y, c4.z, c4.w};
-  philox4x32_10(c, (uint32_t)P.seed, (uint32_t)(P.seed >> 32));
+  philox4x32_10(c, P.pk);
   const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]);
   const float Er = bilin_mix(qEr, wr, fz);
   const float Ez = bilin_mix(qEz, fr, wz);
@@ -994,8 +1004,8 @@ __device__ __forceinline__ void deposit_global32(const SimParams &P, int ir, int
                                                  float fz, float ur, float uz, float ig) {
   int ca, cb, ra, rb, vr[4], vz[4];
   deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, ca, cb, ra, rb, vr, vz);
-  const int64_t a[4] = {ca + (int64_t)ra * P.nr, cb + (int64_t)ra * P.nr,
-                        ca + (int64_t)rb * P.nr, cb + (int64_t)rb * P.nr};
+  const int64_t a[4] = {ca + (int64_t)ra * P.ldj, cb + (int64_t)ra * P.ldj,
+                        ca + (int64_t)rb * P.ldj, cb + (int64_t)rb * P.ldj};
   deposit_atomic<int>(a, vr, vz, P.Jr, P.Jz);
 }
 
@@ -1079,7 +1089,7 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
 // FP32 particle pass of step `step` (modes as push32).  Its blocks first take
 // the collision candidates queued by the previous pass, one per warp (a long
 // serial chain each, so blocks in order take eight at a time), then all other
-// particles in chunks of at most kChunk handed out in order, so the blocks
+// particles in chunks of P.chunk handed out in order, so the blocks
 // that ran a candidate simply take fewer chunks.  Counters are committed by
 // the field kernel of the next step.
 __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fields<float> F,
@@ -1087,6 +1097,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
                                                       const SimParams *__restrict__ Pg) {
   __shared__ int win_r[kWinNodes], win_z[kWinNodes];
   __shared__ int win_row0, win_rows;
+  __shared__ int box_cmax;                       // highest window column the chunk touched
   __shared__ long long chunk_at;
   const long long n0 = (long long)cnt->n_total;   // births of this pass land beyond
   const long long step = cnt->step;
@@ -1094,6 +1105,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
   const uint32_t parbit = par ? kSign : 0u;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned lost = 0;
+  // the window starts zeroed; each chunk's flush leaves it zeroed again
+  for (int i = threadIdx.x; i < kWinNodes; i += kBlock) { win_r[i] = 0; win_z[i] = 0; }
   if (mode != 1) {
     const long long nq = (long long)cnt->n_cand[par ^ 1];
     const int *qin = queue + (long long)(par ^ 1) * P.cap;
@@ -1105,11 +1118,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
   }
   const int ws = win_stride(P.nr);
   const int maxrows = min(kWinNodes / ws, P.nz);
-  const long long nchunk = (n0 + kChunk - 1) / kChunk;
+  const int chunk = P.chunk;
+  const long long nchunk = (n0 + chunk - 1) / chunk;
   // window rows of a chunk: the node rows of its first and last particles,
   // with a margin for the drift since the last sort
   auto chunk_rows = [&](long long ch, int &row0, int &rows) {
-    const long long beg = ch * kChunk, end = min(beg + kChunk, n0);
+    const long long beg = ch * chunk, end = min(beg + chunk, n0);
     const uint32_t k0 = reinterpret_cast<const uint32_t *>(S.a + beg)[0];
     const uint32_t k1 = reinterpret_cast<const uint32_t *>(S.a + end - 1)[0];
     int lo = P.nz, hi = -1;
@@ -1139,16 +1153,14 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
       chunk_at = next_ch;
       win_row0 = next_row0;
       win_rows = next_rows;
+      box_cmax = -1;
       if (next_ch < nchunk) next_ch = (long long)atomicAdd(&cnt->chunk_next, 1ull);
     }
     __syncthreads();
     const long long ch = chunk_at;
     if (ch >= nchunk) break;
-    const long long beg = ch * kChunk, end = min(beg + kChunk, n0);
+    const long long beg = ch * chunk, end = min(beg + chunk, n0);
     const Win32 w{win_r, win_z, win_row0, win_rows, ws};
-    const int nwin = w.rows * ws;
-    for (int i = threadIdx.x; i < nwin; i += kBlock) { win_r[i] = 0; win_z[i] = 0; }
-    __syncthreads();
     // the next iteration's particle is loaded one iteration ahead, so its
     // HBM latency overlaps the current particle's arithmetic
     long long base = beg + (threadIdx.x & ~31);
@@ -1156,6 +1168,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
     float2 Bn = make_float2(0.f, 0.f);
     uint64_t idn = 0;
     if (base + lane < end) { An = S.a[base + lane]; Bn = S.b[base + lane]; idn = S.id[base + lane]; }
+    int wc_max = -1;                 // highest window column this lane touched
     for (; base < end; base += blockDim.x) {
       const long long p = base + lane;
       uint4 A = An;
@@ -1185,47 +1198,56 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
         act = alive && mode != 2;
       }
       queue_push(cand, p, &cnt->n_cand[par], queue + (long long)par * P.cap);
+      // Deposit: the lanes that share a node quad (sorted particles put one to
+      // a few quads in a warp) sum their eight integer contributions with
+      // redux.sync, and the first lane of each quad adds the sums - one
+      // shared-memory atomic per node and quad instead of one per particle
+      const unsigned dm = __ballot_sync(0xFFFFFFFFu, act);
       if (act) {
         int ca, cb, ra, rb, vr[4], vz[4];
-        deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, ca, cb, ra, rb, vr, vz);
-        const unsigned la = (unsigned)(ra - w.row0), lb = (unsigned)(rb - w.row0);
-        if (la < (unsigned)w.rows && lb < (unsigned)w.rows) {
-          // each lane visits its four nodes in an order permuted by lane & 3
-          // (swap the columns on bit 0, the rows on bit 1), so lanes on the
-          // same node quad hit four different nodes in each atomic
-          const bool sc = lane & 1, sr = lane & 2;
-          int k0 = (int)la * ws, k1 = (int)lb * ws, c0 = ca, c1 = cb;
-          int r0 = sc ? vr[1] : vr[0], r1 = sc ? vr[0] : vr[1];
-          int r2 = sc ? vr[3] : vr[2], r3 = sc ? vr[2] : vr[3];
-          int z0 = sc ? vz[1] : vz[0], z1 = sc ? vz[0] : vz[1];
-          int z2 = sc ? vz[3] : vz[2], z3 = sc ? vz[2] : vz[3];
-          if (sc) { c0 = cb; c1 = ca; }
-          if (sr) {
-            const int tk = k0; k0 = k1; k1 = tk;
-            int t = r0; r0 = r2; r2 = t; t = r1; r1 = r3; r3 = t;
-            t = z0; z0 = z2; z2 = t; t = z1; z1 = z3; z3 = t;
+        const unsigned key = deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, ca, cb, ra, rb, vr, vz);
+        const unsigned grp = __match_any_sync(dm, key);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          vr[k] = __reduce_add_sync(grp, vr[k]);
+          vz[k] = __reduce_add_sync(grp, vz[k]);
+        }
+        if (lane == __ffs(grp) - 1) {
+          const unsigned la = (unsigned)(ra - w.row0), lb = (unsigned)(rb - w.row0);
+          if (la < (unsigned)w.rows && lb < (unsigned)w.rows) {
+            const int k0 = (int)la * ws, k1 = (int)lb * ws;
+            atomicAdd(win_r + k0 + ca, vr[0]); atomicAdd(win_z + k0 + ca, vz[0]);
+            atomicAdd(win_r + k0 + cb, vr[1]); atomicAdd(win_z + k0 + cb, vz[1]);
+            atomicAdd(win_r + k1 + ca, vr[2]); atomicAdd(win_z + k1 + ca, vz[2]);
+            atomicAdd(win_r + k1 + cb, vr[3]); atomicAdd(win_z + k1 + cb, vz[3]);
+            wc_max = max(wc_max, cb);
+          } else {
+            win_node(w, P, ca, ra, vr[0], vz[0]);
+            win_node(w, P, cb, ra, vr[1], vz[1]);
+            win_node(w, P, ca, rb, vr[2], vz[2]);
+            win_node(w, P, cb, rb, vr[3], vz[3]);
+            wc_max = max(wc_max, cb);     // win_node may use the window for one row
           }
-          atomicAdd(win_r + k0 + c0, r0); atomicAdd(win_z + k0 + c0, z0);
-          atomicAdd(win_r + k0 + c1, r1); atomicAdd(win_z + k0 + c1, z1);
-          atomicAdd(win_r + k1 + c0, r2); atomicAdd(win_z + k1 + c0, z2);
-          atomicAdd(win_r + k1 + c1, r3); atomicAdd(win_z + k1 + c1, z3);
-        } else {
-          win_node(w, P, ca, ra, vr[0], vz[0]);
-          win_node(w, P, cb, ra, vr[1], vz[1]);
-          win_node(w, P, ca, rb, vr[2], vz[2]);
-          win_node(w, P, cb, rb, vr[3], vz[3]);
         }
       }
     }
+    // the window columns this warp touched, merged into the block's
+    wc_max = __reduce_max_sync(0xFFFFFFFFu, wc_max);
+    if (lane == 0 && wc_max >= 0) atomicMax(&box_cmax, wc_max);
     if (threadIdx.x == 0 && next_ch < nchunk) chunk_rows(next_ch, next_row0, next_rows);
     __syncthreads();
-    for (int i = threadIdx.x; i < nwin; i += kBlock) {
-      const int vr = win_r[i], vz = win_z[i];
-      if (vr | vz) {                 // the padding words stay zero
-        const int row = i / ws;
-        const int64_t g = (int64_t)(w.row0 + row) * P.nr + (i - row * ws);
+    // add the touched columns of the window rows to the grid (one 64-bit
+    // atomic per nonzero node) and zero them for the next chunk
+    const int bw = box_cmax + 1, nb = bw > 0 ? bw * w.rows : 0;
+    for (int i = threadIdx.x; i < nb; i += kBlock) {
+      const int row = i / bw, col = i - row * bw;
+      const int k = row * ws + col;
+      const int vr = win_r[k], vz = win_z[k];
+      if (vr | vz) {
+        const int64_t g = (int64_t)(w.row0 + row) * P.ldj + col;
         if (vr) atomicAdd(P.Jr + g, (unsigned long long)(long long)vr);
         if (vz) atomicAdd(P.Jz + g, (unsigned long long)(long long)vz);
+        win_r[k] = 0; win_z[k] = 0;
       }
     }
     __syncthreads();
@@ -1253,34 +1275,47 @@ __global__ void __launch_bounds__(kMccBlock) k_collide32(const SimParams *__rest
 }
 
 // ------------------------------------------------------------- FDTD
-// One fused field sub-cycle per step (fdtd_tiled).
-// R1: the fdtd_ratio 1 specialisation (the two variants need their own
-// kernels: each declares a 40 KB patch)
-template <typename T, bool R1>
+// FP32 form (cnt given): commit the previous pass and open step s - the
+// births of the last pass join the slots, the queue that pass consumed is
+// emptied, the chunk counter rewinds; no other kernel runs meanwhile
+__device__ __forceinline__ void commit_pass32(SimCounters *cnt) {
+  const long long ns = cnt->step + 1;
+  const unsigned long long nt = cnt->n_total + cnt->n_births;
+  cnt->n_total = nt < cnt->cap ? nt : cnt->cap;
+  cnt->n_births = 0;
+  cnt->n_cand[ns & 1] = 0;
+  cnt->chunk_next = 0;
+  cnt->step = ns;
+}
+
+// The field sub-cycle of one step for fdtd_ratio 1: the persistent TMA-fed
+// kernel of fdtd_tma.cuh.
+template <typename T>
+__global__ void __launch_bounds__(32 * kTmaRows, 1) k_sim_fdtd_tma(
+    const __grid_constant__ TmaMaps M, T *Er, T *Ez, T *H, unsigned long long *Jr_next,
+    unsigned long long *Jz_next, int nr, int nz, int ldf, int ldj, FdtdCoef c,
+    const double *invV, double mu, double dt, unsigned flags, SimCounters *cnt,
+    ExtraCurrent ion, FieldQuads quads, int ph, int tiles_x, int ntiles, unsigned *err) {
+  if (cnt && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) commit_pass32(cnt);
+  fdtd_tma_body<T>(M, Er, Ez, H, Jr_next, Jz_next, nr, nz, ldf, ldj, c, invV, mu, dt, flags, ion,
+                   quads, ph, tiles_x, ntiles, err);
+}
+
+// The general sub-cycle (fdtd_ratio > 1): one 32 x 32 patch per block
+// (fdtd_tiled).
+template <typename T>
 __global__ void __launch_bounds__(32 * kFdtdRows, 3) k_sim_fdtd(T *Er, T *Ez, T *H, const unsigned long long *Jr,
                                                   const unsigned long long *Jz,
                                                   unsigned long long *Jr_next,
                                                   unsigned long long *Jz_next, int nr, int nz,
-                                                  FdtdCoef c, const double *invV, double mu,
+                                                  int ldf, int ldj, FdtdCoef c, const double *invV, double mu,
                                                   double dt, int R, unsigned flags,
                                                   SimCounters *cnt, ExtraCurrent ion,
                                                   FieldQuads quads) {
-  // FP32 form (cnt given): commit the previous pass and open step s - the
-  // births of the last pass join the slots, the queue that pass consumed is
-  // emptied, the chunk counter rewinds; no other kernel runs meanwhile
-  if (cnt && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
-    const long long ns = cnt->step + 1;
-    const unsigned long long nt = cnt->n_total + cnt->n_births;
-    cnt->n_total = nt < cnt->cap ? nt : cnt->cap;
-    cnt->n_births = 0;
-    cnt->n_cand[ns & 1] = 0;
-    cnt->chunk_next = 0;
-    cnt->step = ns;
-  }
-  if (R1)
-    fdtd_tiled1<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, c, invV, mu, dt, flags, ion, quads);
-  else
-    fdtd_tiled<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, c, invV, mu, dt, R, flags, ion, quads);
+  if (cnt && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0)
+    commit_pass32(cnt);
+  fdtd_tiled<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, ldf, ldj, c, invV, mu, dt, R, flags, ion,
+                quads);
 }
 
 // ---------------------------------------------------------- load/read
@@ -1469,6 +1504,88 @@ __global__ void k_sort_scatter(State64 A64, State64 B64, State32 A32, State32 B3
   }
 }
 
+// ------------------------------------------------------------ scan
+// Exclusive prefix sum of n ints in one pass (decoupled look-back): each
+// block takes a tile of kScanTile counts by ticket, so a tile's predecessors
+// are always running or done; it publishes its tile total (flag 1), looks
+// back over the predecessors' published totals until it meets an inclusive
+// prefix (flag 2), publishes its own inclusive prefix and writes its tile.
+// A published word is (flag << 62) | value, written in one 64-bit store.
+// The look-back wait on a tile that has published nothing yet is bounded;
+// past the bound the scan sets *err and takes 0 for that tile.
+constexpr int kScanThreads = 256, kScanItems = 16, kScanTile = kScanThreads * kScanItems;
+constexpr unsigned kScanWaitLimit = 1u << 24;
+
+struct ScanState {
+  unsigned long long *tile;   // ceil(n / kScanTile) published words, zeroed before each scan
+  unsigned *ticket;           // tile ticket, zeroed before each scan
+  unsigned *err;
+};
+
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.volatile.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan(const int *in, int *out, int n, ScanState S) {
+  __shared__ int warp_sum[kScanThreads / 32];
+  __shared__ unsigned tile_s;
+  __shared__ long long excl_s;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) tile_s = atomicAdd(S.ticket, 1u);
+  __syncthreads();
+  const unsigned t = tile_s;
+  const long long base = (long long)t * kScanTile + (long long)threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = base + k < n ? in[base + k] : 0;
+    sum += v[k];
+  }
+  // block scan of the thread sums
+  int incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_sum[warp] = incl;
+  __syncthreads();
+  int wbase = 0, total = 0;
+#pragma unroll
+  for (int w = 0; w < kScanThreads / 32; ++w) {
+    wbase += w < warp ? warp_sum[w] : 0;
+    total += warp_sum[w];
+  }
+  if (threadIdx.x == 0) {
+    long long excl = 0;
+    if (t == 0) {
+      atomicExch(S.tile, (2ull << 62) | (unsigned long long)total);
+    } else {
+      atomicExch(S.tile + t, (1ull << 62) | (unsigned long long)total);
+      for (long long p = (long long)t - 1; p >= 0; --p) {
+        unsigned long long w = ld_volatile_u64(S.tile + p);
+        unsigned it = 0;
+        while ((w >> 62) == 0 && ++it < kScanWaitLimit) w = ld_volatile_u64(S.tile + p);
+        if ((w >> 62) == 0) { atomicOr(S.err, 1u); break; }
+        excl += (long long)(w & ((1ull << 62) - 1));
+        if ((w >> 62) == 2) break;
+      }
+      atomicExch(S.tile + t, (2ull << 62) | (unsigned long long)(excl + total));
+    }
+    excl_s = excl;
+  }
+  __syncthreads();
+  int run = (int)excl_s + wbase + incl - sum;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n) out[base + k] = run;
+    run += v[k];
+  }
+}
+
 __global__ void k_sort_finish(SimCounters *cnt, const int *offset, int ncell) {
   cnt->n_total = (unsigned long long)offset[ncell];
   cnt->n_births = 0;
@@ -1514,8 +1631,8 @@ __global__ void k_diag(State64 S64, State32 S32, SimCounters *cnt, double c, dou
 // trapezoid-weighted field energy (electricmagneticfield6.m:153-154),
 // per-block partial sums in a fixed order
 template <typename T>
-__global__ void k_field_energy(const T *Er, const T *Ez, const T *H, int nr, int nz, double dr,
-                               double dz, double *partial) {
+__global__ void k_field_energy(const T *Er, const T *Ez, const T *H, int nr, int nz, int ld,
+                               double dr, double dz, double *partial) {
   __shared__ double sh[kBlock];
   const int64_t nE = (int64_t)nr * (nz + 1), nZ = (int64_t)(nr + 1) * nz, nH = (int64_t)nr * nz;
   double acc[3] = {0, 0, 0};
@@ -1531,7 +1648,7 @@ __global__ void k_field_energy(const T *Er, const T *Ez, const T *H, int nr, int
     const int i = (int)(k % ncol), j = (int)(k / ncol);
     const double wi = (i == 0 || i == ncol - 1) ? 0.5 : 1.0;
     const double wj = (j == 0 || j == nrow - 1) ? 0.5 : 1.0;
-    const double v = (double)A[k];
+    const double v = (double)A[i + (int64_t)j * ld];
     acc[f] += wi * wj * v * v * (r0 + i * dr) * dr * dz;
   }
   for (int f = 0; f < 2; ++f) {
@@ -1560,6 +1677,18 @@ struct gasatt_sim {
   State32 s32[2]{};
   int cur = 0;
   void *Er = nullptr, *Ez = nullptr, *H = nullptr;
+  // field update of fdtd_ratio 1: tensor maps of the fields and of the
+  // current buffer the step reads (index = that buffer), patch rows, tiles
+  TmaMaps tmaps[2];
+  int tma_rows = 0, tma_tiles_x = 0, tma_ntiles = 0;
+  unsigned tma_grid = 0;
+  size_t tma_smem = 0;
+  // Internal grid layout: column-major like the reference's arrays, with row
+  // strides padded so that every row starts on a 16-byte boundary (the field
+  // update stages its tiles with TMA).  Er(i, j) at i + j ldf (j <= n_z),
+  // Ez(i, j) at i + j ldf (i <= n_r), H(i, j) at i + j ldf; currents
+  // J(i, j) at i + j ldj.  The padding stays zero.
+  int ldf = 0, ldj = 0;
   // current accumulators, double-buffered: the field update of step s reads
   // buffer s & 1 and clears the other one, which the pass of step s fills
   unsigned long long *Jr[2] = {nullptr, nullptr}, *Jz[2] = {nullptr, nullptr};
@@ -1568,8 +1697,9 @@ struct gasatt_sim {
   SimCounters *cnt = nullptr;
   SimCounters *h_cnt = nullptr;   // pinned
   int *cell_count = nullptr, *cell_offset = nullptr, *cell_cursor = nullptr;
-  void *scan_tmp = nullptr;
-  size_t scan_bytes = 0;
+  // the sort's scan: one published word per tile of counts, then the tile ticket
+  unsigned long long *scan_tiles = nullptr;
+  int scan_ntiles_max = 0;
   double *partial = nullptr;
   int partial_blocks = 0;
   std::vector<void *> allocs;
@@ -1611,6 +1741,9 @@ int sim_alloc(gasatt_sim *s, T **p, size_t n) {
 
 #define SIM_TRY(x) do { int rc__ = (x); if (rc__) return rc__; } while (0)
 
+// bytes of one current grid (n_z rows of ldj 64-bit counters)
+size_t jbytes(const gasatt_sim *s) { return (size_t)s->ldj * s->cfg.n_z * 8; }
+
 FdtdCoef fdtd_coef(const gasatt_sim *s) {
   const auto &c = s->cfg;
   const double dt = c.dt / c.fdtd_ratio, eps = c.eps0;
@@ -1628,22 +1761,40 @@ int launch_fdtd(gasatt_sim *s, cudaStream_t st, int q) {
   const auto &c = s->cfg;
   const int nr = c.n_r, nz = c.n_z, R = c.fdtd_ratio;
   const FdtdCoef fc = fdtd_coef(s);
-  const int tile = fdtd_tile(R);
-  const dim3 grid((nr + 1 + tile - 1) / tile, (nz + 1 + tile - 1) / tile);
-  const dim3 block(32, kFdtdRows);
   const double dt = c.dt / R;
   // the held ion current, in the electron current's fixed-point units
   const ExtraCurrent ion{s->Jir, s->Jiz, s->scale / s->ion_scale};
-  auto k64 = R == 1 ? k_sim_fdtd<double, true> : k_sim_fdtd<double, false>;
-  auto k32 = R == 1 ? k_sim_fdtd<float, true> : k_sim_fdtd<float, false>;
+  unsigned *err = &s->cnt->fdtd_err;
+  if (R == 1) {
+    const dim3 block(32, kTmaRows);
+    if (s->form == 0)
+      k_sim_fdtd_tma<double><<<s->tma_grid, block, s->tma_smem, st>>>(
+          s->tmaps[q], (double *)s->Er, (double *)s->Ez, (double *)s->H, s->Jr[1 - q], s->Jz[1 - q],
+          nr, nz, s->ldf, s->ldj, fc, s->invV, c.mu0, dt, c.flags, nullptr, ion, FieldQuads{},
+          s->tma_rows, s->tma_tiles_x, s->tma_ntiles, err);
+    else
+      k_sim_fdtd_tma<float><<<s->tma_grid, block, s->tma_smem, st>>>(
+          s->tmaps[q], (float *)s->Er, (float *)s->Ez, (float *)s->H, s->Jr[1 - q], s->Jz[1 - q],
+          nr, nz, s->ldf, s->ldj, fc, s->invV, c.mu0, dt, c.flags, s->cnt, ion, s->quads,
+          s->tma_rows, s->tma_tiles_x, s->tma_ntiles, err);
+    s->ctx->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(s->ctx, e, "fdtd launch");
+    return GASATT_OK;
+  }
+  const int tile = fdtd_tile(R);
+  const dim3 grid((nr + 1 + tile - 1) / tile, (nz + 1 + tile - 1) / tile);
+  const dim3 block(32, kFdtdRows);
+  auto k64 = k_sim_fdtd<double>;
+  auto k32 = k_sim_fdtd<float>;
   if (s->form == 0)
     k64<<<grid, block, 0, st>>>(
         (double *)s->Er, (double *)s->Ez, (double *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
-        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, nullptr, ion, FieldQuads{});
+        s->Jz[1 - q], nr, nz, s->ldf, s->ldj, fc, s->invV, c.mu0, dt, R, c.flags, nullptr, ion, FieldQuads{});
   else
     k32<<<grid, block, 0, st>>>(
         (float *)s->Er, (float *)s->Ez, (float *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
-        s->Jz[1 - q], nr, nz, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt, ion, s->quads);
+        s->Jz[1 - q], nr, nz, s->ldf, s->ldj, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt, ion, s->quads);
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "fdtd launch");
@@ -1710,27 +1861,38 @@ int flush_collisions(gasatt_sim *s) {
   return GASATT_OK;
 }
 
+// exclusive prefix sum of n counts (k_scan), its tile words and ticket cleared first
+int launch_scan(gasatt_sim *s, cudaStream_t st, const int *in, int *out, int n) {
+  const int ntiles = (n + kScanTile - 1) / kScanTile;
+  if (ntiles > s->scan_ntiles_max) return fail(s->ctx, GASATT_E_ARG, "scan longer than its tile words");
+  GASATT_CUDA(s->ctx, cudaMemsetAsync(s->scan_tiles, 0, ((size_t)ntiles + 1) * 8, st));
+  k_scan<<<ntiles, kScanThreads, 0, st>>>(
+      in, out, n, ScanState{s->scan_tiles, reinterpret_cast<unsigned *>(s->scan_tiles + ntiles), &s->cnt->scan_err});
+  s->ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(s->ctx, e, "scan launch");
+  return GASATT_OK;
+}
+
 // Ion push after step host_step when it completes a sub-cycle.  Collisions
 // still queued are applied first, so that the ions born in the step just
 // taken are pushed with the others.
 int launch_ion_push(gasatt_sim *s, cudaStream_t st) {
   SIM_TRY(flush_collisions(s));
   const auto &c = s->cfg;
-  const size_t nc = (size_t)c.n_r * c.n_z;
   const int nbin = (c.n_r + 1) * (c.n_z + 1);
   const unsigned g = grid_for(c.ion_capacity, kBlock) < s->pass_grid ? grid_for(c.ion_capacity, kBlock) : s->pass_grid;
   // sort the store into the scratch store (the electrons' sort buffers are free here)
   GASATT_CUDA(s->ctx, cudaMemsetAsync(s->cell_count, 0, (size_t)(nbin + 1) * 4, st));
   GASATT_CUDA(s->ctx, cudaMemsetAsync(s->cell_cursor, 0, (size_t)nbin * 4, st));
   k_ion_hist<<<g, kBlock, 0, st>>>(s->P.ion, s->cnt, c.ion_capacity, c.n_r, c.n_z, c.dr, c.dz, s->cell_count);
-  size_t nb = s->scan_bytes;
-  GASATT_CUDA(s->ctx, cub::DeviceScan::ExclusiveSum(s->scan_tmp, nb, s->cell_count, s->cell_offset, nbin + 1, st));
+  SIM_TRY(launch_scan(s, st, s->cell_count, s->cell_offset, nbin + 1));
   k_ion_scatter<<<g, kBlock, 0, st>>>(s->P.ion, s->ion_tmp, s->cnt, c.ion_capacity, c.n_r, c.n_z, c.dr,
                                       c.dz, s->cell_offset, s->cell_cursor);
   k_ion_sort_finish<<<1, 1, 0, st>>>(s->cnt, s->cell_offset, nbin);
-  s->ctx->launches += 4;
-  GASATT_CUDA(s->ctx, cudaMemsetAsync(s->Jir, 0, nc * 8, st));
-  GASATT_CUDA(s->ctx, cudaMemsetAsync(s->Jiz, 0, nc * 8, st));
+  s->ctx->launches += 3;
+  GASATT_CUDA(s->ctx, cudaMemsetAsync(s->Jir, 0, jbytes(s), st));
+  GASATT_CUDA(s->ctx, cudaMemsetAsync(s->Jiz, 0, jbytes(s), st));
   SimParams PI = s->P;
   PI.dt = c.dt * c.ion_subcycle;
   PI.qm_dt2 = c.q_e / c.m_ion * PI.dt / 2;
@@ -1762,9 +1924,7 @@ int launch_sort(gasatt_sim *s, cudaStream_t st, int from) {
   else
     k_sort_hist<1><<<g, kBlock, 0, st>>>(s->s64[from], s->s32[from], s->cnt, c.n_r, c.n_z, c.dr, c.dz, s->cell_count);
   s->ctx->launches++;
-  size_t nb = s->scan_bytes;
-  GASATT_CUDA(s->ctx, cub::DeviceScan::ExclusiveSum(s->scan_tmp, nb, s->cell_count, s->cell_offset, ncell + 1, st));
-  s->ctx->launches++;
+  SIM_TRY(launch_scan(s, st, s->cell_count, s->cell_offset, ncell + 1));
   if (s->form == 0)
     k_sort_scatter<0><<<g, kBlock, 0, st>>>(s->s64[from], s->s64[1 - from], s->s32[from], s->s32[1 - from],
                                             s->cnt, c.n_r, c.n_z, c.dr, c.dz, s->cell_offset, s->cell_cursor);
@@ -1803,12 +1963,12 @@ int sim_reset(gasatt_sim *s, int64_t n) {
   zc.cap = (unsigned long long)s->cfg.capacity;
   GASATT_CUDA(ctx, cudaMemcpyAsync(s->cnt, &zc, sizeof(zc), cudaMemcpyHostToDevice, st));
   for (int q = 0; q < 2; ++q) {
-    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
-    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr[q], 0, jbytes(s), st));
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz[q], 0, jbytes(s), st));
   }
   if (s->Jir) {                    // a new run: no ions, no ion current
-    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jir, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
-    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jiz, 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jir, 0, jbytes(s), st));
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jiz, 0, jbytes(s), st));
   }
   GASATT_CUDA(ctx, cudaStreamSynchronize(st));
   s->primed = false;
@@ -1830,6 +1990,75 @@ void set_collision_bound(gasatt_sim *s, double n_max) {
   while ((2.0 * (double)t + 1.0) * 0x1.0p-53 < P.P_null) ++t;
   while (t > 0 && !((2.0 * (double)(t - 1) + 1.0) * 0x1.0p-53 < P.P_null)) --t;
   P.cand_below = t;
+}
+
+// cuTensorMapEncodeTiled from the driver (looked up once)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// A 2D tensor map over a w x h grid of elements with row stride ld_bytes
+// (a multiple of 16), box bw x bh; out-of-bounds boxes fill with zeros.
+int encode_map(gasatt_sim *s, CUtensorMap *m, CUtensorMapDataType type, void *base, int w, int h,
+               size_t ld_bytes, int bw, int bh) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return fail(s->ctx, GASATT_E_CUDA, "cuTensorMapEncodeTiled not available from the driver");
+  const cuuint64_t dims[2] = {(cuuint64_t)w, (cuuint64_t)h};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld_bytes};
+  const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+  const cuuint32_t es[2] = {1, 1};
+  const CUresult r = enc(m, type, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return fail(s->ctx, GASATT_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return GASATT_OK;
+}
+
+// The field update of fdtd_ratio 1: patch rows, tiles, grid, shared memory
+// and the tensor maps of the fields and of both current buffers.
+template <typename T>
+int setup_fdtd_tma(gasatt_sim *s, int nsm) {
+  const auto &c = s->cfg;
+  int ph = c.fdtd_tile_rows > 0 ? c.fdtd_tile_rows : 48;
+  const int max_rows = sizeof(T) == 4 ? 64 : 48;
+  if (ph % kTmaRows || ph < 16 || ph > max_rows)
+    return fail(s->ctx, GASATT_E_ARG, "fdtd_tile_rows: a multiple of 16 in [16, " +
+                                          std::to_string(max_rows) + "]");
+  const TmaSmem<T> L(ph);
+  s->tma_rows = ph;
+  s->tma_smem = L.total();
+  s->tma_tiles_x = (c.n_r + 1 + kTmaTileW - 1) / kTmaTileW;
+  const int tiles_y = (c.n_z + 1 + (ph - 2 * kTmaHalo) - 1) / (ph - 2 * kTmaHalo);
+  s->tma_ntiles = s->tma_tiles_x * tiles_y;
+  GASATT_CUDA(s->ctx, cudaFuncSetAttribute(k_sim_fdtd_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)s->tma_smem));
+  int occ = 0;
+  GASATT_CUDA(s->ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sim_fdtd_tma<T>, 32 * kTmaRows,
+                                                                    s->tma_smem));
+  if (occ < 1) return fail(s->ctx, GASATT_E_ARG, "field update: patch does not fit in shared memory");
+  const long long slots = (long long)nsm * occ;
+  s->tma_grid = (unsigned)(slots < s->tma_ntiles ? slots : s->tma_ntiles);
+  const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const size_t ldb = (size_t)s->ldf * sizeof(T), ldjb = (size_t)s->ldj * 8;
+  const int bw = TmaBox<T>::w;
+  for (int q = 0; q < 2; ++q) {
+    TmaMaps &M = s->tmaps[q];
+    SIM_TRY(encode_map(s, &M.er, ft, s->Er, c.n_r, c.n_z + 1, ldb, bw, ph));
+    SIM_TRY(encode_map(s, &M.ez, ft, s->Ez, c.n_r + 1, c.n_z, ldb, bw, ph));
+    SIM_TRY(encode_map(s, &M.h, ft, s->H, c.n_r, c.n_z, ldb, bw, ph));
+    SIM_TRY(encode_map(s, &M.jr, CU_TENSOR_MAP_DATA_TYPE_INT64, s->Jr[q], c.n_r, c.n_z, ldjb, 34, ph));
+    SIM_TRY(encode_map(s, &M.jz, CU_TENSOR_MAP_DATA_TYPE_INT64, s->Jz[q], c.n_r, c.n_z, ldjb, 34, ph));
+  }
+  return GASATT_OK;
 }
 
 // device copies of P (current buffers 0 and 1) for the kernels that read it
@@ -1880,20 +2109,17 @@ int build_graphs(gasatt_sim *s) {
       GASATT_CUDA(s->ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
       if (s->form == 1) {
         // FP32: the field kernel commits the previous pass, the pass runs the
-        // previous step's collisions itself
+        // previous step's collisions itself.  Timing: one event before, one
+        // between and one after the two kernels (the pass's collisions have
+        // no kernel of their own)
         cudaError_t e = cudaSuccess;
         if (s->timing) e = cudaEventRecordWithFlags(s->ev[0], cs, cudaEventRecordExternal);
         if (e == cudaSuccess) rc = launch_fdtd(s, cs, q);
-        if (e == cudaSuccess && !rc && s->timing) {
+        if (e == cudaSuccess && !rc && s->timing)
           e = cudaEventRecordWithFlags(s->ev[1], cs, cudaEventRecordExternal);
-          if (e == cudaSuccess) e = cudaEventRecordWithFlags(s->ev[2], cs, cudaEventRecordExternal);
-        }
         if (e == cudaSuccess && !rc) rc = launch_pass(s, cs, 0, 1 - q, q);
-        if (e == cudaSuccess && !rc && s->timing) {
+        if (e == cudaSuccess && !rc && s->timing)
           e = cudaEventRecordWithFlags(s->ev[3], cs, cudaEventRecordExternal);
-          if (e == cudaSuccess) e = cudaEventRecordWithFlags(s->ev[4], cs, cudaEventRecordExternal);
-          if (e == cudaSuccess) e = cudaEventRecordWithFlags(s->ev[5], cs, cudaEventRecordExternal);
-        }
         cudaError_t e2 = cudaStreamEndCapture(cs, &g);
         if (!rc && e != cudaSuccess) rc = cuda_fail(s->ctx, e, "capture step");
         if (!rc && e2 != cudaSuccess) rc = cuda_fail(s->ctx, e2, "capture step");
@@ -1986,11 +2212,14 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   const gasatt_sim_config &c = *cfg;
   if (c.n_r < 2 || c.n_z < 2 || c.n_r > 65535 || c.n_z > 65535 ||
       (int64_t)(c.n_r + 1) * (c.n_z + 1) > 0x7FFFFFFFLL || !(c.dr > 0) || !(c.dz > 0) ||
-      !(c.dt > 0) || c.fdtd_ratio < 1 || c.capacity < 1 ||
+      !(c.dt > 0) || c.fdtd_ratio < 1 || c.capacity < 1 || c.capacity > 0x7FFFFFFFLL ||
       (c.precision != GASATT_FP64 && c.precision != GASATT_FP32_SPLIT))
     return fail(ctx, GASATT_E_ARG, "sim config out of range");
   if (c.flags & ~(unsigned)(GASATT_Q_ER_END_COPY | GASATT_Q_EZ_AXIS_JSIGN | GASATT_Q_EZ_RSHIFT))
     return fail(ctx, GASATT_E_ARG, "the resident simulation accepts only the field quirk flags");
+  if (c.pass_chunk < 0 || c.pass_chunk > kChunkMax || c.pass_chunk % kBlock)
+    return fail(ctx, GASATT_E_ARG, "pass_chunk: a multiple of 256 in [256, 1792] (0: 1792)");
+  if (c.fdtd_tile_rows < 0) return fail(ctx, GASATT_E_ARG, "fdtd_tile_rows: >= 0");
   if (c.ion_capacity < 0 || (c.ion_capacity > 0 && (c.ion_subcycle < 1 || !(c.m_ion > 0) ||
                                                      !(c.gas_temperature >= 0))))
     return fail(ctx, GASATT_E_ARG, "ion species: ion_capacity >= 0, ion_subcycle >= 1, m_ion > 0");
@@ -2004,7 +2233,10 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
                             c.m_e, c.q_e, s->tabs, err);
   if (rc) { delete s; return fail(ctx, rc, err); }
   const int64_t cap = c.capacity;
-  const int nr = c.n_r, nz = c.n_z, ncell = nr * nz, nbin = (nr + 1) * (nz + 1);
+  const int nr = c.n_r, nz = c.n_z, nbin = (nr + 1) * (nz + 1);
+  s->ldf = (nr + 1 + 3) & ~3;       // 16-byte rows for float and double
+  s->ldj = (nr + 1) & ~1;           // 16-byte rows of 64-bit counters
+  const size_t ncur = (size_t)s->ldj * nz;
   auto cleanup = [&](int code) { gasatt_sim_destroy(s); return code; };
   for (int b = 0; b < 2; ++b) {
     if (s->form == 0) {
@@ -2027,17 +2259,17 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
         (rc = sim_alloc(s, &I.q, ic)) || (rc = sim_alloc(s, &s->ion_tmp.rz, ic)) ||
         (rc = sim_alloc(s, &s->ion_tmp.urt, ic)) || (rc = sim_alloc(s, &s->ion_tmp.uz, ic)) ||
         (rc = sim_alloc(s, &s->ion_tmp.id, ic)) || (rc = sim_alloc(s, &s->ion_tmp.q, ic)) ||
-        (rc = sim_alloc(s, &s->Jir, (size_t)c.n_r * c.n_z)) ||
-        (rc = sim_alloc(s, &s->Jiz, (size_t)c.n_r * c.n_z)))
+        (rc = sim_alloc(s, &s->Jir, ncur)) || (rc = sim_alloc(s, &s->Jiz, ncur)))
       return cleanup(rc);
   }
   const size_t esz = s->form == 0 ? 8 : 4;
   double *tmpd;
-  if ((rc = sim_alloc(s, (char **)&s->Er, (size_t)nr * (nz + 1) * esz)) ||
-      (rc = sim_alloc(s, (char **)&s->Ez, (size_t)(nr + 1) * nz * esz)) ||
-      (rc = sim_alloc(s, (char **)&s->H, (size_t)nr * nz * esz)) ||
-      (rc = sim_alloc(s, &s->Jr[0], (size_t)ncell)) || (rc = sim_alloc(s, &s->Jz[0], (size_t)ncell)) ||
-      (rc = sim_alloc(s, &s->Jr[1], (size_t)ncell)) || (rc = sim_alloc(s, &s->Jz[1], (size_t)ncell)) ||
+  const size_t nfE = (size_t)s->ldf * (nz + 1), nfZ = (size_t)s->ldf * nz, nfH = (size_t)s->ldf * nz;
+  if ((rc = sim_alloc(s, (char **)&s->Er, nfE * esz)) ||
+      (rc = sim_alloc(s, (char **)&s->Ez, nfZ * esz)) ||
+      (rc = sim_alloc(s, (char **)&s->H, nfH * esz)) ||
+      (rc = sim_alloc(s, &s->Jr[0], ncur)) || (rc = sim_alloc(s, &s->Jz[0], ncur)) ||
+      (rc = sim_alloc(s, &s->Jr[1], ncur)) || (rc = sim_alloc(s, &s->Jz[1], ncur)) ||
       (rc = sim_alloc(s, &s->cnt, 1)) || (rc = sim_alloc(s, &s->cell_count, (size_t)nbin + 1)) ||
       (rc = sim_alloc(s, &s->cell_offset, (size_t)nbin + 1)) ||
       (rc = sim_alloc(s, &s->cell_cursor, (size_t)nbin)) ||
@@ -2054,8 +2286,8 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
     cudaMemset(s->quads.ez, 0, (size_t)nr * (nz + 1) * 16);
     cudaMemset(s->quads.h, 0, (size_t)(nr + 1) * (nz + 1) * 16);
   }
-  cub::DeviceScan::ExclusiveSum(nullptr, s->scan_bytes, s->cell_count, s->cell_offset, nbin + 1);
-  if ((rc = sim_alloc(s, (char **)&s->scan_tmp, s->scan_bytes))) return cleanup(rc);
+  s->scan_ntiles_max = (nbin + 1 + kScanTile - 1) / kScanTile;
+  if ((rc = sim_alloc(s, &s->scan_tiles, (size_t)s->scan_ntiles_max + 1))) return cleanup(rc);
   s->partial_blocks = 296;
   if ((rc = sim_alloc(s, &s->partial, (size_t)2 * s->partial_blocks))) return cleanup(rc);
   if (cudaMallocHost((void **)&s->h_cnt, sizeof(SimCounters)) != cudaSuccess)
@@ -2071,12 +2303,13 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
     return cleanup(fail(ctx, GASATT_E_CUDA, "table upload"));
   // parameters
   SimParams &P = s->P;
-  P.nr = nr; P.nz = nz; P.dr = c.dr; P.dz = c.dz; P.dt = c.dt; P.c = c.c; P.qe = c.q_e;
+  P.nr = nr; P.nz = nz; P.ldf = s->ldf; P.ldj = s->ldj; P.dr = c.dr; P.dz = c.dz; P.dt = c.dt; P.c = c.c; P.qe = c.q_e;
   P.me = c.m_e; P.mu0 = c.mu0; P.FN = c.FN; P.PHIp = c.PHIp; P.n_gas = c.gas_density;
   P.gas = nullptr;
   P.ion_sig = nullptr;
   P.Rp = nr * c.dr; P.Lp = nz * c.dz; P.kb = c.kb; P.m_ion = c.m_ion; P.T_gas = c.gas_temperature;
-  P.seed = c.seed; P.secondaries = c.secondaries; P.cap = cap;
+  P.chunk = c.pass_chunk > 0 ? c.pass_chunk : kChunkMax;
+  P.seed = c.seed; P.pk = philox_keys(c.seed); P.secondaries = c.secondaries; P.cap = cap;
   P.ion_cap = c.ion_capacity;
   P.ion_sigma = c.ion_capacity > 0 ? std::sqrt(c.kb * c.gas_temperature / c.m_ion) : 0.0;
   P.qm_dt2 = -c.q_e / c.m_e * c.dt / 2;
@@ -2112,6 +2345,10 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
     return cleanup(fail(ctx, GASATT_E_ARG, "fdtd_ratio too large for the fused field update (max 6)"));
   int dev = ctx->device, nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (c.fdtd_ratio == 1) {
+    if ((rc = s->form == 0 ? setup_fdtd_tma<double>(s, nsm) : setup_fdtd_tma<float>(s, nsm)))
+      return cleanup(rc);
+  }
   int occ = 4;
   if (s->form == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass64, kBlock, 0);
   else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass32, kBlock, 0);
@@ -2119,7 +2356,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   if (s->form == 1) {
     // FP32 blocks take chunks from a counter: no more blocks than chunks the
     // capacity can hold (small instances then leave the GPU to others)
-    const long long chunks = (cap + kChunk - 1) / kChunk;
+    const long long chunks = (cap + P.chunk - 1) / P.chunk;
     if ((long long)s->pass_grid > chunks) s->pass_grid = (unsigned)(chunks > 0 ? chunks : 1);
   }
   // as many collision warps as fit on the device at once
@@ -2133,16 +2370,16 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   z.cap = (unsigned long long)cap;
   if (cudaMemcpy(s->cnt, &z, sizeof(z), cudaMemcpyHostToDevice) != cudaSuccess)
     return cleanup(fail(ctx, GASATT_E_CUDA, "counter init"));
-  cudaMemset(s->Er, 0, (size_t)nr * (nz + 1) * esz);
-  cudaMemset(s->Ez, 0, (size_t)(nr + 1) * nz * esz);
-  cudaMemset(s->H, 0, (size_t)nr * nz * esz);
+  cudaMemset(s->Er, 0, nfE * esz);
+  cudaMemset(s->Ez, 0, nfZ * esz);
+  cudaMemset(s->H, 0, nfH * esz);
   for (int q = 0; q < 2; ++q) {
-    cudaMemset(s->Jr[q], 0, (size_t)ncell * 8);
-    cudaMemset(s->Jz[q], 0, (size_t)ncell * 8);
+    cudaMemset(s->Jr[q], 0, ncur * 8);
+    cudaMemset(s->Jz[q], 0, ncur * 8);
   }
   if (s->Jir) {
-    cudaMemset(s->Jir, 0, (size_t)ncell * 8);
-    cudaMemset(s->Jiz, 0, (size_t)ncell * 8);
+    cudaMemset(s->Jir, 0, ncur * 8);
+    cudaMemset(s->Jiz, 0, ncur * 8);
   }
   for (int i = 0; i < 6; ++i)
     if (cudaEventCreate(&s->ev[i]) != cudaSuccess) return cleanup(fail(ctx, GASATT_E_CUDA, "event"));
@@ -2393,9 +2630,8 @@ int gasatt_sim_load_ions(gasatt_sim *s, const double *r, const double *z, const 
   const unsigned long long zc[3] = {(unsigned long long)n, 0ull, 0ull};   // n_ions, overflow, lost
   GASATT_CUDA(ctx, cudaMemcpyAsync((char *)s->cnt + offsetof(SimCounters, n_ions), zc, sizeof(zc),
                                    cudaMemcpyHostToDevice, st));
-  const size_t nc = (size_t)s->cfg.n_r * s->cfg.n_z;
-  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jir, 0, nc * 8, st));
-  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jiz, 0, nc * 8, st));
+  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jir, 0, jbytes(s), st));
+  GASATT_CUDA(ctx, cudaMemsetAsync(s->Jiz, 0, jbytes(s), st));
   GASATT_CUDA(ctx, cudaStreamSynchronize(st));    // the host arrays zc and charge go out of scope
   return GASATT_OK;
 }
@@ -2446,72 +2682,99 @@ int gasatt_sim_read_ions(gasatt_sim *s, double *r, double *z, double *ur, double
 namespace {
 // the gather quads of whole float fields (after the fields are set from outside)
 __global__ void k_build_quads(const float *Er, const float *Ez, const float *H, int nr, int nz,
-                              FieldQuads q) {
+                              int ld, FieldQuads q) {
   const int64_t nE = (int64_t)nr * (nz + 1), nZ = (int64_t)(nr + 1) * nz, nH = (int64_t)nr * nz;
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nE + nZ + nH;
        k += (int64_t)gridDim.x * blockDim.x) {
     if (k < nE) {
       const int i = (int)(k % nr), j = (int)(k / nr);
-      quad_put(q.er, nr + 1, quad_axis_shifted(i, nr), quad_axis_plain(j, nz), Er[k]);
+      quad_put(q.er, nr + 1, quad_axis_shifted(i, nr), quad_axis_plain(j, nz), Er[i + (int64_t)j * ld]);
     } else if (k < nE + nZ) {
       const int64_t m = k - nE;
       const int i = (int)(m % (nr + 1)), j = (int)(m / (nr + 1));
-      quad_put(q.ez, nr, quad_axis_plain(i, nr), quad_axis_shifted(j, nz), Ez[m]);
+      quad_put(q.ez, nr, quad_axis_plain(i, nr), quad_axis_shifted(j, nz), Ez[i + (int64_t)j * ld]);
     } else {
       const int64_t m = k - nE - nZ;
       const int i = (int)(m % nr), j = (int)(m / nr);
-      quad_put(q.h, nr + 1, quad_axis_shifted(i, nr), quad_axis_shifted(j, nz), H[m]);
+      quad_put(q.h, nr + 1, quad_axis_shifted(i, nr), quad_axis_shifted(j, nz), H[i + (int64_t)j * ld]);
     }
   }
 }
 
-__global__ void k_f64_to_f32(const double *a, float *b, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    b[i] = (float)a[i];
+// dense column-major double (ncol x nrow, the reference's layout) <-> the
+// padded internal float layout (row stride ld)
+__global__ void k_dense_to_strided(const double *src, float *dst, int ncol, int nrow, int ld) {
+  const int64_t n = (int64_t)ncol * nrow;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(k % ncol), j = (int)(k / ncol);
+    dst[i + (int64_t)j * ld] = (float)src[k];
+  }
 }
-__global__ void k_f32_to_f64(const float *a, double *b, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    b[i] = (double)a[i];
+__global__ void k_strided_to_dense(const float *src, double *dst, int ncol, int nrow, int ld) {
+  const int64_t n = (int64_t)ncol * nrow;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(k % ncol), j = (int)(k / ncol);
+    dst[k] = (double)src[i + (int64_t)j * ld];
+  }
 }
-__global__ void k_j_to_density(const unsigned long long *J, int nr, int nz, double inv_scale,
-                               double dr, double dz, double PHIp, double *out) {
+__global__ void k_j_to_density(const unsigned long long *J, int nr, int nz, int ldj,
+                               double inv_scale, double dr, double dz, double PHIp, double *out) {
   const int64_t n = (int64_t)nr * nz;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = (double)(long long)J[i] * inv_scale / shell_volume((int)(i % nr), dr, dz, PHIp);
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(k % nr), j = (int)(k / nr);
+    out[k] = (double)(long long)J[i + (int64_t)j * ldj] * inv_scale / shell_volume(i, dr, dz, PHIp);
+  }
 }
 
 int fields_io(gasatt_sim *s, double *Er, double *Ez, double *H, int on_device, bool set) {
   gasatt_ctx *ctx = s->ctx;
   GASATT_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
-  const int nr = s->cfg.n_r, nz = s->cfg.n_z;
-  const int64_t n[3] = {(int64_t)nr * (nz + 1), (int64_t)(nr + 1) * nz, (int64_t)nr * nz};
+  const int nr = s->cfg.n_r, nz = s->cfg.n_z, ld = s->ldf;
+  const int ncol[3] = {nr, nr + 1, nr}, nrow[3] = {nz + 1, nz, nz};
   double *u[3] = {Er, Ez, H};
   void *dev[3] = {s->Er, s->Ez, s->H};
+  if (s->form == 0) {
+    // FP64: a pitched copy between the caller's dense array and the padded grid
+    for (int f = 0; f < 3; ++f) {
+      const size_t w = (size_t)ncol[f] * 8;
+      if (set)
+        GASATT_CUDA(ctx, cudaMemcpy2DAsync(dev[f], (size_t)ld * 8, u[f], w, w, nrow[f],
+                                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+      else
+        GASATT_CUDA(ctx, cudaMemcpy2DAsync(u[f], w, dev[f], (size_t)ld * 8, w, nrow[f],
+                                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    }
+    GASATT_CUDA(ctx, cudaStreamSynchronize(st));
+    return GASATT_OK;
+  }
+  // FP32: through a dense double stage on the device when the caller's
+  // arrays are host memory
   void *buf = nullptr;
-  if (!on_device || s->form == 1) {
-    int rc = scratch(ctx, (size_t)(n[0] + n[1] + n[2]) * 8, &buf);
+  if (!on_device) {
+    int rc = scratch(ctx, (size_t)((int64_t)ncol[0] * nrow[0] + (int64_t)ncol[1] * nrow[1] +
+                                   (int64_t)ncol[2] * nrow[2]) * 8, &buf);
     if (rc) return rc;
   }
   int64_t off = 0;
   for (int f = 0; f < 3; ++f) {
+    const int64_t n = (int64_t)ncol[f] * nrow[f];
     double *stage = on_device ? u[f] : (double *)buf + off;
     if (set) {
-      if (!on_device)
-        GASATT_CUDA(ctx, cudaMemcpyAsync(stage, u[f], n[f] * 8, cudaMemcpyHostToDevice, st));
-      if (s->form == 0) GASATT_CUDA(ctx, cudaMemcpyAsync(dev[f], stage, n[f] * 8, cudaMemcpyDeviceToDevice, st));
-      else { k_f64_to_f32<<<grid_for(n[f], kBlock), kBlock, 0, st>>>(stage, (float *)dev[f], n[f]); GASATT_LAUNCHED(ctx); }
+      if (!on_device) GASATT_CUDA(ctx, cudaMemcpyAsync(stage, u[f], n * 8, cudaMemcpyHostToDevice, st));
+      k_dense_to_strided<<<grid_for(n, kBlock), kBlock, 0, st>>>(stage, (float *)dev[f], ncol[f], nrow[f], ld);
+      GASATT_LAUNCHED(ctx);
     } else {
-      if (s->form == 0) GASATT_CUDA(ctx, cudaMemcpyAsync(stage, dev[f], n[f] * 8, cudaMemcpyDeviceToDevice, st));
-      else { k_f32_to_f64<<<grid_for(n[f], kBlock), kBlock, 0, st>>>((float *)dev[f], stage, n[f]); GASATT_LAUNCHED(ctx); }
-      if (!on_device)
-        GASATT_CUDA(ctx, cudaMemcpyAsync(u[f], stage, n[f] * 8, cudaMemcpyDeviceToHost, st));
+      k_strided_to_dense<<<grid_for(n, kBlock), kBlock, 0, st>>>((const float *)dev[f], stage, ncol[f], nrow[f], ld);
+      GASATT_LAUNCHED(ctx);
+      if (!on_device) GASATT_CUDA(ctx, cudaMemcpyAsync(u[f], stage, n * 8, cudaMemcpyDeviceToHost, st));
     }
-    off += n[f];
+    off += n;
   }
-  if (set && s->form == 1) {
-    k_build_quads<<<grid_for(n[0] + n[1] + n[2], kBlock), kBlock, 0, st>>>(
-        (const float *)s->Er, (const float *)s->Ez, (const float *)s->H, nr, nz, s->quads);
+  if (set) {
+    const int64_t n = (int64_t)nr * (nz + 1) + (int64_t)(nr + 1) * nz + (int64_t)nr * nz;
+    k_build_quads<<<grid_for(n, kBlock), kBlock, 0, st>>>(
+        (const float *)s->Er, (const float *)s->Ez, (const float *)s->H, nr, nz, ld, s->quads);
     GASATT_LAUNCHED(ctx);
   }
   GASATT_CUDA(ctx, cudaStreamSynchronize(st));
@@ -2547,8 +2810,8 @@ int gasatt_sim_get_current(gasatt_sim *s, double *jr, double *jz, int on_device)
   const int q = (int)(s->host_step & 1);   // buffer of the most recent deposit
   const unsigned long long *J[2] = {s->Jr[q], s->Jz[q]};
   for (int f = 0; f < 2; ++f) {
-    k_j_to_density<<<grid_for(n, kBlock), kBlock, 0, st>>>(J[f], nr, nz, 1.0 / s->scale, s->cfg.dr,
-                                                           s->cfg.dz, s->cfg.PHIp, d[f]);
+    k_j_to_density<<<grid_for(n, kBlock), kBlock, 0, st>>>(J[f], nr, nz, s->ldj, 1.0 / s->scale,
+                                                           s->cfg.dr, s->cfg.dz, s->cfg.PHIp, d[f]);
     GASATT_LAUNCHED(ctx);
   }
   if (!on_device) {
@@ -2609,9 +2872,9 @@ int gasatt_sim_diag(gasatt_sim *s, gasatt_diag *d) {
   }
   const int nr = s->cfg.n_r, nz = s->cfg.n_z;
   if (s->form == 0)
-    k_field_energy<double><<<s->partial_blocks, kBlock, 0, st>>>((double *)s->Er, (double *)s->Ez, (double *)s->H, nr, nz, s->cfg.dr, s->cfg.dz, s->partial);
+    k_field_energy<double><<<s->partial_blocks, kBlock, 0, st>>>((double *)s->Er, (double *)s->Ez, (double *)s->H, nr, nz, s->ldf, s->cfg.dr, s->cfg.dz, s->partial);
   else
-    k_field_energy<float><<<s->partial_blocks, kBlock, 0, st>>>((float *)s->Er, (float *)s->Ez, (float *)s->H, nr, nz, s->cfg.dr, s->cfg.dz, s->partial);
+    k_field_energy<float><<<s->partial_blocks, kBlock, 0, st>>>((float *)s->Er, (float *)s->Ez, (float *)s->H, nr, nz, s->ldf, s->cfg.dr, s->cfg.dz, s->partial);
   GASATT_LAUNCHED(ctx);
   std::vector<double> part(2 * s->partial_blocks);
   GASATT_CUDA(ctx, cudaMemcpyAsync(s->h_cnt, s->cnt, sizeof(SimCounters), cudaMemcpyDeviceToHost, st));
@@ -2631,7 +2894,8 @@ int gasatt_sim_diag(gasatt_sim *s, gasatt_diag *d) {
   d->kinetic_ev = (double)h.kin_fx / 65536.0;
   d->field_energy_j = s->cfg.PHIp * 0.5 * s->cfg.eps0 * we + s->cfg.PHIp * 0.5 * s->cfg.mu0 * wm;
   d->steps = s->host_step;
-  d->status_flags = (h.cap_overflow ? 2 : 0) | (h.ion_overflow ? 4 : 0);
+  d->status_flags = (h.cap_overflow ? 2 : 0) | (h.ion_overflow ? 4 : 0) |
+                    (h.fdtd_err || h.scan_err ? 8 : 0);
   d->n_ion_lost_wall = (int64_t)h.ion_lost;
   d->ion_kinetic_ev = (double)h.ion_kin_fx / 4294967296.0;
   d->net_charge_c = s->cfg.q_e * s->cfg.FN * ((double)h.ion_charge - (double)h.alive);
@@ -2671,8 +2935,13 @@ int gasatt_sim_last_timing(gasatt_sim *s, float *fdtd_ms, float *pass_ms, float 
   GASATT_CUDA(s->ctx, cudaEventSynchronize(s->ev[3]));
   float a = 0, b = 0, m = 0;
   GASATT_CUDA(s->ctx, cudaEventElapsedTime(&a, s->ev[0], s->ev[1]));
-  GASATT_CUDA(s->ctx, cudaEventElapsedTime(&b, s->ev[2], s->ev[3]));
-  GASATT_CUDA(s->ctx, cudaEventElapsedTime(&m, s->ev[4], s->ev[5]));
+  if (s->form == 1) {
+    // FP32: the pass runs the collisions itself; no separate collision kernel
+    GASATT_CUDA(s->ctx, cudaEventElapsedTime(&b, s->ev[1], s->ev[3]));
+  } else {
+    GASATT_CUDA(s->ctx, cudaEventElapsedTime(&b, s->ev[2], s->ev[3]));
+    GASATT_CUDA(s->ctx, cudaEventElapsedTime(&m, s->ev[4], s->ev[5]));
+  }
   if (fdtd_ms) *fdtd_ms = a;
   if (pass_ms) *pass_ms = b;
   if (mcc_ms) *mcc_ms = m;
@@ -2759,8 +3028,8 @@ int gasatt_sim_run_host(gasatt_sim *s, double *pos, double *vel, int64_t *n_io, 
   h.step += 1;                               // never reuse the last pass's step
   GASATT_CUDA(ctx, cudaMemcpyAsync(s->cnt, &h, sizeof(h), cudaMemcpyHostToDevice, st));
   for (int q = 0; q < 2; ++q) {
-    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
-    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz[q], 0, (size_t)s->cfg.n_r * s->cfg.n_z * 8, st));
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jr[q], 0, jbytes(s), st));
+    GASATT_CUDA(ctx, cudaMemsetAsync(s->Jz[q], 0, jbytes(s), st));
   }
   s->primed = false;
   s->mcc_pending = false;

@@ -4,7 +4,7 @@ import os
 
 import numpy as np
 
-from ._lib import Tables
+from .abi import Tables
 
 DATA = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "data",
                     "n2_tables.npz")

@@ -49,6 +49,7 @@
  *     mexcuda -R2018a gasatt_mex.c -I<repo>/include -L<repo>/gas-atenuator_b200 -lgasatt
  */
 #include <stdint.h>
+#include <math.h>
 #include <string.h>
 
 #include <cuda_runtime.h>
@@ -252,6 +253,14 @@ static void cmd_rebond(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[
   mxGPUDestroyGPUArray(phi.g); mxGPUDestroyGPUArray(vel.g);
 }
 
+/* particle_density's cell count: a positive integer, checked before MATLAB is
+   asked for the output gpuArray */
+static int64_t cell_count(const mxArray *a) {
+  const double v = scalar(a, "ncell");
+  if (!(v >= 1 && v <= 9.0e15) || v != floor(v)) fail("particle_density: ncell must be a positive integer");
+  return (int64_t)v;
+}
+
 /* the density of particles at (r, phi, z) on the sector cells; the variant
    without device allocation leaves MATLAB's pool alone when the grid fits it */
 static mxArray *density(const mxArray *dr, const mxArray *dz, const gpu_in *dphi,
@@ -260,7 +269,7 @@ static mxArray *density(const mxArray *dr, const mxArray *dz, const gpu_in *dphi
                         const mxArray *FN, const mxArray *ncell_a) {
   gpu_in sum_cell = gpu_copy(sum_cell_a, "sum_cell must be a double gpuArray");
   gpu_in VC = gpu_copy(VC_a, "VC must be a double gpuArray");
-  const int64_t ncell = (int64_t)scalar(ncell_a, "ncell");
+  const int64_t ncell = cell_count(ncell_a);
   double *d;
   mxGPUArray *g = gpu_new(ncell, 1, &d);
   check((ncell <= GASATT_DENSITY_NOALLOC_MAX_CELLS ? gasatt_particle_density_noalloc
@@ -274,6 +283,7 @@ static mxArray *density(const mxArray *dr, const mxArray *dz, const gpu_in *dphi
 static void cmd_particle_density(mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
   gpu_in dphi, r, phi, z;
   nargs(nrhs, 12, "particle_density(dr, dz, dphi, r, phi, z, cellnumxy, sum_cell, VC, FN, ncell)");
+  cell_count(prhs[11]);
   dphi = gpu_copy(prhs[3], "dphi must be a double gpuArray");
   r = gpu_copy(prhs[4], "r must be a double gpuArray");
   phi = gpu_copy(prhs[5], "phi must be a double gpuArray");
@@ -288,6 +298,7 @@ static void cmd_particle_density(mxArray *plhs[], int nrhs, const mxArray *prhs[
 static void cmd_particle_density0(mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
   gpu_in dphi, pos;
   nargs(nrhs, 10, "particle_density0(dr, dz, dphi, position, cellnumxy, sum_cell, VC, FN, ncell)");
+  cell_count(prhs[9]);
   dphi = gpu_copy(prhs[3], "dphi must be a double gpuArray");
   pos = gpu_copy(prhs[4], "position must be an n x 3 double gpuArray");
   if (pos.rows && pos.cols != 3) fail("particle_density0: position must be n x 3");

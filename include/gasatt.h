@@ -182,8 +182,11 @@ int gasatt_particle_density(gasatt_ctx *ctx, double dr, double dz,
  *  - Arguments and result are those of gasatt_particle_density.
  *  - ncell > GASATT_DENSITY_NOALLOC_MAX_CELLS is rejected with
  *    GASATT_E_CAPACITY (nothing is launched).
- *  - The first call on a device looks up the array's device address
- *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - Every call looks up the array's device address on the context's device
+ *    (cudaGetSymbolAddress), so the call stays valid after that device's
+ *    context is reset (the array then starts over, zeroed).  The first call
+ *    on a device also loads the library's device code there; make that first
+ *    call before any stream capture.
  *  - The counters are zeroed on the context's stream at the start of every
  *    call.  All calls on a device share the one array, so calls whose work
  *    overlaps on the GPU (other streams, other contexts, other host threads)
@@ -268,6 +271,12 @@ typedef struct gasatt_sim_config {
   int      table_n;         /* log-energy grid points (2048) */
   double   table_emin_ev, table_emax_ev;  /* 0.1 eV, 30 keV */
   int      ion_subcycle;    /* electron steps per ion push (50); the ion step is ion_subcycle*dt */
+  /* launch-shape knobs (results do not depend on them; 0 = the default, and
+   * the autotuner of the Python package picks them per workload): */
+  int      fdtd_tile_rows;  /* rows of the field update's TMA patch, a multiple of 16
+                               (16..64; the FP64 form at most 48); default 48 */
+  int      pass_chunk;      /* FP32 particle pass: particles per chunk a block takes,
+                               a multiple of 256 (256..1792); default 1792 */
 } gasatt_sim_config;
 
 typedef struct gasatt_diag {
@@ -280,7 +289,9 @@ typedef struct gasatt_diag {
   double  kinetic_ev;       /* sum of electron kinetic energy [eV] (x FN not applied) */
   double  field_energy_j;   /* electromagnetic field energy [J] */
   int64_t steps;            /* steps taken */
-  int32_t status_flags;     /* bit0 NaN seen, bit1 capacity overflow, bit2 ion capacity overflow */
+  int32_t status_flags;     /* bit0 NaN seen, bit1 capacity overflow, bit2 ion capacity overflow,
+                               bit3 a bounded device wait gave up (field-update tile copy or
+                               sort scan): the results since are not to be trusted */
   int64_t n_ion_lost_wall;  /* cumulative ions absorbed at r = Rp */
   double  ion_kinetic_ev;   /* sum of ion kinetic energy [eV] (x FN not applied) */
   double  net_charge_c;     /* charge of the macro-particles in the domain [C]:
@@ -384,9 +395,11 @@ int gasatt_sim_run_host(gasatt_sim *sim, double *pos, double *vel,
 int gasatt_sim_counts(gasatt_sim *sim, int64_t *n_slots, int64_t *n_ionizations,
                       int64_t *n_lost);
 /* device-side phase timing: with timing enabled the step graphs record CUDA
- * events around the field sub-cycle, the particle pass and the collision
- * branch (commit + collision kernel, which runs beside the field sub-cycle);
- * last_timing gives their durations in the most recent step (ms) */
+ * events around the field sub-cycle, the particle pass and (FP64 form) the
+ * collision branch (commit + collision kernel, which runs beside the field
+ * sub-cycle); last_timing gives their durations in the most recent step (ms).
+ * The FP32 split form runs the collisions inside its particle pass and
+ * reports mcc_ms = 0. */
 int gasatt_sim_enable_timing(gasatt_sim *sim, int enable);
 int gasatt_sim_last_timing(gasatt_sim *sim, float *fdtd_ms, float *pass_ms, float *mcc_ms);
 

@@ -1335,3 +1335,201 @@ const double *orc_xs_array(const orc_xs *xs, int which) {
     default: return xs->cdf;
   }
 }
+
+/* ========================================= the MATLAB CPU path (one call)
+ * electricmagneticfield3.m:111-319 restated for electrons.  Constants of that
+ * file (:4-11): m_e 9.1096e-31, c 3e8, eps 8.854187817e-12, mu 4 pi 1e-7,
+ * e 1.6e-19.  Its REBOND calls (:113, :303) pass (position, velocity, dt, r,
+ * z, phi), an older argument order than REBOND.m:1 declares; the restatement
+ * applies what both mean: the azimuth atan2(y, x) wrapped into [0, PHIp] one
+ * wedge at a time with (vx, vy) turned by the wedge angle and (x, y) rebuilt
+ * from r and the new azimuth (REBOND.m:7-46), then z reflected at Lp and at 0
+ * with vz flipped (REBOND.m:50-64). */
+static const double MC_ME = 9.1096e-31, MC_C = 3e8, MC_EPS = 8.854187817e-12, MC_E = 1.6e-19;
+#define MC_MU (4 * 3.141592653589793 * 1e-7)
+
+/* half drift, wall deletion (r > R), wedge and z rules of one electron */
+static void mcpu_drift(double *x, double *y, double *z, double *vx, double *vy, double vz_in,
+                       double *vz_out, uint8_t *alive, double h, double R, double Lp, double PHIp) {
+  double X = *x + h * *vx, Y = *y + h * *vy, Z = *z + h * vz_in, vz = vz_in;
+  const double r = sqrt(X * X + Y * Y);
+  if (r > R) { *alive = 0; return; }
+  double ph = atan2(Y, X), v1 = *vx, v2 = *vy;
+  const double cP = cos(PHIp), sP = sin(PHIp);
+  if (ph < 0) {
+    for (int k = 0; ph < 0 && k < 4096; ++k) {
+      ph += PHIp;
+      const double w = v1 * cP - v2 * sP;
+      v2 = v1 * sP + v2 * cP;
+      v1 = w;
+    }
+    X = r * cos(ph); Y = r * sin(ph);
+  }
+  if (ph > PHIp) {
+    for (int k = 0; ph > PHIp && k < 4096; ++k) {
+      ph -= PHIp;
+      const double w = v1 * cP + v2 * sP;
+      v2 = -v1 * sP + v2 * cP;
+      v1 = w;
+    }
+    X = r * cos(ph); Y = r * sin(ph);
+  }
+  if (Z > Lp) { Z = 2 * Lp - Z; vz = -vz; }
+  if (Z < 0) { Z = -Z; vz = -vz; }
+  *x = X; *y = Y; *z = Z; *vx = v1; *vy = v2; *vz_out = vz;
+}
+
+/* MATLAB round (half away from zero) */
+static inline double mround(double a) { return a < 0 ? -floor(-a + 0.5) : floor(a + 0.5); }
+
+/* One axis of interp2's grids: "padded" knots 0, d/2, 3d/2, ..., L - d/2, L
+ * (m cells; :221-223, :240-241) or "plain" knots 0, d, ..., m d.  Sets the
+ * lower knot k and the weight t of the upper one; 0 outside (interp2 gives
+ * NaN there). */
+static int mcpu_axis(double q, double d, int m, int padded, int *k, double *t) {
+  const double L = m * d;
+  if (!(q >= 0 && q <= L)) return 0;
+  if (!padded) {
+    int i = (int)floor(q / d);
+    if (i > m - 1) i = m - 1;
+    *k = i; *t = q / d - i;
+    return 1;
+  }
+  if (q <= d / 2) { *k = 0; *t = q / (d / 2); return 1; }
+  if (q >= L - d / 2) { *k = m; *t = (q - (L - d / 2)) / (d / 2); return 1; }
+  int i = (int)floor(q / d + 0.5);
+  if (i < 1) i = 1;
+  if (i > m - 1) i = m - 1;
+  *k = i; *t = q / d + 0.5 - i;
+  return 1;
+}
+
+/* value of interp2's extended grid of a field at knot (a, b) */
+typedef double (*mcpu_val)(const double *F, int nr, int nz, int a, int b);
+static double mc_er(const double *F, int nr, int nz, int a, int b) {   /* :224-228 */
+  if (a == nr + 1) return 0.0;
+  return F[(a == 0 ? 0 : a - 1) + (int64_t)b * nr];
+}
+static double mc_ez(const double *F, int nr, int nz, int a, int b) {   /* :232-236 */
+  if (b == 0 || b == nz + 1) return 0.0;
+  return F[a + (int64_t)(b - 1) * (nr + 1)];
+}
+static double mc_h(const double *F, int nr, int nz, int a, int b) {    /* :240-252 */
+  a = a < 1 ? 1 : (a > nr ? nr : a);
+  b = b < 1 ? 1 : (b > nz ? nz : b);
+  return F[(a - 1) + (int64_t)(b - 1) * nr];
+}
+static double mcpu_interp2(const double *F, mcpu_val val, int nr, int nz, int pr, int pz,
+                           double d, double r, double z) {
+  int a, b;
+  double tr, tz;
+  if (!mcpu_axis(r, d, nr, pr, &a, &tr) || !mcpu_axis(z, d, nz, pz, &b, &tz)) return NAN;
+  const double v00 = val(F, nr, nz, a, b), v10 = val(F, nr, nz, a + 1, b);
+  const double v01 = val(F, nr, nz, a, b + 1), v11 = val(F, nr, nz, a + 1, b + 1);
+  return (1 - tz) * ((1 - tr) * v00 + tr * v10) + tz * ((1 - tr) * v01 + tr * v11);
+}
+
+int64_t orc_mcpu_step(int64_t n, double *x, double *y, double *z, double *vx, double *vy,
+                      double *vz, uint8_t *alive, double *Er, double *Ez, double *H, double *jr,
+                      double *jz, int nr, int nz, double delta, double dt, double PHIp, double W) {
+  const double R = nr * delta, Lp = nz * delta, d = delta;
+  const int64_t ncell = (int64_t)nr * nz;
+  /* :111-116 half drift, deletion, REBOND */
+#pragma omp parallel for num_threads(g_threads) schedule(static)
+  for (int64_t p = 0; p < n; ++p)
+    if (alive[p]) mcpu_drift(&x[p], &y[p], &z[p], &vx[p], &vy[p], vz[p], &vz[p], &alive[p],
+                             0.5 * dt, R, Lp, PHIp);
+  /* :150-167 nearest-cell current (ind2vec), divided by W / shell volume */
+  memset(jr, 0, ncell * sizeof(double));
+  memset(jz, 0, ncell * sizeof(double));
+#pragma omp parallel for num_threads(g_threads) schedule(static)
+  for (int64_t p = 0; p < n; ++p) {
+    if (!alive[p]) continue;
+    const double r = sqrt(x[p] * x[p] + y[p] * y[p]);
+    const double vr = vx[p] * (x[p] / r) + vy[p] * (y[p] / r);
+    int ar = (int)mround(r / d + 0.5), az = (int)mround(z[p] / d + 0.5);
+    ar = ar < 1 ? 1 : (ar > nr ? nr : ar);
+    az = az < 1 ? 1 : (az > nz ? nz : az);
+    const int64_t c = (ar - 1) + (int64_t)(az - 1) * nr;
+    const double q = -MC_E;
+#pragma omp atomic
+    jr[c] += q * vr;
+#pragma omp atomic
+    jz[c] += q * vz[p];
+  }
+  for (int64_t c = 0; c < ncell; ++c) {
+    const double Rc = (c % nr + 0.5) * d;
+    const double V = PHIp * ((Rc + d / 2) * (Rc + d / 2) - (Rc - d / 2) * (Rc - d / 2)) * d;
+    jr[c] = W * jr[c] / V;
+    jz[c] = W * jz[c] / V;
+  }
+  /* :176-205 the field update: H(-dt/4), [H(dt/2), E(dt/2)] x 2, H(dt/4) */
+  const int repeat = 2;
+  const double dtr = dt / repeat;
+  const int ldr = nr, ldz = nr + 1;
+#define ER(i, j) Er[(i) + (int64_t)(j) * ldr]
+#define EZ(i, j) Ez[(i) + (int64_t)(j) * ldz]
+#define HH(i, j) H[(i) + (int64_t)(j) * ldr]
+#define JR(i, j) jr[(i) + (int64_t)(j) * ldr]
+#define JZ(i, j) jz[(i) + (int64_t)(j) * ldr]
+  double *er1 = malloc(sizeof(double) * nr), *ern = malloc(sizeof(double) * nr);
+  for (int sub = 0; sub <= 2 * repeat + 1; ++sub) {
+    /* sub 0: H(-dtr/2); odd: H(dtr) then E(dtr); last: H(dtr/2) */
+    const int last = sub == 2 * repeat + 1;
+    if (sub == 0 || last || (sub & 1)) {
+      const double h = sub == 0 ? -dtr / 2 : (last ? dtr / 2 : dtr);
+#pragma omp parallel for num_threads(g_threads) schedule(static)
+      for (int j = 0; j < nz; ++j)
+        for (int i = 0; i < nr; ++i)
+          HH(i, j) = HH(i, j) + h / (MC_MU * d) * (EZ(i + 1, j) - EZ(i, j)) -
+                     h / (MC_MU * d) * (ER(i, j + 1) - ER(i, j));
+    }
+    if (!(sub & 1) || sub == 0 || last) continue;
+    for (int i = 0; i < nr; ++i) { er1[i] = ER(i, 1); ern[i] = ER(i, nz - 1); }
+#pragma omp parallel for num_threads(g_threads) schedule(static)
+    for (int j = 1; j < nz; ++j)
+      for (int i = 0; i < nr; ++i)
+        ER(i, j) = ER(i, j) - dtr / MC_EPS * (JR(i, j - 1) + JR(i, j)) / 2 -
+                   dtr / (MC_EPS * d) * (HH(i, j) - HH(i, j - 1));
+#pragma omp parallel for num_threads(g_threads) schedule(static)
+    for (int j = 0; j < nz; ++j) {
+      for (int i = 1; i < nr; ++i) {
+        const double ri = i * d;
+        EZ(i, j) = EZ(i, j) - dtr / MC_EPS * (JZ(i - 1, j) + JZ(i, j)) / 2 +
+                   dtr / MC_EPS * (1 / (2 * ri) + 1 / d) * HH(i, j) +
+                   dtr / MC_EPS * (1 / (2 * ri) - 1 / d) * HH(i - 1, j);
+      }
+      EZ(0, j) = EZ(0, j) + dtr / MC_EPS * JZ(0, j) + 4 * dtr / (MC_EPS * d) * HH(0, j);
+    }
+    for (int i = 0; i < nr; ++i) { ER(i, 0) = er1[i]; ER(i, nz) = ern[i]; }
+  }
+  free(er1);
+  free(ern);
+#undef ER
+#undef EZ
+#undef HH
+#undef JR
+#undef JZ
+  /* :216-281 interp2 gather, explicit kick; :285-319 second half drift */
+  int64_t left = 0;
+#pragma omp parallel for num_threads(g_threads) schedule(static) reduction(+ : left)
+  for (int64_t p = 0; p < n; ++p) {
+    if (!alive[p]) continue;
+    const double r = sqrt(x[p] * x[p] + y[p] * y[p]);
+    const double cs = x[p] / r, sn = y[p] / r;
+    const double vr = vx[p] * cs + vy[p] * sn;
+    const double e_r = mcpu_interp2(Er, mc_er, nr, nz, 1, 0, d, r, z[p]);
+    const double e_z = mcpu_interp2(Ez, mc_ez, nr, nz, 0, 1, d, r, z[p]);
+    const double h = mcpu_interp2(H, mc_h, nr, nz, 1, 1, d, r, z[p]);
+    const double q = -MC_E;
+    const double Fr = q * (e_r + (-vz[p] * h * MC_MU)), Fz = q * (e_z + (vr * h * MC_MU));
+    const double g = 1 / sqrt(1 - (vx[p] * vx[p] + vy[p] * vy[p] + vz[p] * vz[p]) / (MC_C * MC_C));
+    const double ux = g * vx[p] + Fr * cs / MC_ME * dt, uy = g * vy[p] + Fr * sn / MC_ME * dt;
+    const double uz = g * vz[p] + Fz / MC_ME * dt;
+    const double g2 = sqrt(1 + (ux * ux + uy * uy + uz * uz) / (MC_C * MC_C));
+    vx[p] = ux / g2; vy[p] = uy / g2; vz[p] = uz / g2;
+    mcpu_drift(&x[p], &y[p], &z[p], &vx[p], &vy[p], vz[p], &vz[p], &alive[p], 0.5 * dt, R, Lp, PHIp);
+    left += alive[p];
+  }
+  return left;
+}

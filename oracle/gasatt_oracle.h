@@ -162,6 +162,20 @@ void orc_sim_fdtd(const gasatt_sim_config *cfg, double *Er, double *Ez, double *
 double orc_field_energy(const gasatt_sim_config *cfg, const double *Er, const double *Ez,
                         const double *H);
 
+/* The reference's MATLAB CPU path, one call of electricmagneticfield3.m:111-319
+ * for electrons (charge -e, mass m_e of that file): half drift, deletion
+ * beyond the wall and the wedge/z rules (REBOND), nearest-cell current
+ * (ind2vec), the field update in two halves, interp2 gather, explicit
+ * relativistic kick, second half drift with the same rules.  Particles are
+ * (x, y, z) and v (not gamma v); deleted ones get alive = 0 instead of being
+ * removed.  Grids dense column-major: Er n_r x (n_z+1), Ez (n_r+1) x n_z,
+ * H n_r x n_z; jr, jz (n_r x n_z) receive the step's current density.
+ * delta: cell size, dt: particle step, PHIp: wedge angle, W: particles per
+ * macro-particle.  Returns the electrons alive afterwards. */
+int64_t orc_mcpu_step(int64_t n, double *x, double *y, double *z, double *vx, double *vy,
+                      double *vz, uint8_t *alive, double *Er, double *Ez, double *H, double *jr,
+                      double *jz, int nr, int nz, double delta, double dt, double PHIp, double W);
+
 #ifdef __cplusplus
 }
 #endif

@@ -206,6 +206,36 @@ def electron_collision(e_pos, e_vel, i1_pos, i1_vel, tab, kin, sum_cell, cellnum
     return E[:ne.value], EV[:ne.value], I[:ni.value], IV[:ni.value]
 
 
+# ------------------------------------------------ the MATLAB CPU path
+class MatlabCpuPath:
+    """electricmagneticfield3.m:111-319 (the reference's CPU push, deposit and
+    field update) for electrons, one call per step (orc_mcpu_step).  Particles
+    are Cartesian positions and velocities v; the grids are the reference's
+    dense column-major arrays."""
+
+    def __init__(self, nr, nz, delta, dt, PHIp=2 * np.pi, W=1.0):
+        self.nr, self.nz, self.delta, self.dt, self.PHIp, self.W = nr, nz, delta, dt, PHIp, W
+        self.Er = np.zeros((nr, nz + 1), order="F")
+        self.Ez = np.zeros((nr + 1, nz), order="F")
+        self.H = np.zeros((nr, nz), order="F")
+        self.jr = np.zeros((nr, nz), order="F")
+        self.jz = np.zeros((nr, nz), order="F")
+        self.n = 0
+
+    def load(self, x, y, z, vx, vy, vz):
+        self.x, self.y, self.z = (np.array(a, dtype=np.float64) for a in (x, y, z))
+        self.vx, self.vy, self.vz = (np.array(a, dtype=np.float64) for a in (vx, vy, vz))
+        self.n = len(self.x)
+        self.alive = np.ones(self.n, np.uint8)
+
+    def step(self):
+        lib.orc_mcpu_step.restype = c_i64
+        return lib.orc_mcpu_step(c_i64(self.n), P(self.x), P(self.y), P(self.z), P(self.vx),
+                                 P(self.vy), P(self.vz), P(self.alive), P(self.Er), P(self.Ez),
+                                 P(self.H), P(self.jr), P(self.jz), c_i(self.nr), c_i(self.nz),
+                                 c_d(self.delta), c_d(self.dt), c_d(self.PHIp), c_d(self.W))
+
+
 # ------------------------------------------------------------ resident step
 class OrcIons(ctypes.Structure):
     _fields_ = [("x", c_p), ("y", c_p), ("z", c_p), ("ux", c_p), ("uy", c_p), ("uz", c_p),

@@ -48,3 +48,33 @@ def test_product_path_never_imports_oracle():
             if f.endswith((".py", ".cu", ".cuh", ".cpp", ".h")):
                 txt = open(os.path.join(dirpath, f), errors="ignore").read()
                 assert "pyoracle" not in txt and "liboracle" not in txt and "orc_" not in txt, f
+
+
+def test_python_default_config_matches_the_library():
+    """gasatt.abi.default_config restates gasatt_sim_default_config (host
+    code, callable without a device) field by field."""
+    from gasatt import _lib
+    from gasatt.abi import default_config
+    want = _lib.SimConfig()
+    assert _lib.lib.gasatt_sim_default_config(ctypes.byref(want)) == _lib.OK
+    got = default_config()
+    for name, _ in _lib.SimConfig._fields_:
+        assert getattr(got, name) == getattr(want, name), name
+
+
+def test_workload_builders_load_no_library():
+    """The workload builders (births, configs, tables) and the CPU oracle are
+    importable without libgasatt.so being mapped: the CPU reference arm of
+    bench.py builds its inputs this way."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path[:0] = [%r, %r]\n"
+            "import gasatt.workload, gasatt.tables, gasatt.abi, pyoracle\n"
+            "cfg = gasatt.workload.config(16, 32, 5e-6, 1e-14, 1.0)\n"
+            "p = gasatt.workload.births(10, 8.0, 32 * 5e-6, seed=1)\n"
+            "o = pyoracle.Sim(cfg, gasatt.tables.N2Tables(), cap=64)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libgasatt' not in maps, 'libgasatt.so mapped'\n"
+            "assert 'gasatt._lib' not in sys.modules\n"
+            % (os.path.join(ROOT, "gas-atenuator_b200"), os.path.join(ROOT, "oracle")))
+    subprocess.run([sys.executable, "-c", code], check=True)

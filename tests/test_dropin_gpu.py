@@ -80,7 +80,7 @@ def test_electricmagneticfield6(name, flags):
     names = ["e_pos", "e_vel", "i1_pos", "i1_vel", "i2_pos", "i2_vel", "Er", "Ez", "Hphi", "kin"]
     assert len(np_(got[0])) == len(want[0]) < 3000       # wall losses happened, same survivors
     for g, w, k in zip(got, want, names):
-        close(np_(g), w, 1e-10, k)
+        close(np_(g), w, 1e-12, k)
 
 
 def collision_inputs(seed, n=5000, PHIp=0.1, Rp=1e-2, rmax=20, zmax=5, Lp=0.05):
@@ -120,7 +120,7 @@ def test_electron_collision(tables, name, flags):
                                 se, si, sx, 2e-10, cs["draws"], flags)
     assert len(np_(got[0])) == len(want[0]) > 5000 + 100     # secondaries appended
     assert len(np_(got[2])) == len(want[2]) == len(want[0]) - 5000 + 7
-    rtol = 1e-6 if flags & _lib.Q_EXC_POWF else 1e-11
+    rtol = 1e-6 if flags & _lib.Q_EXC_POWF else 1e-12
     for g, w, k in zip(got, want, ("e_pos", "e_vel", "i_pos", "i_vel")):
         close(np_(g), w, rtol, k)
 

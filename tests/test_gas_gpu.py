@@ -81,13 +81,13 @@ def test_fp64_graded_density_matches_oracle(tables, switch_at):
     have = by_id(got["id"][g_alive], got["r"][g_alive], got["z"][g_alive], got["ur"][g_alive],
                  got["ut"][g_alive], got["uz"][g_alive])
     for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
-        close(h, w, 1e-10, k)
+        close(h, w, 1e-12, k)
     d = sim.diag()
     ion, ela, exc, nul, lost, ovf = orc.counters
     assert (d["n_ionizations"], d["n_elastic"], d["n_excitation"], d["n_null"]) == (ion, ela, exc, nul)
     assert ion > 10 and ela > 10
     jr, jz = sim.current()
-    close(jr, orc.jr, 1e-10, "jr"); close(jz, orc.jz, 1e-10, "jz")
+    close(jr, orc.jr, 1e-12, "jr"); close(jz, orc.jz, 1e-12, "jz")
     # the graded run differs from the uniform one (the map is really used)
     uni = oracle_run(cfg, tables, parts, flds, steps)
     assert tuple(uni.counters[:4]) != (ion, ela, exc, nul)

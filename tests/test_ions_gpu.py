@@ -68,7 +68,7 @@ def test_fp64_ions_match_oracle(tables):
     assert hset == set(ids[a].tolist())
     want = by_id(ids[a], r[a], z[a], ur[a], ut[a], uz[a])
     for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
-        close(h, w, 1e-10, "ion " + k)
+        close(h, w, 1e-12, "ion " + k)
     assert np.all(gi["charge"] == 1)
     # electrons and fields (the held ion current enters the field update)
     ge = sim.read()
@@ -78,9 +78,9 @@ def test_fp64_ions_match_oracle(tables):
     assert hset == set(ids[a].tolist())
     want = by_id(ids[a], r[a], z[a], ur[a], ut[a], uz[a])
     for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
-        close(h, w, 1e-10, k)
+        close(h, w, 1e-12, k)
     Er, Ez, H = sim.fields()
-    close(Er, orc.Er, 1e-10, "Er"); close(Ez, orc.Ez, 1e-10, "Ez"); close(H, orc.H, 1e-10, "H")
+    close(Er, orc.Er, 1e-12, "Er"); close(Ez, orc.Ez, 1e-12, "Ez"); close(H, orc.H, 1e-12, "H")
 
 
 @pytest.mark.parametrize("precision", [_lib.FP64, _lib.FP32_SPLIT])
@@ -106,7 +106,7 @@ def test_ion_current_drives_the_fields_like_the_oracle(tables, precision):
     orc.prologue()
     for _ in range(steps):
         orc.step()
-    tol = 1e-10 if precision == _lib.FP64 else 1e-5
+    tol = 1e-12 if precision == _lib.FP64 else 1e-5
     Er, Ez, H = sim.fields()
     assert np.abs(orc.Ez).max() > 0
     close(Er, orc.Er, tol, "Er"); close(Ez, orc.Ez, tol, "Ez"); close(H, orc.H, tol, "H")
@@ -118,7 +118,7 @@ def test_ion_current_drives_the_fields_like_the_oracle(tables, precision):
     assert hset == set(ids[a].tolist())
     want = by_id(ids[a], r[a], z[a], ur[a], ut[a], uz[a])
     for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
-        close(h, w, 1e-10 if precision == _lib.FP64 else 1e-6, "ion " + k)
+        close(h, w, 1e-12 if precision == _lib.FP64 else 1e-6, "ion " + k)
 
 
 @pytest.mark.parametrize("precision", [_lib.FP64, _lib.FP32_SPLIT])
@@ -288,7 +288,7 @@ def test_gas_temperature_map_sets_the_newborn_ions_spread(tables):
     have, _ = alive_by_id(gi)
     want = by_id(ids, r, z, ur, ut, uz)
     for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
-        close(h, w, 1e-10, "ion " + k)
+        close(h, w, 1e-12, "ion " + k)
     hot = gi["z"] >= NZ // 2 * D
     s_hot, s_cold = gi["uz"][hot].std(), gi["uz"][~hot].std()
     assert hot.sum() > 100 and (~hot).sum() > 100

@@ -120,6 +120,16 @@ def test_gateway_turns_bad_calls_into_matlab_errors(mex, tables):
     register_tables(mex, tables)                          # host-only: works without a GPU
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("ncell", [0.0, -3.0, 2.5])
+def test_gateway_rejects_a_bad_cell_count_before_allocating(mex, ncell):
+    """particle_density's ncell is checked before the gateway asks MATLAB for
+    the output gpuArray."""
+    g = Gpu([1.0])
+    with pytest.raises(MexError, match="ncell must be a positive integer"):
+        mex.call(1, "particle_density", 1.0, 1.0, g, g, g, g, 1.0, g, g, 1.0, ncell)
+
+
 @pytest.mark.skipif(has_gpu(), reason="checks the error path of a machine without a GPU")
 def test_gateway_reports_a_missing_gpu(mex, tables):
     register_tables(mex, tables)

@@ -63,7 +63,7 @@ def test_fp64_matches_oracle(tables, steps):
     have = by_id(got["id"][g_alive], got["r"][g_alive], got["z"][g_alive], got["ur"][g_alive],
                  got["ut"][g_alive], got["uz"][g_alive])
     for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
-        close(h, w, 1e-10, k)
+        close(h, w, 1e-12, k)
     d = sim.diag()
     ion, ela, exc, nul, lost, ovf = orc.counters
     assert (d["n_ionizations"], d["n_elastic"], d["n_excitation"], d["n_null"]) == (ion, ela, exc, nul)
@@ -71,16 +71,16 @@ def test_fp64_matches_oracle(tables, steps):
     if steps > 1:
         assert ion > 10 and ela > 10 and exc > 10
     Er, Ez, H = sim.fields()
-    close(Er, orc.Er, 1e-10, "Er"); close(Ez, orc.Ez, 1e-10, "Ez"); close(H, orc.H, 1e-10, "H")
+    close(Er, orc.Er, 1e-12, "Er"); close(Ez, orc.Ez, 1e-12, "Ez"); close(H, orc.H, 1e-12, "H")
     jr, jz = sim.current()
-    close(jr, orc.jr, 1e-10, "jr"); close(jz, orc.jz, 1e-10, "jz")
+    close(jr, orc.jr, 1e-12, "jr"); close(jz, orc.jz, 1e-12, "jz")
 
 
 def test_fp64_field_energy_diag_matches_oracle(tables):
     cfg, sim, parts, flds = start(_lib.FP64)
     sim.step(2)
     orc = oracle_run(cfg, tables, parts, flds, 2)
-    close(sim.diag()["field_energy_j"], orc.field_energy(), 1e-10, "field energy")
+    close(sim.diag()["field_energy_j"], orc.field_energy(), 1e-12, "field energy")
 
 
 @pytest.mark.parametrize("precision", [_lib.FP64, _lib.FP32_SPLIT])
@@ -146,12 +146,12 @@ def test_fp64_matches_oracle_multi_window(tables):
     want = by_id(oid[a], rr[a], zz[a], urr[a], utt[a], uzz[a])
     have = by_id(got["id"][ga], got["r"][ga], got["z"][ga], got["ur"][ga], got["ut"][ga], got["uz"][ga])
     for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
-        close(h, w, 1e-10, k)
+        close(h, w, 1e-12, k)
     jr, jz = sim.current()
-    close(jr, orc.jr, 1e-10, "jr"); close(jz, orc.jz, 1e-10, "jz")
+    close(jr, orc.jr, 1e-12, "jr"); close(jz, orc.jz, 1e-12, "jz")
     f = sim.fields()
     for g, w, k in zip(f, (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
-        close(g, w, 1e-10, k)
+        close(g, w, 1e-12, k)
     d = sim.diag()
     assert (d["n_ionizations"], d["n_elastic"], d["n_excitation"]) == tuple(orc.counters[:3])
 
@@ -227,24 +227,44 @@ def test_free_drift_keeps_kinetic_energy(precision, tol):
     assert abs(d["kinetic_ev"] / e0 - 1) < tol, d["kinetic_ev"] / e0 - 1
 
 
-def test_c1_full_size_fp64_matches_oracle(tables):
-    """The reference's CPU-runnable case at full size (20,000 electrons, 64 x
-    256 cells at 10 um, 1 Torr, dt 2e-14 s) for 500 steps: the FP64 form and
-    the oracle keep the same population and event counts, and agree to 1e-10."""
-    nr, nz, d = 64, 256, 10e-6
-    cfg = config(nr, nz, d, 2e-14, 1.0, precision=_lib.FP64, capacity=200_000, seed=0,
-                 sort_period=30)
-    parts = births(10_000, 8.0, nz * d, seed=0, Rp=nr * d)
-    sim = Sim(cfg)
-    sim.load(*parts)
-    sim.step(500)
-    got = sim.read()
+C1 = dict(nr=64, nz=256, d=10e-6, dt=2e-14, torr=1.0, photo=10_000, steps=500, seed=0)
+
+
+def c1_cfg(precision):
+    return config(C1["nr"], C1["nz"], C1["d"], C1["dt"], C1["torr"], precision=precision,
+                  capacity=200_000, seed=C1["seed"], sort_period=30)
+
+
+@pytest.fixture(scope="module")
+def c1_oracle(tables):
+    """The oracle's run of the reference's CPU-runnable case at full size:
+    20,000 electrons (10,000 photoionizations at 8 keV), 64 x 256 cells at
+    10 um, 1 Torr, dt 2e-14 s, 500 steps."""
+    cfg = c1_cfg(_lib.FP64)
+    parts = births(C1["photo"], 8.0, C1["nz"] * C1["d"], seed=C1["seed"], Rp=C1["nr"] * C1["d"])
     orc = O.Sim(cfg, tables, cap=cfg.capacity)
     orc.load(*parts)
     orc.prologue()
-    for _ in range(500):
+    for _ in range(C1["steps"]):
         orc.step()
-    dg = sim.diag()
+    return parts, orc
+
+
+def c1_gpu(precision, parts):
+    sim = Sim(c1_cfg(precision))
+    sim.load(*parts)
+    sim.step(C1["steps"])
+    out = (sim.read(), sim.fields(), sim.diag())
+    sim.close()
+    return out
+
+
+def test_c1_full_size_fp64_matches_oracle(c1_oracle):
+    """C1 at full size for 500 steps: the FP64 form and the oracle keep the
+    same population and event counts, and agree to 1e-12 (particles: max
+    |a - b| / max |b| per component; fields likewise)."""
+    parts, orc = c1_oracle
+    got, flds, dg = c1_gpu(_lib.FP64, parts)
     ion, ela, exc, nul, lost, ovf = orc.counters
     assert (dg["n_ionizations"], dg["n_elastic"], dg["n_excitation"], dg["n_null"],
             dg["n_lost_wall"]) == (ion, ela, exc, nul, lost)
@@ -257,9 +277,43 @@ def test_c1_full_size_fp64_matches_oracle(tables):
     have = by_id(got["id"][ga], got["r"][ga], got["z"][ga], got["ur"][ga], got["ut"][ga],
                  got["uz"][ga])
     for h, w, k in zip(have, want, ("r", "z", "ur", "ut", "uz")):
-        close(h, w, 1e-10, k)
-    for g, w, k in zip(sim.fields(), (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
-        close(g, w, 1e-10, k)
+        close(h, w, 1e-12, k)
+    for g, w, k in zip(flds, (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
+        close(g, w, 1e-12, k)
+
+
+def test_c1_full_size_fp32_product_against_oracle(c1_oracle):
+    """The FP32 split form (the product) against the FP64 oracle directly, C1
+    at full size for 500 steps: ionization yield within 0.5%, fields within
+    1e-4 (||F32 - F64||_2 / ||F64||_2, worst of Er, Ez, H; the max-abs form
+    within 1e-3), and the electron energy distribution (40 log bins from 0.1
+    eV to 10 keV) and the mean energy within 3 sigma of their Monte Carlo
+    error."""
+    parts, orc = c1_oracle
+    got, flds, dg = c1_gpu(_lib.FP32_SPLIT, parts)
+    ion = int(orc.counters[0])
+    assert ion > 500
+    assert abs(dg["n_ionizations"] - ion) <= 0.005 * ion, (dg["n_ionizations"], ion)
+    for g, w, k in zip(flds, (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
+        assert np.linalg.norm(g - w) <= 1e-4 * np.linalg.norm(w), k
+        close(g, w, 1e-3, k)
+    me, c, qe = 9.1093837015e-31, 299792458.0, 1.602176634e-19
+
+    def energies(ur, ut, uz):
+        u2 = (ur ** 2 + ut ** 2 + uz ** 2) / c ** 2
+        return me * c * c * (u2 / (np.sqrt(1 + u2) + 1)) / qe
+
+    r, z, ur, ut, uz, ids, alive = orc.state_rz()
+    a = alive.astype(bool)
+    ga = got["r"] >= 0
+    E64 = energies(ur[a], ut[a], uz[a])
+    E32 = energies(got["ur"][ga], got["ut"][ga], got["uz"][ga])
+    assert abs(len(E32) - len(E64)) <= 0.005 * len(E64)
+    bins = np.logspace(-1, 4, 41)
+    h64, _ = np.histogram(E64, bins)
+    h32, _ = np.histogram(E32, bins)
+    assert np.all(np.abs(h32 - h64) <= 3 * np.sqrt(h64 + 1) + 1)
+    assert abs(E32.mean() - E64.mean()) <= 3 * E64.std() / np.sqrt(len(E64))
 
 
 def test_fp32_energy_distribution_within_3_sigma_of_fp64():
@@ -310,7 +364,7 @@ def test_field_subcycle_ratio_matches_oracle(tables, ratio):
     f64, d64, cfg, parts, flds = out[_lib.FP64]
     orc = oracle_run(cfg, tables, parts, flds, 4)
     for g, w, k in zip(f64, (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
-        close(g, w, 1e-10, k)
+        close(g, w, 1e-12, k)
     assert d64["n_ionizations"] == orc.counters[0]
     f32, d32 = out[_lib.FP32_SPLIT][:2]
     for g, w, k in zip(f32, f64, ("Er", "Ez", "H")):
@@ -344,7 +398,7 @@ def test_fields_set_between_steps(tables, precision):
         orc.step()
     f64, i64 = out[_lib.FP64]
     for g, w, k in zip(f64, (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
-        close(g, w, 1e-10, k)
+        close(g, w, 1e-12, k)
     assert i64 == orc.counters[0]
     f, i = out[precision]
     for g, w, k in zip(f, f64, ("Er", "Ez", "H")):

@@ -19,3 +19,66 @@ def test_tune_sort_period_returns_the_fastest_candidate(precision):
     assert all(v > 0 for v in table.values())
     assert best in table and table[best] == min(table.values())
     assert cfg.sort_period == 20            # the caller's config is left alone
+
+
+@pytest.mark.parametrize("precision", [_lib.FP64, _lib.FP32_SPLIT])
+def test_tune_every_knob_by_coordinate_descent(precision):
+    """tune() times every candidate of every knob (field patch rows, FP32
+    chunk size, sort period) and keeps the fastest of each."""
+    from gasatt.tune import knob_candidates, tune
+    cfg = config(48, 200, 5e-6, 1e-14, 300.0, precision=precision, capacity=60000, seed=7)
+    parts = births(6000, 8.0, 200 * 5e-6, seed=3, sigma_r=40e-6, Rp=48 * 5e-6)
+    knobs = knob_candidates(cfg)
+    if precision == _lib.FP32_SPLIT:
+        assert set(knobs) == {"fdtd_tile_rows", "pass_chunk", "sort_period"}
+    else:
+        assert set(knobs) == {"fdtd_tile_rows", "sort_period"}
+        assert max(knobs["fdtd_tile_rows"]) <= 48
+    best, table = tune(cfg, parts, steps=20)
+    for name, cands in knobs.items():
+        assert set(table[name]) == set(cands)
+        assert getattr(best, name) == min(table[name], key=table[name].get)
+    assert cfg.fdtd_tile_rows == 0 and cfg.pass_chunk == 0 and cfg.sort_period == 20
+
+
+@pytest.mark.parametrize("precision", [_lib.FP64, _lib.FP32_SPLIT])
+def test_launch_knobs_leave_results_bit_identical(precision):
+    """The tuned knobs change only launch shapes: fields, currents and event
+    counts are the same bits for every patch height and chunk size."""
+    import numpy as np
+    from _cases import grid_fields
+    from gasatt.sim import Sim
+    outs = []
+    shapes = [(16, 256), (32, 1792), (48, 1024)]
+    if precision == _lib.FP32_SPLIT:
+        shapes.append((64, 512))
+    for rows, chunk in shapes:
+        cfg = config(40, 150, 5e-6, 1e-14, 300.0, precision=precision, capacity=60000, seed=7,
+                     sort_period=7)
+        cfg.fdtd_tile_rows, cfg.pass_chunk = rows, chunk
+        sim = Sim(cfg)
+        sim.load(*births(5000, 8.0, 150 * 5e-6, seed=3, sigma_r=40e-6, Rp=40 * 5e-6))
+        Er, Ez, H = grid_fields(40, 150, np.random.default_rng(4), E0=3e6, H0=2e3)
+        Er[:, 0] = 0; Er[:, -1] = 0; Ez[-1, :] = 0
+        sim.set_fields(Er, Ez, H)
+        sim.step(12)
+        d = sim.diag()
+        outs.append((*sim.fields(), *sim.current(), d["n_ionizations"], d["n_alive"],
+                     d["status_flags"]))
+        sim.close()
+    for o in outs[1:]:
+        for a, b in zip(outs[0], o):
+            assert np.array_equal(a, b)
+    assert outs[0][-1] == 0
+
+
+def test_bad_launch_knobs_are_rejected():
+    from gasatt._lib import GasattError
+    from gasatt.sim import Sim
+    for prec, rows, chunk in ((_lib.FP32_SPLIT, 40, 0), (_lib.FP32_SPLIT, 80, 0),
+                              (_lib.FP64, 64, 0), (_lib.FP32_SPLIT, 0, 300),
+                              (_lib.FP32_SPLIT, 0, 2048)):
+        cfg = config(32, 64, 5e-6, 1e-14, 1.0, precision=prec, capacity=1000)
+        cfg.fdtd_tile_rows, cfg.pass_chunk = rows, chunk
+        with pytest.raises(GasattError):
+            Sim(cfg)

@@ -83,3 +83,29 @@ def test_noalloc_density_rejects_grids_beyond_its_fixed_scratch():
         assert torch.count_nonzero(out).item() == 0           # nothing was written
     finally:
         ctx.close()
+
+
+def test_noalloc_density_allocates_nothing():
+    """On a fresh context, after one call that loads the library's device code
+    (and with it the fixed array), further no-allocation calls leave the
+    device's free memory unchanged: they take nothing from the context's
+    scratch (which a fresh context would have to cudaMalloc) nor from
+    anywhere else."""
+    warm = Context(0)
+    fresh = Context(0)
+    try:
+        c = _case(24, 200000, 8)
+        out = torch.zeros(c["ncell"], dtype=torch.float64, device="cuda")
+        assert _call(lib.gasatt_particle_density_noalloc, warm, c, 1.0, out) == _lib.OK
+        assert lib.gasatt_synchronize(warm.handle) == _lib.OK
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        for FN in (1.0, 2.0, 4.0):
+            assert _call(lib.gasatt_particle_density_noalloc, fresh, c, FN, out) == _lib.OK, \
+                lib.gasatt_last_error(fresh.handle)
+            assert lib.gasatt_synchronize(fresh.handle) == _lib.OK
+            assert torch.cuda.mem_get_info()[0] == free0
+        assert torch.count_nonzero(out).item() > 0
+    finally:
+        fresh.close()
+        warm.close()
