@@ -407,6 +407,8 @@ def run_ours(args):
         accuracy_legs[prec] = accuracy_run(prec, local, rank, torch, args.accuracy_steps, knobs)
     e2e = e2e_run("fp32_split", local, rank, torch, steps_per_call=200,
                   knobs=tuned["fp32_split"][0])
+    # the batched workload (48 uneven cells in one batch) in both forms
+    c3 = {prec: c3_batched(prec, local, torch) for prec in ("fp32_split", "fp64")}
 
     pk, pk_src = peaks()
     hbm = float(pk.get("hbm_gbs", 6650.0))
@@ -436,6 +438,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
+        cpu["matlab_path"] = matlab_path_baseline()
     # DRAM bytes (read + write) of one k_pass32 launch from an ncu capture of
     # this workload, scaled from the captured launch's electron count to this
     # run's mean count (the traffic is per particle: state and id)
@@ -487,6 +490,15 @@ def run_ours(args):
                  "mcc_ms": f64["mcc_ms"], "fdtd_ms": f64["fdtd_ms"],
                  "achieved_gbs": f64["achieved_gbs"], "frac": f64["achieved_gbs"] / hbm},
         "fp32_over_fp64": f32["value"] / f64["value"],
+        "batched": {"workload": "48 gas cells: p log-U(0.1, 10) Torr, grid from {64x256, 128x512, "
+                                "256x1024, 512x2048} at 10 um, dt 2e-14 s, photon U(2, 20) keV, "
+                                "photoionizations log-U(1e4, 1e6), seed 2; births drawn on the GPU; "
+                                "one batch step = every cell one step",
+                    "fp32_split": {k: c3["fp32_split"][k] for k in ("value", "ms_per_step", "electrons")},
+                    "fp64": {k: c3["fp64"][k] for k in ("value", "ms_per_step", "electrons")},
+                    "fp32_batched_over_fp64_batched": c3["fp32_split"]["value"] / c3["fp64"]["value"],
+                    "steps": c3["fp32_split"]["steps"],
+                    "l2": "not flushed (the 48 cells' state exceeds the L2)"},
         "accuracy": accuracy,
         "fdtd": {"cell_updates_per_s": f32["cell_updates_per_s"], "ms": f32["fdtd_ms"],
                  "note": "one cell-update = one cell advanced by a full particle step (H, E, H, E, H sub-updates)"},
@@ -520,6 +532,43 @@ def oracle_workload(cap):
     return O, orc
 
 
+def matlab_path_baseline(target_s=8.0, max_steps=None):
+    """The reference's MATLAB CPU path restated in C (electricmagneticfield3.m:
+    111-319: half drifts with the wall and wedge/z rules, nearest-cell current,
+    the field update in two halves, interp2 gather, explicit kick), OpenMP on
+    every host core, on the full workload (electrons placed at azimuth 0 with
+    v = u / gamma).  Its collisions come once per 1000 pushes
+    (electron_transport_field2.m:157-160), outside a sample this short."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    from gasatt.workload import births
+    w = WORKLOAD
+    threads = os.cpu_count() or 1
+    O.lib.orc_set_threads(threads)
+    r, z, ur, ut, uz, _ = births(w["photo"], w["e_keV"], w["n_z"] * w["delta"], seed=w["seed"],
+                                 Rp=w["n_r"] * w["delta"])
+    g = np.sqrt(1 + (ur * ur + ut * ut + uz * uz) / 299792458.0 ** 2)
+    m = O.MatlabCpuPath(w["n_r"], w["n_z"], w["delta"], w["dt"])
+    m.load(r, np.zeros_like(r), z, ur / g, ut / g, uz / g)
+    t0 = time.perf_counter()
+    m.step()
+    one = time.perf_counter() - t0
+    steps = max(1, min(200, int(target_s / max(one, 1e-3))))
+    if max_steps:
+        steps = min(steps, max_steps)
+    n0 = int(m.alive.sum())
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        m.step()
+    dt = time.perf_counter() - t0
+    n1 = int(m.alive.sum())
+    return {"value": 0.5 * (n0 + n1) * steps / dt, "unit": UNIT, "cores": threads,
+            "kind": "matlab-path port",
+            "sample": f"full workload ({n0:,} electrons), {steps} steps after 1 warm-up step; "
+                      f"the reference's MATLAB CPU push/deposit/field step "
+                      f"(electricmagneticfield3.m:111-319) restated in C, OpenMP {threads} threads"}
+
+
 ORACLE_WHAT = ("plain C FP64 restatement of the same corrected step (Boris push, null-collision "
                "MCC, fixed-point deposit, FDTD); the reference's own CPU path is MATLAB, "
                "which is not installed")
@@ -545,6 +594,7 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     alive1 = int(orc.alive[:orc.n].sum())
     value = 0.5 * (alive0 + alive1) * args.steps / dt
+    mpath = matlab_path_baseline(max_steps=max(args.steps, 3))
     sample = (f"the full workload ({alive0:,} electrons at the first timed step, 256x1024 grid, FDTD "
               f"every step), {args.steps} steps after {args.warmup} warm-up steps; {ORACLE_WHAT}; "
               f"OpenMP {threads} threads")
@@ -555,7 +605,7 @@ def run_reference(args):
             "config": {"workload": WORKLOAD_NAME, "precision": "fp64",
                        "global_electrons": alive0, "parallelism": "host threads x%d" % threads},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": sample},
+                             "sample": sample, "matlab_path": mpath},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -575,6 +625,45 @@ def c3_cells(n=48, seed=2):
                           torr=float(10 ** rng.uniform(-1, 1)), e_keV=float(rng.uniform(2, 20)),
                           photo=int(round(10 ** rng.uniform(4, 6))), seed=seed * 1000 + i))
     return cells
+
+
+def c3_batched(precision, device, torch, steps=100, warmup=5, sort_period=30):
+    """The 48 C3 gas cells (c3_cells) stepped as one batch in the given form:
+    births drawn on the GPU with the workload's laws, `steps` whole steps
+    timed with CUDA events after `warmup`.  Returns the rate (mean electrons
+    x steps / time), ms per step and the electron count."""
+    from gasatt import abi
+    from gasatt.dropin import Context
+    from gasatt.sim import Batch, Sim
+    from gasatt.workload import config
+    prec = abi.FP32_SPLIT if precision == "fp32_split" else abi.FP64
+    ctx = Context(device)
+    ctx.bind_stream()
+    sims = []
+    for c in c3_cells():
+        cfg = config(c["n_r"], c["n_z"], c["delta"], c["dt"], c["torr"], precision=prec,
+                     capacity=6 * c["photo"], seed=c["seed"], sort_period=sort_period)
+        sim = Sim(cfg, ctx=ctx, device=device)
+        sim.birth_photo(c["photo"], c["e_keV"], seed=c["seed"])
+        sims.append(sim)
+    batch = Batch(sims, sort_period=sort_period)
+    stream = torch.cuda.current_stream(device)
+    batch.step(warmup)
+    torch.cuda.synchronize()
+    a0 = sum(s.diag()["n_alive"] for s in sims)
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    a1 = sum(s.diag()["n_alive"] for s in sims)
+    batch.close()
+    for s in sims:
+        s.close()
+    ctx.close()
+    return {"value": 0.5 * (a0 + a1) * steps / (ms / 1e3), "ms_per_step": ms / steps,
+            "electrons": int(a1), "steps": steps}
 
 
 def run_c3(args):

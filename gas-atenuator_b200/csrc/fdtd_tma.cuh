@@ -29,8 +29,8 @@
 // grid (negative or beyond the extent) arrive as zeros and are never updated.
 //
 // Every wait on an mbarrier is bounded; a block whose copy has not completed
-// after the bound sets *err, waits (bounded) for its other copy in flight and
-// returns.
+// after the bound sets the cell's *err, waits (bounded) for its other copy in
+// flight and returns.
 #pragma once
 #include <cuda.h>
 #include "fdtd.cuh"
@@ -116,6 +116,40 @@ struct TmaMaps {
   CUtensorMap er, ez, h, jr, jz;
 };
 
+// One gas cell's field update as the kernel sees it: its tensor maps (the
+// fields and the current buffer read in this step), where the tile is written
+// back (fields in T, the other current buffer cleared, FP32 gather quads),
+// the coefficients and its tile grid.  A single cell passes it as a kernel
+// parameter; a batch keeps one per cell in global memory.
+struct FdtdInst {
+  TmaMaps maps;
+  void *Er, *Ez, *H;
+  unsigned long long *Jr_next, *Jz_next;
+  const double *invV;
+  ExtraCurrent xj;
+  FieldQuads q;
+  FdtdCoef c;
+  double mu, dt;
+  int nr, nz, ldf, ldj;
+  unsigned flags;
+  int tiles_x, ntiles;
+  unsigned *err;              // set when a tile copy of this cell did not complete
+};
+
+// Work of a launch: tile t of one cell, or entry t of a table of (cell, tile)
+// pairs over the cells of a batch.
+struct FdtdWork {
+  const FdtdInst *inst;       // one cell, or the batch's cells
+  const int2 *table;          // null for one cell; else (cell, tile) per work item
+  int ntiles;                 // work items
+  __device__ __forceinline__ const FdtdInst &at(int t, int &lt) const {
+    if (!table) { lt = t; return *inst; }
+    const int2 e = table[t];
+    lt = e.y;
+    return inst[e.x];
+  }
+};
+
 // tile t of a tiles_x-wide row-major tile grid -> the patch origin (x0, y0)
 __device__ __forceinline__ void tma_patch_origin(int t, int tiles_x, int ph, int &x0, int &y0) {
   const int ty = t / tiles_x, tx = t - ty * tiles_x;
@@ -136,19 +170,21 @@ __device__ __forceinline__ void tma_issue(const TmaMaps &M, unsigned char *stage
   tma_load_2d(stage + 3 * L.field_bytes() + L.cur_bytes(), &M.jz, xj, y0, bar);
 }
 
-// The sub-cycle on the tiles of an n_r x n_z grid in the padded layout
-// (row strides ldf for the fields, ldj for the currents).  The field
-// arithmetic is that of fdtd_tiled1 (fdtd.cuh).
+// issue the copies of work item t (thread 0)
 template <typename T>
-__device__ __forceinline__ void fdtd_tma_body(const TmaMaps &M, T *__restrict__ Er,
-                                              T *__restrict__ Ez, T *__restrict__ H,
-                                              unsigned long long *__restrict__ Jr_next,
-                                              unsigned long long *__restrict__ Jz_next, int nr,
-                                              int nz, int ldf, int ldj, const FdtdCoef &c,
-                                              const double *__restrict__ invV, double mu,
-                                              double dt, unsigned flags, ExtraCurrent xj,
-                                              FieldQuads q, int ph, int tiles_x, int ntiles,
-                                              unsigned *err) {
+__device__ __forceinline__ void tma_issue_item(const FdtdWork &W, int t, unsigned char *stage,
+                                               uint64_t *bar, const TmaSmem<T> &L) {
+  int lt, x0, y0;
+  const FdtdInst &I = W.at(t, lt);
+  tma_patch_origin(lt, I.tiles_x, L.ph, x0, y0);
+  tma_issue<T>(I.maps, stage, bar, L, x0, y0);
+}
+
+// The sub-cycle on the work items of W (cells on the padded layout: row
+// strides ldf for the fields, ldj for the currents).  The field arithmetic is
+// that of fdtd_tiled1 (fdtd.cuh).
+template <typename T>
+__device__ __forceinline__ void fdtd_tma_body(const FdtdWork &W, int ph) {
   constexpr int PW = kTmaPatchW;
   constexpr int al = 16 / (int)sizeof(T);
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -159,9 +195,7 @@ __device__ __forceinline__ void fdtd_tma_body(const TmaMaps &M, T *__restrict__ 
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L.bar_off());
   const int li = threadIdx.x, tid = threadIdx.y * PW + threadIdx.x;
   const int nrow_t = ph / kTmaRows;                  // patch rows per thread
-  const bool endcopy = (flags & GASATT_Q_ER_END_COPY) != 0;
-  const bool jsign = (flags & GASATT_Q_EZ_AXIS_JSIGN) != 0;
-  const double dt_eps = c.dt_eps, dt_eps_dz = c.dt_eps_dz, axis = c.axis, inv_dr = 1 / c.dr;
+  const int ntiles = W.ntiles;
   if (tid == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
@@ -171,30 +205,35 @@ __device__ __forceinline__ void fdtd_tma_body(const TmaMaps &M, T *__restrict__ 
   int t = blockIdx.x;
   bool issued0 = false, issued1 = false;             // thread 0: a copy of buffer 0 / 1 in flight
   if (tid == 0 && t < ntiles) {
-    int x0, y0;
-    tma_patch_origin(t, tiles_x, ph, x0, y0);
-    tma_issue<T>(M, stage[0], &bar[0], L, x0, y0);
+    tma_issue_item<T>(W, t, stage[0], &bar[0], L);
     issued0 = true;
   }
   for (int k = 0; t < ntiles; t += gridDim.x, ++k) {
     const int b = k & 1;
-    // the next tile's copies go out now, into the buffer the previous tile
+    // the next item's copies go out now, into the buffer the previous item
     // has finished with (every thread read it before the barriers below)
     if (tid == 0 && t + (int)gridDim.x < ntiles) {
-      int x0, y0;
-      tma_patch_origin(t + gridDim.x, tiles_x, ph, x0, y0);
       fence_proxy_async_smem();
-      tma_issue<T>(M, stage[b ^ 1], &bar[b ^ 1], L, x0, y0);
+      tma_issue_item<T>(W, t + gridDim.x, stage[b ^ 1], &bar[b ^ 1], L);
       if (b) issued0 = true; else issued1 = true;
     }
     const bool ok = mbar_wait(&bar[b], (uint32_t)((k >> 1) & 1));
     if (tid == 0 && ok) { if (b) issued1 = false; else issued0 = false; }
     if (__syncthreads_or(!ok)) {
-      if (tid == 0) atomicOr(err, 1u);
+      int lt;
+      if (tid == 0) atomicOr(W.at(t, lt).err, 1u);
       break;
     }
-    int x0, y0;
-    tma_patch_origin(t, tiles_x, ph, x0, y0);
+    int lt, x0, y0;
+    const FdtdInst &I = W.at(t, lt);
+    tma_patch_origin(lt, I.tiles_x, ph, x0, y0);
+    const int nr = I.nr, nz = I.nz;
+    const FdtdCoef &c = I.c;
+    const unsigned flags = I.flags;
+    const bool endcopy = (flags & GASATT_Q_ER_END_COPY) != 0;
+    const bool jsign = (flags & GASATT_Q_EZ_AXIS_JSIGN) != 0;
+    const double dt_eps = c.dt_eps, dt_eps_dz = c.dt_eps_dz, axis = c.axis, inv_dr = 1 / c.dr;
+    const double mu = I.mu, dt = I.dt;
     const int col = x0 + li;
     const int of = x0 - (x0 & ~(al - 1)), oj = x0 - (x0 & ~1);
     // widen the staged tile into the working arrays
@@ -205,16 +244,17 @@ __device__ __forceinline__ void fdtd_tma_body(const TmaMaps &M, T *__restrict__ 
       const long long *gJr = reinterpret_cast<const long long *>(stage[b] + 3 * L.field_bytes());
       const long long *gJz =
           reinterpret_cast<const long long *>(stage[b] + 3 * L.field_bytes() + L.cur_bytes());
-      const double iv = (col >= 0 && col < nr) ? invV[col] : 0.0;
+      const double iv = (col >= 0 && col < nr) ? I.invV[col] : 0.0;
+      const ExtraCurrent xj = I.xj;
       for (int m = 0; m < nrow_t; ++m) {
         const int r = threadIdx.y + kTmaRows * m, s = li + r * PW;
         const int sf = li + of + r * TmaBox<T>::w, sj = li + oj + r * 34;
         sEr[s] = (double)gEr[sf];
         sEz[s] = (double)gEz[sf];
         sH[s] = (double)gH[sf];
-        const int row = y0 + r;
-        if (xj.Jr && col >= 0 && col < nr && row >= 0 && row < nz) {
-          const int64_t g = col + (int64_t)row * ldj;
+        const int jrow = y0 + r;
+        if (xj.Jr && col >= 0 && col < nr && jrow >= 0 && jrow < nz) {
+          const int64_t g = col + (int64_t)jrow * I.ldj;
           sJr[s] = ((double)gJr[sj] + (double)(long long)xj.Jr[g] * xj.rel) * iv;
           sJz[s] = ((double)gJz[sj] + (double)(long long)xj.Jz[g] * xj.rel) * iv;
         } else {
@@ -277,6 +317,10 @@ __device__ __forceinline__ void fdtd_tma_body(const TmaMaps &M, T *__restrict__ 
     h_update(dt / 4);
     __syncthreads();
     // write back the tile: columns [3, 29) and rows [3, ph - 3) of the patch
+    T *Er = reinterpret_cast<T *>(I.Er), *Ez = reinterpret_cast<T *>(I.Ez), *H = reinterpret_cast<T *>(I.H);
+    unsigned long long *Jr_next = I.Jr_next, *Jz_next = I.Jz_next;
+    const int ldf = I.ldf, ldj = I.ldj;
+    const FieldQuads q = I.q;
     if (li >= kTmaHalo && li < kTmaHalo + kTmaTileW && col <= nr) {
       const int c0 = col > 0 ? li - 1 : li, c1 = col > nr - 1 ? li - 1 : li;   // quad columns
       for (int m = 0; m < nrow_t; ++m) {

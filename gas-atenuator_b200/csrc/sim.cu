@@ -388,7 +388,7 @@ __device__ __forceinline__ void queue_push(bool want, long long p, unsigned long
 // advances.  Idempotent: only the first commit after a pass does anything.
 // (Done at the end of the pass itself, by its last block, the atomics of 592
 // blocks on the counters' cache line slowed the pass by a tenth.)
-__global__ void k_commit(SimCounters *cnt, int q) {
+__device__ __forceinline__ void k_commit_body(SimCounters *cnt, int q) {
   if (!cnt->uncommitted) return;
   const unsigned long long nt = cnt->n_total + cnt->n_births;
   cnt->n_total = nt < cnt->cap ? nt : cnt->cap;
@@ -398,6 +398,7 @@ __global__ void k_commit(SimCounters *cnt, int q) {
   cnt->step += 1;
   cnt->uncommitted = 0;
 }
+__global__ void k_commit(SimCounters *cnt, int q) { k_commit_body(cnt, q); }
 
 // ------------------------------------------------------ deposit
 // Each particle's four node contributions (q FN v w, both components) are
@@ -492,21 +493,16 @@ __device__ __forceinline__ void deposit_values64(const SimParams &P, double r, d
   }
 }
 
-// mode 0: full step - kick, drift (two half drifts), deposit; collision
-// candidates go to queue q for k_mcc64; mode 1: half drift + deposit only
-// (start of a run); mode 2: kick + half drift only, ending at integer time
-// (end of a run)
-__global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fields<double> F,
-                                                      SimCounters *cnt, int *queue, int mode,
-                                                      int q) {
-  const long long n0 = slots_in_use(cnt);
-  const long long step = cnt->step;
+// The particles [beg, end) of the FP64 pass of step `step` (beg a multiple
+// of 32 apart from the block's first warp): mode 0: full step - kick, drift
+// (two half drifts), deposit; collision candidates go to queue q for k_mcc64;
+// mode 1: half drift + deposit only (start of a run); mode 2: kick + half
+// drift only, ending at integer time (end of a run).
+__device__ __forceinline__ void range64(const SimParams &P, const State64 &S,
+                                        const Fields<double> &F, SimCounters *cnt, int *queue,
+                                        int mode, int q, long long step, long long beg,
+                                        long long end) {
   const int lane = threadIdx.x & 31;
-  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->uncommitted = 1;
-  // each block takes a contiguous chunk of the (cell-sorted) particles, so its
-  // field reads stay in a narrow band of grid rows
-  const long long chunk = (n0 + gridDim.x - 1) / gridDim.x;
-  const long long beg = (long long)blockIdx.x * chunk, end = min(beg + chunk, n0);
   unsigned lost = 0;
   for (long long base = beg + (threadIdx.x & ~31); base < end; base += blockDim.x) {
     const long long p = base + lane;
@@ -552,6 +548,49 @@ __global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fi
   if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
 }
 
+__global__ void __launch_bounds__(kBlock, 3) k_pass64(SimParams P, State64 S, Fields<double> F,
+                                                      SimCounters *cnt, int *queue, int mode,
+                                                      int q) {
+  const long long n0 = slots_in_use(cnt);
+  const long long step = cnt->step;
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->uncommitted = 1;
+  // each block takes a contiguous chunk of the (cell-sorted) particles, so its
+  // field reads stay in a narrow band of grid rows
+  const long long chunk = (n0 + gridDim.x - 1) / gridDim.x;
+  const long long beg = (long long)blockIdx.x * chunk, end = min(beg + chunk, n0);
+  range64(P, S, F, cnt, queue, mode, q, step, beg, end);
+}
+
+// The collision of candidate slot p queued at step `step` (FP64 form): MCC,
+// the ion and the secondary's birth at the parent's position.  n0: the
+// committed slots (births land beyond).
+__device__ __forceinline__ void mcc64_one(const SimParams &P, const State64 &S, SimCounters *cnt,
+                                          long long p, long long step, long long n0) {
+  const double2 rz = S.rz[p], urt = S.urt[p];
+  double ur = urt.x, ut = urt.y, uz = S.uz[p];
+  const uint64_t id = S.id[p];
+  Birth b;
+  const double ng = gas_density(P, (int)floor(rz.x / P.dr), (int)floor(rz.y / P.dz));
+  const int ev = mcc_event<false>(P, id, step, ur, ut, uz, b, ng);
+  count_event(cnt, ev, b);
+  if (ev == 2 && P.ion_cap > 0)
+    ion_birth(P.ion, P.ion_cap, ion_spread(P, (int)floor(rz.x / P.dr), (int)floor(rz.y / P.dz)),
+              P.seed, cnt, id, step, rz.x, rz.y);
+  if (b.born) {
+    const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
+    const long long slot = n0 + (long long)kb;
+    if (slot < P.cap) {
+      S.rz[slot] = rz;
+      S.urt[slot] = make_double2(b.ux, b.uy);
+      S.uz[slot] = b.uz;
+      S.id[slot] = child_id(id, step);
+    } else {
+      atomicAdd(&cnt->cap_overflow, 1ull);
+    }
+  }
+  S.urt[p] = make_double2(ur, ut); S.uz[p] = uz;
+}
+
 // The collisions of the pass that filled queue q, at the end of its step
 // (after the drift and the deposit): the MCC changes the velocity, and an
 // ionization appends its secondary at the parent's position.  Nothing here
@@ -567,31 +606,91 @@ __global__ void __launch_bounds__(kMccBlock) k_mcc64(SimParams P, State64 S, Sim
   const long long nq = (long long)cnt->n_cand[q];
   const int *qu = queue + (long long)q * P.cap;
   const long long nwarps = (long long)gridDim.x * (kMccBlock / 32);
+  for (long long k = (blockIdx.x * (long long)kMccBlock + threadIdx.x) >> 5; k < nq; k += nwarps)
+    mcc64_one(P, S, cnt, qu[k], step, n0);
+}
+
+constexpr int kMaxBatch = 256;               // cells a batch holds at most
+
+// the cell of work item k: the last c with prefix[c] <= k (prefix ascending,
+// prefix[0] = 0, n cells)
+__device__ __forceinline__ int cell_of_item(const long long *prefix, int n, long long k) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (prefix[mid] <= k) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// ------------------------------------------------------- batched FP64 step
+struct BatchCell64 {
+  SimParams P[2];             // deposit into current buffer 0 / 1
+  State64 S[2];
+  SimCounters *cnt;
+  int *queue;
+  Fields<double> F;
+};
+constexpr int kChunk64 = 2048;               // particles per work item of the batched FP64 pass
+
+__global__ void k_batch_commit64(const BatchCell64 *__restrict__ cells, int ncell, int q) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x)
+    k_commit_body(cells[c].cnt, q);
+}
+
+// the collisions queued (parity q) by every cell's last pass, one per warp
+__global__ void __launch_bounds__(kMccBlock) k_batch_mcc64(const BatchCell64 *__restrict__ cells,
+                                                           int ncell, int cur, int q) {
+  __shared__ long long pre[kMaxBatch + 1];
+  for (int c = threadIdx.x; c < ncell; c += blockDim.x) pre[c + 1] = (long long)cells[c].cnt->n_cand[q];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    pre[0] = 0;
+    for (int c = 0; c < ncell; ++c) pre[c + 1] += pre[c];
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) != 0) return;
+  const long long nq = pre[ncell];
+  const long long nwarps = (long long)gridDim.x * (kMccBlock / 32);
   for (long long k = (blockIdx.x * (long long)kMccBlock + threadIdx.x) >> 5; k < nq; k += nwarps) {
-    const long long p = qu[k];
-    const double2 rz = S.rz[p], urt = S.urt[p];
-    double ur = urt.x, ut = urt.y, uz = S.uz[p];
-    const uint64_t id = S.id[p];
-    Birth b;
-    const double ng = gas_density(P, (int)floor(rz.x / P.dr), (int)floor(rz.y / P.dz));
-    const int ev = mcc_event<false>(P, id, step, ur, ut, uz, b, ng);
-    count_event(cnt, ev, b);
-    if (ev == 2 && P.ion_cap > 0)
-      ion_birth(P.ion, P.ion_cap, ion_spread(P, (int)floor(rz.x / P.dr), (int)floor(rz.y / P.dz)),
-                P.seed, cnt, id, step, rz.x, rz.y);
-    if (b.born) {
-      const unsigned long long kb = atomicAdd(&cnt->n_births, 1ull);
-      const long long slot = n0 + (long long)kb;
-      if (slot < P.cap) {
-        S.rz[slot] = rz;
-        S.urt[slot] = make_double2(b.ux, b.uy);
-        S.uz[slot] = b.uz;
-        S.id[slot] = child_id(id, step);
-      } else {
-        atomicAdd(&cnt->cap_overflow, 1ull);
-      }
-    }
-    S.urt[p] = make_double2(ur, ut); S.uz[p] = uz;
+    const int c = cell_of_item(pre, ncell, k);
+    const BatchCell64 &C = cells[c];
+    SimCounters *cc = C.cnt;
+    const int *qu = C.queue + (long long)q * C.P[0].cap;
+    mcc64_one(C.P[0], C.S[cur], cc, qu[k - pre[c]], cc->cand_step[q], (long long)cc->n_total);
+  }
+}
+
+// The FP64 pass of every cell of a batch: (cell, chunk of kChunk64) work
+// items from one counter (*chunk_next, zeroed before the launch).
+__global__ void __launch_bounds__(kBlock, 3) k_batch_pass64(const BatchCell64 *__restrict__ cells,
+                                                            int ncell, int cur, int jb, int mode,
+                                                            int q, unsigned long long *chunk_next) {
+  __shared__ long long pre[kMaxBatch + 1];
+  __shared__ long long item_at;
+  for (int c = threadIdx.x; c < ncell; c += blockDim.x)
+    pre[c + 1] = (slots_in_use(cells[c].cnt) + kChunk64 - 1) / kChunk64;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    pre[0] = 0;
+    for (int c = 0; c < ncell; ++c) pre[c + 1] += pre[c];
+    if (blockIdx.x == 0)
+      for (int c = 0; c < ncell; ++c) cells[c].cnt->uncommitted = 1;
+  }
+  __syncthreads();
+  const long long nitem = pre[ncell];
+  for (;;) {
+    if (threadIdx.x == 0) item_at = (long long)atomicAdd(chunk_next, 1ull);
+    __syncthreads();
+    const long long g = item_at;
+    __syncthreads();
+    if (g >= nitem) break;
+    const int c = cell_of_item(pre, ncell, g);
+    const BatchCell64 &C = cells[c];
+    SimCounters *cc = C.cnt;
+    const long long n0 = slots_in_use(cc);
+    const long long beg = (g - pre[c]) * kChunk64, end = min(beg + kChunk64, n0);
+    range64(C.P[jb], C.S[cur], C.F, cc, C.queue, mode, q, cc->step, beg, end);
   }
 }
 
@@ -1086,12 +1185,142 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
   S.b[p] = make_float2(ut, uz);
 }
 
+// Window rows of chunk ch (particles [ch chunk, min(ch chunk + chunk, n0))):
+// the node rows of its first and last particles, with a margin for the drift
+// since the last sort.  maxrows: rows the window holds for this grid.
+__device__ __forceinline__ void chunk_rows32(const SimParams &P, const State32 &S, long long n0,
+                                             int chunk, long long ch, int maxrows, int &row0,
+                                             int &rows) {
+  const long long beg = ch * chunk, end = min(beg + chunk, n0);
+  const uint32_t k0 = reinterpret_cast<const uint32_t *>(S.a + beg)[0];
+  const uint32_t k1 = reinterpret_cast<const uint32_t *>(S.a + end - 1)[0];
+  int lo = P.nz, hi = -1;
+  if (k0 != kDead) { lo = min(lo, (int)(k0 >> 16)); hi = max(hi, (int)(k0 >> 16)); }
+  if (k1 != kDead) { lo = min(lo, (int)(k1 >> 16)); hi = max(hi, (int)(k1 >> 16)); }
+  row0 = 0; rows = maxrows;
+  if (hi >= 0) {
+    // the chunk's own deposit rows lo-1 .. hi+1 first, then up to three
+    // rows either side for the drift since the last sort (a wide grid
+    // leaves room for few rows)
+    const int core = hi - lo + 3;
+    const int below = maxrows >= core + 6 ? 3 : max(1, 1 + (maxrows - core) / 2);
+    row0 = min(max(0, lo - below), P.nz - maxrows);
+    rows = min(maxrows, hi + 4 - row0);
+  }
+}
+
+// The particles [beg, end) of one chunk of the FP32 pass of step `step`:
+// push (push32), collision candidates queued, deposit into the window w (one
+// shared-memory atomic per node and deposit quad of a warp; nodes outside the
+// window straight to the grid).  The highest window column touched is merged
+// into *box_cmax; electrons absorbed at the wall are counted into cnt.
+__device__ __forceinline__ void chunk32(const SimParams &P, const State32 &S, const Fields<float> &F,
+                                        SimCounters *cnt, int *queue, long long step, int mode,
+                                        int beg, int end, const Win32 &w, int *box_cmax) {
+  const int par = (int)(step & 1);
+  const uint32_t parbit = par ? kSign : 0u;
+  const int lane = threadIdx.x & 31;
+  unsigned lost = 0;
+  int wc_max = -1;                 // highest window column this lane touched
+  // the next iteration's particle is loaded one iteration ahead, so its
+  // HBM latency overlaps the current particle's arithmetic
+  int base = beg + (int)(threadIdx.x & ~31);
+  uint4 An = make_uint4(kDead, 0, 0, 0);
+  float2 Bn = make_float2(0.f, 0.f);
+  uint64_t idn = 0;
+  if (base + lane < end) { An = S.a[base + lane]; Bn = S.b[base + lane]; idn = S.id[base + lane]; }
+  for (; base < end; base += kBlock) {
+    const int p = base + lane;
+    uint4 A = An;
+    const float2 B = Bn;
+    const uint64_t id = idn;
+    {
+      const int pn = p + kBlock;
+      An = make_uint4(kDead, 0, 0, 0);
+      if (pn < end) { An = S.a[pn]; Bn = S.b[pn]; idn = S.id[pn]; }
+    }
+    // skip the dead, the pending collisions and those already pushed in
+    // this step (the candidates the pass has taken)
+    bool act = p < end && A.x != kDead && !(A.y & kSign) && (A.z & kSign) != parbit;
+    int ir = (int)(A.x & 0xFFFFu), iz = (int)(A.x >> 16);
+    float fr = __uint_as_float(A.y & ~kSign), fz = __uint_as_float(A.z & ~kSign);
+    float ur = __uint_as_float(A.w), ut = B.x, uz = B.y, ig = 1.f;
+    bool cand = false;
+    if (act) {
+      bool alive = true;
+      cand = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive, ig);
+      if (!alive) {
+        lost++;
+        count_wall_loss(cnt, (double)ur * ur + (double)ut * ut + (double)uz * uz, P.me * P.c * P.c / P.qe);
+      }
+      S.a[p] = pack32(ir, iz, fr, fz, ur, alive, cand, par);
+      S.b[p] = make_float2(ut, uz);
+      act = alive && mode != 2;
+    }
+    queue_push(cand, p, &cnt->n_cand[par], queue + (long long)par * P.cap);
+    // Deposit: the lanes that share a node quad (sorted particles put one to
+    // a few quads in a warp) sum their eight integer contributions with
+    // redux.sync, and the first lane of each quad adds the sums - one
+    // shared-memory atomic per node and quad instead of one per particle
+    const unsigned dm = __ballot_sync(0xFFFFFFFFu, act);
+    if (act) {
+      int ca, cb, ra, rb, vr[4], vz[4];
+      const unsigned key = deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, ca, cb, ra, rb, vr, vz);
+      const unsigned grp = __match_any_sync(dm, key);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        vr[k] = __reduce_add_sync(grp, vr[k]);
+        vz[k] = __reduce_add_sync(grp, vz[k]);
+      }
+      if (lane == __ffs(grp) - 1) {
+        const unsigned la = (unsigned)(ra - w.row0), lb = (unsigned)(rb - w.row0);
+        if (la < (unsigned)w.rows && lb < (unsigned)w.rows) {
+          const int k0 = (int)la * w.ws, k1 = (int)lb * w.ws;
+          atomicAdd(w.r + k0 + ca, vr[0]); atomicAdd(w.z + k0 + ca, vz[0]);
+          atomicAdd(w.r + k0 + cb, vr[1]); atomicAdd(w.z + k0 + cb, vz[1]);
+          atomicAdd(w.r + k1 + ca, vr[2]); atomicAdd(w.z + k1 + ca, vz[2]);
+          atomicAdd(w.r + k1 + cb, vr[3]); atomicAdd(w.z + k1 + cb, vz[3]);
+        } else {
+          win_node(w, P, ca, ra, vr[0], vz[0]);
+          win_node(w, P, cb, ra, vr[1], vz[1]);
+          win_node(w, P, ca, rb, vr[2], vz[2]);
+          win_node(w, P, cb, rb, vr[3], vz[3]);
+        }
+        wc_max = max(wc_max, cb);       // (win_node may use the window for one row)
+      }
+    }
+  }
+  // the window columns this warp touched, merged into the block's; the wall
+  // losses of the warp
+  wc_max = __reduce_max_sync(0xFFFFFFFFu, wc_max);
+  if (lane == 0 && wc_max >= 0) atomicMax(box_cmax, wc_max);
+  lost = __reduce_add_sync(0xFFFFFFFFu, lost);
+  if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
+}
+
+// Add the window columns [0, bw) of every window row to the grid (one 64-bit
+// atomic per nonzero node) and zero them for the next chunk.
+__device__ __forceinline__ void flush32(const SimParams &P, const Win32 &w, int bw) {
+  const int nb = bw > 0 ? bw * w.rows : 0;
+  for (int i = threadIdx.x; i < nb; i += kBlock) {
+    const int row = i / bw, col = i - row * bw;
+    const int k = row * w.ws + col;
+    const int vr = w.r[k], vz = w.z[k];
+    if (vr | vz) {
+      const int64_t g = (int64_t)(w.row0 + row) * P.ldj + col;
+      if (vr) atomicAdd(P.Jr + g, (unsigned long long)(long long)vr);
+      if (vz) atomicAdd(P.Jz + g, (unsigned long long)(long long)vz);
+      w.r[k] = 0; w.z[k] = 0;
+    }
+  }
+}
+
 // FP32 particle pass of step `step` (modes as push32).  Its blocks first take
 // the collision candidates queued by the previous pass, one per warp (a long
 // serial chain each, so blocks in order take eight at a time), then all other
-// particles in chunks of P.chunk handed out in order, so the blocks
-// that ran a candidate simply take fewer chunks.  Counters are committed by
-// the field kernel of the next step.
+// particles in chunks of P.chunk handed out in order, so the blocks that ran
+// a candidate simply take fewer chunks.  Counters are committed by the field
+// kernel of the next step.
 __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fields<float> F,
                                                       SimCounters *cnt, int *queue, int mode,
                                                       const SimParams *__restrict__ Pg) {
@@ -1102,51 +1331,31 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
   const long long n0 = (long long)cnt->n_total;   // births of this pass land beyond
   const long long step = cnt->step;
   const int par = (int)(step & 1);
-  const uint32_t parbit = par ? kSign : 0u;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned lost = 0;
   // the window starts zeroed; each chunk's flush leaves it zeroed again
   for (int i = threadIdx.x; i < kWinNodes; i += kBlock) { win_r[i] = 0; win_z[i] = 0; }
   if (mode != 1) {
     const long long nq = (long long)cnt->n_cand[par ^ 1];
     const int *qin = queue + (long long)(par ^ 1) * P.cap;
+    unsigned lost = 0;
     for (long long k = (long long)blockIdx.x * (kBlock / 32) + warp; k < nq;
          k += (long long)gridDim.x * (kBlock / 32)) {
       if (lane == 0) candidate32(Pg, F, S, cnt, queue, qin[k], step, mode, true, n0, lost);
       __syncwarp();
     }
+    if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
   }
   const int ws = win_stride(P.nr);
   const int maxrows = min(kWinNodes / ws, P.nz);
   const int chunk = P.chunk;
   const long long nchunk = (n0 + chunk - 1) / chunk;
-  // window rows of a chunk: the node rows of its first and last particles,
-  // with a margin for the drift since the last sort
-  auto chunk_rows = [&](long long ch, int &row0, int &rows) {
-    const long long beg = ch * chunk, end = min(beg + chunk, n0);
-    const uint32_t k0 = reinterpret_cast<const uint32_t *>(S.a + beg)[0];
-    const uint32_t k1 = reinterpret_cast<const uint32_t *>(S.a + end - 1)[0];
-    int lo = P.nz, hi = -1;
-    if (k0 != kDead) { lo = min(lo, (int)(k0 >> 16)); hi = max(hi, (int)(k0 >> 16)); }
-    if (k1 != kDead) { lo = min(lo, (int)(k1 >> 16)); hi = max(hi, (int)(k1 >> 16)); }
-    row0 = 0; rows = maxrows;
-    if (hi >= 0) {
-      // the chunk's own deposit rows lo-1 .. hi+1 first, then up to three
-      // rows either side for the drift since the last sort (a wide grid
-      // leaves room for few rows)
-      const int core = hi - lo + 3;
-      const int below = maxrows >= core + 6 ? 3 : max(1, 1 + (maxrows - core) / 2);
-      row0 = min(max(0, lo - below), P.nz - maxrows);
-      rows = min(maxrows, hi + 4 - row0);
-    }
-  };
   // thread 0 fetches the next chunk (index and window rows) while the block
   // works on the current one
   long long next_ch = 0;
   int next_row0 = 0, next_rows = 0;
   if (threadIdx.x == 0) {
     next_ch = (long long)atomicAdd(&cnt->chunk_next, 1ull);
-    if (next_ch < nchunk) chunk_rows(next_ch, next_row0, next_rows);
+    if (next_ch < nchunk) chunk_rows32(P, S, n0, chunk, next_ch, maxrows, next_row0, next_rows);
   }
   for (;;) {
     if (threadIdx.x == 0) {
@@ -1159,101 +1368,128 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
     __syncthreads();
     const long long ch = chunk_at;
     if (ch >= nchunk) break;
-    const long long beg = ch * chunk, end = min(beg + chunk, n0);
+    // 32-bit slot indices: the capacity is below 2^31
+    const int beg = (int)(ch * chunk), end = (int)min((long long)beg + chunk, n0);
     const Win32 w{win_r, win_z, win_row0, win_rows, ws};
-    // the next iteration's particle is loaded one iteration ahead, so its
-    // HBM latency overlaps the current particle's arithmetic
-    long long base = beg + (threadIdx.x & ~31);
-    uint4 An = make_uint4(kDead, 0, 0, 0);
-    float2 Bn = make_float2(0.f, 0.f);
-    uint64_t idn = 0;
-    if (base + lane < end) { An = S.a[base + lane]; Bn = S.b[base + lane]; idn = S.id[base + lane]; }
-    int wc_max = -1;                 // highest window column this lane touched
-    for (; base < end; base += blockDim.x) {
-      const long long p = base + lane;
-      uint4 A = An;
-      const float2 B = Bn;
-      const uint64_t id = idn;
-      {
-        const long long pn = p + blockDim.x;
-        An = make_uint4(kDead, 0, 0, 0);
-        if (pn < end) { An = S.a[pn]; Bn = S.b[pn]; idn = S.id[pn]; }
-      }
-      // skip the dead, the pending collisions and those already pushed in
-      // this step (the candidates the pass has taken)
-      bool act = p < end && A.x != kDead && !(A.y & kSign) && (A.z & kSign) != parbit;
-      int ir = (int)(A.x & 0xFFFFu), iz = (int)(A.x >> 16);
-      float fr = __uint_as_float(A.y & ~kSign), fz = __uint_as_float(A.z & ~kSign);
-      float ur = __uint_as_float(A.w), ut = B.x, uz = B.y, ig = 1.f;
-      bool cand = false;
-      if (act) {
-        bool alive = true;
-        cand = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive, ig);
-        if (!alive) {
-          lost++;
-          count_wall_loss(cnt, (double)ur * ur + (double)ut * ut + (double)uz * uz, P.me * P.c * P.c / P.qe);
-        }
-        S.a[p] = pack32(ir, iz, fr, fz, ur, alive, cand, par);
-        S.b[p] = make_float2(ut, uz);
-        act = alive && mode != 2;
-      }
-      queue_push(cand, p, &cnt->n_cand[par], queue + (long long)par * P.cap);
-      // Deposit: the lanes that share a node quad (sorted particles put one to
-      // a few quads in a warp) sum their eight integer contributions with
-      // redux.sync, and the first lane of each quad adds the sums - one
-      // shared-memory atomic per node and quad instead of one per particle
-      const unsigned dm = __ballot_sync(0xFFFFFFFFu, act);
-      if (act) {
-        int ca, cb, ra, rb, vr[4], vz[4];
-        const unsigned key = deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, ca, cb, ra, rb, vr, vz);
-        const unsigned grp = __match_any_sync(dm, key);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          vr[k] = __reduce_add_sync(grp, vr[k]);
-          vz[k] = __reduce_add_sync(grp, vz[k]);
-        }
-        if (lane == __ffs(grp) - 1) {
-          const unsigned la = (unsigned)(ra - w.row0), lb = (unsigned)(rb - w.row0);
-          if (la < (unsigned)w.rows && lb < (unsigned)w.rows) {
-            const int k0 = (int)la * ws, k1 = (int)lb * ws;
-            atomicAdd(win_r + k0 + ca, vr[0]); atomicAdd(win_z + k0 + ca, vz[0]);
-            atomicAdd(win_r + k0 + cb, vr[1]); atomicAdd(win_z + k0 + cb, vz[1]);
-            atomicAdd(win_r + k1 + ca, vr[2]); atomicAdd(win_z + k1 + ca, vz[2]);
-            atomicAdd(win_r + k1 + cb, vr[3]); atomicAdd(win_z + k1 + cb, vz[3]);
-            wc_max = max(wc_max, cb);
-          } else {
-            win_node(w, P, ca, ra, vr[0], vz[0]);
-            win_node(w, P, cb, ra, vr[1], vz[1]);
-            win_node(w, P, ca, rb, vr[2], vz[2]);
-            win_node(w, P, cb, rb, vr[3], vz[3]);
-            wc_max = max(wc_max, cb);     // win_node may use the window for one row
-          }
-        }
-      }
-    }
-    // the window columns this warp touched, merged into the block's
-    wc_max = __reduce_max_sync(0xFFFFFFFFu, wc_max);
-    if (lane == 0 && wc_max >= 0) atomicMax(&box_cmax, wc_max);
-    if (threadIdx.x == 0 && next_ch < nchunk) chunk_rows(next_ch, next_row0, next_rows);
+    chunk32(P, S, F, cnt, queue, step, mode, beg, end, w, &box_cmax);
+    if (threadIdx.x == 0 && next_ch < nchunk)
+      chunk_rows32(P, S, n0, chunk, next_ch, maxrows, next_row0, next_rows);
     __syncthreads();
-    // add the touched columns of the window rows to the grid (one 64-bit
-    // atomic per nonzero node) and zero them for the next chunk
-    const int bw = box_cmax + 1, nb = bw > 0 ? bw * w.rows : 0;
-    for (int i = threadIdx.x; i < nb; i += kBlock) {
-      const int row = i / bw, col = i - row * bw;
-      const int k = row * ws + col;
-      const int vr = win_r[k], vz = win_z[k];
-      if (vr | vz) {
-        const int64_t g = (int64_t)(w.row0 + row) * P.ldj + col;
-        if (vr) atomicAdd(P.Jr + g, (unsigned long long)(long long)vr);
-        if (vz) atomicAdd(P.Jz + g, (unsigned long long)(long long)vz);
-        win_r[k] = 0; win_z[k] = 0;
-      }
-    }
+    flush32(P, w, box_cmax + 1);
     __syncthreads();
   }
-  lost = __reduce_add_sync(0xFFFFFFFFu, lost);
-  if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
+}
+
+// ------------------------------------------------------- batched FP32 pass
+// One cell of a batch as the batched FP32 pass sees it (global memory): its
+// parameters with the current buffer 0 / 1 as the deposit target, its two
+// state buffers, counters, candidate queues and fields.
+struct BatchCell32 {
+  SimParams P[2];
+  State32 S[2];
+  SimCounters *cnt;
+  int *queue;
+  Fields<float> F;
+};
+
+// The FP32 pass of one step for every cell of a batch in one launch: each
+// block reads the cells' counters and forms the prefix sums of their
+// collision candidates and chunks; the candidates of all cells go first, one
+// per warp, then the blocks take (cell, chunk) work items from one counter
+// (*chunk_next, zeroed before the launch), copying the cell's parameters into
+// shared memory when the cell changes.  Every cell gives what its own
+// k_pass32 gives.
+__global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *__restrict__ cells,
+                                                            int ncell, int cur, int jb, int mode,
+                                                            unsigned long long *chunk_next) {
+  __shared__ int win_r[kWinNodes], win_z[kWinNodes];
+  __shared__ int win_row0, win_rows, box_cmax, cell_at;
+  __shared__ long long chunk_at;
+  __shared__ long long cand_pre[kMaxBatch + 1], chunk_pre[kMaxBatch + 1];
+  __shared__ __align__(16) unsigned char sP_raw[sizeof(SimParams)];
+  SimParams &sP = *reinterpret_cast<SimParams *>(sP_raw);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < kWinNodes; i += kBlock) { win_r[i] = 0; win_z[i] = 0; }
+  // per-cell candidates (of the previous pass) and chunks, then prefix sums
+  for (int c = threadIdx.x; c < ncell; c += kBlock) {
+    const SimCounters *cc = cells[c].cnt;
+    const long long step = cc->step;
+    cand_pre[c + 1] = mode != 1 ? (long long)cc->n_cand[(int)(step & 1) ^ 1] : 0;
+    const long long n0 = (long long)cc->n_total;
+    const int chunk = cells[c].P[jb].chunk;
+    chunk_pre[c + 1] = (n0 + chunk - 1) / chunk;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cand_pre[0] = 0; chunk_pre[0] = 0;
+    for (int c = 0; c < ncell; ++c) {
+      cand_pre[c + 1] += cand_pre[c];
+      chunk_pre[c + 1] += chunk_pre[c];
+    }
+  }
+  __syncthreads();
+  const long long nq = cand_pre[ncell], nchunk = chunk_pre[ncell];
+  for (long long k = (long long)blockIdx.x * (kBlock / 32) + warp; k < nq;
+       k += (long long)gridDim.x * (kBlock / 32)) {
+    if (lane == 0) {
+      const int c = cell_of_item(cand_pre, ncell, k);
+      const BatchCell32 &C = cells[c];
+      SimCounters *cc = C.cnt;
+      const long long step = cc->step;
+      const int *qin = C.queue + (long long)((int)(step & 1) ^ 1) * C.P[jb].cap;
+      unsigned lost = 0;
+      candidate32(&C.P[jb], C.F, C.S[cur], cc, C.queue, qin[k - cand_pre[c]], step, mode, true,
+                  (long long)cc->n_total, lost);
+      if (lost) atomicAdd(&cc->lost, (unsigned long long)lost);
+    }
+    __syncwarp();
+  }
+  // (cell, chunk) work items
+  long long next = 0;
+  int next_c = -1, next_row0 = 0, next_rows = 0;
+  auto fetch = [&]() {           // thread 0: the next item and its window rows
+    next = (long long)atomicAdd(chunk_next, 1ull);
+    if (next < nchunk) {
+      next_c = cell_of_item(chunk_pre, ncell, next);
+      const BatchCell32 &C = cells[next_c];
+      const SimParams &Pc = C.P[jb];
+      const int ws = win_stride(Pc.nr), maxrows = min(kWinNodes / ws, Pc.nz);
+      chunk_rows32(Pc, C.S[cur], (long long)C.cnt->n_total, Pc.chunk, next - chunk_pre[next_c],
+                   maxrows, next_row0, next_rows);
+    }
+  };
+  if (threadIdx.x == 0) { fetch(); cell_at = -1; }
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      chunk_at = next;
+      win_row0 = next_row0;
+      win_rows = next_rows;
+      box_cmax = -1;
+    }
+    __syncthreads();
+    const long long g = chunk_at;
+    if (g >= nchunk) break;
+    const int c = cell_of_item(chunk_pre, ncell, g);
+    if (c != cell_at) {          // this block's first chunk of cell c: its parameters
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(&cells[c].P[jb]);
+      uint32_t *dst = reinterpret_cast<uint32_t *>(sP_raw);
+      for (int i = threadIdx.x; i < (int)(sizeof(SimParams) / 4); i += kBlock) dst[i] = src[i];
+      __syncthreads();
+      if (threadIdx.x == 0) cell_at = c;
+    }
+    if (threadIdx.x == 0 && next < nchunk) fetch();
+    const BatchCell32 &C = cells[c];
+    SimCounters *cc = C.cnt;
+    const long long n0 = (long long)cc->n_total, step = cc->step;
+    const int chunk = sP.chunk;
+    const long long ch = g - chunk_pre[c];
+    const int beg = (int)(ch * chunk), end = (int)min((long long)beg + chunk, n0);
+    const Win32 w{win_r, win_z, win_row0, win_rows, win_stride(sP.nr)};
+    chunk32(sP, C.S[cur], C.F, cc, C.queue, step, mode, beg, end, w, &box_cmax);
+    __syncthreads();
+    flush32(sP, w, box_cmax + 1);
+  }
 }
 
 // The collisions still queued by the last FP32 pass, without the next push
@@ -1291,14 +1527,23 @@ __device__ __forceinline__ void commit_pass32(SimCounters *cnt) {
 // The field sub-cycle of one step for fdtd_ratio 1: the persistent TMA-fed
 // kernel of fdtd_tma.cuh.
 template <typename T>
-__global__ void __launch_bounds__(32 * kTmaRows, 1) k_sim_fdtd_tma(
-    const __grid_constant__ TmaMaps M, T *Er, T *Ez, T *H, unsigned long long *Jr_next,
-    unsigned long long *Jz_next, int nr, int nz, int ldf, int ldj, FdtdCoef c,
-    const double *invV, double mu, double dt, unsigned flags, SimCounters *cnt,
-    ExtraCurrent ion, FieldQuads quads, int ph, int tiles_x, int ntiles, unsigned *err) {
+__global__ void __launch_bounds__(32 * kTmaRows, 1) k_sim_fdtd_tma(const __grid_constant__ FdtdInst I,
+                                                               SimCounters *cnt, int ph) {
   if (cnt && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) commit_pass32(cnt);
-  fdtd_tma_body<T>(M, Er, Ez, H, Jr_next, Jz_next, nr, nz, ldf, ldj, c, invV, mu, dt, flags, ion,
-                   quads, ph, tiles_x, ntiles, err);
+  fdtd_tma_body<T>(FdtdWork{&I, nullptr, I.ntiles}, ph);
+}
+
+// The field update of every cell of a batch in one launch: the blocks walk a
+// table of (cell, tile) work items; FP32 form (commit given): the blocks first
+// commit the previous pass of every cell.
+template <typename T>
+__global__ void __launch_bounds__(32 * kTmaRows, 1) k_batch_fdtd_tma(const FdtdInst *insts,
+                                                                 const int2 *table, int nitems,
+                                                                 SimCounters *const *commit,
+                                                                 int ninst, int ph) {
+  if (commit && threadIdx.x == 0 && threadIdx.y == 0)
+    for (int i = blockIdx.x; i < ninst; i += gridDim.x) commit_pass32(commit[i]);
+  fdtd_tma_body<T>(FdtdWork{insts, table, nitems}, ph);
 }
 
 // The general sub-cycle (fdtd_ratio > 1): one 32 x 32 patch per block
@@ -1677,10 +1922,11 @@ struct gasatt_sim {
   State32 s32[2]{};
   int cur = 0;
   void *Er = nullptr, *Ez = nullptr, *H = nullptr;
-  // field update of fdtd_ratio 1: tensor maps of the fields and of the
-  // current buffer the step reads (index = that buffer), patch rows, tiles
-  TmaMaps tmaps[2];
-  int tma_rows = 0, tma_tiles_x = 0, tma_ntiles = 0;
+  // field update of fdtd_ratio 1: the cell's descriptor for the steps that
+  // read current buffer 0 / 1 (tensor maps, write-back targets, tiles), the
+  // patch rows, the grid and its shared memory
+  FdtdInst fdtd_inst[2];
+  int tma_rows = 0;
   unsigned tma_grid = 0;
   size_t tma_smem = 0;
   // Internal grid layout: column-major like the reference's arrays, with row
@@ -1709,6 +1955,7 @@ struct gasatt_sim {
   cudaGraphExec_t g_step[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [state buffer][step parity]
   cudaGraph_t gr_step[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};     // the same, not instantiated
   cudaGraphExec_t g_sort[2] = {nullptr, nullptr};
+  cudaGraph_t gr_sort[2] = {nullptr, nullptr};       // the same, not instantiated
   double scale = 1.0;
   unsigned pass_grid = 0, mcc_grid = 0;
   int *queue = nullptr;           // collision candidates, two queues of capacity slots
@@ -1764,19 +2011,14 @@ int launch_fdtd(gasatt_sim *s, cudaStream_t st, int q) {
   const double dt = c.dt / R;
   // the held ion current, in the electron current's fixed-point units
   const ExtraCurrent ion{s->Jir, s->Jiz, s->scale / s->ion_scale};
-  unsigned *err = &s->cnt->fdtd_err;
   if (R == 1) {
     const dim3 block(32, kTmaRows);
     if (s->form == 0)
-      k_sim_fdtd_tma<double><<<s->tma_grid, block, s->tma_smem, st>>>(
-          s->tmaps[q], (double *)s->Er, (double *)s->Ez, (double *)s->H, s->Jr[1 - q], s->Jz[1 - q],
-          nr, nz, s->ldf, s->ldj, fc, s->invV, c.mu0, dt, c.flags, nullptr, ion, FieldQuads{},
-          s->tma_rows, s->tma_tiles_x, s->tma_ntiles, err);
+      k_sim_fdtd_tma<double><<<s->tma_grid, block, s->tma_smem, st>>>(s->fdtd_inst[q], nullptr,
+                                                                      s->tma_rows);
     else
-      k_sim_fdtd_tma<float><<<s->tma_grid, block, s->tma_smem, st>>>(
-          s->tmaps[q], (float *)s->Er, (float *)s->Ez, (float *)s->H, s->Jr[1 - q], s->Jz[1 - q],
-          nr, nz, s->ldf, s->ldj, fc, s->invV, c.mu0, dt, c.flags, s->cnt, ion, s->quads,
-          s->tma_rows, s->tma_tiles_x, s->tma_ntiles, err);
+      k_sim_fdtd_tma<float><<<s->tma_grid, block, s->tma_smem, st>>>(s->fdtd_inst[q], s->cnt,
+                                                                     s->tma_rows);
     s->ctx->launches++;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(s->ctx, e, "fdtd launch");
@@ -1949,6 +2191,8 @@ void drop_graphs(gasatt_sim *s) {
     }
     if (s->g_sort[i]) cudaGraphExecDestroy(s->g_sort[i]);
     s->g_sort[i] = nullptr;
+    if (s->gr_sort[i]) cudaGraphDestroy(s->gr_sort[i]);
+    s->gr_sort[i] = nullptr;
   }
 }
 
@@ -2036,9 +2280,9 @@ int setup_fdtd_tma(gasatt_sim *s, int nsm) {
   const TmaSmem<T> L(ph);
   s->tma_rows = ph;
   s->tma_smem = L.total();
-  s->tma_tiles_x = (c.n_r + 1 + kTmaTileW - 1) / kTmaTileW;
+  const int tiles_x = (c.n_r + 1 + kTmaTileW - 1) / kTmaTileW;
   const int tiles_y = (c.n_z + 1 + (ph - 2 * kTmaHalo) - 1) / (ph - 2 * kTmaHalo);
-  s->tma_ntiles = s->tma_tiles_x * tiles_y;
+  const int ntiles = tiles_x * tiles_y;
   GASATT_CUDA(s->ctx, cudaFuncSetAttribute(k_sim_fdtd_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)s->tma_smem));
   int occ = 0;
@@ -2046,17 +2290,32 @@ int setup_fdtd_tma(gasatt_sim *s, int nsm) {
                                                                     s->tma_smem));
   if (occ < 1) return fail(s->ctx, GASATT_E_ARG, "field update: patch does not fit in shared memory");
   const long long slots = (long long)nsm * occ;
-  s->tma_grid = (unsigned)(slots < s->tma_ntiles ? slots : s->tma_ntiles);
+  s->tma_grid = (unsigned)(slots < ntiles ? slots : ntiles);
   const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
   const size_t ldb = (size_t)s->ldf * sizeof(T), ldjb = (size_t)s->ldj * 8;
   const int bw = TmaBox<T>::w;
   for (int q = 0; q < 2; ++q) {
-    TmaMaps &M = s->tmaps[q];
+    FdtdInst &I = s->fdtd_inst[q];
+    std::memset(&I, 0, sizeof(I));
+    TmaMaps &M = I.maps;
     SIM_TRY(encode_map(s, &M.er, ft, s->Er, c.n_r, c.n_z + 1, ldb, bw, ph));
     SIM_TRY(encode_map(s, &M.ez, ft, s->Ez, c.n_r + 1, c.n_z, ldb, bw, ph));
     SIM_TRY(encode_map(s, &M.h, ft, s->H, c.n_r, c.n_z, ldb, bw, ph));
     SIM_TRY(encode_map(s, &M.jr, CU_TENSOR_MAP_DATA_TYPE_INT64, s->Jr[q], c.n_r, c.n_z, ldjb, 34, ph));
     SIM_TRY(encode_map(s, &M.jz, CU_TENSOR_MAP_DATA_TYPE_INT64, s->Jz[q], c.n_r, c.n_z, ldjb, 34, ph));
+    I.Er = s->Er; I.Ez = s->Ez; I.H = s->H;
+    I.Jr_next = s->Jr[1 - q]; I.Jz_next = s->Jz[1 - q];
+    I.invV = s->invV;
+    I.xj = ExtraCurrent{s->Jir, s->Jiz, s->scale / s->ion_scale};
+    I.q = sizeof(T) == 4 ? s->quads : FieldQuads{};
+    I.c = fdtd_coef(s);
+    I.mu = c.mu0;
+    I.dt = c.dt;
+    I.nr = c.n_r; I.nz = c.n_z; I.ldf = s->ldf; I.ldj = s->ldj;
+    I.flags = c.flags;
+    I.tiles_x = tiles_x;
+    I.ntiles = ntiles;
+    I.err = &s->cnt->fdtd_err;
   }
   return GASATT_OK;
 }
@@ -2167,7 +2426,9 @@ int build_graphs(gasatt_sim *s) {
       e = cudaGraphInstantiate(&s->g_sort[b], g, 0);
       if (e != cudaSuccess) rc = cuda_fail(s->ctx, e, "instantiate sort");
     }
-    if (captured) cudaGraphDestroy(g);
+    if (captured) {
+      if (!rc) s->gr_sort[b] = g; else cudaGraphDestroy(g);
+    }
   }
   s->cur = save;
   s->ctx->launches = save_launch;
@@ -3070,29 +3331,243 @@ int gasatt_sim_run_host(gasatt_sim *s, double *pos, double *vel, int64_t *n_io, 
 }
 
 // ================================================================ batches
-// Many independent gas cells stepped together: one CUDA graph holds the step
-// graphs of all instances side by side (no dependencies between them), so
-// small cells fill the GPU together and one launch advances them all.  The
-// instances share a sort period, so they swap state buffers in lockstep; if
-// one is ever out of step (stepped on its own in between), the batch steps
-// each instance with its own graph.
+// Many independent gas cells stepped together.  Cells of the same precision
+// form and field patch (fdtd_ratio 1) form a group that runs each step as a
+// few launches for the whole group - the field update over every cell's
+// tiles (k_batch_fdtd_tma), (FP64: the commits and the collisions beside it,)
+// then the particle pass over every cell's candidates and chunks
+// (k_batch_pass32 / k_batch_pass64) - instead of one set of launches per
+// cell, so the blocks of each launch share all cells' work and small cells
+// do not leave the GPU idle.  Groups, and any cell that fits no group
+// (fdtd_ratio > 1), run side by side as branches of one graph.  The cells
+// share a sort period, so they swap state buffers in lockstep; if one is
+// ever out of step (stepped on its own in between), the batch steps each
+// cell with its own graph.
+struct BatchGroup {
+  int form = 0, ph = 0;
+  std::vector<gasatt_sim *> sims;
+  void *cells = nullptr;                 // BatchCell32 / BatchCell64 per cell
+  FdtdInst *insts[2] = {nullptr, nullptr};   // per step parity (the current buffer read)
+  int2 *table = nullptr;                 // (cell, tile) work items of the field update
+  int nitems = 0;
+  SimCounters **commit = nullptr;        // FP32: counters the field update commits
+  unsigned long long *chunk_next = nullptr;
+  unsigned fdtd_grid = 0, pass_grid = 0, mcc_grid = 0;
+  size_t fdtd_smem = 0;
+};
+
 struct gasatt_batch {
   gasatt_ctx *ctx = nullptr;
   std::vector<gasatt_sim *> sims;
+  std::vector<BatchGroup> groups;
+  std::vector<gasatt_sim *> singles;     // cells stepped by their own step graph
+  std::vector<void *> allocs;
   int sort_period = 0;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   cudaGraphExec_t g[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [state buffer][parity]
+  cudaGraphExec_t g_sort[2] = {nullptr, nullptr};   // every cell's sort side by side [state buffer]
 };
 
 int gasatt_batch_destroy(gasatt_batch *b) {
   if (!b) return GASATT_OK;
   cudaSetDevice(b->ctx->device);
   cudaStreamSynchronize(b->ctx->stream);
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < 2; ++i) {
     for (int q = 0; q < 2; ++q)
       if (b->g[i][q]) cudaGraphExecDestroy(b->g[i][q]);
+    if (b->g_sort[i]) cudaGraphExecDestroy(b->g_sort[i]);
+  }
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+  if (b->join_ev) cudaEventDestroy(b->join_ev);
+  for (void *p : b->allocs) cudaFree(p);
   delete b;
   return GASATT_OK;
 }
+
+extern "C++" {
+namespace {
+
+template <typename T>
+int batch_alloc(gasatt_batch *b, T **p, size_t n) {
+  cudaError_t e = cudaMalloc((void **)p, (n ? n : 1) * sizeof(T));
+  if (e != cudaSuccess) return cuda_fail(b->ctx, e, "cudaMalloc (batch)");
+  b->allocs.push_back((void *)*p);
+  return GASATT_OK;
+}
+
+// device tables of a group: the cells' pass and field-update descriptors,
+// the field update's work items, the commit list, the chunk counter, grids
+int batch_group_setup(gasatt_batch *b, BatchGroup &G) {
+  gasatt_ctx *ctx = b->ctx;
+  const int n = (int)G.sims.size();
+  if (G.form == 1) {
+    std::vector<BatchCell32> h(n);
+    std::vector<SimCounters *> cm(n);
+    for (int i = 0; i < n; ++i) {
+      gasatt_sim *s = G.sims[i];
+      for (int jb = 0; jb < 2; ++jb) {
+        h[i].P[jb] = s->P;
+        h[i].P[jb].Jr = s->Jr[jb]; h[i].P[jb].Jz = s->Jz[jb];
+      }
+      h[i].S[0] = s->s32[0]; h[i].S[1] = s->s32[1];
+      h[i].cnt = s->cnt; h[i].queue = s->queue;
+      h[i].F = Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H};
+      cm[i] = s->cnt;
+    }
+    BatchCell32 *d;
+    SIM_TRY(batch_alloc(b, &d, (size_t)n));
+    GASATT_CUDA(ctx, cudaMemcpy(d, h.data(), sizeof(BatchCell32) * n, cudaMemcpyHostToDevice));
+    G.cells = d;
+    SIM_TRY(batch_alloc(b, &G.commit, (size_t)n));
+    GASATT_CUDA(ctx, cudaMemcpy(G.commit, cm.data(), sizeof(SimCounters *) * n, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<BatchCell64> h(n);
+    for (int i = 0; i < n; ++i) {
+      gasatt_sim *s = G.sims[i];
+      for (int jb = 0; jb < 2; ++jb) {
+        h[i].P[jb] = s->P;
+        h[i].P[jb].Jr = s->Jr[jb]; h[i].P[jb].Jz = s->Jz[jb];
+      }
+      h[i].S[0] = s->s64[0]; h[i].S[1] = s->s64[1];
+      h[i].cnt = s->cnt; h[i].queue = s->queue;
+      h[i].F = Fields<double>{(double *)s->Er, (double *)s->Ez, (double *)s->H};
+    }
+    BatchCell64 *d;
+    SIM_TRY(batch_alloc(b, &d, (size_t)n));
+    GASATT_CUDA(ctx, cudaMemcpy(d, h.data(), sizeof(BatchCell64) * n, cudaMemcpyHostToDevice));
+    G.cells = d;
+  }
+  std::vector<int2> table;
+  for (int i = 0; i < n; ++i)
+    for (int t = 0; t < G.sims[i]->fdtd_inst[0].ntiles; ++t) table.push_back(make_int2(i, t));
+  G.nitems = (int)table.size();
+  SIM_TRY(batch_alloc(b, &G.table, table.size()));
+  GASATT_CUDA(ctx, cudaMemcpy(G.table, table.data(), sizeof(int2) * table.size(), cudaMemcpyHostToDevice));
+  for (int q = 0; q < 2; ++q) {
+    std::vector<FdtdInst> hi(n);
+    for (int i = 0; i < n; ++i) hi[i] = G.sims[i]->fdtd_inst[q];
+    SIM_TRY(batch_alloc(b, &G.insts[q], (size_t)n));
+    GASATT_CUDA(ctx, cudaMemcpy(G.insts[q], hi.data(), sizeof(FdtdInst) * n, cudaMemcpyHostToDevice));
+  }
+  SIM_TRY(batch_alloc(b, &G.chunk_next, 1));
+  int nsm = 148, occ = 1;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+  G.fdtd_smem = G.sims[0]->tma_smem;
+  if (G.form == 1) {
+    GASATT_CUDA(ctx, cudaFuncSetAttribute(k_batch_fdtd_tma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.fdtd_smem));
+    GASATT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_fdtd_tma<float>, 32 * kTmaRows, G.fdtd_smem));
+  } else {
+    GASATT_CUDA(ctx, cudaFuncSetAttribute(k_batch_fdtd_tma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.fdtd_smem));
+    GASATT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_fdtd_tma<double>, 32 * kTmaRows, G.fdtd_smem));
+  }
+  const long long fslots = (long long)nsm * (occ > 0 ? occ : 1);
+  G.fdtd_grid = (unsigned)(fslots < G.nitems ? fslots : (G.nitems > 0 ? G.nitems : 1));
+  occ = 1;
+  if (G.form == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_pass32, kBlock, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_pass64, kBlock, 0);
+  G.pass_grid = (unsigned)(nsm * (occ > 0 ? occ : 1));
+  occ = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_mcc64, kMccBlock, 0);
+  G.mcc_grid = (unsigned)(nsm * (occ > 0 ? occ : 1));
+  return GASATT_OK;
+}
+
+// one step of group G (state buffer cur, step parity q) onto the capturing
+// stream cs (side: a second stream for the FP64 collision branch)
+int batch_group_launch(gasatt_batch *b, BatchGroup &G, cudaStream_t cs, cudaStream_t side, int cur,
+                       int q) {
+  gasatt_ctx *ctx = b->ctx;
+  const int n = (int)G.sims.size();
+  const dim3 fb(32, kTmaRows);
+  if (G.form == 1) {
+    k_batch_fdtd_tma<float><<<G.fdtd_grid, fb, G.fdtd_smem, cs>>>(G.insts[q], G.table, G.nitems, G.commit,
+                                                                 n, G.ph);
+    GASATT_CUDA(ctx, cudaGetLastError());
+    GASATT_CUDA(ctx, cudaMemsetAsync(G.chunk_next, 0, 8, cs));
+    k_batch_pass32<<<G.pass_grid, kBlock, 0, cs>>>((const BatchCell32 *)G.cells, n, cur, 1 - q, 0,
+                                                   G.chunk_next);
+    GASATT_CUDA(ctx, cudaGetLastError());
+    return GASATT_OK;
+  }
+  GASATT_CUDA(ctx, cudaEventRecord(b->fork_ev, cs));
+  GASATT_CUDA(ctx, cudaStreamWaitEvent(side, b->fork_ev, 0));
+  k_batch_commit64<<<1, 256, 0, side>>>((const BatchCell64 *)G.cells, n, 1 - q);
+  k_batch_mcc64<<<G.mcc_grid, kMccBlock, 0, side>>>((const BatchCell64 *)G.cells, n, cur, 1 - q);
+  GASATT_CUDA(ctx, cudaGetLastError());
+  GASATT_CUDA(ctx, cudaEventRecord(b->join_ev, side));
+  k_batch_fdtd_tma<double><<<G.fdtd_grid, fb, G.fdtd_smem, cs>>>(G.insts[q], G.table, G.nitems, nullptr,
+                                                                n, G.ph);
+  GASATT_CUDA(ctx, cudaGetLastError());
+  GASATT_CUDA(ctx, cudaStreamWaitEvent(cs, b->join_ev, 0));
+  GASATT_CUDA(ctx, cudaMemsetAsync(G.chunk_next, 0, 8, cs));
+  k_batch_pass64<<<G.pass_grid, kBlock, 0, cs>>>((const BatchCell64 *)G.cells, n, cur, 1 - q, 0, q,
+                                                 G.chunk_next);
+  GASATT_CUDA(ctx, cudaGetLastError());
+  return GASATT_OK;
+}
+
+int batch_build_graphs(gasatt_batch *b) {
+  gasatt_ctx *ctx = b->ctx;
+  cudaStream_t cs, side;
+  GASATT_CUDA(ctx, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  if (cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaStreamDestroy(cs);
+    return fail(ctx, GASATT_E_CUDA, "batch: stream");
+  }
+  int rc = GASATT_OK;
+  for (int bi = 0; bi < 2 && !rc; ++bi) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) { rc = cuda_fail(ctx, e, "batch sort graph"); break; }
+    for (size_t i = 0; i < b->sims.size() && !rc; ++i) {
+      cudaGraphNode_t node;
+      e = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, b->sims[i]->gr_sort[bi]);
+      if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batch sort graph");
+    }
+    if (!rc) {
+      e = cudaGraphInstantiate(&b->g_sort[bi], g, 0);
+      if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batch sort graph");
+    }
+    cudaGraphDestroy(g);
+  }
+  for (int bi = 0; bi < 2 && !rc; ++bi)
+    for (int q = 0; q < 2 && !rc; ++q) {
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaGraphCreate(&g, 0);
+      if (e != cudaSuccess) { rc = cuda_fail(ctx, e, "batch graph"); break; }
+      for (BatchGroup &G : b->groups) {
+        cudaGraph_t child = nullptr;
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) { rc = cuda_fail(ctx, e, "batch capture"); break; }
+        rc = batch_group_launch(b, G, cs, side, bi, q);
+        const cudaError_t e2 = cudaStreamEndCapture(cs, &child);
+        if (!rc && e2 != cudaSuccess) rc = cuda_fail(ctx, e2, "batch capture");
+        if (!rc) {
+          cudaGraphNode_t node;
+          e = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, child);
+          if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batch graph");
+        }
+        if (child) cudaGraphDestroy(child);
+        if (rc) break;
+      }
+      for (size_t i = 0; i < b->singles.size() && !rc; ++i) {
+        cudaGraphNode_t node;
+        e = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, b->singles[i]->gr_step[bi][q]);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batch graph");
+      }
+      if (!rc) {
+        e = cudaGraphInstantiate(&b->g[bi][q], g, 0);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batch graph");
+      }
+      cudaGraphDestroy(g);
+    }
+  cudaStreamDestroy(side);
+  cudaStreamDestroy(cs);
+  return rc;
+}
+
+}  // namespace
+}  // extern "C++"
 
 int gasatt_batch_create(gasatt_ctx *ctx, gasatt_sim *const *sims, int n, int sort_period,
                         gasatt_batch **out) {
@@ -3112,21 +3587,30 @@ int gasatt_batch_create(gasatt_ctx *ctx, gasatt_sim *const *sims, int n, int sor
   b->sims.assign(sims, sims + n);
   b->sort_period = sort_period;
   for (gasatt_sim *s : b->sims) s->cfg.sort_period = sort_period;
-  for (int bi = 0; bi < 2; ++bi)
-    for (int q = 0; q < 2; ++q) {
-      cudaGraph_t g = nullptr;
-      cudaError_t e = cudaGraphCreate(&g, 0);
-      for (int i = 0; i < n && e == cudaSuccess; ++i) {
-        cudaGraphNode_t node;
-        e = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, b->sims[i]->gr_step[bi][q]);
-      }
-      if (e == cudaSuccess) e = cudaGraphInstantiate(&b->g[bi][q], g, 0);
-      if (g) cudaGraphDestroy(g);
-      if (e != cudaSuccess) {
-        gasatt_batch_destroy(b);
-        return cuda_fail(ctx, e, "batch graph");
-      }
+  // groups of cells with the same form and field patch; up to kMaxBatch each
+  for (gasatt_sim *s : b->sims) {
+    if (s->cfg.fdtd_ratio != 1) { b->singles.push_back(s); continue; }
+    BatchGroup *G = nullptr;
+    for (BatchGroup &g : b->groups)
+      if (g.form == s->form && g.ph == s->tma_rows && (int)g.sims.size() < kMaxBatch) G = &g;
+    if (!G) {
+      b->groups.emplace_back();
+      G = &b->groups.back();
+      G->form = s->form;
+      G->ph = s->tma_rows;
     }
+    G->sims.push_back(s);
+  }
+  int rc = GASATT_OK;
+  if (cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->join_ev, cudaEventDisableTiming) != cudaSuccess)
+    rc = fail(ctx, GASATT_E_CUDA, "batch: event");
+  for (size_t i = 0; i < b->groups.size() && !rc; ++i) rc = batch_group_setup(b, b->groups[i]);
+  if (!rc) rc = batch_build_graphs(b);
+  if (rc) {
+    gasatt_batch_destroy(b);
+    return rc;
+  }
   *out = b;
   return GASATT_OK;
 }
@@ -3138,8 +3622,25 @@ int gasatt_batch_step(gasatt_batch *b, int nsteps) {
   cudaStream_t st = ctx->stream;
   for (int k = 0; k < nsteps; ++k) {
     for (gasatt_sim *s : b->sims) SIM_TRY(sim_prime(s));
-    for (gasatt_sim *s : b->sims)
-      if (b->sort_period > 0 && s->since_sort >= b->sort_period) SIM_TRY(gasatt_sim_sort(s));
+    if (b->sort_period > 0) {
+      // every cell due at once (the batch keeps them in lockstep): one graph
+      // sorts them all side by side
+      bool all_due = true;
+      for (const gasatt_sim *s : b->sims)
+        all_due = all_due && s->since_sort >= b->sort_period && s->cur == b->sims[0]->cur;
+      if (all_due) {
+        for (gasatt_sim *s : b->sims) SIM_TRY(flush_collisions(s));
+        GASATT_CUDA(ctx, cudaGraphLaunch(b->g_sort[b->sims[0]->cur], st));
+        for (gasatt_sim *s : b->sims) {
+          ctx->launches += 4;
+          s->cur = 1 - s->cur;
+          s->since_sort = 0;
+        }
+      } else {
+        for (gasatt_sim *s : b->sims)
+          if (s->since_sort >= b->sort_period) SIM_TRY(gasatt_sim_sort(s));
+      }
+    }
     const gasatt_sim *s0 = b->sims[0];
     bool lockstep = true;
     for (const gasatt_sim *s : b->sims)
@@ -3147,12 +3648,15 @@ int gasatt_batch_step(gasatt_batch *b, int nsteps) {
                  !s->timing;
     if (lockstep) {
       GASATT_CUDA(ctx, cudaGraphLaunch(b->g[s0->cur][s0->host_step & 1], st));
+      for (const BatchGroup &G : b->groups) ctx->launches += G.form == 0 ? 4 : 2;
+      for (const gasatt_sim *s : b->singles) ctx->launches += s->form == 0 ? 4 : 2;
     } else {
-      for (gasatt_sim *s : b->sims)
+      for (gasatt_sim *s : b->sims) {
         GASATT_CUDA(ctx, cudaGraphLaunch(s->g_step[s->cur][s->host_step & 1], st));
+        ctx->launches += s->form == 0 ? 4 : 2;
+      }
     }
     for (gasatt_sim *s : b->sims) {
-      ctx->launches += s->form == 0 ? 4 : 2;
       s->host_step++;
       s->since_sort++;
       s->mcc_pending = true;

@@ -103,3 +103,57 @@ def test_batch_with_ions_and_gas_maps_equals_instances_alone():
     batch.close()
     for s in sims:
         s.close()
+
+
+def test_batch_groups_share_launches_and_keep_cells_exact():
+    """Twelve FP32 cells of uneven grids and populations, four FP64 cells and
+    one cell with a field sub-cycle of 2 (which fits no group and keeps its own
+    step graph): each batch step launches the group kernels once per group
+    (FP32: field update + pass; FP64: commit, collisions, field update, pass)
+    plus the odd cell's own, and every cell ends bit for bit where it ends
+    alone."""
+    rng = np.random.default_rng(5)
+    cells = []
+    for i in range(16):
+        nr, nz = [(16, 48), (32, 64), (24, 120), (48, 96)][i % 4]
+        cells.append((nr, nz, 5e-6, float(10 ** rng.uniform(0.5, 2.5)), int(rng.integers(300, 3000)),
+                      float(rng.uniform(3, 15)), _lib.FP32_SPLIT if i < 12 else _lib.FP64, 100 + i))
+    ctx = Context(0)
+
+    def make_any(cell, ratio=1):
+        nr, nz, d, torr, photo, kev, prec, seed = cell
+        cfg = config(nr, nz, d, 1e-14, torr, precision=prec, capacity=8 * photo, seed=seed,
+                     sort_period=50, fdtd_ratio=ratio)
+        sim = Sim(cfg, ctx=ctx)
+        sim.load(*births(photo, kev, nz * d, seed=seed, sigma_r=nr * d / 4, Rp=nr * d))
+        return sim
+
+    odd = (32, 64, 5e-6, 50.0, 1500, 8.0, _lib.FP32_SPLIT, 99)
+    alone = []
+    for cell in cells:
+        sim = make_any(cell)
+        sim.step(9)
+        alone.append(snapshot(sim))
+        sim.close()
+    sim = make_any(odd, 2)
+    sim.step(9)
+    alone.append(snapshot(sim))
+    sim.close()
+    sims = [make_any(c) for c in cells] + [make_any(odd, 2)]
+    batch = Batch(sims, sort_period=50)
+    batch.step(1)                                    # primes and sorts every cell
+    l0 = ctx.launches
+    batch.step(8)
+    assert ctx.launches - l0 == 8 * (2 + 4 + 2)      # FP32 group, FP64 group, the odd cell
+    for sim, ref in zip(sims, alone):
+        got = snapshot(sim)
+        for a, b in zip(got[1] + got[2], ref[1] + ref[2]):
+            np.testing.assert_array_equal(a, b)
+        assert got[3] == ref[3]
+        for k in ref[0]:
+            np.testing.assert_array_equal(got[0][k], ref[0][k], err_msg=k)
+    assert sum(r[3][0] for r in alone) > 100
+    batch.close()
+    for s in sims:
+        s.close()
+    ctx.close()
