@@ -33,9 +33,11 @@ WORKLOAD_NAME = ("2,000,000 e- from 1,000,000 photoionizations at 8 keV (photoel
                  "dipole about x; Auger 360 eV isotropic), N2 1 Torr 300 K, 256x1024 cells at 5 um, "
                  "dt 1e-14 s, Rayleigh sigma 50 um, secondaries on, seed 1")
 L2_FLUSH_BYTES = 256 << 20
-# algorithmic bytes: per alive particle-step, FP32 split: 24 B state read + 24 B written
-# + 8 B id read; FP64: 40 + 40 + 8.  Grid term per step: field gather (3 fields) + current.
-BYTES_PER_PARTICLE = {"fp32_split": 56, "fp64": 88}
+# algorithmic bytes: per alive particle-step, twice the state (read + written): FP32 split
+# 24 B (int32 cell key, 2 x f32 offsets, 3 x f32 gamma*v), FP64 40 B (r, z, 3 x gamma*v); the
+# id the random streams are keyed on is not counted.  Grid term per step: field gather
+# (3 fields) + current (2 x int64).
+BYTES_PER_PARTICLE = {"fp32_split": 48, "fp64": 80}
 GRID_BYTES_PER_CELL = {"fp32_split": 3 * 4 + 2 * 8, "fp64": 3 * 8 + 2 * 8}
 
 
