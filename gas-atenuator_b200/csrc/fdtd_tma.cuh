@@ -1,5 +1,5 @@
-// fdtd_tma.cuh - the field sub-cycle of the resident simulation (fdtd_ratio 1)
-// as a persistent kernel fed by TMA tile copies.
+// fdtd_tma.cuh - the field sub-cycle of the resident simulation (fdtd_ratio 1):
+// one warp per patch, the patch staged by TMA, the sub-cycle in registers.
 //
 // One launch advances the fields by one particle step: H(dt/4), E(dt/2),
 // H(dt/2), E(dt/2), H(dt/4) (EM3_1.cu:2-17 and EM3.cu:2-43, called as the
@@ -7,30 +7,32 @@
 // the reference-layout kernels of fdtd.cuh.
 //
 // Work: the grid (n_r + 1 columns x n_z + 1 rows of Yee points) is cut into
-// tiles of 26 columns x (PH - 6) rows.  A block owns a patch of 32 columns x
-// PH rows around its tile (3 halo columns and rows on each side: the five
+// tiles of 26 columns x (R - 6) rows.  A warp owns a patch of 32 columns x R
+// rows around its tile (3 halo columns and rows on each side: the five
 // sub-updates need two on the low side and three on the high side, and one
-// more on the low side lets the block assemble every gather quad of its tile
-// from values it computed).  Blocks are persistent and walk the tiles
-// block-stride; for each tile one thread issues five 2D tensor copies (Er,
-// Ez, H as stored, Jr, Jz as 64-bit fixed point) into a staging buffer in
-// shared memory, completing on an mbarrier.  The copies of the next tile go
-// out before the current one is computed (two staging buffers), so a block's
-// loads overlap its arithmetic.  The staged values are widened into double
-// working arrays (the current scaled by 1 / shell volume), the five
-// sub-updates run there, and the tile is written back: the fields in their
-// storage type, zeros into the other current buffer, and - FP32 form - the
-// whole gather quads of the tile.
+// more on the low side lets the warp assemble every gather quad of its tile
+// from values it computed).  Lane l holds column l of the patch - Er, Ez, H
+// and the two current terms of all R rows - in registers: vertical
+// neighbours are registers, horizontal ones are warp shuffles, so the warps
+// never wait on one another (no block barrier) and the halo is recomputed by
+// each warp instead of exchanged.
+//
+// Staging: one lane of each warp issues five 2D tensor copies (Er, Ez, H as
+// stored, Jr, Jz as 64-bit fixed point) of its patch into the warp's own
+// staging area, completing on the warp's mbarrier.  Once the lanes hold the
+// patch in registers the area is free, and the copies of the warp's next
+// patch go out before the current one is computed.  Warps walk the work items
+// warp-stride.
 //
 // TMA copies want 16-byte aligned starting columns: each box starts at the
 // patch's first column rounded down to a 16-byte boundary and is wide enough
 // (36 floats, 34 doubles or 64-bit counters) to cover the 32 patch columns
-// from there; a thread reads its column at that offset.  Points outside the
+// from there; a lane reads its column at that offset.  Points outside the
 // grid (negative or beyond the extent) arrive as zeros and are never updated.
 //
-// Every wait on an mbarrier is bounded; a block whose copy has not completed
-// after the bound sets the cell's *err, waits (bounded) for its other copy in
-// flight and returns.
+// Every wait on an mbarrier is bounded; a warp whose copy has not completed
+// after the bound sets the cell's *err, waits (bounded) once more for that
+// copy and returns.
 #pragma once
 #include <cuda.h>
 #include "fdtd.cuh"
@@ -39,8 +41,8 @@ namespace gasatt {
 
 constexpr int kTmaTileW = 26;                 // output columns per tile
 constexpr int kTmaPatchW = 32;                // patch columns (one per lane)
-constexpr int kTmaRows = 16;                  // blockDim = (32, kTmaRows)
 constexpr int kTmaHalo = 3;                   // halo columns / rows on each side
+constexpr int kTmaWarps = 1;                  // warps per block (each on its own patches)
 constexpr unsigned kTmaWaitLimit = 1u << 22;  // try_wait rounds before giving up
 
 // staging box widths (elements): 32 columns from an aligned start below the
@@ -91,25 +93,19 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
 }
 
 // ------------------------------------------------------------ layout
-// Byte offsets of the dynamic shared memory of k_fdtd_tma for PH patch rows:
-// two staging buffers (Er, Ez, H in T, Jr, Jz in 64 bits; each 128-byte
-// aligned), the double working arrays, two mbarriers.
-template <typename T>
-struct TmaSmem {
-  int ph;
-  __host__ __device__ explicit TmaSmem(int ph_) : ph(ph_) {}
-  __host__ __device__ static size_t up(size_t b) { return (b + 127) & ~(size_t)127; }
-  __host__ __device__ size_t field_bytes() const { return up((size_t)TmaBox<T>::w * ph * sizeof(T)); }
-  __host__ __device__ size_t cur_bytes() const { return up((size_t)34 * ph * 8); }
-  __host__ __device__ size_t stage_bytes() const { return 3 * field_bytes() + 2 * cur_bytes(); }
-  __host__ __device__ size_t work_bytes() const { return (size_t)ph * kTmaPatchW * 8; }
-  __host__ __device__ size_t work_off() const { return 2 * stage_bytes(); }
-  __host__ __device__ size_t bar_off() const { return work_off() + 5 * work_bytes(); }
-  __host__ __device__ size_t total() const { return bar_off() + 16; }
-  // bytes one tile's five copies deliver (whole boxes, out-of-bounds fill included)
-  __host__ __device__ uint32_t tx_bytes() const {
-    return (uint32_t)(3 * (size_t)TmaBox<T>::w * ph * sizeof(T) + 2 * (size_t)34 * ph * 8);
-  }
+// One warp's staging area for R patch rows (Er, Ez, H in T, Jr, Jz in 64 bits;
+// each 128-byte aligned).  A block holds kTmaWarps areas, then one mbarrier
+// per warp.
+template <typename T, int R>
+struct TmaStage {
+  static constexpr size_t up(size_t b) { return (b + 127) & ~(size_t)127; }
+  static constexpr size_t field_bytes = up((size_t)TmaBox<T>::w * R * sizeof(T));
+  static constexpr size_t cur_bytes = up((size_t)34 * R * 8);
+  static constexpr size_t bytes = 3 * field_bytes + 2 * cur_bytes;
+  static constexpr size_t block_bytes = kTmaWarps * bytes + 128;
+  // bytes one patch's five copies deliver (whole boxes, out-of-bounds fill included)
+  static constexpr uint32_t tx_bytes =
+      (uint32_t)(3 * (size_t)TmaBox<T>::w * R * sizeof(T) + 2 * (size_t)34 * R * 8);
 };
 
 struct TmaMaps {
@@ -125,11 +121,14 @@ struct FdtdInst {
   TmaMaps maps;
   void *Er, *Ez, *H;
   unsigned long long *Jr_next, *Jz_next;
-  const double *invV;
+  // per column i in [0, n_r]: {1/V scaled from fixed point, coefficient of
+  // H(i) and of H(i-1) in the Ez update} (FdtdColumn), precomputed on the host
+  // with the expressions the kernels of fdtd.cuh evaluate per thread
+  const double *colc;
   ExtraCurrent xj;
   FieldQuads q;
   FdtdCoef c;
-  double mu, dt;
+  double chr4, chz4, chr2, chz2;   // H update factors h/(mu dr), h/(mu dz) for h = dt/4, dt/2
   int nr, nz, ldf, ldj;
   unsigned flags;
   int tiles_x, ntiles;
@@ -151,214 +150,252 @@ struct FdtdWork {
 };
 
 // tile t of a tiles_x-wide row-major tile grid -> the patch origin (x0, y0)
-__device__ __forceinline__ void tma_patch_origin(int t, int tiles_x, int ph, int &x0, int &y0) {
+__device__ __forceinline__ void tma_patch_origin(int t, int tiles_x, int rows, int &x0, int &y0) {
   const int ty = t / tiles_x, tx = t - ty * tiles_x;
   x0 = tx * kTmaTileW - kTmaHalo;
-  y0 = ty * (ph - 2 * kTmaHalo) - kTmaHalo;
+  y0 = ty * (rows - 2 * kTmaHalo) - kTmaHalo;
 }
 
-template <typename T>
-__device__ __forceinline__ void tma_issue(const TmaMaps &M, unsigned char *stage, uint64_t *bar,
-                                          const TmaSmem<T> &L, int x0, int y0) {
-  constexpr int al = 16 / (int)sizeof(T);
-  const int xf = x0 & ~(al - 1), xj = x0 & ~1;       // floor to a 16-byte column
-  mbar_expect_tx(bar, L.tx_bytes());
-  tma_load_2d(stage, &M.er, xf, y0, bar);
-  tma_load_2d(stage + L.field_bytes(), &M.ez, xf, y0, bar);
-  tma_load_2d(stage + 2 * L.field_bytes(), &M.h, xf, y0, bar);
-  tma_load_2d(stage + 3 * L.field_bytes(), &M.jr, xj, y0, bar);
-  tma_load_2d(stage + 3 * L.field_bytes() + L.cur_bytes(), &M.jz, xj, y0, bar);
-}
-
-// issue the copies of work item t (thread 0)
-template <typename T>
+// issue the copies of work item t into a warp's staging area (one lane)
+template <typename T, int R>
 __device__ __forceinline__ void tma_issue_item(const FdtdWork &W, int t, unsigned char *stage,
-                                               uint64_t *bar, const TmaSmem<T> &L) {
+                                               uint64_t *bar) {
+  using S = TmaStage<T, R>;
+  constexpr int al = 16 / (int)sizeof(T);
   int lt, x0, y0;
   const FdtdInst &I = W.at(t, lt);
-  tma_patch_origin(lt, I.tiles_x, L.ph, x0, y0);
-  tma_issue<T>(I.maps, stage, bar, L, x0, y0);
+  tma_patch_origin(lt, I.tiles_x, R, x0, y0);
+  const int xf = x0 & ~(al - 1), xj = x0 & ~1;       // floor to a 16-byte column
+  const TmaMaps &M = I.maps;
+  mbar_expect_tx(bar, S::tx_bytes);
+  tma_load_2d(stage, &M.er, xf, y0, bar);
+  tma_load_2d(stage + S::field_bytes, &M.ez, xf, y0, bar);
+  tma_load_2d(stage + 2 * S::field_bytes, &M.h, xf, y0, bar);
+  tma_load_2d(stage + 3 * S::field_bytes, &M.jr, xj, y0, bar);
+  tma_load_2d(stage + 3 * S::field_bytes + S::cur_bytes, &M.jz, xj, y0, bar);
 }
 
 // The sub-cycle on the work items of W (cells on the padded layout: row
-// strides ldf for the fields, ldj for the currents).  The field arithmetic is
-// that of fdtd_tiled1 (fdtd.cuh).
-template <typename T>
-__device__ __forceinline__ void fdtd_tma_body(const FdtdWork &W, int ph) {
-  constexpr int PW = kTmaPatchW;
-  constexpr int al = 16 / (int)sizeof(T);
-  extern __shared__ __align__(1024) unsigned char smem[];
-  const TmaSmem<T> L(ph);
-  unsigned char *stage[2] = {smem, smem + L.stage_bytes()};
-  double *sEr = reinterpret_cast<double *>(smem + L.work_off());
-  double *sEz = sEr + ph * PW, *sH = sEz + ph * PW, *sJr = sH + ph * PW, *sJz = sJr + ph * PW;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L.bar_off());
-  const int li = threadIdx.x, tid = threadIdx.y * PW + threadIdx.x;
-  const int nrow_t = ph / kTmaRows;                  // patch rows per thread
-  const int ntiles = W.ntiles;
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+// strides ldf for the fields, ldj for the currents), R patch rows per warp.
+// The field arithmetic is that of fdtd_tiled1 (fdtd.cuh); the per-column
+// coefficients come from the cell's table, the current terms of the two E
+// updates are formed once per patch.
+template <typename T, int R>
+__device__ __forceinline__ void fdtd_warp_body(const FdtdWork &W) {
+  using S = TmaStage<T, R>;
+  static_assert(R > 2 * kTmaHalo && R <= 32, "patch rows");
+  constexpr int BW = TmaBox<T>::w, al = 16 / (int)sizeof(T);
+  constexpr unsigned FULL = 0xFFFFFFFFu;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  unsigned char *stage = smem + wib * S::bytes;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kTmaWarps * S::bytes) + wib;
+  const int ntiles = W.ntiles, stride = gridDim.x * kTmaWarps;
+  int t = blockIdx.x * kTmaWarps + wib;
+  if (lane == 0) {
+    mbar_init(bar, 1);
     mbar_fence_init();
   }
-  __syncthreads();
-  int t = blockIdx.x;
-  bool issued0 = false, issued1 = false;             // thread 0: a copy of buffer 0 / 1 in flight
-  if (tid == 0 && t < ntiles) {
-    tma_issue_item<T>(W, t, stage[0], &bar[0], L);
-    issued0 = true;
-  }
-  for (int k = 0; t < ntiles; t += gridDim.x, ++k) {
-    const int b = k & 1;
-    // the next item's copies go out now, into the buffer the previous item
-    // has finished with (every thread read it before the barriers below)
-    if (tid == 0 && t + (int)gridDim.x < ntiles) {
-      fence_proxy_async_smem();
-      tma_issue_item<T>(W, t + gridDim.x, stage[b ^ 1], &bar[b ^ 1], L);
-      if (b) issued0 = true; else issued1 = true;
-    }
-    const bool ok = mbar_wait(&bar[b], (uint32_t)((k >> 1) & 1));
-    if (tid == 0 && ok) { if (b) issued1 = false; else issued0 = false; }
-    if (__syncthreads_or(!ok)) {
-      int lt;
-      if (tid == 0) atomicOr(W.at(t, lt).err, 1u);
-      break;
-    }
+  __syncwarp();
+  if (lane == 0 && t < ntiles) tma_issue_item<T, R>(W, t, stage, bar);
+  for (int k = 0; t < ntiles; t += stride, ++k) {
     int lt, x0, y0;
     const FdtdInst &I = W.at(t, lt);
-    tma_patch_origin(lt, I.tiles_x, ph, x0, y0);
+    tma_patch_origin(lt, I.tiles_x, R, x0, y0);
     const int nr = I.nr, nz = I.nz;
-    const FdtdCoef &c = I.c;
     const unsigned flags = I.flags;
     const bool endcopy = (flags & GASATT_Q_ER_END_COPY) != 0;
     const bool jsign = (flags & GASATT_Q_EZ_AXIS_JSIGN) != 0;
-    const double dt_eps = c.dt_eps, dt_eps_dz = c.dt_eps_dz, axis = c.axis, inv_dr = 1 / c.dr;
-    const double mu = I.mu, dt = I.dt;
-    const int col = x0 + li;
+    const double dt_eps = I.c.dt_eps, dt_eps_dz = I.c.dt_eps_dz, axis = I.c.axis;
+    const int col = x0 + lane;
     const int of = x0 - (x0 & ~(al - 1)), oj = x0 - (x0 & ~1);
-    // widen the staged tile into the working arrays
+    const bool colH = col >= 0 && col < nr;
+    // Every point of the patch is updated by the same expression: no in-grid
+    // update reads a point outside the grid (the boundary rules never reach
+    // past the edge), so the values those points take do not matter.  The
+    // rules that keep an in-grid point from the interior expression become
+    // coefficients: Ez on the axis (col 0) takes (+J term, axis factor, 0),
+    // Ez at col n_r and beyond is left as it is (0, 0, 0); Er rows 0 and n_z
+    // are fixed up after each E update.  (Read while the copies are in flight.)
+    double iv = 0.0, ezp = 0.0, ezm = 0.0;
+    if (colH) {
+      iv = I.colc[3 * col];
+      ezp = col == 0 ? axis : I.colc[3 * col + 1];
+      ezm = I.colc[3 * col + 2];            // 0 on the axis
+    }
+    const bool ok = __all_sync(FULL, mbar_wait(bar, (uint32_t)(k & 1)));
+    if (!ok) {
+      if (lane == 0) {
+        atomicOr(I.err, 1u);
+        mbar_wait(bar, (uint32_t)(k & 1));          // the copy still owns the area
+      }
+      break;
+    }
+    // the column's patch: fields, and the current terms of the E updates
+    // (jr: dt/eps (J_r(j-1) + J_r(j)) / 2; jz: the same over columns i-1, i,
+    // or on the axis minus the signed dt/eps J_z term)
+    double er[R], ez[R], h[R], jr[R], jz[R];
     {
-      const T *gEr = reinterpret_cast<const T *>(stage[b]);
-      const T *gEz = reinterpret_cast<const T *>(stage[b] + L.field_bytes());
-      const T *gH = reinterpret_cast<const T *>(stage[b] + 2 * L.field_bytes());
-      const long long *gJr = reinterpret_cast<const long long *>(stage[b] + 3 * L.field_bytes());
-      const long long *gJz =
-          reinterpret_cast<const long long *>(stage[b] + 3 * L.field_bytes() + L.cur_bytes());
-      const double iv = (col >= 0 && col < nr) ? I.invV[col] : 0.0;
+      const T *gEr = reinterpret_cast<const T *>(stage);
+      const T *gEz = reinterpret_cast<const T *>(stage + S::field_bytes);
+      const T *gH = reinterpret_cast<const T *>(stage + 2 * S::field_bytes);
+      const long long *gJr = reinterpret_cast<const long long *>(stage + 3 * S::field_bytes);
+      const long long *gJz = reinterpret_cast<const long long *>(stage + 3 * S::field_bytes + S::cur_bytes);
       const ExtraCurrent xj = I.xj;
-      for (int m = 0; m < nrow_t; ++m) {
-        const int r = threadIdx.y + kTmaRows * m, s = li + r * PW;
-        const int sf = li + of + r * TmaBox<T>::w, sj = li + oj + r * 34;
-        sEr[s] = (double)gEr[sf];
-        sEz[s] = (double)gEz[sf];
-        sH[s] = (double)gH[sf];
-        const int jrow = y0 + r;
-        if (xj.Jr && col >= 0 && col < nr && jrow >= 0 && jrow < nz) {
-          const int64_t g = col + (int64_t)jrow * I.ldj;
-          sJr[s] = ((double)gJr[sj] + (double)(long long)xj.Jr[g] * xj.rel) * iv;
-          sJz[s] = ((double)gJz[sj] + (double)(long long)xj.Jz[g] * xj.rel) * iv;
-        } else {
-          sJr[s] = (double)gJr[sj] * iv;
-          sJz[s] = (double)gJz[sj] * iv;
+      double below = 0.0;
+      if (xj.Jr) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int sf = lane + of + r * BW, sj = lane + oj + r * 34, row = y0 + r;
+          er[r] = (double)gEr[sf];
+          ez[r] = (double)gEz[sf];
+          h[r] = (double)gH[sf];
+          double a = (double)gJr[sj], b = (double)gJz[sj];
+          if (colH && row >= 0 && row < nz) {
+            const int64_t g = col + (int64_t)row * I.ldj;
+            a = a + (double)(long long)xj.Jr[g] * xj.rel;
+            b = b + (double)(long long)xj.Jz[g] * xj.rel;
+          }
+          a = a * iv;
+          b = b * iv;
+          jr[r] = dt_eps * (below + a) / 2;
+          below = a;
+          jz[r] = b;
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int sf = lane + of + r * BW, sj = lane + oj + r * 34;
+          er[r] = (double)gEr[sf];
+          ez[r] = (double)gEz[sf];
+          h[r] = (double)gH[sf];
+          const double a = (double)gJr[sj] * iv;
+          jr[r] = dt_eps * (below + a) / 2;
+          below = a;
+          jz[r] = (double)gJz[sj] * iv;
         }
       }
     }
-    // which updates each cell takes (the grid's boundary rules; the patch's
-    // last column and row have no upper neighbours and are left alone)
-    const double ri = ((flags & GASATT_Q_EZ_RSHIFT) ? (col + 1) : col) * c.dr;
-    const double ezp = col > 0 ? dt_eps * (1 / (2 * ri) + inv_dr) : 0.0;   // coefficient of H(i)
-    const double ezm = col > 0 ? dt_eps * (1 / (2 * ri) - inv_dr) : 0.0;   // coefficient of H(i-1)
-    const bool colH = col >= 0 && col < nr;
-    __syncthreads();
-    auto h_update = [&](double h) {
-      const double chr = h / (mu * c.dr), chz = h / (mu * c.dz);
-      for (int m = 0; m < nrow_t; ++m) {
-        const int r = threadIdx.y + kTmaRows * m, s = li + r * PW, row = y0 + r;
-        if (colH && li + 1 < PW && row >= 0 && row < nz && r + 1 < ph)
-          sH[s] = sH[s] + (chr * (sEz[s + 1] - sEz[s]) - chz * (sEr[s + PW] - sEr[s]));
+    __syncwarp();
+    // the area is free: the warp's next patch is fetched while this one is computed
+    if (lane == 0 && t + stride < ntiles) {
+      fence_proxy_async_smem();
+      tma_issue_item<T, R>(W, t + stride, stage, bar);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const double left = __shfl_up_sync(FULL, jz[r], 1);
+      const double jt = jsign ? dt_eps * jz[r] : -(dt_eps * jz[r]);
+      jz[r] = col == 0 ? -jt : (colH ? dt_eps * (left + jz[r]) / 2 : 0.0);
+    }
+    // patch rows of grid rows 0 and n_z (Er there: zero, or the end copies)
+    const int r0 = -y0, rn = nz - y0;
+    const bool edge_rows = (r0 >= 0 && r0 < R) || (rn >= 0 && rn < R);
+    auto h_update = [&](double chr, double chz) {
+#pragma unroll
+      for (int r = 0; r + 1 < R; ++r) {
+        const double ezr = __shfl_down_sync(FULL, ez[r], 1);
+        h[r] = h[r] + (chr * (ezr - ez[r]) - chz * (er[r + 1] - er[r]));
       }
     };
     auto e_update = [&]() {
-      for (int m = 0; m < nrow_t; ++m) {
-        const int r = threadIdx.y + kTmaRows * m, s = li + r * PW, row = y0 + r;
-        if (colH) {
-          if (row >= 1 && row < nz) {
-            if (r >= 1) {
-              const double old = sEr[s];
-              sEr[s] = old - dt_eps * (sJr[s - PW] + sJr[s]) / 2 - dt_eps_dz * (sH[s] - sH[s - PW]);
-              if (endcopy) {
-                if (row == 1) sEr[s - PW] = old;
-                if (row == nz - 1 && r + 1 < ph) sEr[s + PW] = old;
-              }
-            }
-          } else if (!endcopy && (row == 0 || row == nz)) {
-            sEr[s] = 0.0;
-          }
-        }
-        if (row >= 0 && row < nz) {
-          if (col == 0) {
-            const double jz0 = sJz[s];
-            const double jterm = jsign ? dt_eps * jz0 : -(dt_eps * jz0);
-            sEz[s] = sEz[s] + jterm + axis * sH[s];
-          } else if (col > 0 && col < nr && li >= 1) {
-            sEz[s] = sEz[s] - dt_eps * (sJz[s - 1] + sJz[s]) / 2 + ezp * sH[s] + ezm * sH[s - 1];
-          }
+      double ne[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int rm = r > 0 ? r - 1 : 0;
+        const double hl = __shfl_up_sync(FULL, h[r], 1);
+        ne[r] = er[r] - jr[r] - dt_eps_dz * (h[r] - h[rm]);
+        ez[r] = ez[r] - jz[r] + ezp * h[r] + ezm * hl;
+      }
+      if (edge_rows) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int rm = r > 0 ? r - 1 : r, rp = r + 1 < R ? r + 1 : r;
+          if (r == r0) ne[r] = endcopy ? er[rp] : 0.0;
+          if (r == rn) ne[r] = endcopy ? er[rm] : 0.0;
         }
       }
+#pragma unroll
+      for (int r = 0; r < R; ++r) er[r] = ne[r];
     };
-    h_update(dt / 4);
-    __syncthreads();
+    h_update(I.chr4, I.chz4);
     e_update();
-    __syncthreads();
-    h_update(dt / 2);
-    __syncthreads();
+    h_update(I.chr2, I.chz2);
     e_update();
-    __syncthreads();
-    h_update(dt / 4);
-    __syncthreads();
-    // write back the tile: columns [3, 29) and rows [3, ph - 3) of the patch
+    h_update(I.chr4, I.chz4);
+    // write back the tile: columns [3, 29) and rows [3, R - 3) of the patch
     T *Er = reinterpret_cast<T *>(I.Er), *Ez = reinterpret_cast<T *>(I.Ez), *H = reinterpret_cast<T *>(I.H);
     unsigned long long *Jr_next = I.Jr_next, *Jz_next = I.Jz_next;
     const int ldf = I.ldf, ldj = I.ldj;
-    const FieldQuads q = I.q;
-    if (li >= kTmaHalo && li < kTmaHalo + kTmaTileW && col <= nr) {
-      const int c0 = col > 0 ? li - 1 : li, c1 = col > nr - 1 ? li - 1 : li;   // quad columns
-      for (int m = 0; m < nrow_t; ++m) {
-        const int r = threadIdx.y + kTmaRows * m, row = y0 + r;
-        if (r < kTmaHalo || r >= ph - kTmaHalo || row > nz) continue;
-        const int s = li + r * PW;
-        if (col < nr) Er[col + (int64_t)row * ldf] = (T)sEr[s];
-        if (row < nz) Ez[col + (int64_t)row * ldf] = (T)sEz[s];
+    const bool out_col = lane >= kTmaHalo && lane < kTmaHalo + kTmaTileW && col <= nr;
+    if (sizeof(T) == 4) {
+      // FP32 form: the fields rounded to float once; whole gather quads from
+      // those floats (corner columns from the lane below by shuffle)
+      const FieldQuads q = I.q;
+      float fe[R], fz[R], fh[R];
+#pragma unroll
+      for (int r = kTmaHalo - 1; r <= R - kTmaHalo; ++r) {
+        fe[r] = (float)er[r];
+        fz[r] = (float)ez[r];
+        fh[r] = (float)h[r];
+      }
+      const bool lo0 = col > 0, hi0 = col > nr - 1;   // corner column c0 = col - 1, c1 = col - 1
+#pragma unroll
+      for (int r = kTmaHalo; r < R - kTmaHalo; ++r) {
+        const int row = y0 + r;
+        const float eu0 = __shfl_up_sync(FULL, fe[r], 1), eu1 = __shfl_up_sync(FULL, fe[r + 1], 1);
+        const float zd0 = __shfl_down_sync(FULL, fz[r - 1], 1), zd1 = __shfl_down_sync(FULL, fz[r], 1);
+        const float hu0 = __shfl_up_sync(FULL, fh[r - 1], 1), hu1 = __shfl_up_sync(FULL, fh[r], 1);
+        if (!out_col || row > nz) continue;
+        if (col < nr) reinterpret_cast<float *>(Er)[col + (int64_t)row * ldf] = fe[r];
+        if (row < nz) reinterpret_cast<float *>(Ez)[col + (int64_t)row * ldf] = fz[r];
         if (col < nr && row < nz) {
-          H[col + (int64_t)row * ldf] = (T)sH[s];
+          reinterpret_cast<float *>(H)[col + (int64_t)row * ldf] = fh[r];
           const int64_t g = col + (int64_t)row * ldj;
           Jr_next[g] = 0;
           Jz_next[g] = 0;
         }
-        if (q.er) {
-          const int ra = row > 0 ? r - 1 : r, rb = row > nz - 1 ? r - 1 : r;   // quad rows
-          if (row < nz)
-            q.er[col + (int64_t)row * (nr + 1)] =
-                make_float4((float)sEr[c0 + r * PW], (float)sEr[c1 + r * PW],
-                            (float)sEr[c0 + (r + 1) * PW], (float)sEr[c1 + (r + 1) * PW]);
-          if (col < nr)
-            q.ez[col + (int64_t)row * nr] =
-                make_float4((float)sEz[li + ra * PW], (float)sEz[li + 1 + ra * PW],
-                            (float)sEz[li + rb * PW], (float)sEz[li + 1 + rb * PW]);
-          q.h[col + (int64_t)row * (nr + 1)] =
-              make_float4((float)sH[c0 + ra * PW], (float)sH[c1 + ra * PW], (float)sH[c0 + rb * PW],
-                          (float)sH[c1 + rb * PW]);
+        const bool ra_lo = row > 0, rb_lo = row > nz - 1;   // quad rows ra = row - 1, rb = row - 1
+        if (row < nz)
+          q.er[col + (int64_t)row * (nr + 1)] =
+              make_float4(lo0 ? eu0 : fe[r], hi0 ? eu0 : fe[r], lo0 ? eu1 : fe[r + 1], hi0 ? eu1 : fe[r + 1]);
+        if (col < nr)
+          q.ez[col + (int64_t)row * nr] =
+              make_float4(ra_lo ? fz[r - 1] : fz[r], ra_lo ? zd0 : zd1, rb_lo ? fz[r - 1] : fz[r],
+                          rb_lo ? zd0 : zd1);
+        const float ha0 = ra_lo ? hu0 : hu1, ha = ra_lo ? fh[r - 1] : fh[r];
+        const float hb0 = rb_lo ? hu0 : hu1, hb = rb_lo ? fh[r - 1] : fh[r];
+        q.h[col + (int64_t)row * (nr + 1)] =
+            make_float4(lo0 ? ha0 : ha, hi0 ? ha0 : ha, lo0 ? hb0 : hb, hi0 ? hb0 : hb);
+      }
+    } else if (out_col) {
+#pragma unroll
+      for (int r = kTmaHalo; r < R - kTmaHalo; ++r) {
+        const int row = y0 + r;
+        if (row > nz) continue;
+        if (col < nr) Er[col + (int64_t)row * ldf] = (T)er[r];
+        if (row < nz) Ez[col + (int64_t)row * ldf] = (T)ez[r];
+        if (col < nr && row < nz) {
+          H[col + (int64_t)row * ldf] = (T)h[r];
+          const int64_t g = col + (int64_t)row * ldj;
+          Jr_next[g] = 0;
+          Jz_next[g] = 0;
         }
       }
     }
-    __syncthreads();
   }
-  // a block that gave up still owns copies in flight: let them land first
-  if (tid == 0) {
-    // the parity of a buffer's outstanding phase is not tracked here: waiting
-    // for both (bounded) covers the copy in flight
-    if (issued0) { mbar_wait(&bar[0], 0u); mbar_wait(&bar[0], 1u); }
-    if (issued1) { mbar_wait(&bar[1], 0u); mbar_wait(&bar[1], 1u); }
+}
+
+// the per-column table of FdtdInst::colc for n_r columns: {1/V scaled, Ez
+// coefficients of H(i) and H(i-1)} (the expressions fdtd_tiled1 evaluates)
+inline void fdtd_column_table(int nr, const FdtdCoef &c, const double *invV, unsigned flags,
+                              double *out) {
+  const double inv_dr = 1 / c.dr;
+  for (int i = 0; i < nr; ++i) {
+    const double ri = ((flags & GASATT_Q_EZ_RSHIFT) ? (i + 1) : i) * c.dr;
+    out[3 * i] = invV[i];
+    out[3 * i + 1] = i > 0 ? c.dt_eps * (1 / (2 * ri) + inv_dr) : 0.0;
+    out[3 * i + 2] = i > 0 ? c.dt_eps * (1 / (2 * ri) - inv_dr) : 0.0;
   }
 }
 

@@ -868,21 +868,19 @@ __global__ void k_ion_read(IonState I, double *r, double *z, double *ur, double 
 }
 
 // ----------------------------------------------------------- FP32 form
-// bilinear interpolation from the four corners (c0,r0), (c1,r0), (c0,r1),
-// (c1,r1) of a packed gather quad (FieldQuads)
-struct Quad4 { float f00, f10, f01, f11; };
-
-__device__ __forceinline__ float bilin_mix(const Quad4 &q, float wc, float wr) {
-  const float lo = fmaf(wc, q.f10 - q.f00, q.f00), hi = fmaf(wc, q.f11 - q.f01, q.f01);
-  return fmaf(wr, hi - lo, lo);
-}
-
 // 1/sqrt(x) refined by one Newton step: the hardware estimate is biased, and
 // a biased rotation normaliser or gamma makes the FP32 energy drift steadily
 __device__ __forceinline__ float rsqrt_nr(float x) {
   const float y = rsqrtf(x);
   return y * fmaf(-0.5f * x * y, y, 1.5f);
 }
+
+// Packed pairs: Blackwell issues two FP32 operations of a float2 as one
+// instruction (__fadd2/__fmul2/__ffma2, sm_100); the FP32 push pairs its
+// independent r/z (or column/row) operations this way.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 
 // a + d with stochastic rounding.  The per-step velocity changes of the FP32
 // form (a drift rotation by a small angle, a kick in a weak field) are often
@@ -894,34 +892,24 @@ __device__ __forceinline__ float rsqrt_nr(float x) {
 // in a's binade (within |d| of a power of two the grid changes and the split
 // is off by up to a factor 2; there |d| << |a| makes that a rare, tiny
 // error).  a + d + U h is formed exactly enough in one FMA (d and U h are
-// both small against a) and rounded once.  U = (k + 1/2) 2^-16 (k: the low 16
-// bits of r) is built as a float in [1, 2) minus 1; a = 0 gives h = 0 and the
-// exact d.
-__device__ __forceinline__ float sround_add(float a, float d, uint32_t r) {
-  const float h = __int_as_float(__float_as_int(a) & 0x7F800000) * 1.1920928955078125e-07f;   // 2^-23
-  const float u = __uint_as_float(0x3F800040u | ((r & 0xFFFFu) << 7)) - 1.0f;
-  return __fadd_rz(a, fmaf(copysignf(u, a), h, d));
+// both small against a) and rounded once.  U = (k + 1/2) 2^-16, k a 16-bit
+// random number, is built as a float in [1, 2) minus 1; a = 0 gives h = 0
+// and the exact d.  Done on a pair of components: k from the low 16 bits of r
+// for x, from the high 16 for y.
+__device__ __forceinline__ float2 sround_add2(float2 a, float2 d, uint32_t r) {
+  const float2 h = __fmul2_rn(f2(__int_as_float(__float_as_int(a.x) & 0x7F800000),
+                                 __int_as_float(__float_as_int(a.y) & 0x7F800000)),
+                              f2(1.1920928955078125e-07f));
+  const float2 u = __fadd2_rn(f2(__uint_as_float(0x3F800040u | ((r & 0xFFFFu) << 7)),
+                                 __uint_as_float(0x3F800040u | ((r >> 16) << 7))),
+                              f2(-1.0f));
+  return __fadd2_rz(a, __ffma2_rn(f2(copysignf(u.x, a.x), copysignf(u.y, a.y)), h, d));
 }
 
-// floor(x) for |x| < 2^22, subtracted from x and returned as an int: x + 1.5
-// 2^23 rounded down is 1.5 2^23 + floor(x) exactly (unit spacing there)
-__device__ __forceinline__ int take_floor(float &x) {
-  const float t = __fadd_rd(x, 12582912.0f);
-  x -= t - 12582912.0f;
-  return __float_as_int(t) - 0x4B400000;
-}
-
-// nearest integer (ties to even) of a * b for |a b| < 2^22, rounded once
-__device__ __forceinline__ int fma_rint(float a, float b) {
-  return __float_as_int(fmaf(a, b, 12582912.0f)) - 0x4B400000;
-}
-
-// 32 fresh bits from a 32-bit input (integer finaliser)
-__device__ __forceinline__ uint32_t mix32(uint32_t x) {
-  x ^= x >> 16; x *= 0x7feb352du;
-  x ^= x >> 15; x *= 0x846ca68bu;
-  return x ^ (x >> 16);
-}
+// Floors and nearest integers in FP32 without conversions: for |x| < 2^22,
+// x + 1.5 2^23 lies where the floats are one apart, so rounding that sum
+// down (or to nearest) gives 1.5 2^23 + floor(x) (or + rint(x)) exactly and
+// its bit pattern minus 0x4B400000 is the integer.
 
 // half-cell staggered index/weight: position ic + f measured from node ic-1/2
 __device__ __forceinline__ void half_shift(int ic, float f, int &a, float &w) {
@@ -956,7 +944,8 @@ __device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, 
                                         float &ut, float &uz, bool &alive, const SimParams &P,
                                         uint32_t rb, float hr, float hz, float &ig) {
   ig = rsqrt_nr(fmaf(ur, ur, fmaf(ut, ut, fmaf(uz, uz, 1.0f))));   // 1/gamma, kept by the turn
-  const float dx = ur * ig * hr, dy = ut * ig * hr, dzz = uz * ig * hz;
+  const float2 dxy = __fmul2_rn(__fmul2_rn(f2(ur, ut), f2(ig)), f2(hr));   // (dx, dy)
+  const float dx = dxy.x, dy = dxy.y, dzz = uz * ig * hz;
   const float rc = (float)ir + fr;
   const float X = rc + dx;
   const float r2 = fmaf(X, X, dy * dy);
@@ -967,44 +956,60 @@ __device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, 
   const float cc = 1.f - s2;                         // cos^2 a
   const float sq = cc > 0.f ? cc * rsqrtf(cc) : 0.f;
   const float c1 = X >= 0.f ? __fdividef(s2, 1.f + sq) : 1.f + sq;   // 1 - cos a
-  const float dur = fmaf(sn, ut, -c1 * ur), dut = fmaf(-sn, ur, -c1 * ut);
-  ur = sround_add(ur, dur, rb);
-  ut = sround_add(ut, dut, rb >> 16);
+  // (du_r, du_theta) = (sn ut - c1 ur, -sn ur - c1 ut)
+  const float2 du = __ffma2_rn(f2(sn, -sn), f2(ut, ur), __fmul2_rn(f2(ur, ut), f2(-c1)));
+  const float2 u2 = sround_add2(f2(ur, ut), du, rb);
+  ur = u2.x;
+  ut = u2.y;
   const float den = rn + rc;
   const float drr = den > 0.f ? __fdividef(fmaf(dx, 2.f * rc + dx, dy * dy), den) : 0.f;
-  fr += drr;
-  ir += take_floor(fr);
+  // floor of both offsets at once (take_floor on a pair)
+  const float2 f = __fadd2_rn(f2(fr, fz), f2(drr, dzz));
+  const float2 t = __fadd2_rd(f, f2(12582912.0f));
+  const float2 g = __fadd2_rn(f, neg2(__fadd2_rn(t, f2(-12582912.0f))));
+  fr = g.x;
+  fz = g.y;
+  ir += __float_as_int(t.x) - 0x4B400000;
+  iz += __float_as_int(t.y) - 0x4B400000;
   if (ir < 0) { ir = 0; fr = 0.f; }
   alive = alive && ir < P.nr;
-  fz += dzz;
-  iz += take_floor(fz);
   reflect_z(iz, fz, uz, P.nz);
 }
 
 // The four deposit nodes (columns ca, cb; rows ra, rb; clamped one-sided at
-// the edges as EM7.cu:56-202) and the fixed-point contributions, node order
-// (ca,ra), (cb,ra), (ca,rb), (cb,rb).  The weights sum to 1, so one particle
-// adds at most 2^20 in magnitude to any node, even where clamped nodes merge.
-// ig: 1/gamma of u (the drift's, which turns u without changing |u|).
-// Returns the quad key (ar + 1) + (az + 1)(n_r + 1): equal keys, equal nodes.
-__device__ __forceinline__ unsigned deposit_nodes32(const SimParams &P, int ir, int iz, float fr,
-                                                    float fz, float ur, float uz, float ig, int &ca,
-                                                    int &cb, int &ra, int &rb, int vr[4], int vz[4]) {
+// the edges as EM7.cu:56-202) and the fixed-point contributions.  perm (0..3)
+// permutes the node order: bit 0 swaps the columns, bit 1 the rows, so the
+// order is (c0,r0), (c1,r0), (c0,r1), (c1,r1) with (c0, c1) = (ca, cb) or
+// (cb, ca) and likewise rows; each node's integer is the same whatever the
+// order (its weight is the same product of the same two factors).  The
+// weights sum to 1, so one particle adds at most 2^20 in magnitude to any
+// node, even where clamped nodes merge.  ig: 1/gamma of u (the drift's,
+// which turns u without changing |u|).
+__device__ __forceinline__ void deposit_nodes32(const SimParams &P, int ir, int iz, float fr,
+                                                float fz, float ur, float uz, float ig, int perm,
+                                                int &c0, int &c1, int &r0, int &r1, int vr[4],
+                                                int vz[4]) {
   int ar, az;
   float wr, wz;
   half_shift(ir, fr, ar, wr);
   half_shift(iz, fz, az, wz);
-  ca = max(ar, 0); cb = min(ar + 1, P.nr - 1);
-  ra = max(az, 0); rb = min(az + 1, P.nz - 1);
-  const unsigned key = (unsigned)(ar + 1) + (unsigned)(az + 1) * (unsigned)(P.nr + 1);
-  const float w[4] = {(1 - wr) * (1 - wz), wr * (1 - wz), (1 - wr) * wz, wr * wz};
-  const float kr = P.depf * ur * ig, kz = P.depf * uz * ig;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    vr[k] = fma_rint(kr, w[k]);
-    vz[k] = fma_rint(kz, w[k]);
-  }
-  return key;
+  const int ca = max(ar, 0), cb = min(ar + 1, P.nr - 1);
+  const int ra = max(az, 0), rb = min(az + 1, P.nz - 1);
+  const bool sc = perm & 1, sr = perm & 2;
+  c0 = sc ? cb : ca; c1 = sc ? ca : cb;
+  r0 = sr ? rb : ra; r1 = sr ? ra : rb;
+  const float2 om = __fadd2_rn(f2(1.f), f2(-wr, -wz));        // (1 - wr, 1 - wz)
+  const float2 A = sc ? f2(wr, om.x) : f2(om.x, wr);         // column factors of c0, c1
+  const float B0 = sr ? wz : om.y, B1 = sr ? om.y : wz;       // row factors of r0, r1
+  const float2 w01 = __fmul2_rn(A, f2(B0)), w23 = __fmul2_rn(A, f2(B1));
+  const float2 k = __fmul2_rn(__fmul2_rn(f2(P.depf), f2(ur, uz)), f2(ig));   // (kr, kz)
+  const float2 C = f2(12582912.0f);
+  const float2 v0 = __ffma2_rn(k, f2(w01.x), C), v1 = __ffma2_rn(k, f2(w01.y), C);
+  const float2 v2 = __ffma2_rn(k, f2(w23.x), C), v3 = __ffma2_rn(k, f2(w23.y), C);
+  vr[0] = __float_as_int(v0.x) - 0x4B400000; vz[0] = __float_as_int(v0.y) - 0x4B400000;
+  vr[1] = __float_as_int(v1.x) - 0x4B400000; vz[1] = __float_as_int(v1.y) - 0x4B400000;
+  vr[2] = __float_as_int(v2.x) - 0x4B400000; vz[2] = __float_as_int(v2.y) - 0x4B400000;
+  vr[3] = __float_as_int(v3.x) - 0x4B400000; vz[3] = __float_as_int(v3.y) - 0x4B400000;
 }
 
 // FP32-form deposit window: int32 sums of one chunk of particles on the grid
@@ -1060,11 +1065,11 @@ __device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &
                                        float &fz, float &ur, float &ut, float &uz, bool &alive,
                                        float &ig) {
   // block 0 of this particle's stream: words 0-1 decide the null-collision
-  // candidate, words 2-3 (mixed) drive the stochastic rounding
+  // candidate, words 2-3 drive the stochastic rounding of the kick and the turn
   uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
   if (mode == 1) {
     philox4x32_10(c, P.pk);
-    drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, mix32(c[3]), P.hdr, P.hdz, ig);
+    drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, c[3], P.hdr, P.hdz, ig);
     return false;
   }
   int ar, az;
@@ -1076,24 +1081,30 @@ __device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &
   const float4 a4 = __ldg(P.qEr + ((ar + 1) + iz * (P.nr + 1)));
   const float4 b4 = __ldg(P.qEz + (ir + (az + 1) * P.nr));
   const float4 c4 = __ldg(P.qH + ((ar + 1) + (az + 1) * (P.nr + 1)));
-  const Quad4 qEr{a4.x, a4.y, a4.z, a4.w}, qEz{b4.x, b4.y, b4.z, b4.w}, qH{c4.x, c4.y, c4.z, c4.w};
   philox4x32_10(c, P.pk);
-  const uint32_t rb0 = mix32(c[2]), rb1 = mix32(c[3]);
-  const float Er = bilin_mix(qEr, wr, fz);
-  const float Ez = bilin_mix(qEz, fr, wz);
-  const float H = bilin_mix(qH, wr, wz);
+  // bilinear mixes from the quads' corners (c0,r0), (c1,r0), (c0,r1), (c1,r1)
+  // = (x, y, z, w), paired: the low and high rows of each quad along its
+  // columns, then Er and Ez along their rows
+  const float2 cE = __ffma2_rn(f2(wr), __fadd2_rn(f2(a4.y, a4.w), f2(-a4.x, -a4.z)), f2(a4.x, a4.z));
+  const float2 cZ = __ffma2_rn(f2(fr), __fadd2_rn(f2(b4.y, b4.w), f2(-b4.x, -b4.z)), f2(b4.x, b4.z));
+  const float2 cH = __ffma2_rn(f2(wr), __fadd2_rn(f2(c4.y, c4.w), f2(-c4.x, -c4.z)), f2(c4.x, c4.z));
+  const float2 E = __ffma2_rn(f2(fz, wz), __fadd2_rn(f2(cE.y, cZ.y), f2(-cE.x, -cZ.x)), f2(cE.x, cZ.x));
+  const float H = fmaf(wz, cH.y - cH.x, cH.x);
   // Boris in gamma*beta units: E = (Er, 0, Ez), B = (0, mu0 H, 0); the
   // increment u+ - u is formed first, then added with stochastic rounding
-  const float her = P.aE * Er, hez = P.aE * Ez;
-  const float umr = ur + her, umz = uz + hez;
-  const float igm = rsqrt_nr(fmaf(umr, umr, fmaf(ut, ut, fmaf(umz, umz, 1.0f))));
+  // (random bits: Philox words 2 and 3)
+  const float2 he = __fmul2_rn(f2(P.aE), E);                  // (her, hez)
+  const float2 um = __fadd2_rn(f2(ur, uz), he);               // (umr, umz)
+  const float igm = rsqrt_nr(fmaf(um.x, um.x, fmaf(ut, ut, fmaf(um.y, um.y, 1.0f))));
   const float t = P.aB * H * igm;
   const float s = __fdividef(2.f * t, fmaf(t, t, 1.f));
-  const float upr = fmaf(-umz, t, umr), upz = fmaf(umr, t, umz);
-  ur = sround_add(ur, fmaf(-upz, s, 2.f * her), rb0);
-  uz = sround_add(uz, fmaf(upr, s, 2.f * hez), rb0 >> 16);
+  const float2 up = __ffma2_rn(f2(-um.y, um.x), f2(t), um);   // (upr, upz)
+  const float2 du = __ffma2_rn(f2(-up.y, up.x), f2(s), __fadd2_rn(he, he));
+  const float2 uk = sround_add2(f2(ur, uz), du, c[2]);
+  ur = uk.x;
+  uz = uk.y;
   const float h = mode == 0 ? 2.f : 1.f;
-  drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, rb1, h * P.hdr, h * P.hdz, ig);
+  drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, c[3], h * P.hdr, h * P.hdz, ig);
   return alive && mode == 0 && (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
 }
 
@@ -1102,7 +1113,7 @@ __device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &
 __device__ __forceinline__ void deposit_global32(const SimParams &P, int ir, int iz, float fr,
                                                  float fz, float ur, float uz, float ig) {
   int ca, cb, ra, rb, vr[4], vz[4];
-  deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, ca, cb, ra, rb, vr, vz);
+  deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, 0, ca, cb, ra, rb, vr, vz);
   const int64_t a[4] = {ca + (int64_t)ra * P.ldj, cb + (int64_t)ra * P.ldj,
                         ca + (int64_t)rb * P.ldj, cb + (int64_t)rb * P.ldj};
   deposit_atomic<int>(a, vr, vz, P.Jr, P.Jz);
@@ -1209,10 +1220,24 @@ __device__ __forceinline__ void chunk_rows32(const SimParams &P, const State32 &
   }
 }
 
+// Bring the state of particles [beg, end) into L2 ahead of their chunk (one
+// thread; cp.async.bulk.prefetch.L2, a hint that completes on its own).  beg
+// is a multiple of the chunk size, hence even, so every range starts on a
+// 16-byte boundary; the sizes are rounded down to 16 bytes.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+  if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void prefetch_chunk32(const State32 &S, long long beg, long long end) {
+  const long long n = end - beg;
+  if (n <= 0) return;
+  prefetch_l2(S.a + beg, (uint32_t)(n * 16));
+  prefetch_l2(S.b + beg, (uint32_t)((n * 8) & ~15ll));
+  prefetch_l2(S.id + beg, (uint32_t)((n * 8) & ~15ll));
+}
+
 // The particles [beg, end) of one chunk of the FP32 pass of step `step`:
-// push (push32), collision candidates queued, deposit into the window w (one
-// shared-memory atomic per node and deposit quad of a warp; nodes outside the
-// window straight to the grid).  The highest window column touched is merged
+// push (push32), collision candidates queued, deposit into the window w
+// (nodes outside the window straight to the grid).  The highest window column touched is merged
 // into *box_cmax; electrons absorbed at the wall are counted into cnt.
 __device__ __forceinline__ void chunk32(const SimParams &P, const State32 &S, const Fields<float> &F,
                                         SimCounters *cnt, int *queue, long long step, int mode,
@@ -1258,36 +1283,29 @@ __device__ __forceinline__ void chunk32(const SimParams &P, const State32 &S, co
       act = alive && mode != 2;
     }
     queue_push(cand, p, &cnt->n_cand[par], queue + (long long)par * P.cap);
-    // Deposit: the lanes that share a node quad (sorted particles put one to
-    // a few quads in a warp) sum their eight integer contributions with
-    // redux.sync, and the first lane of each quad adds the sums - one
-    // shared-memory atomic per node and quad instead of one per particle
-    const unsigned dm = __ballot_sync(0xFFFFFFFFu, act);
+    // Deposit: each lane adds its own eight contributions to the window,
+    // visiting its four nodes in an order permuted by lane & 3 (columns
+    // swapped on bit 0, rows on bit 1), so lanes on the same node quad -
+    // sorted particles put one to a few quads in a warp - hit four different
+    // nodes in each atomic.  (Summing the lanes of a quad first with
+    // match.any / redux.sync made this pass two to four times slower on B200.)
     if (act) {
-      int ca, cb, ra, rb, vr[4], vz[4];
-      const unsigned key = deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, ca, cb, ra, rb, vr, vz);
-      const unsigned grp = __match_any_sync(dm, key);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        vr[k] = __reduce_add_sync(grp, vr[k]);
-        vz[k] = __reduce_add_sync(grp, vz[k]);
+      int c0, c1, r0, r1, vr[4], vz[4];
+      deposit_nodes32(P, ir, iz, fr, fz, ur, uz, ig, lane & 3, c0, c1, r0, r1, vr, vz);
+      const unsigned l0 = (unsigned)(r0 - w.row0), l1 = (unsigned)(r1 - w.row0);
+      if (l0 < (unsigned)w.rows && l1 < (unsigned)w.rows) {
+        const int k0 = (int)l0 * w.ws, k1 = (int)l1 * w.ws;
+        atomicAdd(w.r + k0 + c0, vr[0]); atomicAdd(w.z + k0 + c0, vz[0]);
+        atomicAdd(w.r + k0 + c1, vr[1]); atomicAdd(w.z + k0 + c1, vz[1]);
+        atomicAdd(w.r + k1 + c0, vr[2]); atomicAdd(w.z + k1 + c0, vz[2]);
+        atomicAdd(w.r + k1 + c1, vr[3]); atomicAdd(w.z + k1 + c1, vz[3]);
+      } else {
+        win_node(w, P, c0, r0, vr[0], vz[0]);
+        win_node(w, P, c1, r0, vr[1], vz[1]);
+        win_node(w, P, c0, r1, vr[2], vz[2]);
+        win_node(w, P, c1, r1, vr[3], vz[3]);
       }
-      if (lane == __ffs(grp) - 1) {
-        const unsigned la = (unsigned)(ra - w.row0), lb = (unsigned)(rb - w.row0);
-        if (la < (unsigned)w.rows && lb < (unsigned)w.rows) {
-          const int k0 = (int)la * w.ws, k1 = (int)lb * w.ws;
-          atomicAdd(w.r + k0 + ca, vr[0]); atomicAdd(w.z + k0 + ca, vz[0]);
-          atomicAdd(w.r + k0 + cb, vr[1]); atomicAdd(w.z + k0 + cb, vz[1]);
-          atomicAdd(w.r + k1 + ca, vr[2]); atomicAdd(w.z + k1 + ca, vz[2]);
-          atomicAdd(w.r + k1 + cb, vr[3]); atomicAdd(w.z + k1 + cb, vz[3]);
-        } else {
-          win_node(w, P, ca, ra, vr[0], vz[0]);
-          win_node(w, P, cb, ra, vr[1], vz[1]);
-          win_node(w, P, ca, rb, vr[2], vz[2]);
-          win_node(w, P, cb, rb, vr[3], vz[3]);
-        }
-        wc_max = max(wc_max, cb);       // (win_node may use the window for one row)
-      }
+      wc_max = max(wc_max, max(c0, c1));   // (win_node may use the window for one row)
     }
   }
   // the window columns this warp touched, merged into the block's; the wall
@@ -1334,6 +1352,19 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // the window starts zeroed; each chunk's flush leaves it zeroed again
   for (int i = threadIdx.x; i < kWinNodes; i += kBlock) { win_r[i] = 0; win_z[i] = 0; }
+  const int ws = win_stride(P.nr);
+  const int maxrows = min(kWinNodes / ws, P.nz);
+  const int chunk = P.chunk;
+  const long long nchunk = (n0 + chunk - 1) / chunk;
+  // thread 0 claims the block's next chunk (index and window rows) a chunk
+  // ahead and has its state brought into L2 meanwhile; the first one before
+  // the candidates, so that it has their time to arrive
+  long long next_ch = 0;
+  int next_row0 = 0, next_rows = 0;
+  if (threadIdx.x == 0) {
+    next_ch = (long long)atomicAdd(&cnt->chunk_next, 1ull);
+    if (next_ch < nchunk) prefetch_chunk32(S, next_ch * chunk, min((next_ch + 1) * chunk, n0));
+  }
   if (mode != 1) {
     const long long nq = (long long)cnt->n_cand[par ^ 1];
     const int *qin = queue + (long long)(par ^ 1) * P.cap;
@@ -1345,25 +1376,17 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
     }
     if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
   }
-  const int ws = win_stride(P.nr);
-  const int maxrows = min(kWinNodes / ws, P.nz);
-  const int chunk = P.chunk;
-  const long long nchunk = (n0 + chunk - 1) / chunk;
-  // thread 0 fetches the next chunk (index and window rows) while the block
-  // works on the current one
-  long long next_ch = 0;
-  int next_row0 = 0, next_rows = 0;
-  if (threadIdx.x == 0) {
-    next_ch = (long long)atomicAdd(&cnt->chunk_next, 1ull);
-    if (next_ch < nchunk) chunk_rows32(P, S, n0, chunk, next_ch, maxrows, next_row0, next_rows);
-  }
+  if (threadIdx.x == 0 && next_ch < nchunk) chunk_rows32(P, S, n0, chunk, next_ch, maxrows, next_row0, next_rows);
   for (;;) {
     if (threadIdx.x == 0) {
       chunk_at = next_ch;
       win_row0 = next_row0;
       win_rows = next_rows;
       box_cmax = -1;
-      if (next_ch < nchunk) next_ch = (long long)atomicAdd(&cnt->chunk_next, 1ull);
+      if (next_ch < nchunk) {
+        next_ch = (long long)atomicAdd(&cnt->chunk_next, 1ull);
+        if (next_ch < nchunk) prefetch_chunk32(S, next_ch * chunk, min((next_ch + 1) * chunk, n0));
+      }
     }
     __syncthreads();
     const long long ch = chunk_at;
@@ -1429,6 +1452,23 @@ __global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *_
   }
   __syncthreads();
   const long long nq = cand_pre[ncell], nchunk = chunk_pre[ncell];
+  // (cell, chunk) work items; the block's first one is claimed (and its state
+  // brought into L2) before the candidates
+  long long next = 0;
+  int next_c = -1, next_row0 = 0, next_rows = 0;
+  auto fetch = [&]() {           // thread 0: the next item and its window rows
+    next = (long long)atomicAdd(chunk_next, 1ull);
+    if (next < nchunk) {
+      next_c = cell_of_item(chunk_pre, ncell, next);
+      const BatchCell32 &C = cells[next_c];
+      const SimParams &Pc = C.P[jb];
+      const int ws = win_stride(Pc.nr), maxrows = min(kWinNodes / ws, Pc.nz);
+      const long long n0c = (long long)C.cnt->n_total, chc = next - chunk_pre[next_c];
+      prefetch_chunk32(C.S[cur], chc * Pc.chunk, min((chc + 1) * Pc.chunk, n0c));
+      chunk_rows32(Pc, C.S[cur], n0c, Pc.chunk, chc, maxrows, next_row0, next_rows);
+    }
+  };
+  if (threadIdx.x == 0) { fetch(); cell_at = -1; }
   for (long long k = (long long)blockIdx.x * (kBlock / 32) + warp; k < nq;
        k += (long long)gridDim.x * (kBlock / 32)) {
     if (lane == 0) {
@@ -1444,21 +1484,6 @@ __global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *_
     }
     __syncwarp();
   }
-  // (cell, chunk) work items
-  long long next = 0;
-  int next_c = -1, next_row0 = 0, next_rows = 0;
-  auto fetch = [&]() {           // thread 0: the next item and its window rows
-    next = (long long)atomicAdd(chunk_next, 1ull);
-    if (next < nchunk) {
-      next_c = cell_of_item(chunk_pre, ncell, next);
-      const BatchCell32 &C = cells[next_c];
-      const SimParams &Pc = C.P[jb];
-      const int ws = win_stride(Pc.nr), maxrows = min(kWinNodes / ws, Pc.nz);
-      chunk_rows32(Pc, C.S[cur], (long long)C.cnt->n_total, Pc.chunk, next - chunk_pre[next_c],
-                   maxrows, next_row0, next_rows);
-    }
-  };
-  if (threadIdx.x == 0) { fetch(); cell_at = -1; }
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1524,26 +1549,47 @@ __device__ __forceinline__ void commit_pass32(SimCounters *cnt) {
   cnt->step = ns;
 }
 
-// The field sub-cycle of one step for fdtd_ratio 1: the persistent TMA-fed
-// kernel of fdtd_tma.cuh.
-template <typename T>
-__global__ void __launch_bounds__(32 * kTmaRows, 1) k_sim_fdtd_tma(const __grid_constant__ FdtdInst I,
-                                                               SimCounters *cnt, int ph) {
-  if (cnt && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) commit_pass32(cnt);
-  fdtd_tma_body<T>(FdtdWork{&I, nullptr, I.ntiles}, ph);
+// The field sub-cycle of one step for fdtd_ratio 1: one warp per patch of R
+// rows (fdtd_tma.cuh).
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * kTmaWarps, 2) k_sim_fdtd_tma(const __grid_constant__ FdtdInst I,
+                                                                SimCounters *cnt) {
+  if (cnt && blockIdx.x == 0 && threadIdx.x == 0) commit_pass32(cnt);
+  fdtd_warp_body<T, R>(FdtdWork{&I, nullptr, I.ntiles});
 }
 
-// The field update of every cell of a batch in one launch: the blocks walk a
+// The field update of every cell of a batch in one launch: the warps walk a
 // table of (cell, tile) work items; FP32 form (commit given): the blocks first
 // commit the previous pass of every cell.
-template <typename T>
-__global__ void __launch_bounds__(32 * kTmaRows, 1) k_batch_fdtd_tma(const FdtdInst *insts,
-                                                                 const int2 *table, int nitems,
-                                                                 SimCounters *const *commit,
-                                                                 int ninst, int ph) {
-  if (commit && threadIdx.x == 0 && threadIdx.y == 0)
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * kTmaWarps, 2) k_batch_fdtd_tma(const FdtdInst *insts,
+                                                                  const int2 *table, int nitems,
+                                                                  SimCounters *const *commit,
+                                                                  int ninst) {
+  if (commit && threadIdx.x == 0)
     for (int i = blockIdx.x; i < ninst; i += gridDim.x) commit_pass32(commit[i]);
-  fdtd_tma_body<T>(FdtdWork{insts, table, nitems}, ph);
+  fdtd_warp_body<T, R>(FdtdWork{insts, table, nitems});
+}
+
+using SimFdtdTmaFn = void (*)(const FdtdInst, SimCounters *);
+using BatchFdtdTmaFn = void (*)(const FdtdInst *, const int2 *, int, SimCounters *const *, int);
+
+// the patch heights (rows) the field update is built for
+__host__ __device__ constexpr bool tma_rows_ok(int rows) { return rows == 12 || rows == 16 || rows == 20; }
+
+// the instance of each kernel, and its dynamic shared memory, for `rows`
+template <typename T>
+SimFdtdTmaFn sim_fdtd_tma_fn(int rows) {
+  return rows == 12 ? k_sim_fdtd_tma<T, 12> : rows == 20 ? k_sim_fdtd_tma<T, 20> : k_sim_fdtd_tma<T, 16>;
+}
+template <typename T>
+BatchFdtdTmaFn batch_fdtd_tma_fn(int rows) {
+  return rows == 12 ? k_batch_fdtd_tma<T, 12> : rows == 20 ? k_batch_fdtd_tma<T, 20> : k_batch_fdtd_tma<T, 16>;
+}
+template <typename T>
+size_t tma_block_bytes(int rows) {
+  return rows == 12 ? TmaStage<T, 12>::block_bytes
+                    : rows == 20 ? TmaStage<T, 20>::block_bytes : TmaStage<T, 16>::block_bytes;
 }
 
 // The general sub-cycle (fdtd_ratio > 1): one 32 x 32 patch per block
@@ -1940,6 +1986,7 @@ struct gasatt_sim {
   unsigned long long *Jr[2] = {nullptr, nullptr}, *Jz[2] = {nullptr, nullptr};
   double *d_tab = nullptr;
   double *invV = nullptr;         // per column: 2^-S / shell volume
+  double *fdtd_colc = nullptr;    // per column: {invV, Ez coefficients} (fdtd_column_table)
   SimCounters *cnt = nullptr;
   SimCounters *h_cnt = nullptr;   // pinned
   int *cell_count = nullptr, *cell_offset = nullptr, *cell_cursor = nullptr;
@@ -2012,13 +2059,11 @@ int launch_fdtd(gasatt_sim *s, cudaStream_t st, int q) {
   // the held ion current, in the electron current's fixed-point units
   const ExtraCurrent ion{s->Jir, s->Jiz, s->scale / s->ion_scale};
   if (R == 1) {
-    const dim3 block(32, kTmaRows);
+    const dim3 block(32 * kTmaWarps);
     if (s->form == 0)
-      k_sim_fdtd_tma<double><<<s->tma_grid, block, s->tma_smem, st>>>(s->fdtd_inst[q], nullptr,
-                                                                      s->tma_rows);
+      sim_fdtd_tma_fn<double>(s->tma_rows)<<<s->tma_grid, block, s->tma_smem, st>>>(s->fdtd_inst[q], nullptr);
     else
-      k_sim_fdtd_tma<float><<<s->tma_grid, block, s->tma_smem, st>>>(s->fdtd_inst[q], s->cnt,
-                                                                     s->tma_rows);
+      sim_fdtd_tma_fn<float>(s->tma_rows)<<<s->tma_grid, block, s->tma_smem, st>>>(s->fdtd_inst[q], s->cnt);
     s->ctx->launches++;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(s->ctx, e, "fdtd launch");
@@ -2272,25 +2317,22 @@ int encode_map(gasatt_sim *s, CUtensorMap *m, CUtensorMapDataType type, void *ba
 template <typename T>
 int setup_fdtd_tma(gasatt_sim *s, int nsm) {
   const auto &c = s->cfg;
-  int ph = c.fdtd_tile_rows > 0 ? c.fdtd_tile_rows : 48;
-  const int max_rows = sizeof(T) == 4 ? 64 : 48;
-  if (ph % kTmaRows || ph < 16 || ph > max_rows)
-    return fail(s->ctx, GASATT_E_ARG, "fdtd_tile_rows: a multiple of 16 in [16, " +
-                                          std::to_string(max_rows) + "]");
-  const TmaSmem<T> L(ph);
+  const int ph = c.fdtd_tile_rows > 0 ? c.fdtd_tile_rows : 16;
+  if (!tma_rows_ok(ph)) return fail(s->ctx, GASATT_E_ARG, "fdtd_tile_rows: 12, 16 or 20");
   s->tma_rows = ph;
-  s->tma_smem = L.total();
+  s->tma_smem = tma_block_bytes<T>(ph);
   const int tiles_x = (c.n_r + 1 + kTmaTileW - 1) / kTmaTileW;
   const int tiles_y = (c.n_z + 1 + (ph - 2 * kTmaHalo) - 1) / (ph - 2 * kTmaHalo);
   const int ntiles = tiles_x * tiles_y;
-  GASATT_CUDA(s->ctx, cudaFuncSetAttribute(k_sim_fdtd_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const SimFdtdTmaFn kern = sim_fdtd_tma_fn<T>(ph);
+  GASATT_CUDA(s->ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)s->tma_smem));
   int occ = 0;
-  GASATT_CUDA(s->ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sim_fdtd_tma<T>, 32 * kTmaRows,
+  GASATT_CUDA(s->ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 * kTmaWarps,
                                                                     s->tma_smem));
   if (occ < 1) return fail(s->ctx, GASATT_E_ARG, "field update: patch does not fit in shared memory");
-  const long long slots = (long long)nsm * occ;
-  s->tma_grid = (unsigned)(slots < ntiles ? slots : ntiles);
+  const long long slots = (long long)nsm * occ, blocks = (ntiles + kTmaWarps - 1) / kTmaWarps;
+  s->tma_grid = (unsigned)(slots < blocks ? slots : blocks);
   const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
   const size_t ldb = (size_t)s->ldf * sizeof(T), ldjb = (size_t)s->ldj * 8;
   const int bw = TmaBox<T>::w;
@@ -2305,12 +2347,15 @@ int setup_fdtd_tma(gasatt_sim *s, int nsm) {
     SIM_TRY(encode_map(s, &M.jz, CU_TENSOR_MAP_DATA_TYPE_INT64, s->Jz[q], c.n_r, c.n_z, ldjb, 34, ph));
     I.Er = s->Er; I.Ez = s->Ez; I.H = s->H;
     I.Jr_next = s->Jr[1 - q]; I.Jz_next = s->Jz[1 - q];
-    I.invV = s->invV;
+    I.colc = s->fdtd_colc;
     I.xj = ExtraCurrent{s->Jir, s->Jiz, s->scale / s->ion_scale};
     I.q = sizeof(T) == 4 ? s->quads : FieldQuads{};
     I.c = fdtd_coef(s);
-    I.mu = c.mu0;
-    I.dt = c.dt;
+    const double h4 = c.dt / 4, h2 = c.dt / 2;
+    I.chr4 = h4 / (c.mu0 * I.c.dr);
+    I.chz4 = h4 / (c.mu0 * I.c.dz);
+    I.chr2 = h2 / (c.mu0 * I.c.dr);
+    I.chz2 = h2 / (c.mu0 * I.c.dz);
     I.nr = c.n_r; I.nz = c.n_z; I.ldf = s->ldf; I.ldj = s->ldj;
     I.flags = c.flags;
     I.tiles_x = tiles_x;
@@ -2537,7 +2582,8 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
       (rc = sim_alloc(s, &tmpd, (size_t)4 * c.table_n + (size_t)181 * c.table_n)))
     return cleanup(rc);
   s->d_tab = tmpd;
-  if ((rc = sim_alloc(s, &s->invV, (size_t)nr))) return cleanup(rc);
+  if ((rc = sim_alloc(s, &s->invV, (size_t)nr)) || (rc = sim_alloc(s, &s->fdtd_colc, (size_t)3 * nr)))
+    return cleanup(rc);
   if (s->form == 1) {
     if ((rc = sim_alloc(s, &s->quads.er, (size_t)(nr + 1) * nz)) ||
         (rc = sim_alloc(s, &s->quads.ez, (size_t)nr * (nz + 1))) ||
@@ -2598,7 +2644,10 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   {
     std::vector<double> iv(nr);
     for (int i = 0; i < nr; ++i) iv[i] = (1.0 / s->scale) / shell_volume(i, c.dr, c.dz, c.PHIp);
-    if (cudaMemcpy(s->invV, iv.data(), (size_t)nr * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+    std::vector<double> colc((size_t)3 * nr);
+    fdtd_column_table(nr, fdtd_coef(s), iv.data(), c.flags, colc.data());
+    if (cudaMemcpy(s->invV, iv.data(), (size_t)nr * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(s->fdtd_colc, colc.data(), (size_t)3 * nr * 8, cudaMemcpyHostToDevice) != cudaSuccess)
       return cleanup(fail(ctx, GASATT_E_CUDA, "volume table upload"));
   }
   if ((rc = sim_alloc(s, &s->d_P, 2)) || (rc = upload_params(s))) return cleanup(rc);
@@ -3453,15 +3502,12 @@ int batch_group_setup(gasatt_batch *b, BatchGroup &G) {
   int nsm = 148, occ = 1;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
   G.fdtd_smem = G.sims[0]->tma_smem;
-  if (G.form == 1) {
-    GASATT_CUDA(ctx, cudaFuncSetAttribute(k_batch_fdtd_tma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.fdtd_smem));
-    GASATT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_fdtd_tma<float>, 32 * kTmaRows, G.fdtd_smem));
-  } else {
-    GASATT_CUDA(ctx, cudaFuncSetAttribute(k_batch_fdtd_tma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.fdtd_smem));
-    GASATT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_fdtd_tma<double>, 32 * kTmaRows, G.fdtd_smem));
-  }
+  const BatchFdtdTmaFn fk = G.form == 1 ? batch_fdtd_tma_fn<float>(G.ph) : batch_fdtd_tma_fn<double>(G.ph);
+  GASATT_CUDA(ctx, cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.fdtd_smem));
+  GASATT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fk, 32 * kTmaWarps, G.fdtd_smem));
   const long long fslots = (long long)nsm * (occ > 0 ? occ : 1);
-  G.fdtd_grid = (unsigned)(fslots < G.nitems ? fslots : (G.nitems > 0 ? G.nitems : 1));
+  const long long fblocks = (G.nitems + kTmaWarps - 1) / kTmaWarps;
+  G.fdtd_grid = (unsigned)(fslots < fblocks ? fslots : (fblocks > 0 ? fblocks : 1));
   occ = 1;
   if (G.form == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_pass32, kBlock, 0);
   else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_pass64, kBlock, 0);
@@ -3478,10 +3524,10 @@ int batch_group_launch(gasatt_batch *b, BatchGroup &G, cudaStream_t cs, cudaStre
                        int q) {
   gasatt_ctx *ctx = b->ctx;
   const int n = (int)G.sims.size();
-  const dim3 fb(32, kTmaRows);
+  const dim3 fb(32 * kTmaWarps);
   if (G.form == 1) {
-    k_batch_fdtd_tma<float><<<G.fdtd_grid, fb, G.fdtd_smem, cs>>>(G.insts[q], G.table, G.nitems, G.commit,
-                                                                 n, G.ph);
+    batch_fdtd_tma_fn<float>(G.ph)<<<G.fdtd_grid, fb, G.fdtd_smem, cs>>>(G.insts[q], G.table, G.nitems,
+                                                                        G.commit, n);
     GASATT_CUDA(ctx, cudaGetLastError());
     GASATT_CUDA(ctx, cudaMemsetAsync(G.chunk_next, 0, 8, cs));
     k_batch_pass32<<<G.pass_grid, kBlock, 0, cs>>>((const BatchCell32 *)G.cells, n, cur, 1 - q, 0,
@@ -3495,8 +3541,8 @@ int batch_group_launch(gasatt_batch *b, BatchGroup &G, cudaStream_t cs, cudaStre
   k_batch_mcc64<<<G.mcc_grid, kMccBlock, 0, side>>>((const BatchCell64 *)G.cells, n, cur, 1 - q);
   GASATT_CUDA(ctx, cudaGetLastError());
   GASATT_CUDA(ctx, cudaEventRecord(b->join_ev, side));
-  k_batch_fdtd_tma<double><<<G.fdtd_grid, fb, G.fdtd_smem, cs>>>(G.insts[q], G.table, G.nitems, nullptr,
-                                                                n, G.ph);
+  batch_fdtd_tma_fn<double>(G.ph)<<<G.fdtd_grid, fb, G.fdtd_smem, cs>>>(G.insts[q], G.table, G.nitems,
+                                                                       nullptr, n);
   GASATT_CUDA(ctx, cudaGetLastError());
   GASATT_CUDA(ctx, cudaStreamWaitEvent(cs, b->join_ev, 0));
   GASATT_CUDA(ctx, cudaMemsetAsync(G.chunk_next, 0, 8, cs));

@@ -7,10 +7,11 @@ update's arithmetic is the same for every patch):
   sort_period     steps between cell re-sorts: a sort costs a pass over the
                   state, while the particles' drift away from their sorted
                   order slowly makes the gather and the deposit less local;
-  fdtd_tile_rows  rows of the field update's TMA patch (26 columns x rows - 6
-                  per tile): the rows per thread of the update (rows / 16,
-                  so 1/16 to 1/4 of a thread per cell) against the halo
-                  overhead and the number of tiles for the blocks to share;
+  fdtd_tile_rows  rows R of the field update's per-warp patch (12, 16 or 20;
+                  a warp computes 26 columns x R - 6 rows of output from 32 x R
+                  staged points): the halo recomputed per output point against
+                  the registers a warp holds and the number of patches for
+                  the warps to share;
   pass_chunk      particles per chunk of the FP32 particle pass (its deposit
                   window's span against the number of chunks for the blocks
                   to balance).
@@ -28,7 +29,7 @@ from . import abi
 from .sim import Sim
 
 DEFAULT_SORT_PERIODS = (10, 20, 30, 40, 60)
-DEFAULT_TILE_ROWS = (32, 48, 64)
+DEFAULT_TILE_ROWS = (12, 16, 20)
 DEFAULT_CHUNKS = (1024, 1280, 1536, 1792)
 
 
@@ -78,10 +79,9 @@ def tune_sort_period(cfg, particles, candidates=DEFAULT_SORT_PERIODS, steps=200,
 
 def knob_candidates(cfg):
     """The candidates of each knob for this configuration's precision form
-    (the FP64 field update fits at most 48 patch rows; the chunk size is a
-    knob of the FP32 pass only)."""
+    (the chunk size is a knob of the FP32 pass only)."""
     fp32 = cfg.precision == abi.FP32_SPLIT
-    knobs = {"fdtd_tile_rows": tuple(r for r in DEFAULT_TILE_ROWS if fp32 or r <= 48)}
+    knobs = {"fdtd_tile_rows": DEFAULT_TILE_ROWS}
     if cfg.fdtd_ratio != 1:
         knobs = {}                         # only the fdtd_ratio 1 field update has tiles
     if fp32:

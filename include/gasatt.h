@@ -273,8 +273,8 @@ typedef struct gasatt_sim_config {
   int      ion_subcycle;    /* electron steps per ion push (50); the ion step is ion_subcycle*dt */
   /* launch-shape knobs (results do not depend on them; 0 = the default, and
    * the autotuner of the Python package picks them per workload): */
-  int      fdtd_tile_rows;  /* rows of the field update's TMA patch, a multiple of 16
-                               (16..64; the FP64 form at most 48); default 48 */
+  int      fdtd_tile_rows;  /* rows of the field update's per-warp patch: 12, 16 or 20
+                               (output 26 columns x rows - 6 per patch); default 16 */
   int      pass_chunk;      /* FP32 particle pass: particles per chunk a block takes,
                                a multiple of 256 (256..1792); default 1792 */
 } gasatt_sim_config;

@@ -106,7 +106,10 @@ def test_ion_current_drives_the_fields_like_the_oracle(tables, precision):
     orc.prologue()
     for _ in range(steps):
         orc.step()
-    tol = 1e-12 if precision == _lib.FP64 else 1e-5
+    # FP64: the held ion current is 64-bit fixed point at 2^-48 of q_e FN c per
+    # unit, and ions move at |v|/c ~ 1e-3, so each contribution is quantised at
+    # ~5e-12 of itself where the oracle sums doubles (measured: 1.2e-12)
+    tol = 1e-11 if precision == _lib.FP64 else 1e-5
     Er, Ez, H = sim.fields()
     assert np.abs(orc.Ez).max() > 0
     close(Er, orc.Er, tol, "Er"); close(Ez, orc.Ez, tol, "Ez"); close(H, orc.H, tol, "H")

@@ -33,7 +33,7 @@ def test_tune_every_knob_by_coordinate_descent(precision):
         assert set(knobs) == {"fdtd_tile_rows", "pass_chunk", "sort_period"}
     else:
         assert set(knobs) == {"fdtd_tile_rows", "sort_period"}
-        assert max(knobs["fdtd_tile_rows"]) <= 48
+    assert set(knobs["fdtd_tile_rows"]) == {12, 16, 20}
     best, table = tune(cfg, parts, steps=20)
     for name, cands in knobs.items():
         assert set(table[name]) == set(cands)
@@ -49,9 +49,7 @@ def test_launch_knobs_leave_results_bit_identical(precision):
     from _cases import grid_fields
     from gasatt.sim import Sim
     outs = []
-    shapes = [(16, 256), (32, 1792), (48, 1024)]
-    if precision == _lib.FP32_SPLIT:
-        shapes.append((64, 512))
+    shapes = [(12, 256), (16, 1792), (20, 1024), (16, 512)]
     for rows, chunk in shapes:
         cfg = config(40, 150, 5e-6, 1e-14, 300.0, precision=precision, capacity=60000, seed=7,
                      sort_period=7)
@@ -75,8 +73,8 @@ def test_launch_knobs_leave_results_bit_identical(precision):
 def test_bad_launch_knobs_are_rejected():
     from gasatt._lib import GasattError
     from gasatt.sim import Sim
-    for prec, rows, chunk in ((_lib.FP32_SPLIT, 40, 0), (_lib.FP32_SPLIT, 80, 0),
-                              (_lib.FP64, 64, 0), (_lib.FP32_SPLIT, 0, 300),
+    for prec, rows, chunk in ((_lib.FP32_SPLIT, 40, 0), (_lib.FP32_SPLIT, 8, 0),
+                              (_lib.FP64, 24, 0), (_lib.FP32_SPLIT, 0, 300),
                               (_lib.FP32_SPLIT, 0, 2048)):
         cfg = config(32, 64, 5e-6, 1e-14, 1.0, precision=prec, capacity=1000)
         cfg.fdtd_tile_rows, cfg.pass_chunk = rows, chunk
