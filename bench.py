@@ -107,7 +107,7 @@ class ClockSampler:
 
 # ------------------------------------------------------------ ours (GPU)
 SORT_PERIODS = (20, 30, 40, 60)     # candidates of the sort period for the autotuner
-KNOBS = ("fdtd_tile_rows", "pass_chunk", "sort_period")
+KNOBS = ("fdtd_tile_rows", "pass_chunk", "gather", "sort_period")
 
 
 def workload_setup(precision, rank, knobs=None):
@@ -134,7 +134,8 @@ def make_sim(precision, device, rank, torch, knobs=None):
 
 
 def tuned_knobs(precision, device, rank):
-    """The launch-shape knobs (field patch rows, FP32 chunk size, sort period)
+    """The launch-shape knobs (field patch rows, FP32 chunk size and gather
+    source, sort period)
     the autotuner picks for this workload by coordinate descent; results do
     not depend on them (see gasatt.tune).  Returns ({knob: value}, {knob:
     {candidate: ms per step}})."""

@@ -329,8 +329,9 @@ __device__ __forceinline__ void fdtd_warp_body(const FdtdWork &W) {
     const int ldf = I.ldf, ldj = I.ldj;
     const bool out_col = lane >= kTmaHalo && lane < kTmaHalo + kTmaTileW && col <= nr;
     if (sizeof(T) == 4) {
-      // FP32 form: the fields rounded to float once; whole gather quads from
-      // those floats (corner columns from the lane below by shuffle)
+      // FP32 form: the fields rounded to float once; whole gather quads (when
+      // the cell has them) from those floats, corner columns from the lane
+      // below by shuffle
       const FieldQuads q = I.q;
       float fe[R], fz[R], fh[R];
 #pragma unroll
@@ -355,6 +356,7 @@ __device__ __forceinline__ void fdtd_warp_body(const FdtdWork &W) {
           Jr_next[g] = 0;
           Jz_next[g] = 0;
         }
+        if (!q.er) continue;                                 // no gather quads in this cell
         const bool ra_lo = row > 0, rb_lo = row > nz - 1;   // quad rows ra = row - 1, rb = row - 1
         if (row < nz)
           q.er[col + (int64_t)row * (nr + 1)] =

@@ -949,12 +949,14 @@ __device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, 
   const float rc = (float)ir + fr;
   const float X = rc + dx;
   const float r2 = fmaf(X, X, dy * dy);
+  // (products that feed a sum are __fmul_rn: never contracted into an FMA,
+  // so every kernel that inlines this rounds the same way)
   const float irn = rsqrt_nr(r2);                    // 1/r' (inf at r' = 0)
-  const float rn = r2 * irn;
+  const float rn = __fmul_rn(r2, irn);
   const float sn = r2 > 0.f ? dy * irn : 0.f;
-  const float s2 = sn * sn;
+  const float s2 = __fmul_rn(sn, sn);
   const float cc = 1.f - s2;                         // cos^2 a
-  const float sq = cc > 0.f ? cc * rsqrtf(cc) : 0.f;
+  const float sq = cc > 0.f ? __fmul_rn(cc, rsqrtf(cc)) : 0.f;
   const float c1 = X >= 0.f ? __fdividef(s2, 1.f + sq) : 1.f + sq;   // 1 - cos a
   // (du_r, du_theta) = (sn ut - c1 ur, -sn ur - c1 ut)
   const float2 du = __ffma2_rn(f2(sn, -sn), f2(ut, ur), __fmul2_rn(f2(ur, ut), f2(-c1)));
@@ -1076,11 +1078,24 @@ __device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &
   float wr, wz;
   half_shift(ir, fr, ar, wr);
   half_shift(iz, fz, az, wz);
-  // the field loads go out first (one packed quad per field, corners already
-  // clamped at the edges); their latency hides behind Philox
-  const float4 a4 = __ldg(P.qEr + ((ar + 1) + iz * (P.nr + 1)));
-  const float4 b4 = __ldg(P.qEz + (ir + (az + 1) * P.nr));
-  const float4 c4 = __ldg(P.qH + ((ar + 1) + (az + 1) * (P.nr + 1)));
+  // the field loads go out first, their latency hidden behind Philox: one
+  // packed quad per field (corners already clamped at the edges), or the
+  // same four corners from the fields themselves (the same floats)
+  float4 a4, b4, c4;
+  if (P.qEr) {
+    a4 = __ldg(P.qEr + ((ar + 1) + iz * (P.nr + 1)));
+    b4 = __ldg(P.qEz + (ir + (az + 1) * P.nr));
+    c4 = __ldg(P.qH + ((ar + 1) + (az + 1) * (P.nr + 1)));
+  } else {
+    const int c0 = max(ar, 0), c1 = min(ar + 1, P.nr - 1);
+    const int ra = max(az, 0), rb = min(az + 1, P.nz - 1);
+    const float *e0 = F.Er + iz * P.ldf, *e1 = e0 + P.ldf;
+    a4 = make_float4(__ldg(e0 + c0), __ldg(e0 + c1), __ldg(e1 + c0), __ldg(e1 + c1));
+    const float *z0 = F.Ez + ra * P.ldf + ir, *z1 = F.Ez + rb * P.ldf + ir;
+    b4 = make_float4(__ldg(z0), __ldg(z0 + 1), __ldg(z1), __ldg(z1 + 1));
+    const float *h0 = F.H + ra * P.ldf, *h1 = F.H + rb * P.ldf;
+    c4 = make_float4(__ldg(h0 + c0), __ldg(h0 + c1), __ldg(h1 + c0), __ldg(h1 + c1));
+  }
   philox4x32_10(c, P.pk);
   // bilinear mixes from the quads' corners (c0,r0), (c1,r0), (c0,r1), (c1,r1)
   // = (x, y, z, w), paired: the low and high rows of each quad along its
@@ -1751,19 +1766,48 @@ __device__ __forceinline__ int cell_of32(const State32 &S, long long p, int nr) 
   return ar + az * (nr + 1);
 }
 
+// Runs of equal keys among the lanes of a warp (the particles are nearly in
+// key order, so a warp holds few runs): a lane heads a run when its key
+// differs from the lane below's; dead lanes (key -1) end runs.  For each lane:
+// its run's head lane h and, at the head, the run's length.
+__device__ __forceinline__ void key_runs(int c, int lane, int &h, int &len) {
+  const int below = __shfl_up_sync(0xFFFFFFFFu, c, 1);
+  const bool head = c >= 0 && (lane == 0 || below != c);
+  const unsigned heads = __ballot_sync(0xFFFFFFFFu, head);
+  const unsigned ends = __ballot_sync(0xFFFFFFFFu, head || c < 0);
+  const unsigned up = lane == 31 ? 0u : ends & (0xFFFFFFFFu << (lane + 1));
+  len = (up ? __ffs(up) - 1 : 32) - lane;
+  const unsigned le = heads & (lane == 31 ? 0xFFFFFFFFu : ((2u << lane) - 1));
+  h = le ? 31 - __clz(le) : lane;
+}
+
+// Each warp takes segments of kSortSeg particles (kSortSeg / 32 per lane,
+// consecutive groups of 32), loading all of a segment's keys before using
+// them, so that several loads per thread are in flight.
+constexpr int kSortSeg = 128;
+
 template <int FORM>
 __global__ void k_sort_hist(State64 S64, State32 S32, const SimCounters *cnt, int nr, int nz,
                             double dr, double dz, int *count) {
+  constexpr int G = kSortSeg / 32;
   const long long n0 = slots_in_use(cnt);
-  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n0;
-       base += (long long)gridDim.x * blockDim.x) {
-    const long long p = base + (threadIdx.x & 31);
-    int c = -1;
-    if (p < n0) c = FORM == 0 ? cell_of64(S64, p, nr, nz, dr, dz) : cell_of32(S32, p, nr);
-    const unsigned live = __ballot_sync(0xFFFFFFFFu, c >= 0);
-    if (c < 0) continue;
-    const unsigned mask = __match_any_sync(live, c);
-    if ((__ffs(mask) - 1) == (int)(threadIdx.x & 31)) atomicAdd(count + c, __popc(mask));
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+  for (long long seg = (long long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+       seg * kSortSeg < n0; seg += warps) {
+    int c[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const long long p = seg * kSortSeg + g * 32 + lane;
+      c[g] = -1;
+      if (p < n0) c[g] = FORM == 0 ? cell_of64(S64, p, nr, nz, dr, dz) : cell_of32(S32, p, nr);
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      int h, len;
+      key_runs(c[g], lane, h, len);
+      if (c[g] >= 0 && h == lane) atomicAdd(count + c[g], len);
+    }
   }
 }
 
@@ -1771,26 +1815,36 @@ template <int FORM>
 __global__ void k_sort_scatter(State64 A64, State64 B64, State32 A32, State32 B32,
                                SimCounters *cnt, int nr, int nz, double dr, double dz,
                                const int *offset, int *cursor) {
+  constexpr int G = kSortSeg / 32;
   const long long n0 = slots_in_use(cnt);
   const int lane = threadIdx.x & 31;
-  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n0;
-       base += (long long)gridDim.x * blockDim.x) {
-    const long long p = base + lane;
-    int c = -1;
-    if (p < n0) c = FORM == 0 ? cell_of64(A64, p, nr, nz, dr, dz) : cell_of32(A32, p, nr);
-    const unsigned live = __ballot_sync(0xFFFFFFFFu, c >= 0);
-    if (c < 0) continue;
-    const unsigned mask = __match_any_sync(live, c);
-    const int leader = __ffs(mask) - 1;
-    int basepos = 0;
-    if (lane == leader) basepos = atomicAdd(cursor + c, __popc(mask));
-    basepos = __shfl_sync(mask, basepos, leader);
-    const long long dst = (long long)offset[c] + basepos + __popc(mask & ((1u << lane) - 1));
-    if (FORM == 0) {
-      B64.rz[dst] = A64.rz[p]; B64.urt[dst] = A64.urt[p]; B64.uz[dst] = A64.uz[p];
-      B64.id[dst] = A64.id[p];
-    } else {
-      B32.a[dst] = A32.a[p]; B32.b[dst] = A32.b[p]; B32.id[dst] = A32.id[p];
+  const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+  for (long long seg = (long long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+       seg * kSortSeg < n0; seg += warps) {
+    int c[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const long long p = seg * kSortSeg + g * 32 + lane;
+      c[g] = -1;
+      if (p < n0) c[g] = FORM == 0 ? cell_of64(A64, p, nr, nz, dr, dz) : cell_of32(A32, p, nr);
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const long long p = seg * kSortSeg + g * 32 + lane;
+      int h, len;
+      key_runs(c[g], lane, h, len);
+      // the head claims its run's slots in the bin and hands the first one out
+      long long first = 0;
+      if (c[g] >= 0 && h == lane) first = (long long)offset[c[g]] + atomicAdd(cursor + c[g], len);
+      first = __shfl_sync(0xFFFFFFFFu, first, h);
+      if (c[g] < 0) continue;
+      const long long dst = first + (lane - h);
+      if (FORM == 0) {
+        B64.rz[dst] = A64.rz[p]; B64.urt[dst] = A64.urt[p]; B64.uz[dst] = A64.uz[p];
+        B64.id[dst] = A64.id[p];
+      } else {
+        B32.a[dst] = A32.a[p]; B32.b[dst] = A32.b[p]; B32.id[dst] = A32.id[p];
+      }
     }
   }
 }
@@ -1801,9 +1855,10 @@ __global__ void k_sort_scatter(State64 A64, State64 B64, State32 A32, State32 B3
 // are always running or done; it publishes its tile total (flag 1), looks
 // back over the predecessors' published totals until it meets an inclusive
 // prefix (flag 2), publishes its own inclusive prefix and writes its tile.
+// The look-back reads 32 predecessors at a time, one per lane of a warp.
 // A published word is (flag << 62) | value, written in one 64-bit store.
 // The look-back wait on a tile that has published nothing yet is bounded;
-// past the bound the scan sets *err and takes 0 for that tile.
+// past the bound the scan sets *err and takes 0 for the tiles it waited on.
 constexpr int kScanThreads = 256, kScanItems = 16, kScanTile = kScanThreads * kScanItems;
 constexpr unsigned kScanWaitLimit = 1u << 24;
 
@@ -1830,11 +1885,18 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const int *in, int *out, 
   const long long base = (long long)t * kScanTile + (long long)threadIdx.x * kScanItems;
   int v[kScanItems];
   int sum = 0;
+  if (base + kScanItems <= n) {            // whole: four 16-byte loads (base is a multiple of 16)
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    v[k] = base + k < n ? in[base + k] : 0;
-    sum += v[k];
+    for (int k = 0; k < kScanItems; k += 4) {
+      const int4 q = *reinterpret_cast<const int4 *>(in + base + k);
+      v[k] = q.x; v[k + 1] = q.y; v[k + 2] = q.z; v[k + 3] = q.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) v[k] = base + k < n ? in[base + k] : 0;
   }
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) sum += v[k];
   // block scan of the thread sums
   int incl = sum;
 #pragma unroll
@@ -1850,30 +1912,57 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const int *in, int *out, 
     wbase += w < warp ? warp_sum[w] : 0;
     total += warp_sum[w];
   }
-  if (threadIdx.x == 0) {
+  if (warp == 0) {
+    // warp-parallel look-back: lane i reads the word of tile p - i; the
+    // aggregates up to the nearest inclusive prefix are summed in one go
+    constexpr unsigned long long kVal = (1ull << 62) - 1;
     long long excl = 0;
     if (t == 0) {
-      atomicExch(S.tile, (2ull << 62) | (unsigned long long)total);
+      if (lane == 0) atomicExch(S.tile, (2ull << 62) | (unsigned long long)total);
     } else {
-      atomicExch(S.tile + t, (1ull << 62) | (unsigned long long)total);
-      for (long long p = (long long)t - 1; p >= 0; --p) {
-        unsigned long long w = ld_volatile_u64(S.tile + p);
+      if (lane == 0) atomicExch(S.tile + t, (1ull << 62) | (unsigned long long)total);
+      bool failed = false;
+      for (long long p = (long long)t - 1; p >= 0; p -= 32) {
+        const long long q = p - lane;
+        // before tile 0: an inclusive prefix of 0
+        unsigned long long w = q >= 0 ? ld_volatile_u64(S.tile + q) : (2ull << 62);
         unsigned it = 0;
-        while ((w >> 62) == 0 && ++it < kScanWaitLimit) w = ld_volatile_u64(S.tile + p);
-        if ((w >> 62) == 0) { atomicOr(S.err, 1u); break; }
-        excl += (long long)(w & ((1ull << 62) - 1));
-        if ((w >> 62) == 2) break;
+        while (__any_sync(0xFFFFFFFFu, (w >> 62) == 0) && ++it < kScanWaitLimit)
+          if ((w >> 62) == 0) w = ld_volatile_u64(S.tile + q);
+        if (__any_sync(0xFFFFFFFFu, (w >> 62) == 0)) { failed = true; break; }
+        const unsigned inc = __ballot_sync(0xFFFFFFFFu, (w >> 62) == 2);
+        const int stop = inc ? __ffs(inc) - 1 : 31;
+        long long v = lane <= stop ? (long long)(w & kVal) : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        excl += v;
+        if (inc) break;
       }
-      atomicExch(S.tile + t, (2ull << 62) | (unsigned long long)(excl + total));
+      if (lane == 0) {
+        if (failed) atomicOr(S.err, 1u);
+        atomicExch(S.tile + t, (2ull << 62) | (unsigned long long)(excl + total));
+      }
     }
-    excl_s = excl;
+    if (lane == 0) excl_s = excl;
   }
   __syncthreads();
   int run = (int)excl_s + wbase + incl - sum;
+  if (base + kScanItems <= n) {
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    if (base + k < n) out[base + k] = run;
-    run += v[k];
+    for (int k = 0; k < kScanItems; k += 4) {
+      int4 o;
+      o.x = run; run += v[k];
+      o.y = run; run += v[k + 1];
+      o.z = run; run += v[k + 2];
+      o.w = run; run += v[k + 3];
+      *reinterpret_cast<int4 *>(out + base + k) = o;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      if (base + k < n) out[base + k] = run;
+      run += v[k];
+    }
   }
 }
 
@@ -2526,6 +2615,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   if (c.pass_chunk < 0 || c.pass_chunk > kChunkMax || c.pass_chunk % kBlock)
     return fail(ctx, GASATT_E_ARG, "pass_chunk: a multiple of 256 in [256, 1792] (0: 1792)");
   if (c.fdtd_tile_rows < 0) return fail(ctx, GASATT_E_ARG, "fdtd_tile_rows: >= 0");
+  if (c.gather < 0 || c.gather > 2) return fail(ctx, GASATT_E_ARG, "gather: 0 (auto), 1 (quads) or 2 (fields)");
   if (c.ion_capacity < 0 || (c.ion_capacity > 0 && (c.ion_subcycle < 1 || !(c.m_ion > 0) ||
                                                      !(c.gas_temperature >= 0))))
     return fail(ctx, GASATT_E_ARG, "ion species: ion_capacity >= 0, ion_subcycle >= 1, m_ion > 0");
@@ -2584,7 +2674,11 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   s->d_tab = tmpd;
   if ((rc = sim_alloc(s, &s->invV, (size_t)nr)) || (rc = sim_alloc(s, &s->fdtd_colc, (size_t)3 * nr)))
     return cleanup(rc);
-  if (s->form == 1) {
+  // FP32 gather quads: 48 bytes more per cell written by every field update,
+  // against nine fewer loads per electron; worth it where electrons are dense
+  const bool quads = s->form == 1 &&
+                     (c.gather == 1 || (c.gather == 0 && c.capacity >= 4 * (int64_t)(nr + 1) * (nz + 1)));
+  if (quads) {
     if ((rc = sim_alloc(s, &s->quads.er, (size_t)(nr + 1) * nz)) ||
         (rc = sim_alloc(s, &s->quads.ez, (size_t)nr * (nz + 1))) ||
         (rc = sim_alloc(s, &s->quads.h, (size_t)(nr + 1) * (nz + 1))))
@@ -3081,7 +3175,7 @@ int fields_io(gasatt_sim *s, double *Er, double *Ez, double *H, int on_device, b
     }
     off += n;
   }
-  if (set) {
+  if (set && s->quads.er) {
     const int64_t n = (int64_t)nr * (nz + 1) + (int64_t)(nr + 1) * nz + (int64_t)nr * nz;
     k_build_quads<<<grid_for(n, kBlock), kBlock, 0, st>>>(
         (const float *)s->Er, (const float *)s->Ez, (const float *)s->H, nr, nz, ld, s->quads);

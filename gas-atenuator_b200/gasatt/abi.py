@@ -30,6 +30,8 @@ FAITHFUL = 0x0FFF
 POS_IN_CYL = 1 << 16
 MCC_NDRAW = 8
 FP64, FP32_SPLIT = 0, 1
+# SimConfig.gather (FP32 form): automatic, packed quads, direct field loads
+GATHER_AUTO, GATHER_QUADS, GATHER_FIELDS = 0, 1, 2
 
 
 class Tables(ctypes.Structure):
@@ -48,7 +50,8 @@ class SimConfig(ctypes.Structure):
                 ("precision", c_i), ("capacity", c_i64), ("ion_capacity", c_i64),
                 ("seed", c_u64), ("flags", c_u), ("sort_period", c_i), ("secondaries", c_i),
                 ("table_n", c_i), ("table_emin_ev", c_d), ("table_emax_ev", c_d),
-                ("ion_subcycle", c_i), ("fdtd_tile_rows", c_i), ("pass_chunk", c_i)]
+                ("ion_subcycle", c_i), ("fdtd_tile_rows", c_i), ("pass_chunk", c_i),
+                ("gather", c_i)]
 
 
 class Diag(ctypes.Structure):

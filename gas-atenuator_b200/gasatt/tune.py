@@ -1,6 +1,6 @@
 """Autotuning of the resident simulation's launch-shape knobs.
 
-Three knobs change speed and not results (random streams are keyed on
+Four knobs change speed and not results (random streams are keyed on
 particle ids and steps, the deposit is an exact integer sum, and the field
 update's arithmetic is the same for every patch):
 
@@ -14,7 +14,10 @@ update's arithmetic is the same for every patch):
                   the warps to share;
   pass_chunk      particles per chunk of the FP32 particle pass (its deposit
                   window's span against the number of chunks for the blocks
-                  to balance).
+                  to balance);
+  gather          where the FP32 push reads E and H: packed 2 x 2 quads the
+                  field update writes beside the fields (fewer loads per
+                  electron, 48 more bytes written per cell), or the fields.
 
 The best setting depends on the workload (particle speed, cell size, time
 step, population, grid), so it is measured: fresh copies of the same
@@ -86,6 +89,7 @@ def knob_candidates(cfg):
         knobs = {}                         # only the fdtd_ratio 1 field update has tiles
     if fp32:
         knobs["pass_chunk"] = DEFAULT_CHUNKS
+        knobs["gather"] = (abi.GATHER_QUADS, abi.GATHER_FIELDS)
     knobs["sort_period"] = DEFAULT_SORT_PERIODS
     return knobs
 

@@ -277,6 +277,12 @@ typedef struct gasatt_sim_config {
                                (output 26 columns x rows - 6 per patch); default 16 */
   int      pass_chunk;      /* FP32 particle pass: particles per chunk a block takes,
                                a multiple of 256 (256..1792); default 1792 */
+  int      gather;          /* FP32 form, how the push reads E and H: 1 = packed 2 x 2
+                               quads the field update writes beside the fields (three
+                               16-byte loads per electron, 48 more bytes written per
+                               cell), 2 = the four corners straight from the fields;
+                               0 = quads when the capacity is at least 4 electrons per
+                               cell.  Both give the same bits. */
 } gasatt_sim_config;
 
 typedef struct gasatt_diag {
