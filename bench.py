@@ -671,21 +671,23 @@ def c3_batched(precision, device, torch, steps=100, warmup=5, sort_period=30):
 
 def run_c3(args):
     """Batched instances (one graph launch per step for all cells) against the
-    same instances stepped one after another; FP32 split form."""
+    same instances stepped one after another, in the form --precision; births
+    drawn on the GPU as in the bench line's batched leg."""
     import torch
-    from gasatt import _lib
+    from gasatt import abi
     from gasatt.dropin import Context
-    from gasatt.sim import Batch, Sim, births, config
+    from gasatt.sim import Batch, Sim
+    from gasatt.workload import config
     torch.cuda.set_device(0)
+    prec = abi.FP32_SPLIT if args.precision == "fp32_split" else abi.FP64
     ctx = Context(0)
     ctx.bind_stream()
     sims = []
     for c in c3_cells():
-        cfg = config(c["n_r"], c["n_z"], c["delta"], c["dt"], c["torr"], precision=_lib.FP32_SPLIT,
+        cfg = config(c["n_r"], c["n_z"], c["delta"], c["dt"], c["torr"], precision=prec,
                      capacity=6 * c["photo"], seed=c["seed"], sort_period=30)
         sim = Sim(cfg, ctx=ctx)
-        sim.load(*births(c["photo"], c["e_keV"], c["n_z"] * c["delta"], seed=c["seed"],
-                         Rp=c["n_r"] * c["delta"]))
+        sim.birth_photo(c["photo"], c["e_keV"], seed=c["seed"])
         sims.append(sim)
     batch = Batch(sims, sort_period=30)
     stream = torch.cuda.current_stream()
@@ -716,7 +718,7 @@ def run_c3(args):
             "config": {"workload": "48 cells: p log-U(0.1, 10) Torr, grid from "
                        "{64x256, 128x512, 256x1024, 512x2048} at 10 um, dt 2e-14 s, photon "
                        "U(2, 20) keV, photoionizations log-U(1e4, 1e6), seed 2",
-                       "precision": "fp32_split", "sort_period": 30, "l2": "not flushed"}}
+                       "precision": args.precision, "sort_period": 30, "l2": "not flushed"}}
     print(json.dumps(line), flush=True)
     batch.close()
     for s in sims:
