@@ -943,7 +943,10 @@ __device__ __forceinline__ void reflect_z(int &iz, float &fz, float &uz, int nz)
 __device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, float &ur,
                                         float &ut, float &uz, bool &alive, const SimParams &P,
                                         uint32_t rb, float hr, float hz, float &ig) {
-  ig = rsqrt_nr(fmaf(ur, ur, fmaf(ut, ut, fmaf(uz, uz, 1.0f))));   // 1/gamma, kept by the turn
+  // 1/gamma, kept by the turn.  (The hardware estimate is enough here: it only
+  // scales the displacement and the current, and the turn keeps |u| whatever
+  // it is; the kick's 1/gamma is refined.)
+  ig = rsqrtf(fmaf(ur, ur, fmaf(ut, ut, fmaf(uz, uz, 1.0f))));
   const float2 dxy = __fmul2_rn(__fmul2_rn(f2(ur, ut), f2(ig)), f2(hr));   // (dx, dy)
   const float dx = dxy.x, dy = dxy.y, dzz = uz * ig * hz;
   const float rc = (float)ir + fr;
@@ -955,9 +958,8 @@ __device__ __forceinline__ void drift32(int &ir, int &iz, float &fr, float &fz, 
   const float rn = __fmul_rn(r2, irn);
   const float sn = r2 > 0.f ? dy * irn : 0.f;
   const float s2 = __fmul_rn(sn, sn);
-  const float cc = 1.f - s2;                         // cos^2 a
-  const float sq = cc > 0.f ? __fmul_rn(cc, rsqrtf(cc)) : 0.f;
-  const float c1 = X >= 0.f ? __fdividef(s2, 1.f + sq) : 1.f + sq;   // 1 - cos a
+  const float cs = r2 > 0.f ? X * irn : 1.f;         // cos a
+  const float c1 = X >= 0.f ? __fdividef(s2, 1.f + cs) : 1.f - cs;   // 1 - cos a
   // (du_r, du_theta) = (sn ut - c1 ur, -sn ur - c1 ut)
   const float2 du = __ffma2_rn(f2(sn, -sn), f2(ut, ur), __fmul2_rn(f2(ur, ut), f2(-c1)));
   const float2 u2 = sround_add2(f2(ur, ut), du, rb);
@@ -1016,16 +1018,17 @@ __device__ __forceinline__ void deposit_nodes32(const SimParams &P, int ir, int 
 
 // FP32-form deposit window: int32 sums of one chunk of particles on the grid
 // rows [row0, row0 + rows) in shared memory.  A chunk holds at most kChunkMax
-// particles, so a node's window sum stays below kChunkMax * 2^20 < 2^31.  Rows
-// are ws >= nr words apart with ws = 3 (mod 32), so the 3 x 3 nodes around a
-// warp's particles sit in 9 different banks.  Nodes outside the window go
-// straight to the grid with 64-bit atomics; the window is added to the grid
-// with one 64-bit atomic per touched node.
-constexpr int kWinNodes = 4096;           // per component
+// particles, so a node's window sum stays below kChunkMax * 2^20 < 2^31.  A
+// node's two sums (r, z) are adjacent words, so one address serves both
+// atomics; rows are ws >= nr nodes apart with ws = 3 (mod 32), so the 3 x 3
+// nodes around a warp's particles sit in 9 different bank pairs.  Nodes
+// outside the window go straight to the grid with 64-bit atomics; the window
+// is added to the grid with one 64-bit atomic per touched node.
+constexpr int kWinNodes = 4096;           // nodes (two int32 sums each)
 constexpr int kChunkMax = 7 * kBlock;     // 1792 particles (the default chunk)
 
 struct Win32 {
-  int *r, *z;
+  int *rz;                  // node k: r at rz[2k], z at rz[2k + 1]
   int row0, rows, ws;
 };
 
@@ -1036,8 +1039,8 @@ __device__ __forceinline__ void win_node(const Win32 &w, const SimParams &P, int
   const unsigned lr = (unsigned)(row - w.row0);
   if (lr < (unsigned)w.rows) {
     const int k = (int)lr * w.ws + col;
-    atomicAdd(w.r + k, vr);
-    atomicAdd(w.z + k, vz);
+    atomicAdd(w.rz + 2 * k, vr);
+    atomicAdd(w.rz + 2 * k + 1, vz);
   } else {
     const int64_t g = col + (int64_t)row * P.ldj;
     if (vr) atomicAdd(P.Jr + g, (unsigned long long)(long long)vr);
@@ -1062,14 +1065,15 @@ __device__ __forceinline__ uint4 pack32(int ir, int iz, float fr, float fz, floa
 // the whole step, null-collision candidate test; mode 1: half drift (start of
 // a run); mode 2: gather, kick, half drift to integer time (end of a run).
 // Returns whether the particle is a collision candidate (alive, mode 0).
+template <int MODE>
 __device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &F, uint64_t id,
-                                       long long step, int mode, int &ir, int &iz, float &fr,
+                                       long long step, int &ir, int &iz, float &fr,
                                        float &fz, float &ur, float &ut, float &uz, bool &alive,
                                        float &ig) {
   // block 0 of this particle's stream: words 0-1 decide the null-collision
   // candidate, words 2-3 drive the stochastic rounding of the kick and the turn
   uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)step, 0u};
-  if (mode == 1) {
+  if (MODE == 1) {
     philox4x32_10(c, P.pk);
     drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, c[3], P.hdr, P.hdz, ig);
     return false;
@@ -1118,9 +1122,9 @@ __device__ __forceinline__ bool push32(const SimParams &P, const Fields<float> &
   const float2 uk = sround_add2(f2(ur, uz), du, c[2]);
   ur = uk.x;
   uz = uk.y;
-  const float h = mode == 0 ? 2.f : 1.f;
+  const float h = MODE == 0 ? 2.f : 1.f;
   drift32(ir, iz, fr, fz, ur, ut, uz, alive, P, c[3], h * P.hdr, h * P.hdz, ig);
-  return alive && mode == 0 && (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
+  return alive && MODE == 0 && (((((uint64_t)c[0]) << 32) | c[1]) >> 12) < P.cand_below;
 }
 
 // ig: the drift's 1/gamma, as in the chunk loop, so that a particle deposits
@@ -1180,7 +1184,9 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
       const uint64_t cid = child_id(id, cstep);
       if (push) {
         float cig;
-        cc = push32(P, F, cid, step, mode, cir, ciz, cfr, cfz, cur, cut, cuz, calive, cig);
+        cc = mode == 0 ? push32<0>(P, F, cid, step, cir, ciz, cfr, cfz, cur, cut, cuz, calive, cig)
+           : mode == 1 ? push32<1>(P, F, cid, step, cir, ciz, cfr, cfz, cur, cut, cuz, calive, cig)
+                       : push32<2>(P, F, cid, step, cir, ciz, cfr, cfz, cur, cut, cuz, calive, cig);
         if (calive && mode != 2) deposit_global32(P, cir, ciz, cfr, cfz, cur, cuz, cig);
         if (!calive) {
           lost++;
@@ -1199,7 +1205,9 @@ __device__ __noinline__ void candidate32(const SimParams *__restrict__ Pg, Field
   bool alive = true, pc = false;
   if (push) {
     float pig;
-    pc = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive, pig);
+    pc = mode == 0 ? push32<0>(P, F, id, step, ir, iz, fr, fz, ur, ut, uz, alive, pig)
+       : mode == 1 ? push32<1>(P, F, id, step, ir, iz, fr, fz, ur, ut, uz, alive, pig)
+                   : push32<2>(P, F, id, step, ir, iz, fr, fz, ur, ut, uz, alive, pig);
     if (alive && mode != 2) deposit_global32(P, ir, iz, fr, fz, ur, uz, pig);
     if (!alive) {
       lost++;
@@ -1254,8 +1262,9 @@ __device__ __forceinline__ void prefetch_chunk32(const State32 &S, long long beg
 // push (push32), collision candidates queued, deposit into the window w
 // (nodes outside the window straight to the grid).  The highest window column touched is merged
 // into *box_cmax; electrons absorbed at the wall are counted into cnt.
+template <int MODE>
 __device__ __forceinline__ void chunk32(const SimParams &P, const State32 &S, const Fields<float> &F,
-                                        SimCounters *cnt, int *queue, long long step, int mode,
+                                        SimCounters *cnt, int *queue, long long step,
                                         int beg, int end, const Win32 &w, int *box_cmax) {
   const int par = (int)(step & 1);
   const uint32_t parbit = par ? kSign : 0u;
@@ -1288,14 +1297,14 @@ __device__ __forceinline__ void chunk32(const SimParams &P, const State32 &S, co
     bool cand = false;
     if (act) {
       bool alive = true;
-      cand = push32(P, F, id, step, mode, ir, iz, fr, fz, ur, ut, uz, alive, ig);
+      cand = push32<MODE>(P, F, id, step, ir, iz, fr, fz, ur, ut, uz, alive, ig);
       if (!alive) {
         lost++;
         count_wall_loss(cnt, (double)ur * ur + (double)ut * ut + (double)uz * uz, P.me * P.c * P.c / P.qe);
       }
       S.a[p] = pack32(ir, iz, fr, fz, ur, alive, cand, par);
       S.b[p] = make_float2(ut, uz);
-      act = alive && mode != 2;
+      act = alive && MODE != 2;
     }
     queue_push(cand, p, &cnt->n_cand[par], queue + (long long)par * P.cap);
     // Deposit: each lane adds its own eight contributions to the window,
@@ -1310,10 +1319,12 @@ __device__ __forceinline__ void chunk32(const SimParams &P, const State32 &S, co
       const unsigned l0 = (unsigned)(r0 - w.row0), l1 = (unsigned)(r1 - w.row0);
       if (l0 < (unsigned)w.rows && l1 < (unsigned)w.rows) {
         const int k0 = (int)l0 * w.ws, k1 = (int)l1 * w.ws;
-        atomicAdd(w.r + k0 + c0, vr[0]); atomicAdd(w.z + k0 + c0, vz[0]);
-        atomicAdd(w.r + k0 + c1, vr[1]); atomicAdd(w.z + k0 + c1, vz[1]);
-        atomicAdd(w.r + k1 + c0, vr[2]); atomicAdd(w.z + k1 + c0, vz[2]);
-        atomicAdd(w.r + k1 + c1, vr[3]); atomicAdd(w.z + k1 + c1, vz[3]);
+        int *n00 = w.rz + 2 * (k0 + c0), *n10 = w.rz + 2 * (k0 + c1);
+        int *n01 = w.rz + 2 * (k1 + c0), *n11 = w.rz + 2 * (k1 + c1);
+        atomicAdd(n00, vr[0]); atomicAdd(n00 + 1, vz[0]);
+        atomicAdd(n10, vr[1]); atomicAdd(n10 + 1, vz[1]);
+        atomicAdd(n01, vr[2]); atomicAdd(n01 + 1, vz[2]);
+        atomicAdd(n11, vr[3]); atomicAdd(n11 + 1, vz[3]);
       } else {
         win_node(w, P, c0, r0, vr[0], vz[0]);
         win_node(w, P, c1, r0, vr[1], vz[1]);
@@ -1338,12 +1349,13 @@ __device__ __forceinline__ void flush32(const SimParams &P, const Win32 &w, int 
   for (int i = threadIdx.x; i < nb; i += kBlock) {
     const int row = i / bw, col = i - row * bw;
     const int k = row * w.ws + col;
-    const int vr = w.r[k], vz = w.z[k];
+    const int2 v = reinterpret_cast<const int2 *>(w.rz)[k];
+    const int vr = v.x, vz = v.y;
     if (vr | vz) {
       const int64_t g = (int64_t)(w.row0 + row) * P.ldj + col;
       if (vr) atomicAdd(P.Jr + g, (unsigned long long)(long long)vr);
       if (vz) atomicAdd(P.Jz + g, (unsigned long long)(long long)vz);
-      w.r[k] = 0; w.z[k] = 0;
+      reinterpret_cast<int2 *>(w.rz)[k] = make_int2(0, 0);
     }
   }
 }
@@ -1354,10 +1366,12 @@ __device__ __forceinline__ void flush32(const SimParams &P, const Win32 &w, int 
 // particles in chunks of P.chunk handed out in order, so the blocks that ran
 // a candidate simply take fewer chunks.  Counters are committed by the field
 // kernel of the next step.
+template <int MODE>
 __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fields<float> F,
-                                                      SimCounters *cnt, int *queue, int mode,
+                                                      SimCounters *cnt, int *queue,
                                                       const SimParams *__restrict__ Pg) {
-  __shared__ int win_r[kWinNodes], win_z[kWinNodes];
+  constexpr int mode = MODE;
+  __shared__ __align__(16) int win_rz[2 * kWinNodes];
   __shared__ int win_row0, win_rows;
   __shared__ int box_cmax;                       // highest window column the chunk touched
   __shared__ long long chunk_at;
@@ -1366,7 +1380,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
   const int par = (int)(step & 1);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // the window starts zeroed; each chunk's flush leaves it zeroed again
-  for (int i = threadIdx.x; i < kWinNodes; i += kBlock) { win_r[i] = 0; win_z[i] = 0; }
+  for (int i = threadIdx.x; i < kWinNodes; i += kBlock) reinterpret_cast<int2 *>(win_rz)[i] = make_int2(0, 0);
   const int ws = win_stride(P.nr);
   const int maxrows = min(kWinNodes / ws, P.nz);
   const int chunk = P.chunk;
@@ -1408,8 +1422,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
     if (ch >= nchunk) break;
     // 32-bit slot indices: the capacity is below 2^31
     const int beg = (int)(ch * chunk), end = (int)min((long long)beg + chunk, n0);
-    const Win32 w{win_r, win_z, win_row0, win_rows, ws};
-    chunk32(P, S, F, cnt, queue, step, mode, beg, end, w, &box_cmax);
+    const Win32 w{win_rz, win_row0, win_rows, ws};
+    chunk32<MODE>(P, S, F, cnt, queue, step, beg, end, w, &box_cmax);
     if (threadIdx.x == 0 && next_ch < nchunk)
       chunk_rows32(P, S, n0, chunk, next_ch, maxrows, next_row0, next_rows);
     __syncthreads();
@@ -1438,16 +1452,17 @@ struct BatchCell32 {
 // shared memory when the cell changes.  Every cell gives what its own
 // k_pass32 gives.
 __global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *__restrict__ cells,
-                                                            int ncell, int cur, int jb, int mode,
+                                                            int ncell, int cur, int jb,
                                                             unsigned long long *chunk_next) {
-  __shared__ int win_r[kWinNodes], win_z[kWinNodes];
+  constexpr int mode = 0;        // a batch only takes whole steps
+  __shared__ __align__(16) int win_rz[2 * kWinNodes];
   __shared__ int win_row0, win_rows, box_cmax, cell_at;
   __shared__ long long chunk_at;
   __shared__ long long cand_pre[kMaxBatch + 1], chunk_pre[kMaxBatch + 1];
   __shared__ __align__(16) unsigned char sP_raw[sizeof(SimParams)];
   SimParams &sP = *reinterpret_cast<SimParams *>(sP_raw);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < kWinNodes; i += kBlock) { win_r[i] = 0; win_z[i] = 0; }
+  for (int i = threadIdx.x; i < kWinNodes; i += kBlock) reinterpret_cast<int2 *>(win_rz)[i] = make_int2(0, 0);
   // per-cell candidates (of the previous pass) and chunks, then prefix sums
   for (int c = threadIdx.x; c < ncell; c += kBlock) {
     const SimCounters *cc = cells[c].cnt;
@@ -1525,8 +1540,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *_
     const int chunk = sP.chunk;
     const long long ch = g - chunk_pre[c];
     const int beg = (int)(ch * chunk), end = (int)min((long long)beg + chunk, n0);
-    const Win32 w{win_r, win_z, win_row0, win_rows, win_stride(sP.nr)};
-    chunk32(sP, C.S[cur], C.F, cc, C.queue, step, mode, beg, end, w, &box_cmax);
+    const Win32 w{win_rz, win_row0, win_rows, win_stride(sP.nr)};
+    chunk32<0>(sP, C.S[cur], C.F, cc, C.queue, step, beg, end, w, &box_cmax);
     __syncthreads();
     flush32(sP, w, box_cmax + 1);
   }
@@ -2189,9 +2204,12 @@ int launch_pass(gasatt_sim *s, cudaStream_t st, int mode, int jb, int q) {
                                               Fields<double>{(double *)s->Er, (double *)s->Ez, (double *)s->H},
                                               s->cnt, s->queue, mode, q);
   else
-    k_pass32<<<s->pass_grid, kBlock, 0, st>>>(P, s->s32[b],
-                                              Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H},
-                                              s->cnt, s->queue, mode, s->d_P + jb);
+  {
+    auto kern = mode == 0 ? k_pass32<0> : mode == 1 ? k_pass32<1> : k_pass32<2>;
+    kern<<<s->pass_grid, kBlock, 0, st>>>(P, s->s32[b],
+                                          Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H},
+                                          s->cnt, s->queue, s->d_P + jb);
+  }
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "particle pass launch");
@@ -2755,7 +2773,7 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   }
   int occ = 4;
   if (s->form == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass64, kBlock, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass32, kBlock, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass32<0>, kBlock, 0);
   s->pass_grid = (unsigned)(nsm * (occ > 0 ? occ : 1));
   if (s->form == 1) {
     // FP32 blocks take chunks from a counter: no more blocks than chunks the
@@ -3624,7 +3642,7 @@ int batch_group_launch(gasatt_batch *b, BatchGroup &G, cudaStream_t cs, cudaStre
                                                                         G.commit, n);
     GASATT_CUDA(ctx, cudaGetLastError());
     GASATT_CUDA(ctx, cudaMemsetAsync(G.chunk_next, 0, 8, cs));
-    k_batch_pass32<<<G.pass_grid, kBlock, 0, cs>>>((const BatchCell32 *)G.cells, n, cur, 1 - q, 0,
+    k_batch_pass32<<<G.pass_grid, kBlock, 0, cs>>>((const BatchCell32 *)G.cells, n, cur, 1 - q,
                                                    G.chunk_next);
     GASATT_CUDA(ctx, cudaGetLastError());
     return GASATT_OK;
