@@ -164,26 +164,27 @@ def aligned_warmup(warmup, sort_period):
     return -(-warmup // sort_period) * sort_period
 
 
-def timed_run(sim, steps, warmup, torch, flush, dist_barrier, sort_period):
-    """K steps, each preceded by an L2 flush (outside its event pair), with the
-    library's phase events on: the same steps give the whole-step time (event
-    pair around the step, the periodic sort included when it falls in it), the
-    field update and the particle pass (event nodes in the step graph right
-    before and after each kernel).  The host waits for each step before
+def timed_run(sim, steps, warmup, torch, flush, dist_barrier, sort_period, phase_steps=300):
+    """K steps, each preceded by an L2 flush (outside its event pair), through
+    the production step graphs: the whole-step time, the periodic sort
+    included when it falls in a step.  The host waits for each step before
     enqueuing the next flush; the flush (256 MiB) runs long enough for the
-    next step's launch to be queued behind it."""
+    next step's launch to be queued behind it.  Then `phase_steps` more
+    flushed steps through the instrumented copies of the step graphs (event
+    nodes right before and after each kernel) give the field update and the
+    particle pass apart; those event nodes cost about 10 us per step, so they
+    are kept out of the headline steps."""
     from gasatt._lib import lib
     stream = torch.cuda.current_stream()
-    lib.gasatt_sim_enable_timing(sim.h, 1)
     pre = aligned_warmup(warmup, sort_period)
+    lib.gasatt_sim_enable_timing(sim.h, 0)
     sim.step(pre)
     torch.cuda.synchronize()
     d0 = sim.diag()
     l0 = sim.ctx.launches
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    fd = ctypes.c_float(); ps = ctypes.c_float(); mc = ctypes.c_float()
-    step_ms, pass_ms, fdtd_ms, mcc_ms = [], [], [], []
+    step_ms = []
     dist_barrier()
     torch.cuda.synchronize()
     for _ in range(steps):
@@ -193,13 +194,22 @@ def timed_run(sim, steps, warmup, torch, flush, dist_barrier, sort_period):
         e1.record(stream)
         e1.synchronize()
         step_ms.append(e0.elapsed_time(e1))
-        lib.gasatt_sim_last_timing(sim.h, ctypes.byref(fd), ctypes.byref(ps), ctypes.byref(mc))
-        fdtd_ms.append(fd.value); pass_ms.append(ps.value); mcc_ms.append(mc.value)
     torch.cuda.synchronize()
     dist_barrier()
     launches = sim.ctx.launches - l0
     d1 = sim.diag()
+    # phases, in the instrumented step graphs
+    fd = ctypes.c_float(); ps = ctypes.c_float(); mc = ctypes.c_float()
+    pass_ms, fdtd_ms, mcc_ms = [], [], []
+    lib.gasatt_sim_enable_timing(sim.h, 1)
+    for _ in range(phase_steps):
+        flush()
+        sim.step(1)
+        torch.cuda.synchronize()
+        lib.gasatt_sim_last_timing(sim.h, ctypes.byref(fd), ctypes.byref(ps), ctypes.byref(mc))
+        fdtd_ms.append(fd.value); pass_ms.append(ps.value); mcc_ms.append(mc.value)
     lib.gasatt_sim_enable_timing(sim.h, 0)
+    dist_barrier()
     sorts = sum(1 for i in range(pre, pre + steps) if sort_period > 0 and i % sort_period == 0)
     return dict(step_ms=step_ms, pass_ms=pass_ms, fdtd_ms=fdtd_ms, mcc_ms=mcc_ms, d0=d0, d1=d1,
                 launches=launches, sorts=sorts, warmup_steps=pre)
@@ -476,9 +486,10 @@ def run_ours(args):
                              f"{results['fp32_split']['warmup_steps']} steps so that the window "
                              f"holds ceil(K / sort period) = {results['fp32_split']['sorts']} sorts"),
                    "sorts_in_timed_steps": results["fp32_split"]["sorts"],
-                   "phases": "pass_ms and fdtd_ms: event nodes right before and after each kernel "
-                             "in the same step graphs as the headline (their sum is below "
-                             "ms_per_step)"},
+                   "phases": "pass_ms and fdtd_ms: 300 more flushed steps through instrumented "
+                             "copies of the step graphs (event nodes right before and after each "
+                             "kernel, which add about 10 us per step and are kept out of the "
+                             "headline steps); roofline.achieved uses this pass_ms"},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"] / e2e["steps"],
                 "d2h_bytes_per_step": e2e["d2h"] / e2e["steps"],
                 "call": f"gasatt_sim_run_host, {e2e['steps']} steps per call, pinned host x,y,z,vx,vy,vz in/out"},
