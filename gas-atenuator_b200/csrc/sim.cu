@@ -1412,20 +1412,22 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
       win_row0 = next_row0;
       win_rows = next_rows;
       box_cmax = -1;
-      if (next_ch < nchunk) {
-        next_ch = (long long)atomicAdd(&cnt->chunk_next, 1ull);
-        if (next_ch < nchunk) prefetch_chunk32(S, next_ch * chunk, min((next_ch + 1) * chunk, n0));
-      }
     }
     __syncthreads();
     const long long ch = chunk_at;
     if (ch >= nchunk) break;
+    // thread 0 claims the next chunk now; the claim's result is first used
+    // after this chunk, so its round trip overlaps the chunk's work instead
+    // of holding the block at the barrier above
+    if (threadIdx.x == 0) next_ch = (long long)atomicAdd(&cnt->chunk_next, 1ull);
     // 32-bit slot indices: the capacity is below 2^31
     const int beg = (int)(ch * chunk), end = (int)min((long long)beg + chunk, n0);
     const Win32 w{win_rz, win_row0, win_rows, ws};
     chunk32<MODE>(P, S, F, cnt, queue, step, beg, end, w, &box_cmax);
-    if (threadIdx.x == 0 && next_ch < nchunk)
+    if (threadIdx.x == 0 && next_ch < nchunk) {
+      prefetch_chunk32(S, next_ch * chunk, min((next_ch + 1) * chunk, n0));
       chunk_rows32(P, S, n0, chunk, next_ch, maxrows, next_row0, next_rows);
+    }
     __syncthreads();
     flush32(P, w, box_cmax + 1);
     __syncthreads();
@@ -1486,8 +1488,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *_
   // brought into L2) before the candidates
   long long next = 0;
   int next_c = -1, next_row0 = 0, next_rows = 0;
-  auto fetch = [&]() {           // thread 0: the next item and its window rows
-    next = (long long)atomicAdd(chunk_next, 1ull);
+  auto resolve = [&]() {         // thread 0: the cell and window rows of the claimed item
     if (next < nchunk) {
       next_c = cell_of_item(chunk_pre, ncell, next);
       const BatchCell32 &C = cells[next_c];
@@ -1498,7 +1499,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *_
       chunk_rows32(Pc, C.S[cur], n0c, Pc.chunk, chc, maxrows, next_row0, next_rows);
     }
   };
-  if (threadIdx.x == 0) { fetch(); cell_at = -1; }
+  if (threadIdx.x == 0) {
+    next = (long long)atomicAdd(chunk_next, 1ull);
+    resolve();
+    cell_at = -1;
+  }
   for (long long k = (long long)blockIdx.x * (kBlock / 32) + warp; k < nq;
        k += (long long)gridDim.x * (kBlock / 32)) {
     if (lane == 0) {
@@ -1533,7 +1538,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *_
       __syncthreads();
       if (threadIdx.x == 0) cell_at = c;
     }
-    if (threadIdx.x == 0 && next < nchunk) fetch();
+    // the next item is claimed now and resolved after this one, so the
+    // claim's round trip and the loads it leads to overlap the chunk's work
+    if (threadIdx.x == 0 && next < nchunk) next = (long long)atomicAdd(chunk_next, 1ull);
     const BatchCell32 &C = cells[c];
     SimCounters *cc = C.cnt;
     const long long n0 = (long long)cc->n_total, step = cc->step;
@@ -1542,6 +1549,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *_
     const int beg = (int)(ch * chunk), end = (int)min((long long)beg + chunk, n0);
     const Win32 w{win_rz, win_row0, win_rows, win_stride(sP.nr)};
     chunk32<0>(sP, C.S[cur], C.F, cc, C.queue, step, beg, end, w, &box_cmax);
+    if (threadIdx.x == 0) resolve();
     __syncthreads();
     flush32(sP, w, box_cmax + 1);
   }
