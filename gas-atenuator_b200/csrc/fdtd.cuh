@@ -276,173 +276,4 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
   }
 }
 
-// quad_put for H (shifted on both axes): the four slots every value has,
-// written directly, then the clamped edges' extra slots
-__device__ __forceinline__ void quad_put_h(float4 *Q, int nr, int nz, int i, int j, float v) {
-  const int ncq = nr + 1;
-  float *f = reinterpret_cast<float *>(Q) + 4 * ((int64_t)(i + 1) + (int64_t)(j + 1) * ncq);
-  f[0] = v;                          // quad (i+1, j+1), corner (c0, r0)
-  f[-4 + 1] = v;                     // quad (i, j+1), corner (c1, r0)
-  f[-4 * ncq + 2] = v;               // quad (i+1, j), corner (c0, r1)
-  f[-4 * ncq - 4 + 3] = v;           // quad (i, j), corner (c1, r1)
-  if (i == 0 || i == nr - 1 || j == 0 || j == nz - 1) {
-    const QuadAxis cx = quad_axis_shifted(i, nr), ry = quad_axis_shifted(j, nz);
-    float *g = reinterpret_cast<float *>(Q);
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b)
-        if ((a >= 2 || b >= 2) && ((cx.m >> a) & 1u) && ((ry.m >> b) & 1u))
-          g[(((int64_t)cx.q[a] + (int64_t)ry.q[b] * ncq) << 2) + cx.d[a] + 2 * ry.d[b]] = v;
-  }
-}
-
-// The fused sub-cycle for fdtd_ratio 1 (the product's): H(dt/4), E(dt/2),
-// H(dt/2), E(dt/2), H(dt/4) on a 32 x 32 patch with a 27 x 27 tile, the same
-// arithmetic as fdtd_tiled, unrolled: each thread owns one column and two rows
-// of the patch, and the boundary tests of its cells are taken once.  FP32 form
-// (q.er non-null): also writes the gather quads of the tile's values.
-template <typename T>
-__device__ __forceinline__ void fdtd_tiled1(T *__restrict__ Er, T *__restrict__ Ez,
-                                            T *__restrict__ H,
-                                            const unsigned long long *__restrict__ Jr,
-                                            const unsigned long long *__restrict__ Jz,
-                                            unsigned long long *__restrict__ Jr_next,
-                                            unsigned long long *__restrict__ Jz_next, int nr,
-                                            int nz, int ldf, int ldj, const FdtdCoef &c,
-                                            const double *__restrict__ invV, double mu, double dt,
-                                            unsigned flags, ExtraCurrent xj, FieldQuads q) {
-  constexpr int TW = kFdtdPatch, RW = kFdtdRows;
-  static_assert(TW == 2 * RW, "two patch rows per thread");
-  __shared__ double sEr[TW * TW], sEz[TW * TW], sH[TW * TW], sJr[TW * TW], sJz[TW * TW];
-  const int tile = fdtd_tile(1);
-  const int i0 = blockIdx.x * tile, j0 = blockIdx.y * tile;
-  const int I0 = max(i0 - 2, 0), J0 = max(j0 - 2, 0);
-  const int I1 = min(i0 + tile + 3, nr + 1), J1 = min(j0 + tile + 3, nz + 1);
-  const int W = I1 - I0, Hn = J1 - J0;
-  const int li = threadIdx.x, i = I0 + li;
-  const bool col = li < W;
-  const bool endcopy = (flags & GASATT_Q_ER_END_COPY) != 0;
-  // the thread's two patch rows
-  int lj[2], j[2], sidx[2];
-  bool row[2];
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    lj[k] = threadIdx.y + RW * k;
-    j[k] = J0 + lj[k];
-    sidx[k] = li + lj[k] * TW;
-    row[k] = col && lj[k] < Hn;
-  }
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    if (!row[k]) continue;
-    const int jj = j[k], s = sidx[k];
-    if (i < nr && jj <= nz) sEr[s] = (double)Er[i + jj * ldf];
-    if (i <= nr && jj < nz) sEz[s] = (double)Ez[i + jj * ldf];
-    if (i < nr && jj < nz) {
-      const int g = i + jj * ldj;
-      sH[s] = (double)H[i + jj * ldf];
-      if (xj.Jr) {
-        sJr[s] = ((double)(long long)Jr[g] + (double)(long long)xj.Jr[g] * xj.rel) * invV[i];
-        sJz[s] = ((double)(long long)Jz[g] + (double)(long long)xj.Jz[g] * xj.rel) * invV[i];
-      } else {
-        sJr[s] = (double)(long long)Jr[g] * invV[i];
-        sJz[s] = (double)(long long)Jz[g] * invV[i];
-      }
-    }
-  }
-  // which update each of the two cells takes
-  bool upH[2], upEr[2], zeroEr[2], upEzAxis[2], upEz[2];
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const int jj = j[k];
-    upH[k] = row[k] && i < nr && i + 1 < I1 && jj < nz && jj + 1 < J1;
-    const bool erin = jj >= 1 && jj < nz;
-    upEr[k] = row[k] && i < nr && erin && jj - 1 >= J0;
-    zeroEr[k] = row[k] && i < nr && !erin && !endcopy && jj <= nz;
-    upEzAxis[k] = row[k] && jj < nz && i == 0;
-    upEz[k] = row[k] && jj < nz && i > 0 && i < nr && i - 1 >= I0;
-  }
-  const double dt_eps = c.dt_eps, dt_eps_dz = c.dt_eps_dz, axis = c.axis, inv_dr = 1 / c.dr;
-  const double ri = ((flags & GASATT_Q_EZ_RSHIFT) ? (i + 1) : i) * c.dr;
-  const double ezp = i > 0 ? dt_eps * (1 / (2 * ri) + inv_dr) : 0.0;   // coefficient of H(i)
-  const double ezm = i > 0 ? dt_eps * (1 / (2 * ri) - inv_dr) : 0.0;   // coefficient of H(i-1)
-  const bool jsign = (flags & GASATT_Q_EZ_AXIS_JSIGN) != 0;
-  __syncthreads();
-  auto h_update = [&](double h) {
-    const double chr = h / (mu * c.dr), chz = h / (mu * c.dz);
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const int s = sidx[k];
-      if (upH[k]) sH[s] = sH[s] + (chr * (sEz[s + 1] - sEz[s]) - chz * (sEr[s + TW] - sEr[s]));
-    }
-  };
-  auto e_update = [&]() {
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const int s = sidx[k], jj = j[k];
-      if (upEr[k]) {
-        const double old = sEr[s];
-        sEr[s] = old - dt_eps * (sJr[s - TW] + sJr[s]) / 2 - dt_eps_dz * (sH[s] - sH[s - TW]);
-        if (endcopy) {
-          if (jj == 1 && J0 == 0) sEr[s - TW] = old;
-          if (jj == nz - 1 && J1 == nz + 1) sEr[s + TW] = old;
-        }
-      } else if (zeroEr[k]) {
-        sEr[s] = 0.0;
-      }
-      if (upEzAxis[k]) {
-        const double jz0 = sJz[s];
-        const double jterm = jsign ? dt_eps * jz0 : -(dt_eps * jz0);
-        sEz[s] = sEz[s] + jterm + axis * sH[s];
-      } else if (upEz[k]) {
-        sEz[s] = sEz[s] - dt_eps * (sJz[s - 1] + sJz[s]) / 2 + ezp * sH[s] + ezm * sH[s - 1];
-      }
-    }
-  };
-  h_update(dt / 4);
-  __syncthreads();
-  e_update();
-  __syncthreads();
-  h_update(dt / 2);
-  __syncthreads();
-  e_update();
-  __syncthreads();
-  h_update(dt / 4);
-  __syncthreads();
-  const int ie = min(i0 + tile, nr + 1), je = min(j0 + tile, nz + 1);
-  if (i >= i0 && i < ie) {
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const int jj = j[k], s = sidx[k];
-      if (!row[k] || jj < j0 || jj >= je) continue;
-      if (i < nr && jj <= nz) Er[i + jj * ldf] = (T)sEr[s];
-      if (i <= nr && jj < nz) Ez[i + jj * ldf] = (T)sEz[s];
-      // whole Er and Ez quads of the tile's quad indices: after the sub-cycle
-      // E is correct one cell beyond the tile (Er one column below it, Ez one
-      // row below it, both one above), which covers their corners
-      if (q.er && jj < nz) {
-        const int sa = (max(i - 1, 0) - I0) + (jj - J0) * TW, sb = (min(i, nr - 1) - I0) + (jj - J0) * TW;
-        q.er[i + jj * (nr + 1)] = make_float4((float)sEr[sa], (float)sEr[sb], (float)sEr[sa + TW],
-                                              (float)sEr[sb + TW]);
-      }
-      if (q.ez && i < nr) {
-        const int s0 = (i - I0) + (max(jj - 1, 0) - J0) * TW, s1 = (i - I0) + (min(jj, nz - 1) - J0) * TW;
-        q.ez[i + jj * nr] = make_float4((float)sEz[s0], (float)sEz[s0 + 1], (float)sEz[s1],
-                                        (float)sEz[s1 + 1]);
-      }
-      if (i < nr && jj < nz) {
-        const int g = i + jj * ldj;
-        const T v = (T)sH[s];
-        H[i + jj * ldf] = v;
-        // H is correct only on the tile, one short of its quads' corners:
-        // each value goes to the quad slots that read it instead
-        if (q.h) quad_put_h(q.h, nr, nz, i, jj, (float)v);
-        Jr_next[g] = 0;
-        Jz_next[g] = 0;
-      }
-    }
-  }
-}
-
 }  // namespace gasatt

@@ -177,7 +177,7 @@ __device__ __forceinline__ void tma_issue_item(const FdtdWork &W, int t, unsigne
 
 // The sub-cycle on the work items of W (cells on the padded layout: row
 // strides ldf for the fields, ldj for the currents), R patch rows per warp.
-// The field arithmetic is that of fdtd_tiled1 (fdtd.cuh); the per-column
+// The field arithmetic is that of fdtd_tiled (fdtd.cuh); the per-column
 // coefficients come from the cell's table, the current terms of the two E
 // updates are formed once per patch.
 template <typename T, int R>
@@ -389,7 +389,7 @@ __device__ __forceinline__ void fdtd_warp_body(const FdtdWork &W) {
 }
 
 // the per-column table of FdtdInst::colc for n_r columns: {1/V scaled, Ez
-// coefficients of H(i) and H(i-1)} (the expressions fdtd_tiled1 evaluates)
+// coefficients of H(i) and H(i-1)} (the expressions fdtd_tiled evaluates)
 inline void fdtd_column_table(int nr, const FdtdCoef &c, const double *invV, unsigned flags,
                               double *out) {
   const double inv_dr = 1 / c.dr;

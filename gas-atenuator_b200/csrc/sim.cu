@@ -453,11 +453,6 @@ __device__ __forceinline__ void warp_deposit(bool act, unsigned key, const int64
   if ((pending >> lane) & 1u) deposit_atomic<VT>(a, vr, vz, Jr, Jz);
 }
 
-template <typename VT>
-__device__ __forceinline__ void deposit_direct(const int64_t a[4], const VT vr[4],
-                                               const VT vz[4], const SimParams &P) {
-  deposit_atomic<VT>(a, vr, vz, P.Jr, P.Jz);
-}
 
 // ----------------------------------------------------------- FP64 form
 __device__ __forceinline__ void halfdrift64(double &r, double &z, double &ur, double &ut,
