@@ -404,3 +404,39 @@ def test_fields_set_between_steps(tables, precision):
     for g, w, k in zip(f, f64, ("Er", "Ez", "H")):
         assert np.linalg.norm(g - w) <= 1e-4 * np.linalg.norm(w), k
     assert abs(i - i64) <= 2
+
+
+@pytest.mark.parametrize("precision", [_lib.FP64, _lib.FP32_SPLIT])
+def test_sort_orders_by_deposit_quad_and_drops_the_dead(precision):
+    """The counting sort (runs of equal keys found with a shuffle and ballots,
+    per-run slot claims, the single-pass scan): after it the slots hold only
+    live electrons, in non-decreasing deposit-quad key (the cell shifted by
+    half a cell), each electron exactly once.  A dense population (most
+    electrons in a few cells: long runs of equal keys) with wall losses
+    (dead slots between them), loaded in random order."""
+    cfg = config(NR, NZ, D, 1e-14, 300.0, precision=precision, capacity=60000, seed=9,
+                 sort_period=0)
+    # a dense core on the axis, and a spread population whose outer part
+    # crosses the wall within the 40 steps
+    dense = births(8000, 8.0, NZ * D, seed=4, sigma_r=D, Rp=NR * D)
+    wide = births(4000, 8.0, NZ * D, seed=5, sigma_r=NR * D, Rp=NR * D, id_base=1 << 40)
+    r, z, ur, ut, uz, ids = (np.concatenate([a, b]) for a, b in zip(dense, wide))
+    perm = np.random.default_rng(2).permutation(len(r))
+    sim = Sim(cfg)
+    sim.load(*(a[perm] for a in (r, z, ur, ut, uz, ids)))
+    sim.step(40)                          # wall losses leave dead slots
+    before = sim.read()
+    live_ids = np.sort(before["id"][before["r"] >= 0])
+    d0 = sim.diag()
+    sim.sort()
+    got = sim.read()
+    d1 = sim.diag()
+    sim.close()
+    assert d0["n_lost_wall"] > 0 and d0["n_total"] > d0["n_alive"]
+    assert len(got["r"]) == d1["n_alive"] == d0["n_alive"] and np.all(got["r"] >= 0)
+    assert np.array_equal(np.sort(got["id"]), live_ids)
+    ar = np.clip(np.floor(got["r"] / D - 0.5).astype(np.int64) + 1, 0, NR)
+    az = np.clip(np.floor(got["z"] / D - 0.5).astype(np.int64) + 1, 0, NZ)
+    key = ar + az * (NR + 1)
+    assert np.all(np.diff(key) >= 0)
+    assert np.max(np.bincount(key)) > 64        # runs longer than a warp
