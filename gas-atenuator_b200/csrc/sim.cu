@@ -2427,7 +2427,7 @@ int encode_map(gasatt_sim *s, CUtensorMap *m, CUtensorMapDataType type, void *ba
 template <typename T>
 int setup_fdtd_tma(gasatt_sim *s, int nsm) {
   const auto &c = s->cfg;
-  const int ph = c.fdtd_tile_rows > 0 ? c.fdtd_tile_rows : 16;
+  const int ph = c.fdtd_tile_rows > 0 ? c.fdtd_tile_rows : 12;
   if (!tma_rows_ok(ph)) return fail(s->ctx, GASATT_E_ARG, "fdtd_tile_rows: 12, 16 or 20");
   s->tma_rows = ph;
   s->tma_smem = tma_block_bytes<T>(ph);

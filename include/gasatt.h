@@ -274,7 +274,7 @@ typedef struct gasatt_sim_config {
   /* launch-shape knobs (results do not depend on them; 0 = the default, and
    * the autotuner of the Python package picks them per workload): */
   int      fdtd_tile_rows;  /* rows of the field update's per-warp patch: 12, 16 or 20
-                               (output 26 columns x rows - 6 per patch); default 16 */
+                               (output 26 columns x rows - 6 per patch); default 12 */
   int      pass_chunk;      /* FP32 particle pass: particles per chunk a block takes,
                                a multiple of 256 (256..1792); default 1792 */
   int      gather;          /* FP32 form, how the push reads E and H: 1 = packed 2 x 2
