@@ -1355,11 +1355,15 @@ __device__ __forceinline__ void flush32(const SimParams &P, const Win32 &w, int 
   }
 }
 
+constexpr int kCandLanes = 8;     // collision candidates a warp of the pass takes at once
+
 // FP32 particle pass of step `step` (modes as push32).  Its blocks first take
-// the collision candidates queued by the previous pass, one per warp (a long
-// serial chain each, so blocks in order take eight at a time), then all other
-// particles in chunks of P.chunk handed out in order, so the blocks that ran
-// a candidate simply take fewer chunks.  Counters are committed by the field
+// the collision candidates queued by the previous pass, kCandLanes per warp,
+// one per lane (a long serial chain each; a warp's chains share its issue but
+// serialise their different collision branches, so a few per warp, not 32,
+// keep the longest warp short), then all other particles in chunks of
+// P.chunk handed out in order, so the blocks that ran candidates simply take
+// fewer chunks.  Counters are committed by the field
 // kernel of the next step.
 template <int MODE>
 __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fields<float> F,
@@ -1392,13 +1396,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_pass32(SimParams P, State32 S, Fi
   if (mode != 1) {
     const long long nq = (long long)cnt->n_cand[par ^ 1];
     const int *qin = queue + (long long)(par ^ 1) * P.cap;
+    // kCandLanes candidates per warp, one per lane
     unsigned lost = 0;
-    for (long long k = (long long)blockIdx.x * (kBlock / 32) + warp; k < nq;
-         k += (long long)gridDim.x * (kBlock / 32)) {
-      if (lane == 0) candidate32(Pg, F, S, cnt, queue, qin[k], step, mode, true, n0, lost);
-      __syncwarp();
-    }
-    if (lane == 0 && lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
+    if (lane < kCandLanes)
+      for (long long k = ((long long)blockIdx.x * (kBlock / 32) + warp) * kCandLanes + lane; k < nq;
+           k += (long long)gridDim.x * (kBlock / 32) * kCandLanes)
+        candidate32(Pg, F, S, cnt, queue, qin[k], step, mode, true, n0, lost);
+    if (lost) atomicAdd(&cnt->lost, (unsigned long long)lost);
   }
   if (threadIdx.x == 0 && next_ch < nchunk) chunk_rows32(P, S, n0, chunk, next_ch, maxrows, next_row0, next_rows);
   for (;;) {
@@ -1499,20 +1503,18 @@ __global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *_
     resolve();
     cell_at = -1;
   }
-  for (long long k = (long long)blockIdx.x * (kBlock / 32) + warp; k < nq;
-       k += (long long)gridDim.x * (kBlock / 32)) {
-    if (lane == 0) {
-      const int c = cell_of_item(cand_pre, ncell, k);
-      const BatchCell32 &C = cells[c];
-      SimCounters *cc = C.cnt;
-      const long long step = cc->step;
-      const int *qin = C.queue + (long long)((int)(step & 1) ^ 1) * C.P[jb].cap;
-      unsigned lost = 0;
-      candidate32(&C.P[jb], C.F, C.S[cur], cc, C.queue, qin[k - cand_pre[c]], step, mode, true,
-                  (long long)cc->n_total, lost);
-      if (lost) atomicAdd(&cc->lost, (unsigned long long)lost);
-    }
-    __syncwarp();
+  // one candidate per lane (the chains of a warp share its instruction issue)
+  for (long long k = ((long long)blockIdx.x * (kBlock / 32) + warp) * 32 + lane; k < nq;
+       k += (long long)gridDim.x * kBlock) {
+    const int c = cell_of_item(cand_pre, ncell, k);
+    const BatchCell32 &C = cells[c];
+    SimCounters *cc = C.cnt;
+    const long long step = cc->step;
+    const int *qin = C.queue + (long long)((int)(step & 1) ^ 1) * C.P[jb].cap;
+    unsigned lost = 0;
+    candidate32(&C.P[jb], C.F, C.S[cur], cc, C.queue, qin[k - cand_pre[c]], step, mode, true,
+                (long long)cc->n_total, lost);
+    if (lost) atomicAdd(&cc->lost, (unsigned long long)lost);
   }
   for (;;) {
     __syncthreads();
@@ -1562,10 +1564,10 @@ __global__ void __launch_bounds__(kMccBlock) k_collide32(const SimParams *__rest
   const int par = (int)(step & 1);
   const long long nq = (long long)cnt->n_cand[par];
   const int *qu = queue + (long long)par * P.cap;
-  const long long nwarps = (long long)gridDim.x * (kMccBlock / 32);
-  unsigned lost = 0;
-  for (long long k = (blockIdx.x * (long long)kMccBlock + threadIdx.x) >> 5; k < nq; k += nwarps)
-    if ((threadIdx.x & 31) == 0) candidate32(Pg, F, S, cnt, queue, qu[k], step, 0, false, n0, lost);
+  unsigned lost = 0;              // (no push here: nothing reaches the wall)
+  for (long long k = blockIdx.x * (long long)kMccBlock + threadIdx.x; k < nq;
+       k += (long long)gridDim.x * kMccBlock)
+    candidate32(Pg, F, S, cnt, queue, qu[k], step, 0, false, n0, lost);
 }
 
 // ------------------------------------------------------------- FDTD
