@@ -1570,6 +1570,43 @@ __global__ void __launch_bounds__(kMccBlock) k_collide32(const SimParams *__rest
     candidate32(Pg, F, S, cnt, queue, qu[k], step, 0, false, n0, lost);
 }
 
+// k_collide32 for every cell of a batch in one launch (before the batch's
+// sort): the cells' queued collisions in one range by prefix sums, one per
+// lane; each cell's are those its own k_collide32 would apply.
+__global__ void __launch_bounds__(kMccBlock) k_batch_collide32(const BatchCell32 *__restrict__ cells,
+                                                               int ncell, int cur) {
+  __shared__ long long pre[kMaxBatch + 1];
+  for (int c = threadIdx.x; c < ncell; c += blockDim.x) {
+    const SimCounters *cc = cells[c].cnt;
+    pre[c + 1] = (long long)cc->n_cand[(int)(cc->step & 1)];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    pre[0] = 0;
+    for (int c = 0; c < ncell; ++c) pre[c + 1] += pre[c];
+  }
+  __syncthreads();
+  const long long nq = pre[ncell];
+  for (long long k = blockIdx.x * (long long)kMccBlock + threadIdx.x; k < nq;
+       k += (long long)gridDim.x * kMccBlock) {
+    const int c = cell_of_item(pre, ncell, k);
+    const BatchCell32 &C = cells[c];
+    SimCounters *cc = C.cnt;
+    const long long step = cc->step;
+    const int *qu = C.queue + (long long)(int)(step & 1) * C.P[0].cap;
+    unsigned lost = 0;
+    candidate32(&C.P[0], C.F, C.S[cur], cc, C.queue, qu[k - pre[c]], step, 0, false,
+                (long long)cc->n_total, lost);
+  }
+}
+
+// every cell's collision queue of parity q emptied, after its collisions ran
+template <typename Cell>
+__global__ void k_batch_clear_cand(const Cell *__restrict__ cells, int ncell, int q) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x)
+    cells[c].cnt->n_cand[q] = 0;
+}
+
 // ------------------------------------------------------------- FDTD
 // FP32 form (cnt given): commit the previous pass and open step s - the
 // births of the last pass join the slots, the queue that pass consumed is
@@ -3729,6 +3766,45 @@ int batch_build_graphs(gasatt_batch *b) {
   return rc;
 }
 
+// flush_collisions for every cell of the batch (before its sort): a group
+// whose cells are at the same step parity and state buffer does it in two
+// launches (FP32: k_batch_collide32) or three (FP64: the commits, then
+// k_batch_mcc64) for all of its cells, then empties their queues; any other
+// cell flushes on its own.  A cell with nothing pending finds an empty queue
+// (its own flush emptied it) and a commit already made.
+int batch_flush_collisions(gasatt_batch *b) {
+  gasatt_ctx *ctx = b->ctx;
+  cudaStream_t st = ctx->stream;
+  for (BatchGroup &G : b->groups) {
+    const gasatt_sim *s0 = G.sims[0];
+    bool same = true, any = false;
+    for (const gasatt_sim *s : G.sims) {
+      same = same && s->cur == s0->cur && (s->host_step & 1) == (s0->host_step & 1);
+      any = any || s->mcc_pending;
+    }
+    if (!any) continue;
+    if (!same) {
+      for (gasatt_sim *s : G.sims) SIM_TRY(flush_collisions(s));
+      continue;
+    }
+    const int n = (int)G.sims.size(), cur = s0->cur, q = (int)((s0->host_step - 1) & 1);
+    if (G.form == 1) {
+      k_batch_collide32<<<G.pass_grid, kMccBlock, 0, st>>>((const BatchCell32 *)G.cells, n, cur);
+      k_batch_clear_cand<<<1, 256, 0, st>>>((const BatchCell32 *)G.cells, n, q);
+      ctx->launches += 2;
+    } else {
+      k_batch_commit64<<<1, 256, 0, st>>>((const BatchCell64 *)G.cells, n, q);
+      k_batch_mcc64<<<G.mcc_grid, kMccBlock, 0, st>>>((const BatchCell64 *)G.cells, n, cur, q);
+      k_batch_clear_cand<<<1, 256, 0, st>>>((const BatchCell64 *)G.cells, n, q);
+      ctx->launches += 3;
+    }
+    GASATT_CUDA(ctx, cudaGetLastError());
+    for (gasatt_sim *s : G.sims) s->mcc_pending = false;
+  }
+  for (gasatt_sim *s : b->singles) SIM_TRY(flush_collisions(s));
+  return GASATT_OK;
+}
+
 }  // namespace
 }  // extern "C++"
 
@@ -3792,7 +3868,7 @@ int gasatt_batch_step(gasatt_batch *b, int nsteps) {
       for (const gasatt_sim *s : b->sims)
         all_due = all_due && s->since_sort >= b->sort_period && s->cur == b->sims[0]->cur;
       if (all_due) {
-        for (gasatt_sim *s : b->sims) SIM_TRY(flush_collisions(s));
+        SIM_TRY(batch_flush_collisions(b));
         GASATT_CUDA(ctx, cudaGraphLaunch(b->g_sort[b->sims[0]->cur], st));
         for (gasatt_sim *s : b->sims) {
           ctx->launches += 4;
