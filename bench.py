@@ -694,7 +694,7 @@ def run_c3(args):
     ctx = Context(0)
     ctx.bind_stream()
     sims = []
-    for c in c3_cells():
+    for c in c3_cells(args.c3_cells):
         cfg = config(c["n_r"], c["n_z"], c["delta"], c["dt"], c["torr"], precision=prec,
                      capacity=6 * c["photo"], seed=c["seed"], sort_period=30)
         sim = Sim(cfg, ctx=ctx)
@@ -726,7 +726,7 @@ def run_c3(args):
             "batched": {"value": v_batch, "ms_per_step": ms_batch},
             "one_after_another": {"value": v_seq, "ms_per_step": ms_seq},
             "batched_over_one_after_another": v_batch / v_seq,
-            "config": {"workload": "48 cells: p log-U(0.1, 10) Torr, grid from "
+            "config": {"workload": f"{len(sims)} cells: p log-U(0.1, 10) Torr, grid from "
                        "{64x256, 128x512, 256x1024, 512x2048} at 10 um, dt 2e-14 s, photon "
                        "U(2, 20) keV, photoionizations log-U(1e4, 1e6), seed 2",
                        "precision": args.precision, "sort_period": 30, "l2": "not flushed"}}
@@ -1047,6 +1047,8 @@ def main():
                     help="workload of --mode profile")
     ap.add_argument("--c5-capacity", type=int, default=80_000_000)
     ap.add_argument("--precision", default="fp32_split", choices=["fp32_split", "fp64"])
+    ap.add_argument("--c3-cells", type=int, default=48,
+                    help="--mode c3: the first N cells of the 48 (a smaller case for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.mode == "profile":
