@@ -157,3 +157,53 @@ def test_batch_groups_share_launches_and_keep_cells_exact():
     for s in sims:
         s.close()
     ctx.close()
+
+
+def test_batch_sort_flushes_each_group_in_one_launch():
+    """Six FP32 and two FP64 cells sorting every 4 steps: before each sort of
+    all cells, each group applies its cells' pending collisions with one
+    kernel (FP32: k_batch_collide32; FP64: the commits and k_batch_mcc64) and
+    one queue clear, not a launch per cell; every cell still ends bit for bit
+    where it ends alone."""
+    rng = np.random.default_rng(9)
+    cells = []
+    for i in range(8):
+        nr, nz = [(16, 48), (32, 64), (24, 120), (48, 96)][i % 4]
+        cells.append((nr, nz, 5e-6, float(10 ** rng.uniform(1.5, 2.5)), int(rng.integers(500, 3000)),
+                      float(rng.uniform(3, 15)), _lib.FP32_SPLIT if i < 6 else _lib.FP64, 200 + i))
+    ctx = Context(0)
+
+    def make_any(cell):
+        nr, nz, d, torr, photo, kev, prec, seed = cell
+        cfg = config(nr, nz, d, 1e-14, torr, precision=prec, capacity=8 * photo, seed=seed,
+                     sort_period=4)
+        sim = Sim(cfg, ctx=ctx)
+        sim.load(*births(photo, kev, nz * d, seed=seed, sigma_r=nr * d / 4, Rp=nr * d))
+        return sim
+
+    alone = []
+    for cell in cells:
+        sim = make_any(cell)
+        sim.step(9)
+        alone.append(snapshot(sim))
+        sim.close()
+    sims = [make_any(c) for c in cells]
+    batch = Batch(sims, sort_period=4)
+    batch.step(1)                                    # primes and sorts every cell
+    l0 = ctx.launches
+    batch.step(8)                                    # all cells sort before steps 5 and 9
+    per_step = 2 + 4                                 # FP32 group, FP64 group
+    per_sort = (2 + 3) + 4 * len(cells)              # group flushes, then every cell's sort
+    assert ctx.launches - l0 == 8 * per_step + 2 * per_sort
+    for sim, ref in zip(sims, alone):
+        got = snapshot(sim)
+        for a, b in zip(got[1] + got[2], ref[1] + ref[2]):
+            np.testing.assert_array_equal(a, b)
+        assert got[3] == ref[3]
+        for k in ref[0]:
+            np.testing.assert_array_equal(got[0][k], ref[0][k], err_msg=k)
+    assert sum(r[3][0] for r in alone) > 50
+    batch.close()
+    for s in sims:
+        s.close()
+    ctx.close()
