@@ -1054,6 +1054,8 @@ def main():
     if args.mode == "profile":
         run_profile(args)
     elif args.mode == "c3":
+        if not 1 <= args.c3_cells <= 48:
+            ap.error("--c3-cells: 1 to 48")
         run_c3(args)
     elif args.mode == "c1":
         run_c1(args)
