@@ -147,7 +147,9 @@ __device__ __forceinline__ void quad_put(float4 *Q, int ncq, const QuadAxis &cx,
 // (32 - 4R - 1)^2 cells plus a halo of 2R cells on the low side and 2R + 1 on
 // the high side (each H update needs E one cell up in r and z, each E update
 // needs H one cell down) into shared memory, runs all sub-updates there, and
-// writes back its tile.  A warp covers one 32-cell row of the patch.  The
+// writes its tile to the output fields (a second buffer: the patches of other
+// blocks, which may run later, still read the old fields around this tile).
+// A warp covers one 32-cell row of the patch.  The
 // current it reads (Jr, Jz, fixed point) was deposited by the previous
 // particle pass; the block clears its tile of the other buffer (Jr_next,
 // Jz_next) for the next pass.  Storage in T; the patch stays in shared
@@ -166,8 +168,9 @@ struct ExtraCurrent {
 };
 
 template <typename T>
-__device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ Ez,
-                                           T *__restrict__ H,
+__device__ __forceinline__ void fdtd_tiled(const T *__restrict__ Er, const T *__restrict__ Ez,
+                                           const T *__restrict__ H, T *__restrict__ Er_out,
+                                           T *__restrict__ Ez_out, T *__restrict__ H_out,
                                            const unsigned long long *__restrict__ Jr,
                                            const unsigned long long *__restrict__ Jz,
                                            unsigned long long *__restrict__ Jr_next,
@@ -256,18 +259,18 @@ __device__ __forceinline__ void fdtd_tiled(T *__restrict__ Er, T *__restrict__ E
       const int s = li + (j - J0) * TW;
       if (i < nr && j <= nz) {
         const T v = (T)sEr[s];
-        Er[i + (int64_t)j * ldf] = v;
+        Er_out[i + (int64_t)j * ldf] = v;
         if (q.er) quad_put(q.er, nr + 1, quad_axis_shifted(i, nr), quad_axis_plain(j, nz), (float)v);
       }
       if (i <= nr && j < nz) {
         const T v = (T)sEz[s];
-        Ez[i + (int64_t)j * ldf] = v;
+        Ez_out[i + (int64_t)j * ldf] = v;
         if (q.ez) quad_put(q.ez, nr, quad_axis_plain(i, nr), quad_axis_shifted(j, nz), (float)v);
       }
       if (i < nr && j < nz) {
         const int64_t g = i + (int64_t)j * ldj;
         const T v = (T)sH[s];
-        H[i + (int64_t)j * ldf] = v;
+        H_out[i + (int64_t)j * ldf] = v;
         if (q.h) quad_put(q.h, nr + 1, quad_axis_shifted(i, nr), quad_axis_shifted(j, nz), (float)v);
         Jr_next[g] = 0;
         Jz_next[g] = 0;

@@ -22,7 +22,9 @@
 // staging area, completing on the warp's mbarrier.  Once the lanes hold the
 // patch in registers the area is free, and the copies of the warp's next
 // patch go out before the current one is computed.  Warps walk the work items
-// warp-stride.
+// warp-stride.  The tiles are written to a second set of fields: a patch
+// staged after its neighbours' tiles were written still reads the old fields
+// in its halo.
 //
 // TMA copies want 16-byte aligned starting columns: each box starts at the
 // patch's first column rounded down to a 16-byte boundary and is wide enough
@@ -113,8 +115,9 @@ struct TmaMaps {
 };
 
 // One gas cell's field update as the kernel sees it: its tensor maps (the
-// fields and the current buffer read in this step), where the tile is written
-// back (fields in T, the other current buffer cleared, FP32 gather quads),
+// field and current buffers read in this step), where the tile is written
+// (the other field buffer in T, the other current buffer cleared, FP32 gather
+// quads),
 // the coefficients and its tile grid.  A single cell passes it as a kernel
 // parameter; a batch keeps one per cell in global memory.
 struct FdtdInst {

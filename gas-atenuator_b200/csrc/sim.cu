@@ -624,7 +624,7 @@ struct BatchCell64 {
   State64 S[2];
   SimCounters *cnt;
   int *queue;
-  Fields<double> F;
+  Fields<double> F[2];        // field buffers 0 / 1 (the pass into current buffer jb reads F[jb])
 };
 constexpr int kChunk64 = 2048;               // particles per work item of the batched FP64 pass
 
@@ -685,7 +685,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_batch_pass64(const BatchCell64 *_
     SimCounters *cc = C.cnt;
     const long long n0 = slots_in_use(cc);
     const long long beg = (g - pre[c]) * kChunk64, end = min(beg + kChunk64, n0);
-    range64(C.P[jb], C.S[cur], C.F, cc, C.queue, mode, q, cc->step, beg, end);
+    range64(C.P[jb], C.S[cur], C.F[jb], cc, C.queue, mode, q, cc->step, beg, end);
   }
 }
 
@@ -1442,7 +1442,7 @@ struct BatchCell32 {
   State32 S[2];
   SimCounters *cnt;
   int *queue;
-  Fields<float> F;
+  Fields<float> F[2];         // field buffers 0 / 1 (the pass into current buffer jb reads F[jb])
 };
 
 // The FP32 pass of one step for every cell of a batch in one launch: each
@@ -1512,7 +1512,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *_
     const long long step = cc->step;
     const int *qin = C.queue + (long long)((int)(step & 1) ^ 1) * C.P[jb].cap;
     unsigned lost = 0;
-    candidate32(&C.P[jb], C.F, C.S[cur], cc, C.queue, qin[k - cand_pre[c]], step, mode, true,
+    candidate32(&C.P[jb], C.F[jb], C.S[cur], cc, C.queue, qin[k - cand_pre[c]], step, mode, true,
                 (long long)cc->n_total, lost);
     if (lost) atomicAdd(&cc->lost, (unsigned long long)lost);
   }
@@ -1545,7 +1545,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_batch_pass32(const BatchCell32 *_
     const long long ch = g - chunk_pre[c];
     const int beg = (int)(ch * chunk), end = (int)min((long long)beg + chunk, n0);
     const Win32 w{win_rz, win_row0, win_rows, win_stride(sP.nr)};
-    chunk32<0>(sP, C.S[cur], C.F, cc, C.queue, step, beg, end, w, &box_cmax);
+    chunk32<0>(sP, C.S[cur], C.F[jb], cc, C.queue, step, beg, end, w, &box_cmax);
     if (threadIdx.x == 0) resolve();
     __syncthreads();
     flush32(sP, w, box_cmax + 1);
@@ -1595,7 +1595,7 @@ __global__ void __launch_bounds__(kMccBlock) k_batch_collide32(const BatchCell32
     const long long step = cc->step;
     const int *qu = C.queue + (long long)(int)(step & 1) * C.P[0].cap;
     unsigned lost = 0;
-    candidate32(&C.P[0], C.F, C.S[cur], cc, C.queue, qu[k - pre[c]], step, 0, false,
+    candidate32(&C.P[0], C.F[0], C.S[cur], cc, C.queue, qu[k - pre[c]], step, 0, false,
                 (long long)cc->n_total, lost);
   }
 }
@@ -1665,9 +1665,10 @@ size_t tma_block_bytes(int rows) {
 }
 
 // The general sub-cycle (fdtd_ratio > 1): one 32 x 32 patch per block
-// (fdtd_tiled).
+// (fdtd_tiled), from the fields `in` to the fields `out`.
 template <typename T>
-__global__ void __launch_bounds__(32 * kFdtdRows, 3) k_sim_fdtd(T *Er, T *Ez, T *H, const unsigned long long *Jr,
+__global__ void __launch_bounds__(32 * kFdtdRows, 3) k_sim_fdtd(Fields<T> in, Fields<T> out,
+                                                  const unsigned long long *Jr,
                                                   const unsigned long long *Jz,
                                                   unsigned long long *Jr_next,
                                                   unsigned long long *Jz_next, int nr, int nz,
@@ -1677,8 +1678,8 @@ __global__ void __launch_bounds__(32 * kFdtdRows, 3) k_sim_fdtd(T *Er, T *Ez, T 
                                                   FieldQuads quads) {
   if (cnt && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0)
     commit_pass32(cnt);
-  fdtd_tiled<T>(Er, Ez, H, Jr, Jz, Jr_next, Jz_next, nr, nz, ldf, ldj, c, invV, mu, dt, R, flags, ion,
-                quads);
+  fdtd_tiled<T>(in.Er, in.Ez, in.H, out.Er, out.Ez, out.H, Jr, Jz, Jr_next, Jz_next, nr, nz, ldf, ldj,
+                c, invV, mu, dt, R, flags, ion, quads);
 }
 
 // ---------------------------------------------------------- load/read
@@ -2113,10 +2114,14 @@ struct gasatt_sim {
   State64 s64[2]{};
   State32 s32[2]{};
   int cur = 0;
-  void *Er = nullptr, *Ez = nullptr, *H = nullptr;
-  // field update of fdtd_ratio 1: the cell's descriptor for the steps that
-  // read current buffer 0 / 1 (tensor maps, write-back targets, tiles), the
-  // patch rows, the grid and its shared memory
+  // fields, double-buffered: the step of parity q reads buffer q and writes
+  // buffer 1 - q (the field update keeps patches of the old fields while
+  // others are written), so the fields of the current time are in buffer
+  // host_step & 1
+  void *Er[2] = {nullptr, nullptr}, *Ez[2] = {nullptr, nullptr}, *H[2] = {nullptr, nullptr};
+  // field update of fdtd_ratio 1: the cell's descriptor for the steps of
+  // parity 0 / 1 (tensor maps of the fields and current read, write-back
+  // targets, tiles), the patch rows, the grid and its shared memory
   FdtdInst fdtd_inst[2];
   int tma_rows = 0;
   unsigned tma_grid = 0;
@@ -2197,6 +2202,16 @@ FdtdCoef fdtd_coef(const gasatt_sim *s) {
 }
 
 // field sub-cycle of step with parity q: reads current buffer q, clears 1 - q
+// field buffer k as the kernels take it
+template <typename T>
+Fields<T> fields_of(const gasatt_sim *s, int k) {
+  return Fields<T>{(T *)s->Er[k], (T *)s->Ez[k], (T *)s->H[k]};
+}
+// the field buffer that holds the fields of the current time
+inline int fcur(const gasatt_sim *s) { return (int)(s->host_step & 1); }
+
+// field update of a step of parity q: reads field buffer q and current
+// buffer q, writes field buffer 1 - q and clears current buffer 1 - q
 int launch_fdtd(gasatt_sim *s, cudaStream_t st, int q) {
   const auto &c = s->cfg;
   const int nr = c.n_r, nz = c.n_z, R = c.fdtd_ratio;
@@ -2222,11 +2237,11 @@ int launch_fdtd(gasatt_sim *s, cudaStream_t st, int q) {
   auto k32 = k_sim_fdtd<float>;
   if (s->form == 0)
     k64<<<grid, block, 0, st>>>(
-        (double *)s->Er, (double *)s->Ez, (double *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
+        fields_of<double>(s, q), fields_of<double>(s, 1 - q), s->Jr[q], s->Jz[q], s->Jr[1 - q],
         s->Jz[1 - q], nr, nz, s->ldf, s->ldj, fc, s->invV, c.mu0, dt, R, c.flags, nullptr, ion, FieldQuads{});
   else
     k32<<<grid, block, 0, st>>>(
-        (float *)s->Er, (float *)s->Ez, (float *)s->H, s->Jr[q], s->Jz[q], s->Jr[1 - q],
+        fields_of<float>(s, q), fields_of<float>(s, 1 - q), s->Jr[q], s->Jz[q], s->Jr[1 - q],
         s->Jz[1 - q], nr, nz, s->ldf, s->ldj, fc, s->invV, c.mu0, dt, R, c.flags, s->cnt, ion, s->quads);
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
@@ -2235,22 +2250,20 @@ int launch_fdtd(gasatt_sim *s, cudaStream_t st, int q) {
 }
 
 // particle pass; its collision candidates (mode 0) go to queue q, its
-// current to buffer jb
-int launch_pass(gasatt_sim *s, cudaStream_t st, int mode, int jb, int q) {
+// current to buffer jb; it gathers from field buffer fb
+int launch_pass(gasatt_sim *s, cudaStream_t st, int mode, int jb, int q, int fb) {
   SimParams P = s->P;
   P.Jr = s->Jr[jb];
   P.Jz = s->Jz[jb];
   const int b = s->cur;
   if (s->form == 0)
-    k_pass64<<<s->pass_grid, kBlock, 0, st>>>(P, s->s64[b],
-                                              Fields<double>{(double *)s->Er, (double *)s->Ez, (double *)s->H},
-                                              s->cnt, s->queue, mode, q);
+    k_pass64<<<s->pass_grid, kBlock, 0, st>>>(P, s->s64[b], fields_of<double>(s, fb), s->cnt,
+                                              s->queue, mode, q);
   else
   {
     auto kern = mode == 0 ? k_pass32<0> : mode == 1 ? k_pass32<1> : k_pass32<2>;
-    kern<<<s->pass_grid, kBlock, 0, st>>>(P, s->s32[b],
-                                          Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H},
-                                          s->cnt, s->queue, s->d_P + jb);
+    kern<<<s->pass_grid, kBlock, 0, st>>>(P, s->s32[b], fields_of<float>(s, fb), s->cnt, s->queue,
+                                          s->d_P + jb);
   }
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
@@ -2273,9 +2286,8 @@ int launch_mcc(gasatt_sim *s, cudaStream_t st, int q) {
   if (s->form == 0)
     k_mcc64<<<s->mcc_grid, kMccBlock, 0, st>>>(s->P, s->s64[b], s->cnt, s->queue, q);
   else
-    k_collide32<<<s->mcc_grid, kMccBlock, 0, st>>>(
-        s->d_P, s->s32[b], Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H}, s->cnt,
-        s->queue);
+    k_collide32<<<s->mcc_grid, kMccBlock, 0, st>>>(s->d_P, s->s32[b], fields_of<float>(s, fcur(s)),
+                                                   s->cnt, s->queue);
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "collision launch");
@@ -2335,9 +2347,9 @@ int launch_ion_push(gasatt_sim *s, cudaStream_t st) {
   PI.dep = s->ion_scale;
   PI.Jr = s->Jir; PI.Jz = s->Jiz;
   if (s->form == 0)
-    k_ion_push<double><<<g, kBlock, 0, st>>>(PI, Fields<double>{(double *)s->Er, (double *)s->Ez, (double *)s->H}, s->cnt, s->ion_tmp);
+    k_ion_push<double><<<g, kBlock, 0, st>>>(PI, fields_of<double>(s, fcur(s)), s->cnt, s->ion_tmp);
   else
-    k_ion_push<float><<<g, kBlock, 0, st>>>(PI, Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H}, s->cnt, s->ion_tmp);
+    k_ion_push<float><<<g, kBlock, 0, st>>>(PI, fields_of<float>(s, fcur(s)), s->cnt, s->ion_tmp);
   s->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "ion push launch");
@@ -2390,6 +2402,19 @@ void drop_graphs(gasatt_sim *s) {
   }
 }
 
+// host_step starts over at 0: the fields of the current time move to field
+// buffer 0 (they are in buffer host_step & 1)
+int restart_steps(gasatt_sim *s, cudaStream_t st) {
+  if (fcur(s) != 0) {
+    const size_t esz = s->form == 0 ? 8 : 4, nz = (size_t)s->cfg.n_z, ld = (size_t)s->ldf;
+    GASATT_CUDA(s->ctx, cudaMemcpyAsync(s->Er[0], s->Er[1], ld * (nz + 1) * esz, cudaMemcpyDeviceToDevice, st));
+    GASATT_CUDA(s->ctx, cudaMemcpyAsync(s->Ez[0], s->Ez[1], ld * nz * esz, cudaMemcpyDeviceToDevice, st));
+    GASATT_CUDA(s->ctx, cudaMemcpyAsync(s->H[0], s->H[1], ld * nz * esz, cudaMemcpyDeviceToDevice, st));
+  }
+  s->host_step = 0;
+  return GASATT_OK;
+}
+
 // A fresh population of n particles sits in state buffer 0: counters, current
 // buffers and the step bookkeeping start over.
 int sim_reset(gasatt_sim *s, int64_t n) {
@@ -2408,10 +2433,10 @@ int sim_reset(gasatt_sim *s, int64_t n) {
     GASATT_CUDA(ctx, cudaMemsetAsync(s->Jir, 0, jbytes(s), st));
     GASATT_CUDA(ctx, cudaMemsetAsync(s->Jiz, 0, jbytes(s), st));
   }
+  SIM_TRY(restart_steps(s, st));
   GASATT_CUDA(ctx, cudaStreamSynchronize(st));
   s->primed = false;
   s->mcc_pending = false;
-  s->host_step = 0;
   s->since_sort = 0;
   return GASATT_OK;
 }
@@ -2489,12 +2514,12 @@ int setup_fdtd_tma(gasatt_sim *s, int nsm) {
     FdtdInst &I = s->fdtd_inst[q];
     std::memset(&I, 0, sizeof(I));
     TmaMaps &M = I.maps;
-    SIM_TRY(encode_map(s, &M.er, ft, s->Er, c.n_r, c.n_z + 1, ldb, bw, ph));
-    SIM_TRY(encode_map(s, &M.ez, ft, s->Ez, c.n_r + 1, c.n_z, ldb, bw, ph));
-    SIM_TRY(encode_map(s, &M.h, ft, s->H, c.n_r, c.n_z, ldb, bw, ph));
+    SIM_TRY(encode_map(s, &M.er, ft, s->Er[q], c.n_r, c.n_z + 1, ldb, bw, ph));
+    SIM_TRY(encode_map(s, &M.ez, ft, s->Ez[q], c.n_r + 1, c.n_z, ldb, bw, ph));
+    SIM_TRY(encode_map(s, &M.h, ft, s->H[q], c.n_r, c.n_z, ldb, bw, ph));
     SIM_TRY(encode_map(s, &M.jr, CU_TENSOR_MAP_DATA_TYPE_INT64, s->Jr[q], c.n_r, c.n_z, ldjb, 34, ph));
     SIM_TRY(encode_map(s, &M.jz, CU_TENSOR_MAP_DATA_TYPE_INT64, s->Jz[q], c.n_r, c.n_z, ldjb, 34, ph));
-    I.Er = s->Er; I.Ez = s->Ez; I.H = s->H;
+    I.Er = s->Er[1 - q]; I.Ez = s->Ez[1 - q]; I.H = s->H[1 - q];
     I.Jr_next = s->Jr[1 - q]; I.Jz_next = s->Jz[1 - q];
     I.colc = s->fdtd_colc;
     I.xj = ExtraCurrent{s->Jir, s->Jiz, s->scale / s->ion_scale};
@@ -2530,7 +2555,7 @@ int sim_prime(gasatt_sim *s) {
   if (s->primed) return GASATT_OK;
   cudaStream_t st = s->ctx->stream;
   if (s->cfg.sort_period > 0) SIM_TRY(gasatt_sim_sort(s));
-  SIM_TRY(launch_pass(s, st, 1, 0, 1));
+  SIM_TRY(launch_pass(s, st, 1, 0, 1, fcur(s)));   // (a half drift reads no field)
   if (s->form == 0) SIM_TRY(launch_commit(s, st, 1));
   s->primed = true;
   return GASATT_OK;
@@ -2570,7 +2595,7 @@ int build_graphs(gasatt_sim *s) {
         if (e == cudaSuccess) rc = launch_fdtd(s, cs, q);
         if (e == cudaSuccess && !rc && s->timing)
           e = cudaEventRecordWithFlags(s->ev[1], cs, cudaEventRecordExternal);
-        if (e == cudaSuccess && !rc) rc = launch_pass(s, cs, 0, 1 - q, q);
+        if (e == cudaSuccess && !rc) rc = launch_pass(s, cs, 0, 1 - q, q, 1 - q);
         if (e == cudaSuccess && !rc && s->timing)
           e = cudaEventRecordWithFlags(s->ev[3], cs, cudaEventRecordExternal);
         cudaError_t e2 = cudaStreamEndCapture(cs, &g);
@@ -2597,7 +2622,7 @@ int build_graphs(gasatt_sim *s) {
       if (e == cudaSuccess && !rc && s->timing) e = cudaEventRecordWithFlags(s->ev[1], cs, cudaEventRecordExternal);
       if (e == cudaSuccess && !rc) e = cudaStreamWaitEvent(cs, s->join_ev, 0);
       if (e == cudaSuccess && !rc && s->timing) e = cudaEventRecordWithFlags(s->ev[2], cs, cudaEventRecordExternal);
-      if (e == cudaSuccess && !rc) rc = launch_pass(s, cs, 0, 1 - q, q);
+      if (e == cudaSuccess && !rc) rc = launch_pass(s, cs, 0, 1 - q, q, 1 - q);
       if (e == cudaSuccess && !rc && s->timing) e = cudaEventRecordWithFlags(s->ev[3], cs, cudaEventRecordExternal);
       cudaError_t e2 = cudaStreamEndCapture(cs, &g);
       if (!rc && e != cudaSuccess) rc = cuda_fail(s->ctx, e, "capture step");
@@ -2721,9 +2746,12 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   const size_t esz = s->form == 0 ? 8 : 4;
   double *tmpd;
   const size_t nfE = (size_t)s->ldf * (nz + 1), nfZ = (size_t)s->ldf * nz, nfH = (size_t)s->ldf * nz;
-  if ((rc = sim_alloc(s, (char **)&s->Er, nfE * esz)) ||
-      (rc = sim_alloc(s, (char **)&s->Ez, nfZ * esz)) ||
-      (rc = sim_alloc(s, (char **)&s->H, nfH * esz)) ||
+  if ((rc = sim_alloc(s, (char **)&s->Er[0], nfE * esz)) ||
+      (rc = sim_alloc(s, (char **)&s->Ez[0], nfZ * esz)) ||
+      (rc = sim_alloc(s, (char **)&s->H[0], nfH * esz)) ||
+      (rc = sim_alloc(s, (char **)&s->Er[1], nfE * esz)) ||
+      (rc = sim_alloc(s, (char **)&s->Ez[1], nfZ * esz)) ||
+      (rc = sim_alloc(s, (char **)&s->H[1], nfH * esz)) ||
       (rc = sim_alloc(s, &s->Jr[0], ncur)) || (rc = sim_alloc(s, &s->Jz[0], ncur)) ||
       (rc = sim_alloc(s, &s->Jr[1], ncur)) || (rc = sim_alloc(s, &s->Jz[1], ncur)) ||
       (rc = sim_alloc(s, &s->cnt, 1)) || (rc = sim_alloc(s, &s->cell_count, (size_t)nbin + 1)) ||
@@ -2834,9 +2862,11 @@ int gasatt_sim_create(gasatt_ctx *ctx, const gasatt_sim_config *cfg, const gasat
   z.cap = (unsigned long long)cap;
   if (cudaMemcpy(s->cnt, &z, sizeof(z), cudaMemcpyHostToDevice) != cudaSuccess)
     return cleanup(fail(ctx, GASATT_E_CUDA, "counter init"));
-  cudaMemset(s->Er, 0, nfE * esz);
-  cudaMemset(s->Ez, 0, nfZ * esz);
-  cudaMemset(s->H, 0, nfH * esz);
+  for (int k = 0; k < 2; ++k) {
+    cudaMemset(s->Er[k], 0, nfE * esz);
+    cudaMemset(s->Ez[k], 0, nfZ * esz);
+    cudaMemset(s->H[k], 0, nfH * esz);
+  }
   for (int q = 0; q < 2; ++q) {
     cudaMemset(s->Jr[q], 0, ncur * 8);
     cudaMemset(s->Jz[q], 0, ncur * 8);
@@ -3197,7 +3227,7 @@ int fields_io(gasatt_sim *s, double *Er, double *Ez, double *H, int on_device, b
   const int nr = s->cfg.n_r, nz = s->cfg.n_z, ld = s->ldf;
   const int ncol[3] = {nr, nr + 1, nr}, nrow[3] = {nz + 1, nz, nz};
   double *u[3] = {Er, Ez, H};
-  void *dev[3] = {s->Er, s->Ez, s->H};
+  void *dev[3] = {s->Er[fcur(s)], s->Ez[fcur(s)], s->H[fcur(s)]};
   if (s->form == 0) {
     // FP64: a pitched copy between the caller's dense array and the padded grid
     for (int f = 0; f < 3; ++f) {
@@ -3238,7 +3268,8 @@ int fields_io(gasatt_sim *s, double *Er, double *Ez, double *H, int on_device, b
   if (set && s->quads.er) {
     const int64_t n = (int64_t)nr * (nz + 1) + (int64_t)(nr + 1) * nz + (int64_t)nr * nz;
     k_build_quads<<<grid_for(n, kBlock), kBlock, 0, st>>>(
-        (const float *)s->Er, (const float *)s->Ez, (const float *)s->H, nr, nz, ld, s->quads);
+        (const float *)s->Er[fcur(s)], (const float *)s->Ez[fcur(s)], (const float *)s->H[fcur(s)], nr, nz, ld,
+        s->quads);
     GASATT_LAUNCHED(ctx);
   }
   GASATT_CUDA(ctx, cudaStreamSynchronize(st));
@@ -3336,9 +3367,9 @@ int gasatt_sim_diag(gasatt_sim *s, gasatt_diag *d) {
   }
   const int nr = s->cfg.n_r, nz = s->cfg.n_z;
   if (s->form == 0)
-    k_field_energy<double><<<s->partial_blocks, kBlock, 0, st>>>((double *)s->Er, (double *)s->Ez, (double *)s->H, nr, nz, s->ldf, s->cfg.dr, s->cfg.dz, s->partial);
+    k_field_energy<double><<<s->partial_blocks, kBlock, 0, st>>>((double *)s->Er[fcur(s)], (double *)s->Ez[fcur(s)], (double *)s->H[fcur(s)], nr, nz, s->ldf, s->cfg.dr, s->cfg.dz, s->partial);
   else
-    k_field_energy<float><<<s->partial_blocks, kBlock, 0, st>>>((float *)s->Er, (float *)s->Ez, (float *)s->H, nr, nz, s->ldf, s->cfg.dr, s->cfg.dz, s->partial);
+    k_field_energy<float><<<s->partial_blocks, kBlock, 0, st>>>((float *)s->Er[fcur(s)], (float *)s->Ez[fcur(s)], (float *)s->H[fcur(s)], nr, nz, s->ldf, s->cfg.dr, s->cfg.dz, s->partial);
   GASATT_LAUNCHED(ctx);
   std::vector<double> part(2 * s->partial_blocks);
   GASATT_CUDA(ctx, cudaMemcpyAsync(s->h_cnt, s->cnt, sizeof(SimCounters), cudaMemcpyDeviceToHost, st));
@@ -3497,14 +3528,15 @@ int gasatt_sim_run_host(gasatt_sim *s, double *pos, double *vel, int64_t *n_io, 
   }
   s->primed = false;
   s->mcc_pending = false;
-  s->host_step = 0;                          // the prologue deposits into buffer 0
+  SIM_TRY(restart_steps(s, st));             // the prologue deposits into buffer 0
   s->since_sort = s->cfg.sort_period;       // sort the fresh population first
   SIM_TRY(gasatt_sim_step(s, nsteps - 1));
   // last step: the pending collisions, the fields, then a push that ends at
   // integer time
   SIM_TRY(flush_collisions(s));
   SIM_TRY(launch_fdtd(s, st, (int)(s->host_step & 1)));
-  SIM_TRY(launch_pass(s, st, 2, (int)((s->host_step + 1) & 1), (int)(s->host_step & 1)));
+  SIM_TRY(launch_pass(s, st, 2, (int)((s->host_step + 1) & 1), (int)(s->host_step & 1),
+                      (int)((s->host_step + 1) & 1)));
   if (s->form == 0) SIM_TRY(launch_commit(s, st, (int)(s->host_step & 1)));
   SIM_TRY(gasatt_sim_sort(s));               // compacts away the dead
   s->host_step++;
@@ -3614,7 +3646,7 @@ int batch_group_setup(gasatt_batch *b, BatchGroup &G) {
       }
       h[i].S[0] = s->s32[0]; h[i].S[1] = s->s32[1];
       h[i].cnt = s->cnt; h[i].queue = s->queue;
-      h[i].F = Fields<float>{(float *)s->Er, (float *)s->Ez, (float *)s->H};
+      for (int k = 0; k < 2; ++k) h[i].F[k] = Fields<float>{(float *)s->Er[k], (float *)s->Ez[k], (float *)s->H[k]};
       cm[i] = s->cnt;
     }
     BatchCell32 *d;
@@ -3633,7 +3665,7 @@ int batch_group_setup(gasatt_batch *b, BatchGroup &G) {
       }
       h[i].S[0] = s->s64[0]; h[i].S[1] = s->s64[1];
       h[i].cnt = s->cnt; h[i].queue = s->queue;
-      h[i].F = Fields<double>{(double *)s->Er, (double *)s->Ez, (double *)s->H};
+      for (int k = 0; k < 2; ++k) h[i].F[k] = Fields<double>{(double *)s->Er[k], (double *)s->Ez[k], (double *)s->H[k]};
     }
     BatchCell64 *d;
     SIM_TRY(batch_alloc(b, &d, (size_t)n));
