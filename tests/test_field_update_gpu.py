@@ -67,3 +67,34 @@ def test_field_update_at_tile_edges_matches_oracle(tables, nr, nz, flags):
         assert np.array_equal(a, b)
     for g, w, k in zip(f32[0], ref, ("Er", "Ez", "H")):
         assert np.linalg.norm(g - w) <= 1e-4 * np.linalg.norm(w), k
+
+
+@pytest.mark.parametrize("ratio", [1, 2])
+def test_field_update_with_several_patches_per_warp_matches_oracle(tables, ratio):
+    """512 x 1024 cells: more patches (or, with a field sub-cycle of 2, more
+    blocks) than the field update keeps resident, so most warps take several
+    patches and later ones are staged after neighbouring tiles were written;
+    the FP64 form still matches the oracle (the tiles go to a second field
+    buffer, so every halo holds the fields of the previous step)."""
+    nr, nz = 512, 1024
+    cfg = config(nr, nz, D, DT, 300.0, precision=abi.FP64, capacity=20000, seed=5,
+                 sort_period=0, fdtd_ratio=ratio)
+    cfg.fdtd_tile_rows = 12
+    parts = births(1500, 8.0, nz * D, seed=11, sigma_r=2 * D, Rp=nr * D)
+    flds = grid_fields(nr, nz, np.random.default_rng(3), E0=3e6, H0=2e3)
+    flds[0][:, 0] = 0; flds[0][:, -1] = 0; flds[1][-1, :] = 0     # the PEC ends and the outer wall
+    sim = Sim(cfg)
+    sim.load(*parts)
+    sim.set_fields(*flds)
+    sim.step(STEPS)
+    got, st = sim.fields(), sim.diag()["status_flags"]
+    sim.close()
+    assert st == 0
+    orc = O.Sim(cfg, tables, cap=cfg.capacity)
+    orc.load(*parts)
+    orc.Er[:], orc.Ez[:], orc.H[:] = flds
+    orc.prologue()
+    for _ in range(STEPS):
+        orc.step()
+    for g, w, k in zip(got, (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
+        close(g, w, 1e-12, k)
