@@ -207,3 +207,33 @@ def test_batch_sort_flushes_each_group_in_one_launch():
     for s in sims:
         s.close()
     ctx.close()
+
+
+def test_batch_of_large_cells_equals_instances_alone():
+    """Four 256 x 512 cells (FP32): alone, each field update fits in one wave
+    of warps; batched, their 3,440 patches take several rounds per warp, so
+    patches are staged after neighbouring tiles (of the same cell) were
+    written.  Every cell still ends bit for bit where it ends alone."""
+    cells = [(256, 512, 10e-6, float(t), 4000, 8.0, _lib.FP32_SPLIT, 300 + i)
+             for i, t in enumerate((3.0, 10.0, 30.0, 100.0))]
+    ctx = Context(0)
+    alone = []
+    for cell in cells:
+        sim = make(ctx, cell)
+        sim.step(10)
+        alone.append(snapshot(sim))
+        sim.close()
+    sims = [make(ctx, cell) for cell in cells]
+    batch = Batch(sims, sort_period=SORT_PERIOD)
+    batch.step(10)
+    for sim, ref in zip(sims, alone):
+        got = snapshot(sim)
+        for a, b in zip(got[1] + got[2], ref[1] + ref[2]):
+            np.testing.assert_array_equal(a, b)
+        assert got[3] == ref[3]
+        for k in ref[0]:
+            np.testing.assert_array_equal(got[0][k], ref[0][k], err_msg=k)
+    batch.close()
+    for s in sims:
+        s.close()
+    ctx.close()

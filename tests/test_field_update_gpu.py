@@ -98,3 +98,26 @@ def test_field_update_with_several_patches_per_warp_matches_oracle(tables, ratio
         orc.step()
     for g, w, k in zip(got, (orc.Er, orc.Ez, orc.H), ("Er", "Ez", "H")):
         close(g, w, 1e-12, k)
+
+
+def test_fp32_run_with_several_patches_per_warp_is_reproducible():
+    """Two FP32 runs of the same 512 x 1024 cell (several field patches per
+    warp) end with the same fields, current and counts, bit for bit."""
+    nr, nz = 512, 1024
+    out = []
+    for _ in range(2):
+        cfg = config(nr, nz, D, DT, 300.0, precision=abi.FP32_SPLIT, capacity=40000, seed=5,
+                     sort_period=4)
+        parts = births(4000, 8.0, nz * D, seed=11, sigma_r=20 * D, Rp=nr * D)
+        flds = grid_fields(nr, nz, np.random.default_rng(3), E0=3e6, H0=2e3)
+        sim = Sim(cfg)
+        sim.load(*parts)
+        sim.set_fields(*flds)
+        sim.step(10)
+        d = sim.diag()
+        out.append((sim.fields(), sim.current(), d["n_ionizations"], d["n_alive"], d["status_flags"]))
+        sim.close()
+    (fa, ja, *ca), (fb, jb, *cb) = out
+    assert ca == cb and ca[-1] == 0
+    for a, b in zip(fa + ja, fb + jb):
+        np.testing.assert_array_equal(a, b)
