@@ -65,4 +65,7 @@ def main(ref_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GASATT_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: make_n2_tables.py REFERENCE_DIR (or set GASATT_REFERENCE_DIR)")
+    main(ref)
